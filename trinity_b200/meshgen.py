@@ -1,0 +1,190 @@
+"""Synthetic inputs for the adaptation round: structured unit-square meshes
+and nodal solution fields, written in the formats trinity reads.
+
+Formats (as parsed by trinity's loader, src/io.cpp:53-161 of the reference):
+  * ``.mesh`` (medit): ``Vertices`` (x y tag), ``Edges`` (1-based pairs, mark
+    boundary vertices), ``Triangles`` (1-based, CCW), ``Corners`` (1-based).
+  * ``.bb``: a header line ``2 1 V 2`` then V values (the header layout is the
+    one trinity's field scripts write, scripts/bench_solut_field.py:99).
+
+Mesh: an n x n grid of the unit square, (n+1)^2 vertices numbered x-fastest,
+each quad (a,b,c,d) = ((i,j),(i+1,j),(i+1,j+1),(i,j+1)) cut along a-c into the
+CCW triangles (a,b,c) and (a,c,d). Interior vertices can be jittered by
+U(-j*h, j*h) per coordinate from ``numpy.random.default_rng(seed)``.
+
+Fields:
+  * ``shock``: tanh(a*(y - 0.5 - b*sin(2 pi x))), a=50, b=0.25 by default;
+  * ``multi``: shock + exp(-200((x-0.3)^2 + (y-0.7)^2)) + 0.1 sin(8 pi x) sin(8 pi y).
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class GridMesh:
+    points: np.ndarray      # (V, 2) float64
+    tris: np.ndarray        # (T, 3) int32, 0-based, CCW
+    edges: np.ndarray       # (E, 2) int32, 0-based boundary edges
+    corners: np.ndarray     # (4,) int32, 0-based
+
+    @property
+    def nb_nodes(self) -> int:
+        return int(self.points.shape[0])
+
+    @property
+    def nb_elems(self) -> int:
+        return int(self.tris.shape[0])
+
+
+def grid_mesh(n: int, jitter: float = 0.0, seed: int = 0) -> GridMesh:
+    """n x n unit-square grid; ``jitter`` in units of the spacing h = 1/n."""
+    h = 1.0 / n
+    idx = np.arange(n + 1)
+    X, Y = np.meshgrid(idx * h, idx * h, indexing="xy")     # rows = y, cols = x
+    pts = np.stack([X.ravel(), Y.ravel()], axis=1).astype(np.float64)
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        d = rng.uniform(-jitter * h, jitter * h, size=pts.shape)
+        ii = np.tile(idx, n + 1)
+        jj = np.repeat(idx, n + 1)
+        interior = (ii > 0) & (ii < n) & (jj > 0) & (jj < n)
+        pts[interior] += d[interior]
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="xy")
+    i = i.ravel()
+    j = j.ravel()
+    a = j * (n + 1) + i
+    b = a + 1
+    c = a + (n + 1) + 1
+    d = a + (n + 1)
+    tris = np.empty((2 * n * n, 3), dtype=np.int32)
+    tris[0::2] = np.stack([a, b, c], axis=1)
+    tris[1::2] = np.stack([a, c, d], axis=1)
+    # boundary edges, counter-clockwise around the square
+    bottom = [(k, k + 1) for k in range(n)]
+    right = [(k * (n + 1) + n, (k + 1) * (n + 1) + n) for k in range(n)]
+    top = [(n * (n + 1) + k + 1, n * (n + 1) + k) for k in range(n)]
+    left = [((k + 1) * (n + 1), k * (n + 1)) for k in range(n)]
+    edges = np.array(bottom + right + top + left, dtype=np.int32)
+    corners = np.array([0, n, n * (n + 1) + n, n * (n + 1)], dtype=np.int32)
+    return GridMesh(pts, tris, edges, corners)
+
+
+def field_shock(pts: np.ndarray, a: float = 50.0, b: float = 0.25) -> np.ndarray:
+    x, y = pts[:, 0], pts[:, 1]
+    return np.tanh(a * (y - 0.5 - b * np.sin(2.0 * np.pi * x)))
+
+
+def field_multi(pts: np.ndarray) -> np.ndarray:
+    x, y = pts[:, 0], pts[:, 1]
+    return (field_shock(pts)
+            + np.exp(-200.0 * ((x - 0.3) ** 2 + (y - 0.7) ** 2))
+            + 0.1 * np.sin(8.0 * np.pi * x) * np.sin(8.0 * np.pi * y))
+
+
+def write_mesh(path: str, m: GridMesh) -> None:
+    """Write a medit ``.mesh`` with full-precision coordinates."""
+    with open(path, "w") as f:
+        f.write("MeshVersionFormatted 1\nDimension 2\n")
+        f.write(f"Vertices\n{m.nb_nodes}\n")
+        f.write("\n".join(f"{x:.17g} {y:.17g} 0" for x, y in m.points.tolist()))
+        f.write(f"\n\nEdges\n{m.edges.shape[0]}\n")
+        f.write("\n".join(f"{u + 1} {v + 1} 1" for u, v in m.edges.tolist()))
+        f.write(f"\n\nTriangles\n{m.nb_elems}\n")
+        f.write("\n".join(f"{a + 1} {b + 1} {c + 1} 0" for a, b, c in m.tris.tolist()))
+        f.write(f"\n\nCorners\n{m.corners.shape[0]}\n")
+        f.write("\n".join(str(c + 1) for c in m.corners.tolist()))
+        f.write("\n\nEnd\n")
+
+
+def write_bb(path: str, u: np.ndarray) -> None:
+    with open(path, "w") as f:
+        f.write(f"2 1 {u.shape[0]} 2\n")
+        f.write("\n".join(f"{v:.17g}" for v in u.tolist()))
+        f.write("\n")
+
+
+# Workloads: (grid side, jitter in h, seed, field, target, norm, rounds, depth, bucket)
+CONFIGS = {
+    "c1": dict(n=100, jitter=0.0, seed=1, field="shock", target=0.9, norm=2,
+               rounds=3, depth=1, bucket=64),
+    "c2": dict(n=1000, jitter=0.2, seed=2, field="multi", target=0.7, norm=2,
+               rounds=3, depth=2, bucket=128),
+    "c3": dict(n=1414, jitter=0.2, seed=3, field="multi", target=0.7, norm=2,
+               rounds=3, depth=2, bucket=128),
+    "c4": dict(n=1000, jitter=0.3, seed=4, field="multi", target=0.7, norm=2,
+               rounds=3, depth=2, bucket=128),
+}
+
+
+def make_config(name: str, n: int | None = None):
+    """Return (mesh, field, params) for a named workload; ``n`` overrides the side."""
+    c = dict(CONFIGS[name])
+    if n is not None:
+        c["n"] = n
+    m = grid_mesh(c["n"], c["jitter"], c["seed"])
+    u = field_shock(m.points) if c["field"] == "shock" else field_multi(m.points)
+    return m, u, c
+
+
+def write_config(name: str, outdir: str, n: int | None = None):
+    m, u, c = make_config(name, n)
+    os.makedirs(outdir, exist_ok=True)
+    tag = name if n is None else f"{name}_n{n}"
+    mp = os.path.join(outdir, f"{tag}.mesh")
+    bp = os.path.join(outdir, f"{tag}.bb")
+    write_mesh(mp, m)
+    write_bb(bp, u)
+    return mp, bp, c
+
+
+def batch_specs(count: int = 256, seed: int = 5, lo: int = 32, hi: int = 512):
+    """Batched workload: per mesh (side, a, b) drawn from one generator; side is
+    log-uniform in [lo, hi]; a ~ U[10, 100], b ~ U[0, 0.3]."""
+    rng = np.random.default_rng(seed)
+    sides = np.exp(rng.uniform(np.log(lo), np.log(hi), size=count)).round().astype(int)
+    a = rng.uniform(10.0, 100.0, size=count)
+    b = rng.uniform(0.0, 0.3, size=count)
+    return [(int(s), float(x), float(y)) for s, x, y in zip(sides, a, b)]
+
+
+def read_mesh(path: str) -> GridMesh:
+    """Read a medit ``.mesh`` (Vertices / Edges / Triangles / Corners)."""
+    toks = open(path).read().split()
+    def section(key):
+        try:
+            i = toks.index(key)
+        except ValueError:
+            return None, None
+        return int(toks[i + 1]), i + 2
+    nv, i = section("Vertices")
+    v = np.array(toks[i:i + 3 * nv], dtype=np.float64).reshape(nv, 3)[:, :2]
+    ne, i = section("Edges")
+    e = (np.array(toks[i:i + 3 * ne], dtype=np.int64).reshape(ne, 3)[:, :2] - 1
+         if ne else np.zeros((0, 2), np.int64))
+    nt, i = section("Triangles")
+    t = np.array(toks[i:i + 4 * nt], dtype=np.int64).reshape(nt, 4)[:, :3] - 1
+    nc, i = section("Corners")
+    c = (np.array(toks[i:i + nc], dtype=np.int64) - 1) if nc else np.zeros(0, np.int64)
+    return GridMesh(v, t.astype(np.int32), e.astype(np.int32), c.astype(np.int32))
+
+
+def read_bb(path: str, nb_nodes: int) -> np.ndarray:
+    """Read a ``.bb`` field: skip the header line, then ``nb_nodes`` values."""
+    with open(path) as f:
+        f.readline()
+        vals = np.array(f.read().split()[:nb_nodes], dtype=np.float64)
+    return vals
+
+
+if __name__ == "__main__":
+    import argparse
+    p = argparse.ArgumentParser(description="write a synthetic workload")
+    p.add_argument("config", choices=sorted(CONFIGS))
+    p.add_argument("outdir")
+    p.add_argument("--n", type=int, default=None)
+    a = p.parse_args()
+    print(write_config(a.config, a.outdir, a.n))
