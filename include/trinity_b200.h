@@ -1,0 +1,112 @@
+/*
+ * trinity_b200.h — C ABI of the B200 implementation of trinity's adaptation
+ * round (metric recovery, refinement, edge collapse, edge flips, smoothing).
+ *
+ * Every entry point replaces one call of trinity's C++ API (include/trinity.h
+ * of the reference, which pulls in include/trinity/<kernel>.h); the reference
+ * interface is named beside each declaration. Plain pointers and sizes only.
+ * All functions return TRN_OK (0) or a TRN_ERR_* code; trn_last_error() gives
+ * the message. One CUDA stream per mesh; every call is blocking, like the
+ * reference's run() methods, and not thread-safe on the same mesh.
+ */
+#ifndef TRINITY_B200_H
+#define TRINITY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  TRN_OK = 0,
+  TRN_ERR_CAPACITY = 1,    /* a capacity (nodes, elements, stencil bucket) is too small */
+  TRN_ERR_IO = 2,          /* file missing or malformed */
+  TRN_ERR_INVALID = 3,     /* bad argument */
+  TRN_ERR_NO_PROGRESS = 4, /* an iterative loop hit its iteration cap */
+  TRN_ERR_CUDA = 5,        /* CUDA runtime error */
+  TRN_ERR_REPLAY = 6,      /* the replay log does not fit this run */
+};
+
+/* Per-kernel statistics: same layout as trinity::Stats (header.h:72-77). */
+typedef struct trn_stats {
+  int eval;     /* entities examined */
+  int task;     /* entities changed */
+  int elap;     /* milliseconds (device time of the call) */
+  int step[5];  /* per-step milliseconds, kernel specific */
+} trn_stats;
+
+typedef struct trn_mesh trn_mesh;
+
+/* replaces Mesh::Mesh(int size[2], int bucket, int depth, int verbosity, int rounds)
+ * (include/trinity/mesh.h:46). size = {vertices, triangles} of the input mesh.
+ * Capacity = scale x size with scale = max(3*(depth-1), 4). */
+int trn_mesh_create(const int size[2], int bucket, int depth, int verbosity, int rounds,
+                    trn_mesh** out);
+/* as above with an explicit capacity scale (>= 1) */
+int trn_mesh_create_ex(const int size[2], int bucket, int depth, int verbosity, int rounds,
+                       int capa_scale, trn_mesh** out);
+/* replaces Mesh::~Mesh (mesh.cpp:47-54) */
+int trn_mesh_destroy(trn_mesh* mesh);
+
+/* replaces Mesh::load(path, solu) (mesh.h:65, io.cpp:53-161): medit .mesh and
+ * .bb solution field, then Mesh::rebuildTopology (mesh.cpp:191-249) */
+int trn_mesh_load(trn_mesh* mesh, const char* mesh_path, const char* solut_path);
+/* the same from arrays: points[2V], tris[3T] 0-based CCW, tags[V] (0, 4 =
+ * boundary, 12 = boundary|corner, header.h:55-60), solut[V] */
+int trn_mesh_load_arrays(trn_mesh* mesh, int nb_nodes, int nb_elems, const double* points,
+                         const int* tris, const uint8_t* tags, const double* solut);
+/* replaces Mesh::store(path) (mesh.h:66, io.cpp:164-255) */
+int trn_mesh_store(trn_mesh* mesh, const char* path);
+/* metric field in medit .sol format (the reference writes none; an addition) */
+int trn_mesh_store_sol(trn_mesh* mesh, const char* path);
+/* copy out the raw state: nb_nodes / nb_elems entries (any pointer may be NULL) */
+int trn_mesh_export(trn_mesh* mesh, double* points, double* tensor, int* tris, uint8_t* alive,
+                    uint8_t* tags);
+/* slot counts (deleted entities included) and live counts */
+int trn_mesh_counts(trn_mesh* mesh, int* nb_nodes, int* nb_elems, int* live_nodes,
+                    int* live_elems);
+
+/* replaces Metrics(Mesh*, target_factor, Lp_norm, h_min, h_max) + Metrics::run
+ * (include/trinity/metric.h:38-44, metric.cpp:24-70) */
+int trn_metric_run(trn_mesh* mesh, double target_factor, int lp_norm, double h_min, double h_max,
+                   trn_stats* stats);
+/* replaces Refine(Mesh*, level) + Refine::run (refinement.h:39-42, refinement.cpp:445-493) */
+int trn_refine_run(trn_mesh* mesh, int depth, trn_stats* stats);
+/* replaces Coarse(Mesh*, Partit*) + Coarse::run (coarsening.h:40-42, coarsening.cpp:463-508);
+ * max_colors mirrors Partit(mesh, max_part_size) (partition.h:46) */
+int trn_coarsen_run(trn_mesh* mesh, int max_colors, trn_stats* stats);
+/* replaces Swap(Mesh*) + Swap::run (swapping.h:39-42, swapping.cpp:383-428) */
+int trn_swap_run(trn_mesh* mesh, trn_stats* stats);
+/* replaces Smooth(Mesh*, Partit*, level) + Smooth::run (smoothing.h:39-42, smoothing.cpp:274-302) */
+int trn_smooth_run(trn_mesh* mesh, int max_colors, int depth, trn_stats* stats);
+/* one full round: refine, coarsen, swap, smooth (main.cpp:52-57) */
+int trn_round_run(trn_mesh* mesh, int depth, trn_stats stats[4]);
+
+/* Replay mode: the independent sets, matchings and colorings are read from a
+ * decision log (int32 stream: 1 = set [n, ids], 2 = matching [n, (k1,k2)*n],
+ * 3 = coloring [parts, (n, ids)*parts]) instead of being computed; the
+ * complexity sum is then taken in element order. Passing n = 0 leaves
+ * replay mode. No counterpart in the reference: it makes the GPU's topology
+ * checkable bit for bit against the reference's 1-thread run. */
+int trn_set_replay(trn_mesh* mesh, const int32_t* log, size_t n);
+/* free-mode options: seed of the hash priorities; exact_sum = 1 takes the
+ * metric complexity sum in element order (bit-compatible with the reference) */
+int trn_set_options(trn_mesh* mesh, uint64_t seed, int exact_sum);
+
+/* last metric complexity (Metrics::field.complexity) */
+double trn_last_complexity(trn_mesh* mesh);
+/* device time of the last run call, milliseconds */
+double trn_last_time_ms(trn_mesh* mesh);
+/* the cudaStream_t every kernel of this mesh runs on */
+void* trn_mesh_stream(trn_mesh* mesh);
+/* message of the last error on this mesh ("" if none) */
+const char* trn_last_error(trn_mesh* mesh);
+/* library version string */
+const char* trn_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

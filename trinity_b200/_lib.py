@@ -1,0 +1,82 @@
+"""ctypes binding of the C ABI in include/trinity_b200.h.
+
+The shared library is built in-tree (``make -C trinity_b200``) and loaded from
+the package directory; there is no CPU fallback, so a missing library is an
+error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libtrinity_b200.so")
+
+TRN_OK = 0
+ERRORS = {
+    1: "TRN_ERR_CAPACITY",
+    2: "TRN_ERR_IO",
+    3: "TRN_ERR_INVALID",
+    4: "TRN_ERR_NO_PROGRESS",
+    5: "TRN_ERR_CUDA",
+    6: "TRN_ERR_REPLAY",
+}
+
+
+class Stats(ctypes.Structure):
+    """trinity::Stats (header.h:72-77)."""
+    _fields_ = [("eval", ctypes.c_int), ("task", ctypes.c_int), ("elap", ctypes.c_int),
+                ("step", ctypes.c_int * 5)]
+
+    def __repr__(self):
+        return f"Stats(eval={self.eval}, task={self.task}, elap={self.elap})"
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `make -C {PKG_DIR}` "
+                "(the GPU path has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip, dp, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+        pmesh = ctypes.c_void_p
+        sp = ctypes.POINTER(Stats)
+        L.trn_mesh_create.argtypes = [vp, ip, ip, ip, ip, ctypes.POINTER(pmesh)]
+        L.trn_mesh_create_ex.argtypes = [vp, ip, ip, ip, ip, ip, ctypes.POINTER(pmesh)]
+        L.trn_mesh_destroy.argtypes = [pmesh]
+        L.trn_mesh_load.argtypes = [pmesh, ctypes.c_char_p, ctypes.c_char_p]
+        L.trn_mesh_load_arrays.argtypes = [pmesh, ip, ip, vp, vp, vp, vp]
+        L.trn_mesh_store.argtypes = [pmesh, ctypes.c_char_p]
+        L.trn_mesh_store_sol.argtypes = [pmesh, ctypes.c_char_p]
+        L.trn_mesh_export.argtypes = [pmesh, vp, vp, vp, vp, vp]
+        L.trn_mesh_counts.argtypes = [pmesh, vp, vp, vp, vp]
+        L.trn_metric_run.argtypes = [pmesh, dp, ip, dp, dp, sp]
+        L.trn_refine_run.argtypes = [pmesh, ip, sp]
+        L.trn_coarsen_run.argtypes = [pmesh, ip, sp]
+        L.trn_swap_run.argtypes = [pmesh, sp]
+        L.trn_smooth_run.argtypes = [pmesh, ip, ip, sp]
+        L.trn_round_run.argtypes = [pmesh, ip, sp]
+        L.trn_set_replay.argtypes = [pmesh, vp, sz]
+        L.trn_set_options.argtypes = [pmesh, ctypes.c_uint64, ip]
+        L.trn_last_complexity.argtypes = [pmesh]
+        L.trn_last_complexity.restype = dp
+        L.trn_last_time_ms.argtypes = [pmesh]
+        L.trn_last_time_ms.restype = dp
+        L.trn_mesh_stream.argtypes = [pmesh]
+        L.trn_mesh_stream.restype = vp
+        L.trn_last_error.argtypes = [pmesh]
+        L.trn_last_error.restype = ctypes.c_char_p
+        L.trn_version.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+class TrinityError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code

@@ -1,0 +1,188 @@
+"""Python mirror of trinity's C++ API (include/trinity.h of the reference):
+``Mesh``, ``Metrics``, ``Partit``, ``Refine``, ``Coarse``, ``Swap``, ``Smooth``
+and ``Stats``, with the same constructor arguments and ``run(stats)`` calls,
+backed by the CUDA library through its C ABI.
+
+    mesh = Mesh(size, bucket, depth, verbosity, rounds)      # mesh.h:46
+    metric = Metrics(mesh, target, norm, h_min, h_max)       # metric.h:38
+    heuris = Partit(mesh, 8)                                 # partition.h:46
+    refine, swap = Refine(mesh, depth), Swap(mesh)           # refinement.h:39, swapping.h:39
+    coarse, smooth = Coarse(mesh, heuris), Smooth(mesh, heuris, depth)
+    mesh.load(input, solut); metric.run(stats[0])
+    for _ in range(rounds): refine.run(); coarse.run(); swap.run(); smooth.run()
+    mesh.store(result)
+
+As in the reference, the mesh must outlive the kernel objects, and calls are
+blocking and not thread-safe on one mesh.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import Stats, TrinityError, lib
+
+__all__ = ["Mesh", "Metrics", "Partit", "Refine", "Coarse", "Swap", "Smooth", "Stats",
+           "TrinityError", "EPSILON", "H_MAX", "find"]
+
+EPSILON = 1.0e-9   # header.h:50, the h_min the CLI passes (parser.cpp:95)
+H_MAX = 0.4        # parser.cpp:96
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def find(key: str, path: str) -> int:
+    """io::find (io.cpp:25-49): the count that follows section ``key``."""
+    with open(path) as f:
+        for line in f:
+            s = line.lstrip()
+            if s.startswith(("#", "%")):
+                continue
+            tok = s.split()
+            if tok and tok[0] == key:
+                for line2 in f:
+                    t2 = line2.split()
+                    if t2:
+                        return int(t2[0])
+    return -1
+
+
+class Mesh:
+    """GPU-resident mesh (Mesh, mesh.h:29-161)."""
+
+    def __init__(self, size, bucket: int = 64, depth: int = 3, verbosity: int = 0,
+                 rounds: int = 1, capa_scale: int | None = None):
+        L = lib()
+        self._L = L
+        sz = (ctypes.c_int * 2)(int(size[0]), int(size[1]))
+        h = ctypes.c_void_p()
+        if capa_scale is None:
+            rc = L.trn_mesh_create(sz, bucket, depth, verbosity, rounds, ctypes.byref(h))
+        else:
+            rc = L.trn_mesh_create_ex(sz, bucket, depth, verbosity, rounds, capa_scale, ctypes.byref(h))
+        if rc:
+            raise TrinityError(rc, "mesh creation failed")
+        self.h = h
+        self.depth = depth
+        self.rounds = rounds
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.trn_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc:
+            raise TrinityError(rc, self._L.trn_last_error(self.h).decode())
+
+    def load(self, path: str, solu: str) -> None:
+        self._check(self._L.trn_mesh_load(self.h, path.encode(), solu.encode() if solu else None))
+
+    def load_arrays(self, points, tris, tags, solut) -> None:
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        tr = np.ascontiguousarray(tris, dtype=np.int32)
+        tg = np.ascontiguousarray(tags, dtype=np.uint8)
+        u = np.ascontiguousarray(solut, dtype=np.float64)
+        self._check(self._L.trn_mesh_load_arrays(self.h, pts.shape[0], tr.shape[0], _p(pts), _p(tr),
+                                                 _p(tg), _p(u)))
+
+    def store(self, path: str) -> None:
+        self._check(self._L.trn_mesh_store(self.h, path.encode()))
+
+    def store_sol(self, path: str) -> None:
+        self._check(self._L.trn_mesh_store_sol(self.h, path.encode()))
+
+    def counts(self):
+        v = [ctypes.c_int() for _ in range(4)]
+        self._check(self._L.trn_mesh_counts(self.h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def export(self):
+        """(points[V,2], tensor[V,3], tris[T,3], alive[V], tags[V]) of all slots in use."""
+        nn, ne, _, _ = self.counts()
+        pts = np.zeros((nn, 2)); ten = np.zeros((nn, 3)); tri = np.zeros((ne, 3), np.int32)
+        alive = np.zeros(nn, np.uint8); tags = np.zeros(nn, np.uint8)
+        self._check(self._L.trn_mesh_export(self.h, _p(pts), _p(ten), _p(tri), _p(alive), _p(tags)))
+        return pts, ten, tri, alive, tags
+
+    def set_replay(self, log) -> None:
+        a = np.ascontiguousarray(log, dtype=np.int32)
+        self._check(self._L.trn_set_replay(self.h, _p(a) if a.size else None, a.size))
+
+    def set_options(self, seed: int = 0x7472696E697479, exact_sum: bool = False) -> None:
+        self._check(self._L.trn_set_options(self.h, seed, 1 if exact_sum else 0))
+
+    def last_time_ms(self) -> float:
+        return self._L.trn_last_time_ms(self.h)
+
+    def stream(self) -> int:
+        return self._L.trn_mesh_stream(self.h)
+
+
+class Metrics:
+    """Metrics(Mesh*, target_factor, Lp_norm, h_min, h_max) (metric.h:38-44)."""
+
+    def __init__(self, mesh: Mesh, target_factor: float, Lp_norm: int, h_min: float = EPSILON,
+                 h_max: float = H_MAX):
+        self.mesh, self.target, self.norm, self.h_min, self.h_max = mesh, target_factor, Lp_norm, h_min, h_max
+
+    def run(self, total: Stats | None = None) -> None:
+        m = self.mesh
+        m._check(m._L.trn_metric_run(m.h, self.target, self.norm, self.h_min, self.h_max,
+                                     ctypes.byref(total) if total is not None else None))
+
+    def complexity(self) -> float:
+        return self.mesh._L.trn_last_complexity(self.mesh.h)
+
+
+class Partit:
+    """Partit(Mesh const*, max_part_size) (partition.h:46): the coloring /
+    independent-set engine shared by Coarse and Smooth."""
+
+    def __init__(self, mesh: Mesh, max_part_size: int = 8):
+        self.mesh = mesh
+        self.max_part = max(6, max_part_size)
+
+
+class Refine:
+    def __init__(self, mesh: Mesh, level: int):
+        self.mesh, self.level = mesh, level
+
+    def run(self, total: Stats | None = None) -> None:
+        m = self.mesh
+        m._check(m._L.trn_refine_run(m.h, self.level, ctypes.byref(total) if total is not None else None))
+
+
+class Coarse:
+    def __init__(self, mesh: Mesh, algo: Partit):
+        self.mesh, self.algo = mesh, algo
+
+    def run(self, total: Stats | None = None) -> None:
+        m = self.mesh
+        m._check(m._L.trn_coarsen_run(m.h, self.algo.max_part,
+                                      ctypes.byref(total) if total is not None else None))
+
+
+class Swap:
+    def __init__(self, mesh: Mesh):
+        self.mesh = mesh
+
+    def run(self, total: Stats | None = None) -> None:
+        m = self.mesh
+        m._check(m._L.trn_swap_run(m.h, ctypes.byref(total) if total is not None else None))
+
+
+class Smooth:
+    def __init__(self, mesh: Mesh, algo: Partit, level: int):
+        self.mesh, self.algo, self.level = mesh, algo, level
+
+    def run(self, total: Stats | None = None) -> None:
+        m = self.mesh
+        m._check(m._L.trn_smooth_run(m.h, self.algo.max_part, self.level,
+                                     ctypes.byref(total) if total is not None else None))

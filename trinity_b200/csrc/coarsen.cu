@@ -1,0 +1,184 @@
+/*
+ * coarsen.cu — edge collapse (Coarse::run body, coarsening.cpp:480-503).
+ *
+ *   k_coarse_pre     activity flags: corners -1, live vertices 1, others 0;
+ *                    clear repair tags (coarsening.cpp:257-281)
+ *   k_coarse_filter  per active vertex: the shortest collapse target among
+ *                    neighbours closer than 1/sqrt(2) whose simulated collapse
+ *                    keeps every surviving element CCW with edges <= sqrt(2)
+ *                    (Coarse::identifyTarget, coarsening.cpp:47-133); ties are
+ *                    broken in adjacency order, like the reference's multimap
+ *   k_collapse       per independent vertex: erase the 1-2 shell elements,
+ *                    move the rest of the stencil to the target, relabel,
+ *                    tag repairs, re-activate the 1-ring (Coarse::collapseEdge,
+ *                    coarsening.cpp:136-254 with Mesh::copyStencil mesh.cpp:497)
+ * Independent sources touch disjoint elements, so the collapses of one level
+ * run in parallel; appends to a shared target's stencil are atomic and the
+ * repair pass sorts them.
+ */
+#include "trn_internal.h"
+#include "trn_numeric.cuh"
+
+namespace trn {
+
+__global__ void k_coarse_pre(DMesh m, int nb_nodes) {
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    if (m.tags[v] & TRN_TAG_CORNER) m.activ[v] = -1;
+    else m.activ[v] = m.alive[v] ? 1 : 0;
+    m.fixes[v] = 0;
+  }
+}
+
+__device__ int identify_target(const DMesh& m, int source) {
+  const bool bound_source = (m.tags[source] & TRN_TAG_BOUND) != 0;
+  double lens[TRN_MAX_DEG];
+  int cands[TRN_MAX_DEG];
+  int nc = 0;
+  const int* vc = m.vic + (size_t) source * m.bucket;
+  const int nv = m.vdeg[source];
+  const double2 ps = m.pts[source];
+  const double4 ts = m.ten[source];
+  for (int b = 0; b < nv; ++b) {
+    int neigh = vc[b];
+    bool bound_destin = (m.tags[neigh] & TRN_TAG_BOUND) != 0;
+    if (bound_source && !bound_destin) continue;
+    double len = trn_dist2(ps, m.pts[neigh], ts, m.ten[neigh]);
+    if (len < TRN_L_MIN) {
+      int p = nc;
+      while (p > 0 && lens[p - 1] > len) {
+        lens[p] = lens[p - 1];
+        cands[p] = cands[p - 1];
+        --p;
+      }
+      lens[p] = len;
+      cands[p] = neigh;
+      nc++;
+    }
+  }
+  const int* st = m.stenc + (size_t) source * m.bucket;
+  const int deg = trn_deg(m, source);
+  int destin = -1;
+  bool skip = true;
+  int next = 0;
+  while (skip && next < nc) {
+    destin = cands[next++];
+    skip = false;
+    int shared = 0;
+    const bool bound_destin = (m.tags[destin] & TRN_TAG_BOUND) != 0;
+    for (int a = 0; !skip && a < deg; ++a) {
+      int4 n = m.tri[st[a]];
+      if ((source == n.x && destin == n.y) || (source == n.y && destin == n.x) ||
+          (source == n.y && destin == n.z) || (source == n.z && destin == n.y) ||
+          (source == n.z && destin == n.x) || (source == n.x && destin == n.z)) {
+        skip = (++shared > 1 && bound_source && bound_destin);
+        continue;
+      }
+      int f0 = (n.x == source ? destin : n.x);
+      int f1 = (n.y == source ? destin : n.y);
+      int f2 = (n.z == source ? destin : n.z);
+      double2 p0 = m.pts[f0], p1 = m.pts[f1], p2 = m.pts[f2];
+      if (trn_ccw(p0, p1, p2)) {
+        double4 t0 = m.ten[f0], t1 = m.ten[f1], t2 = m.ten[f2];
+        double l0 = trn_dist2(p0, p1, t0, t1);
+        double l1 = trn_dist2(p1, p2, t1, t2);
+        double l2 = trn_dist2(p2, p0, t2, t0);
+        skip = (l0 > TRN_L_MAX || l1 > TRN_L_MAX || l2 > TRN_L_MAX);
+        continue;
+      }
+      skip = true;
+    }
+  }
+  return skip ? -1 : destin;
+}
+
+__global__ void k_coarse_filter(DMesh m, int nb_nodes, int* __restrict__ target,
+                                uint8_t* __restrict__ flag) {
+  if (trn_failed(m)) return;
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    uint8_t f = 0;
+    if (m.activ[v] > 0) {
+      m.activ[v] = 0;
+      int t = identify_target(m, v);
+      target[v] = t;
+      f = t > -1 ? 1 : 0;
+    }
+    flag[v] = f;
+  }
+}
+
+__global__ void k_collapse(DMesh m, const int* __restrict__ indep, const int* count,
+                           const int* __restrict__ target, const uint8_t* __restrict__ cand_flag) {
+  if (trn_failed(m)) return;
+  const int n_indep = *count;
+  for (int q = trn_tid(); q < n_indep; q += trn_grid_stride()) {
+    const int source = indep[q];
+    if (source < 0 || source >= m.capa_node || !cand_flag[source]) {
+      trn_set_error(m.err, TRN_DERR_REPLAY);
+      continue;
+    }
+    const int destin = target[source];
+    int* st = m.stenc + (size_t) source * m.bucket;
+    const int deg = trn_deg(m, source);
+    const int limit = (m.tags[source] & TRN_TAG_BOUND) ? 1 : 2;
+    int k = 0, trash0 = -1, trash1 = -1;
+    int opp[2] = {-1, -1};
+    for (int a = 0; k < limit && a < deg; ++a) {
+      int4 n = m.tri[st[a]];
+      int o = -2;
+      if ((source == n.x && destin == n.y) || (destin == n.x && source == n.y)) o = n.z;
+      else if ((source == n.y && destin == n.z) || (destin == n.y && source == n.z)) o = n.x;
+      else if ((source == n.z && destin == n.x) || (destin == n.z && source == n.x)) o = n.y;
+      if (o != -2) {
+        opp[k] = o;
+        if (k == 0) trash0 = a; else trash1 = a;
+        ++k;
+      }
+    }
+    int rest[TRN_MAX_DEG];
+    int nr = 0;
+    for (int a = 0; a < deg; ++a) {
+      int e = st[a];
+      if (a == trash0 || a == trash1) {
+        m.tri[e] = make_int4(-1, -1, -1, 0);
+        continue;
+      }
+      rest[nr++] = e;
+    }
+    for (int j = 0; j < k; ++j)
+      if (opp[j] >= 0) trn_flag_on(m.fixes + opp[j]);
+    trn_stenc_append_n(m, destin, rest, nr);
+    for (int a = 0; a < nr; ++a) {
+      int4 n = m.tri[rest[a]];
+      if (n.x == source) n.x = destin;
+      else if (n.y == source) n.y = destin;
+      else if (n.z == source) n.z = destin;
+      m.tri[rest[a]] = n;
+    }
+    trn_flag_on(m.fixes + destin);
+    const int* vc = m.vic + (size_t) source * m.bucket;
+    const int nv = m.vdeg[source];
+    for (int b = 0; b < nv; ++b) trn_activ_on(m.activ + vc[b]);
+    m.vdeg[source] = 0;
+    m.alive[source] = 0;
+    for (int a = 0; a < deg; ++a) st[a] = -1;
+    m.deg[source] = 0;
+  }
+}
+
+void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s) {
+  k_coarse_pre<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  check_launch("coarsen_pre");
+}
+
+void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, cudaStream_t s) {
+  k_coarse_filter<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, flag);
+  check_launch("coarsen_filter");
+}
+
+void collapse(const DMesh& m, const int* indep, const int* count, const int* target,
+              const uint8_t* cand_flag, cudaStream_t s) {
+  k_collapse<<<grid_for(m.capa_node), TRN_THREADS, 0, s>>>(m, indep, count, target, cand_flag);
+  check_launch("collapse");
+}
+
+}  // namespace trn

@@ -1,0 +1,282 @@
+/*
+ * heuristics.cu — the graph heuristics of the free (non-replay) mode.
+ *
+ * The reference resolves conflicts with a speculative first-fit coloring
+ * (partition.cpp:79-306, independent set = color 1) and a Karp-Sipser-like
+ * greedy matching (matching.cpp:81-135), both sequential in spirit. On the GPU
+ * these become round-synchronous algorithms with seeded hash priorities:
+ *
+ *   mis_jp          Jones-Plassmann maximal independent set on the collapse
+ *                   candidates: a candidate joins when it has the highest
+ *                   priority among its undecided candidate neighbours, and
+ *                   leaves when a neighbour joined.
+ *   match_handshake maximal matching on the swap dual rows: every unmatched
+ *                   candidate points along its heaviest free edge (symmetric
+ *                   hash weight); mutual candidate pairs match, a non-candidate
+ *                   neighbour accepts its heaviest proposer.
+ *   color_jp        Jones-Plassmann first-fit coloring of the interior
+ *                   vertices with colors 1..max_col; a vertex left without a
+ *                   free color is not smoothed, as in the reference.
+ */
+#include "trn_internal.h"
+
+#include <cstdio>
+
+namespace trn {
+
+/* ---------------- independent set ---------------- */
+__global__ void k_mis_init(uint8_t* state, const int* __restrict__ cand, int n) {
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) state[cand[q]] = 1;
+}
+
+__global__ void k_mis_round(DMesh m, uint8_t* state, const int* __restrict__ cand, int n,
+                            uint64_t seed, int* undecided) {
+  if (trn_failed(m)) return;
+  int left = 0;
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int v = cand[q];
+    if (state[v] != 1) continue;
+    const uint64_t pv = trn_prio(seed, v);
+    const int* vc = m.vic + (size_t) v * m.bucket;
+    const int nv = m.vdeg[v];
+    bool is_max = true, out = false;
+    for (int b = 0; b < nv; ++b) {
+      const int w = vc[b];
+      const uint8_t sw = *(volatile uint8_t*) (state + w);
+      if (sw == 2) { out = true; break; }
+      if (sw == 1 && trn_prio(seed, w) > pv) is_max = false;
+    }
+    if (out) state[v] = 0;
+    else if (is_max) state[v] = 2;
+    else ++left;
+  }
+  if (left) atomicAdd(undecided, left);
+}
+
+__global__ void k_mis_collect(const uint8_t* state, const int* __restrict__ cand, int n, int* indep,
+                              int* count) {
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int v = cand[q];
+    if (state[v] == 2) indep[atomicAdd(count, 1)] = v;
+  }
+}
+
+__global__ void k_mis_clear(uint8_t* state, const int* __restrict__ cand, int n) {
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) state[cand[q]] = 0;
+}
+
+void mis_jp(const DMesh& m, int nb_nodes, const uint8_t* cand_flag, const int* cand_list,
+            int ncand, uint64_t seed, HeurWs& ws, int* indep, int* count, ScanWs& scan,
+            cudaStream_t s) {
+  (void) nb_nodes;
+  (void) cand_flag;
+  (void) scan;
+  const int g = grid_for(ncand);
+  k_mis_init<<<g, TRN_THREADS, 0, s>>>(ws.state, cand_list, ncand);
+  int host_left = 1;
+  for (int batch = 0; batch < 64 && host_left; ++batch) {
+    cudaMemsetAsync(ws.cnt, 0, sizeof(int) * 4, s);
+    for (int r = 0; r < 4; ++r)
+      k_mis_round<<<g, TRN_THREADS, 0, s>>>(m, ws.state, cand_list, ncand, seed, ws.cnt + r);
+    cudaMemcpyAsync(&host_left, ws.cnt + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+  }
+  cudaMemsetAsync(count, 0, sizeof(int), s);
+  k_mis_collect<<<g, TRN_THREADS, 0, s>>>(ws.state, cand_list, ncand, indep, count);
+  k_mis_clear<<<g, TRN_THREADS, 0, s>>>(ws.state, cand_list, ncand);
+  check_launch("mis_jp");
+}
+
+/* ---------------- matching ---------------- */
+__device__ __forceinline__ uint32_t edge_weight(uint64_t seed, int a, int b, int round) {
+  int lo = a < b ? a : b, hi = a < b ? b : a;
+  uint64_t h = trn_hash64(seed ^ ((uint64_t) (uint32_t) lo << 32 | (uint32_t) hi) ^
+                          ((uint64_t) round * 0xd1b54a32d192ed03ULL));
+  return (uint32_t) (h >> 32) | 1u;
+}
+
+__global__ void k_match_reset(const int* __restrict__ dual, const int* __restrict__ dual_n,
+                              int ntasks, int* mate, unsigned long long* prop) {
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride())
+    for (int q = 0; q < dual_n[i]; ++q) {
+      int e = dual[i * 4 + q];
+      mate[e] = -1;
+      prop[e] = 0ULL;
+    }
+}
+
+__global__ void k_match_propose(const int* __restrict__ dual, const int* __restrict__ dual_n,
+                                int ntasks, const int* mate, unsigned long long* prop, int* choice,
+                                uint64_t seed, int round) {
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
+    const int c = dual[i * 4];
+    int best = -1;
+    uint32_t bw = 0;
+    if (mate[c] == -1) {
+      for (int q = 1; q < dual_n[i]; ++q) {
+        const int n = dual[i * 4 + q];
+        if (mate[n] != -1) continue;
+        uint32_t w = edge_weight(seed, c, n, round);
+        if (w > bw) { bw = w; best = n; }
+      }
+      if (best >= 0) atomicMax(prop + best, ((unsigned long long) bw << 32) | (uint32_t) c);
+    }
+    choice[i] = best;
+  }
+}
+
+__global__ void k_match_accept(const int* __restrict__ dual, int ntasks, const int* __restrict__ map,
+                               int* mate, const unsigned long long* prop, const int* choice,
+                               uint64_t seed, int round, int* pairs, int* npairs) {
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
+    const int n = choice[i];
+    if (n < 0) continue;
+    const int c = dual[i * 4];
+    const int x = map[n];
+    const bool n_cand = x >= 0 && x < ntasks && dual[x * 4] == n;
+    bool ok;
+    if (n_cand) ok = (choice[x] == c) && (c < n);
+    else ok = prop[n] == (((unsigned long long) edge_weight(seed, c, n, round) << 32) | (uint32_t) c);
+    if (ok) {
+      mate[c] = n;
+      mate[n] = c;
+      int p = atomicAdd(npairs, 1);
+      pairs[2 * p] = c;
+      pairs[2 * p + 1] = n;
+    }
+  }
+}
+
+__global__ void k_match_prop_clear(const int* __restrict__ dual, const int* __restrict__ dual_n,
+                                   int ntasks, unsigned long long* prop) {
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride())
+    for (int q = 1; q < dual_n[i]; ++q) prop[dual[i * 4 + q]] = 0ULL;
+}
+
+void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n, int ntasks,
+                     const int* map, uint64_t seed, HeurWs& ws, int* pairs, int* npairs,
+                     cudaStream_t s) {
+  (void) nb_elems;
+  (void) m;
+  const int g = grid_for(ntasks);
+  cudaMemsetAsync(npairs, 0, sizeof(int), s);
+  k_match_reset<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.mate, ws.prop);
+  for (int r = 0; r < 6; ++r) {
+    k_match_propose<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.mate, ws.prop, ws.choice,
+                                               seed, r);
+    k_match_accept<<<g, TRN_THREADS, 0, s>>>(dual, ntasks, map, ws.mate, ws.prop, ws.choice, seed,
+                                              r, pairs, npairs);
+    k_match_prop_clear<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.prop);
+  }
+  check_launch("match_handshake");
+}
+
+/* ---------------- coloring ---------------- */
+/* color word: 0 = uncolored, else (round + 1) << 8 | color, color 0xff = none */
+__global__ void k_color_round(DMesh m, int nb_nodes, int* color, int max_col, uint64_t seed,
+                              int round, int* undecided) {
+  if (trn_failed(m)) return;
+  int left = 0;
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    if (m.activ[v] != 1 || m.vdeg[v] == 0 || color[v] != 0) continue;
+    const uint64_t pv = trn_prio(seed, v);
+    const int* vc = m.vic + (size_t) v * m.bucket;
+    const int nv = m.vdeg[v];
+    bool is_max = true;
+    unsigned used = 0;
+    for (int b = 0; b < nv; ++b) {
+      const int w = vc[b];
+      if (m.activ[w] != 1 || m.vdeg[w] == 0) continue;
+      const int cw = *(volatile int*) (color + w);
+      const int rw = cw >> 8;
+      if (cw == 0 || rw == round + 1) {
+        if (trn_prio(seed, w) > pv) { is_max = false; break; }
+      } else {
+        used |= 1u << (cw & 0xff & 31);
+      }
+    }
+    if (!is_max) { ++left; continue; }
+    int c = 1;
+    while (c <= max_col && (used & (1u << c))) ++c;
+    color[v] = ((round + 1) << 8) | (c <= max_col ? c : 0xff);
+  }
+  if (left) atomicAdd(undecided, left);
+}
+
+__global__ void k_color_count(DMesh m, int nb_nodes, const int* color, int* cnt, int max_col) {
+  __shared__ int sc[32];
+  if (threadIdx.x < 32) sc[threadIdx.x] = 0;
+  __syncthreads();
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    int c = color[v] & 0xff;
+    if (color[v] != 0 && c >= 1 && c <= max_col) atomicAdd(sc + c, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x >= 1 && threadIdx.x <= max_col && sc[threadIdx.x])
+    atomicAdd(cnt + threadIdx.x, sc[threadIdx.x]);
+}
+
+__global__ void k_color_offsets(const int* cnt, int* part_off, int* cursor, int max_col) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int acc = 0;
+  for (int c = 1; c <= max_col; ++c) {
+    part_off[c - 1] = acc;
+    cursor[c] = acc;
+    acc += cnt[c];
+  }
+  part_off[max_col] = acc;
+}
+
+__global__ void k_color_scatter(int nb_nodes, int* color, int* cursor, int* parts, int max_col) {
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    int cw = color[v];
+    int c = cw & 0xff;
+    if (cw != 0 && c >= 1 && c <= max_col) parts[atomicAdd(cursor + c, 1)] = v;
+    color[v] = 0;
+  }
+}
+
+void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& ws, int* parts,
+              int* part_off, cudaStream_t s) {
+  const int g = grid_for(nb_nodes);
+  int host_left = 1;
+  int round = 0;
+  for (int batch = 0; batch < 64 && host_left; ++batch) {
+    cudaMemsetAsync(ws.cnt, 0, sizeof(int) * 4, s);
+    for (int r = 0; r < 4; ++r, ++round)
+      k_color_round<<<g, TRN_THREADS, 0, s>>>(m, nb_nodes, ws.color, max_col, seed, round, ws.cnt + r);
+    cudaMemcpyAsync(&host_left, ws.cnt + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+  }
+  int* cnt = ws.cnt + 4;      /* 32 slots */
+  int* cursor = ws.cnt + 40;  /* 32 slots */
+  cudaMemsetAsync(cnt, 0, sizeof(int) * 32, s);
+  k_color_count<<<g, TRN_THREADS, 0, s>>>(m, nb_nodes, ws.color, cnt, max_col);
+  k_color_offsets<<<1, 32, 0, s>>>(cnt, part_off, cursor, max_col);
+  k_color_scatter<<<g, TRN_THREADS, 0, s>>>(nb_nodes, ws.color, cursor, parts, max_col);
+  check_launch("color_jp");
+}
+
+void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {
+  size_t big = (size_t) (capa_node > capa_elem ? capa_node : capa_elem);
+  cudaMalloc(&ws->state, big);
+  cudaMemset(ws->state, 0, big);
+  cudaMalloc(&ws->prop, sizeof(unsigned long long) * (size_t) capa_elem);
+  cudaMalloc(&ws->choice, sizeof(int) * (size_t) capa_elem);
+  cudaMalloc(&ws->color, sizeof(int) * (size_t) capa_node);
+  cudaMemset(ws->color, 0, sizeof(int) * (size_t) capa_node);
+  cudaMalloc(&ws->mate, sizeof(int) * (size_t) capa_elem);
+  cudaMalloc(&ws->cnt, sizeof(int) * 128);
+}
+
+void heur_ws_free(HeurWs* ws) {
+  cudaFree(ws->state);
+  cudaFree(ws->prop);
+  cudaFree(ws->choice);
+  cudaFree(ws->color);
+  cudaFree(ws->mate);
+  cudaFree(ws->cnt);
+  *ws = HeurWs();
+}
+
+}  // namespace trn

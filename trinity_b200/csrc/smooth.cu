@@ -1,0 +1,117 @@
+/*
+ * smooth.cu — anisotropic smart-Laplacian smoothing (Smooth::run,
+ * smoothing.cpp:274-302).
+ *
+ *   k_smooth_pre   live vertices: interior ones active, boundary ones not
+ *                  (smoothing.cpp:129-142)
+ *   k_smooth_move  one launch per color class: every listed interior vertex
+ *                  moves to the mean over its neighbours b of
+ *                  p_a + (p_b - p_a)/L_M(a,b), takes the log-Euclidean mean of
+ *                  the neighbours' tensors, and keeps the move only if every
+ *                  incident element stays CCW with quality above the old
+ *                  stencil minimum, backing off the step 1, 1/2, .., 1/16
+ *                  (Smooth::moveSmartLaplacian, smoothing.cpp:40-126).
+ * Vertices of one color share no element, so a class moves in parallel; the
+ * classes run in order, as in the reference.
+ */
+#include "trn_internal.h"
+#include "trn_numeric.cuh"
+
+namespace trn {
+
+__global__ void k_smooth_pre(DMesh m, int nb_nodes) {
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride())
+    if (m.alive[v]) m.activ[v] = (m.tags[v] & TRN_TAG_BOUND) ? 0 : 1;
+}
+
+__device__ int move_laplacian(const DMesh& m, int i) {
+  const int* vc = m.vic + (size_t) i * m.bucket;
+  const int* st = m.stenc + (size_t) i * m.bucket;
+  const int deg = trn_deg(m, i);
+  const int nb_neigh = m.vdeg[i];
+  double q_min = 1.7976931348623157e308;
+  for (int a = 0; a < deg; ++a) q_min = trn_dmin(q_min, m.qual[st[a]]);
+  const double2 pini = m.pts[i];
+  const double4 tini = m.ten[i];
+  double ox = 0, oy = 0;
+  double lm[4] = {0, 0, 0, 0};
+  for (int k = 0; k < nb_neigh; ++k) {
+    const int nb = vc[k];
+    const double2 pb = m.pts[nb];
+    const double4 tb = m.ten[nb];
+    const double len = trn_dist2(pini, pb, tini, tb);
+    ox += pini.x + ((pb.x - pini.x) / len);
+    oy += pini.y + ((pb.y - pini.y) / len);
+    trn_interp_add(lm, tb.x, tb.y, tb.z);
+  }
+  ox /= nb_neigh;
+  oy /= nb_neigh;
+  double tn[3];
+  trn_interp_finish(lm, nb_neigh, tn);
+  const double4 tnew = make_double4(tn[0], tn[1], tn[2], 0.0);
+  m.ten[i] = tnew;
+  double qual[TRN_MAX_DEG];
+  bool valid;
+  int retry = 0;
+  double weight = 1;
+  do {
+    valid = true;
+    double2 pa;
+    pa.x = (1 - weight) * pini.x + weight * ox;
+    pa.y = (1 - weight) * pini.y + weight * oy;
+    m.pts[i] = pa;
+    for (int a = 0; valid && a < deg; ++a) {
+      const int4 n = m.tri[st[a]];
+      const double2 p0 = (n.x == i) ? pa : m.pts[n.x];
+      const double2 p1 = (n.y == i) ? pa : m.pts[n.y];
+      const double2 p2 = (n.z == i) ? pa : m.pts[n.z];
+      valid = false;
+      if (trn_ccw(p0, p1, p2)) {
+        const double4 t0 = (n.x == i) ? tnew : m.ten[n.x];
+        const double4 t1 = (n.y == i) ? tnew : m.ten[n.y];
+        const double4 t2 = (n.z == i) ? tnew : m.ten[n.z];
+        qual[a] = trn_quality(p0, p1, p2, t0, t1, t2);
+        valid = (qual[a] > q_min);
+      }
+    }
+    weight *= 0.5;
+  } while (!valid && ++retry < 5);
+  if (valid) {
+    for (int a = 0; a < deg; ++a) m.qual[st[a]] = qual[a];
+  } else {
+    m.pts[i] = pini;
+    m.ten[i] = tini;
+  }
+  return valid ? 1 : 0;
+}
+
+__global__ void k_smooth_move(DMesh m, const int* __restrict__ list, int n, int* counters) {
+  if (trn_failed(m)) return;
+  int tasks = 0, commit = 0;
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int v = list[q];
+    if (v < 0 || v >= m.capa_node) {
+      trn_set_error(m.err, TRN_DERR_REPLAY);
+      continue;
+    }
+    if (!m.activ[v]) continue;
+    if (m.vdeg[v] == 0) continue;
+    tasks++;
+    commit += move_laplacian(m, v);
+  }
+  if (tasks) atomicAdd(counters, tasks);
+  if (commit) atomicAdd(counters + 1, commit);
+}
+
+void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s) {
+  k_smooth_pre<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  check_launch("smooth_pre");
+}
+
+void smooth_color(const DMesh& m, const int* list, int n, int* counters, cudaStream_t s) {
+  if (n <= 0) return;
+  k_smooth_move<<<grid_for(n, 128), 128, 0, s>>>(m, list, n, counters);
+  check_launch("smooth_color");
+}
+
+}  // namespace trn

@@ -1,0 +1,196 @@
+/*
+ * swap.cu — edge flips (Swap::run, swapping.cpp:383-428).
+ *
+ *   k_swap_init    repair tags off, element -> dual-index map reset, quality
+ *                  cache and activity of every live element (cacheQuality,
+ *                  swapping.cpp:152-178)
+ *   k_swap_filter  active elements lose their flag; those with q < 0.9 become
+ *                  candidates (filterElems, swapping.cpp:181-201)
+ *   k_swap_dual    per candidate: itself plus its edge neighbours, the two at
+ *                  its first vertex found in that vertex's stencil order, then
+ *                  the one across the opposite edge (extractDualGraph,
+ *                  swapping.cpp:204-248); records element -> row index
+ *   k_swap_flip    per matched pair: flip the shared edge when both new
+ *                  elements are CCW and the smaller quality does not drop;
+ *                  stencil appends, repair tags, cached qualities and
+ *                  re-activation of the dual rows (Swap::swap, swapping.cpp:55-149)
+ * The map keeps entries of earlier levels of the same call (it is reset once
+ * per call, like the reference), so re-activation may follow an older row;
+ * rows therefore persist across levels.
+ */
+#include "trn_internal.h"
+#include "trn_numeric.cuh"
+
+namespace trn {
+
+__global__ void k_swap_init_nodes(DMesh m, int nb_nodes) {
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) m.fixes[v] = 0;
+}
+
+__global__ void k_swap_init_elems(DMesh m, int nb_elems, int* __restrict__ map) {
+  if (trn_failed(m)) return;
+  for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
+    map[i] = -1;
+    int4 t = m.tri[i];
+    if (t.x < 0) {
+      m.activ[i] = 0;
+      continue;
+    }
+    m.qual[i] = trn_quality(m.pts[t.x], m.pts[t.y], m.pts[t.z], m.ten[t.x], m.ten[t.y], m.ten[t.z]);
+    m.activ[i] = 1;
+  }
+}
+
+__global__ void k_swap_filter(DMesh m, int nb_elems, uint8_t* __restrict__ flag) {
+  for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
+    uint8_t f = 0;
+    if (m.activ[i]) {
+      m.activ[i] = 0;
+      f = (m.qual[i] < TRN_Q_MIN) ? 1 : 0;
+    }
+    flag[i] = f;
+  }
+}
+
+__global__ void k_swap_dual(DMesh m, const int* __restrict__ list, int ntasks, int* __restrict__ dual,
+                            int* __restrict__ dual_n, int* __restrict__ map) {
+  if (trn_failed(m)) return;
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
+    const int k = list[i];
+    const int4 n = m.tri[k];
+    int row[4] = {k, -1, -1, -1};
+    int dn = 1;
+    const int* s0 = m.stenc + (size_t) n.x * m.bucket;
+    const int d0 = trn_deg(m, n.x);
+    for (int a = 0; dn < 3 && a < d0; ++a) {
+      int t = s0[a];
+      if (t == k) continue;
+      int4 v = m.tri[t];
+      if ((v.x == n.x && v.y == n.z) || (v.x == n.y && v.y == n.x) ||
+          (v.y == n.x && v.z == n.z) || (v.y == n.y && v.z == n.x) ||
+          (v.z == n.x && v.x == n.z) || (v.z == n.y && v.x == n.x))
+        row[dn++] = t;
+    }
+    const int* s2 = m.stenc + (size_t) n.z * m.bucket;
+    const int d2 = trn_deg(m, n.z);
+    for (int a = 0; a < d2; ++a) {
+      int t = s2[a];
+      if (t == k) continue;
+      int4 v = m.tri[t];
+      if ((v.x == n.z && v.y == n.y) || (v.y == n.z && v.z == n.y) || (v.z == n.z && v.x == n.y)) {
+        row[dn++] = t;
+        break;
+      }
+    }
+    reinterpret_cast<int4*>(dual)[i] = make_int4(row[0], row[1], row[2], row[3]);
+    dual_n[i] = dn;
+    map[k] = i;
+  }
+}
+
+/* Swap::swap, swapping.cpp:55-149 */
+__device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int* map,
+                         const int* dual, const int* dual_n) {
+  const int4 a = m.tri[id1], b = m.tri[id2];
+  const int o1[3] = {a.x, a.y, a.z};
+  const int o2[3] = {b.x, b.y, b.z};
+  int c1[3] = {-1, -1, -1}, c2[3] = {-1, -1, -1};
+  for (int i = 0; i < 3; ++i) {
+    int j = (i + 1) % 3, k = (i + 2) % 3;
+    if (o1[i] == o2[1] && o1[j] == o2[0]) {
+      c1[0] = o1[i]; c1[1] = o2[2]; c1[2] = o1[k];
+      c2[0] = o1[k]; c2[1] = o2[2]; c2[2] = o1[j];
+      break;
+    }
+    if (o1[i] == o2[2] && o1[j] == o2[1]) {
+      c1[0] = o1[i]; c1[1] = o2[0]; c1[2] = o1[k];
+      c2[0] = o1[k]; c2[1] = o2[0]; c2[2] = o1[j];
+      break;
+    }
+    if (o1[i] == o2[0] && o1[j] == o2[2]) {
+      c1[0] = o1[i]; c1[1] = o2[1]; c1[2] = o1[k];
+      c2[0] = o1[k]; c2[1] = o2[1]; c2[2] = o1[j];
+      break;
+    }
+  }
+  if (c1[0] < 0) return 0;
+  const double2 p10 = m.pts[c1[0]], p11 = m.pts[c1[1]], p12 = m.pts[c1[2]];
+  const double2 p22 = m.pts[c2[2]];
+  /* c2 = (c1[2], c1[1], c2[2]) */
+  if (!trn_ccw(p10, p11, p12) || !trn_ccw(p12, p11, p22)) return 0;
+  const double4 t10 = m.ten[c1[0]], t11 = m.ten[c1[1]], t12 = m.ten[c1[2]];
+  const double4 t22 = m.ten[c2[2]];
+  const double q0 = trn_quality(p10, p11, p12, t10, t11, t12);
+  const double q1 = trn_quality(p12, p11, p22, t12, t11, t22);
+  const double q_old = trn_dmin(m.qual[id1], m.qual[id2]);
+  const double q_new = trn_dmin(q0, q1);
+  if (q_new < q_old) return 0;
+  m.tri[id1] = make_int4(c1[0], c1[1], c1[2], 0);
+  m.tri[id2] = make_int4(c2[0], c2[1], c2[2], 0);
+  trn_stenc_append(m, c2[0], id2);
+  trn_stenc_append(m, c2[1], id1);
+  trn_flag_on(m.fixes + c1[0]);
+  trn_flag_on(m.fixes + c1[1]);
+  trn_flag_on(m.fixes + c1[2]);
+  trn_flag_on(m.fixes + c2[2]);
+  m.qual[id1] = q0;
+  m.qual[id2] = q1;
+  for (int q = 0; q < dual_n[index]; ++q) trn_activ_on(m.activ + dual[index * 4 + q]);
+  const int x = map[id2];
+  if (x > -1)
+    for (int q = 0; q < dual_n[x]; ++q) trn_activ_on(m.activ + dual[x * 4 + q]);
+  return 2;
+}
+
+__global__ void k_swap_flip(DMesh m, const int* __restrict__ pairs, const int* npairs,
+                            const int* __restrict__ map, const int* __restrict__ dual,
+                            const int* __restrict__ dual_n, int ntasks, int* commit) {
+  if (trn_failed(m)) return;
+  const int np = *npairs;
+  int local = 0;
+  for (int p = trn_tid(); p < np; p += trn_grid_stride()) {
+    const int k1 = pairs[2 * p], k2 = pairs[2 * p + 1];
+    if (k1 < 0 || k1 >= m.capa_elem || k2 < 0 || k2 >= m.capa_elem) {
+      trn_set_error(m.err, TRN_DERR_REPLAY);
+      continue;
+    }
+    const int index = map[k1];
+    bool ok = index >= 0 && index < ntasks && dual[index * 4] == k1;
+    if (ok) {
+      ok = false;
+      for (int q = 1; q < dual_n[index]; ++q) ok |= (dual[index * 4 + q] == k2);
+    }
+    if (!ok) {
+      trn_set_error(m.err, TRN_DERR_REPLAY);
+      continue;
+    }
+    local += flip_pair(m, k1, k2, index, map, dual, dual_n);
+  }
+  if (local) atomicAdd(commit, local);
+}
+
+void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, cudaStream_t s) {
+  k_swap_init_nodes<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  k_swap_init_elems<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, map);
+  check_launch("swap_init");
+}
+
+void swap_filter(const DMesh& m, int nb_elems, uint8_t* flag, cudaStream_t s) {
+  k_swap_filter<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, flag);
+  check_launch("swap_filter");
+}
+
+void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual_n, int* map,
+               cudaStream_t s) {
+  k_swap_dual<<<grid_for(ntasks), TRN_THREADS, 0, s>>>(m, list, ntasks, dual, dual_n, map);
+  check_launch("swap_dual");
+}
+
+void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* map,
+               const int* dual, const int* dual_n, int ntasks, int* commit, cudaStream_t s) {
+  k_swap_flip<<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
+                                                             ntasks, commit);
+  check_launch("swap_flip");
+}
+
+}  // namespace trn

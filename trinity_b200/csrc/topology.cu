@@ -1,0 +1,138 @@
+/*
+ * topology.cu — incidence build and repair.
+ *
+ *   k_count_fill   : vertex -> element stencils from the triangle array
+ *                    (Mesh::rebuildTopology, mesh.cpp:197-210: atomic append)
+ *   k_sort_stencil : sort each stencil (mesh.cpp:244)
+ *   k_build_vicin  : sorted unique vertex adjacency from the stencil
+ *                    (mesh.cpp:214-243 and Mesh::extractPrimalGraph 297-330)
+ *   k_fix_tagged   : the fused stencil repair of Mesh::fixTagged
+ *                    (mesh.cpp:716-760): keep the entries whose element still
+ *                    holds the vertex, sort, drop duplicates, in one pass over
+ *                    the vertex's bucket held in registers/local memory.
+ */
+#include "trn_internal.h"
+#include "trn_numeric.cuh"
+
+namespace trn {
+
+__global__ void k_fill_stencils(DMesh m, int nb_elems) {
+  for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
+    int4 t = m.tri[i];
+    if (t.x < 0) continue;
+    trn_stenc_append(m, t.x, i);
+    trn_stenc_append(m, t.y, i);
+    trn_stenc_append(m, t.z, i);
+  }
+}
+
+__global__ void k_sort_stencils(DMesh m, int nb_nodes) {
+  if (trn_failed(m)) return;
+  int buf[TRN_MAX_DEG];
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    int d = trn_deg(m, v);
+    int* s = m.stenc + (size_t) v * m.bucket;
+    for (int a = 0; a < d; ++a) buf[a] = s[a];
+    trn_isort(buf, d);
+    for (int a = 0; a < d; ++a) s[a] = buf[a];
+  }
+}
+
+/* adjacency of v from its (canonical) stencil */
+__device__ __forceinline__ void build_one_vicin(const DMesh& m, int v) {
+  int buf[2 * TRN_MAX_DEG];
+  int k = 0;
+  if (m.alive[v]) {
+    const int* s = m.stenc + (size_t) v * m.bucket;
+    int d = trn_deg(m, v);
+    for (int a = 0; a < d; ++a) {
+      int4 n = m.tri[s[a]];
+      if (v == n.x) { buf[k++] = n.y; buf[k++] = n.z; }
+      else if (v == n.y) { buf[k++] = n.z; buf[k++] = n.x; }
+      else if (v == n.z) { buf[k++] = n.x; buf[k++] = n.y; }
+    }
+  }
+  trn_isort(buf, k);
+  k = trn_iunique(buf, k);
+  if (k > m.bucket) {
+    trn_set_error(m.err, TRN_DERR_CAPACITY);
+    k = m.bucket;
+  }
+  int* out = m.vic + (size_t) v * m.bucket;
+  for (int a = 0; a < k; ++a) out[a] = buf[a];
+  m.vdeg[v] = k;
+}
+
+__global__ void k_build_vicin(DMesh m, int nb_nodes, int only_flagged) {
+  if (trn_failed(m)) return;
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    if (only_flagged && m.activ[v] == 0) continue;
+    build_one_vicin(m, v);
+  }
+}
+
+__global__ void k_fix_tagged(DMesh m, int nb_nodes) {
+  if (trn_failed(m)) return;
+  int buf[TRN_MAX_DEG];
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    if (!m.fixes[v]) continue;
+    m.fixes[v] = 0;
+    int* s = m.stenc + (size_t) v * m.bucket;
+    int d = trn_deg(m, v);
+    if (d > m.bucket) d = m.bucket;
+    int k = 0;
+    for (int a = 0; a < d; ++a) {
+      int t = s[a];
+      if (t < 0) continue;
+      int4 n = m.tri[t];
+      if (v == n.x || v == n.y || v == n.z) buf[k++] = t;
+    }
+    trn_isort(buf, k);
+    k = trn_iunique(buf, k);
+    for (int a = 0; a < k; ++a) s[a] = buf[a];
+    for (int a = k; a < d; ++a) s[a] = -1;
+    m.deg[v] = k;
+  }
+}
+
+__global__ void k_flag_alive(DMesh m, int nb_nodes) {
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) m.fixes[v] = m.alive[v] ? 1 : 0;
+}
+
+/* cached quality of every live element (swapping.cpp:167-174, smoothing.cpp:145-151) */
+__global__ void k_quality_all(DMesh m, int nb_elems) {
+  if (trn_failed(m)) return;
+  for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
+    int4 t = m.tri[i];
+    if (t.x < 0) continue;
+    m.qual[i] = trn_quality(m.pts[t.x], m.pts[t.y], m.pts[t.z], m.ten[t.x], m.ten[t.y], m.ten[t.z]);
+  }
+}
+
+void build_stencils(const DMesh& m, int nb_nodes, int nb_elems, cudaStream_t s) {
+  cudaMemsetAsync(m.deg, 0, sizeof(int) * (size_t) m.capa_node, s);
+  k_fill_stencils<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems);
+  k_sort_stencils<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  check_launch("build_stencils");
+}
+
+void build_vicin(const DMesh& m, int nb_nodes, bool only_flagged, cudaStream_t s) {
+  k_build_vicin<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, only_flagged ? 1 : 0);
+  check_launch("build_vicin");
+}
+
+void fix_tagged(const DMesh& m, int nb_nodes, cudaStream_t s) {
+  k_fix_tagged<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  check_launch("fix_tagged");
+}
+
+void flag_all_alive(const DMesh& m, int nb_nodes, cudaStream_t s) {
+  k_flag_alive<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+}
+
+void quality_all(const DMesh& m, int nb_elems, cudaStream_t s) {
+  k_quality_all<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems);
+  check_launch("quality_all");
+}
+
+}  // namespace trn

@@ -1,0 +1,754 @@
+/*
+ * trn_api.cu — host orchestration and the C ABI (include/trinity_b200.h).
+ *
+ * The control flow of each run() mirrors the reference's kernel drivers
+ * (Refine::run refinement.cpp:445-493, Coarse::run coarsening.cpp:463-508,
+ * Swap::run swapping.cpp:383-428, Smooth::run smoothing.cpp:274-302); the
+ * loops whose trip count depends on the data read one small status block back
+ * from the device per level (pinned memory, one stream synchronisation).
+ */
+#include "trn_internal.h"
+#include "trn_libm.h"
+#include "../../include/trinity_b200.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace trn;
+
+namespace {
+
+/* status block layout (device and pinned host mirror) */
+enum {
+  S_ERR = 0,
+  S_COMMIT = 1,
+  S_SMOOTH_TASKS = 2,
+  S_SMOOTH_COMMIT = 3,
+  S_NPAIRS = 4,
+  S_NINDEP = 5,
+  S_COUNT = 6,     /* copy of a compaction count */
+  S_PARTS = 8,     /* part offsets, 9 slots */
+  S_SIZE = 32,     /* device status block */
+  H_WIDE = 40,     /* host-only pinned slot for one 8-byte value */
+  H_SIZE = 64,
+};
+
+constexpr int kLoopCap = 100000;
+
+}  // namespace
+
+struct trn_mesh {
+  int nb_nodes = 0, nb_elems = 0;
+  int size0[2] = {0, 0};
+  int capa_node = 0, capa_elem = 0, bucket = 64, depth = 1, verb = 0, rounds = 1;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DMesh d{};
+  double* solut = nullptr;
+  double2* grad = nullptr;
+  double* terms = nullptr;
+  double* complexity = nullptr;
+  int* target = nullptr;
+  uint8_t* flag = nullptr;
+  int* list = nullptr;
+  int* indep = nullptr;
+  int* map = nullptr;
+  int* dual = nullptr;
+  int* dual_n = nullptr;
+  int* pairs = nullptr;
+  int* parts = nullptr;
+  int* status = nullptr;
+  int* h_status = nullptr;
+  ScanWs scan;
+  RefineWs rws;
+  HeurWs hws;
+  /* replay */
+  bool replay = false;
+  std::vector<int32_t> log;
+  int32_t* d_log = nullptr;
+  size_t cursor = 0;
+  /* options */
+  uint64_t seed = 0x7472696e697479ULL;
+  uint64_t calls = 0;
+  bool exact_sum = false;
+  double last_complexity = 0.0;
+  double last_ms = 0.0;
+  std::string err;
+};
+
+namespace {
+
+int fail(trn_mesh* m, int code, const std::string& msg) {
+  if (m) m->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                 \
+  do {                                                                           \
+    cudaError_t e_ = (call);                                                     \
+    if (e_ != cudaSuccess)                                                       \
+      return fail(m, TRN_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+/* copy the status block (and optionally one compaction count) back and sync */
+int sync_status(trn_mesh* m, const int* count = nullptr) {
+  CK(cudaMemcpyAsync(m->h_status, m->status, sizeof(int) * S_SIZE, cudaMemcpyDeviceToHost, m->stream));
+  if (count)
+    CK(cudaMemcpyAsync(m->h_status + S_COUNT, count, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaGetLastError());
+  int e = m->h_status[S_ERR];
+  if (e) {
+    const char* what = e == TRN_DERR_CAPACITY ? "capacity exceeded (stencil bucket, hash or patch)"
+                       : e == TRN_DERR_REPLAY  ? "replay log does not match the mesh"
+                                               : "invalid state";
+    return fail(m, e == TRN_DERR_CAPACITY ? TRN_ERR_CAPACITY
+                   : e == TRN_DERR_REPLAY ? TRN_ERR_REPLAY : TRN_ERR_INVALID,
+                std::string("device: ") + what);
+  }
+  return TRN_OK;
+}
+
+void begin_timing(trn_mesh* m) { cudaEventRecord(m->ev0, m->stream); }
+
+int end_timing(trn_mesh* m, trn_stats* st, int eval, int task) {
+  cudaEventRecord(m->ev1, m->stream);
+  CK(cudaEventSynchronize(m->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, m->ev0, m->ev1);
+  m->last_ms = ms;
+  if (st) {
+    st->eval += eval;
+    st->task += task;
+    st->elap += (int) ms;
+  }
+  return TRN_OK;
+}
+
+/* next replay entry: checks the tag, returns the payload offset and count */
+int replay_take(trn_mesh* m, int tag, size_t* payload, int* n) {
+  if (m->cursor + 2 > m->log.size() || m->log[m->cursor] != tag)
+    return fail(m, TRN_ERR_REPLAY, "replay log: expected entry " + std::to_string(tag) +
+                                       " at " + std::to_string(m->cursor));
+  *n = m->log[m->cursor + 1];
+  *payload = m->cursor + 2;
+  size_t len = 0;
+  if (tag == 1) len = (size_t) *n;
+  else if (tag == 2) len = 2 * (size_t) *n;
+  else {
+    size_t p = *payload;
+    for (int c = 0; c < *n; ++c) {
+      if (p >= m->log.size()) return fail(m, TRN_ERR_REPLAY, "replay log truncated");
+      p += 1 + (size_t) m->log[p];
+    }
+    len = p - *payload;
+  }
+  if (*payload + len > m->log.size()) return fail(m, TRN_ERR_REPLAY, "replay log truncated");
+  m->cursor = *payload + len;
+  return TRN_OK;
+}
+
+template <typename T>
+int dmalloc(trn_mesh* m, T** p, size_t count) {
+  CK(cudaMalloc((void**) p, sizeof(T) * (count ? count : 1)));
+  return TRN_OK;
+}
+
+void release(trn_mesh* m) {
+  if (!m) return;
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  void* bufs[] = {m->d.pts, m->d.ten, m->d.tri, m->d.stenc, m->d.deg, m->d.vic, m->d.vdeg,
+                  m->d.tags, m->d.alive, m->d.fixes, m->d.activ, m->d.qual, m->solut, m->grad,
+                  m->terms, m->complexity, m->target, m->flag, m->list, m->indep, m->map,
+                  m->dual, m->dual_n, m->pairs, m->parts, m->status, m->d_log};
+  for (void* b : bufs) if (b) cudaFree(b);
+  if (m->h_status) cudaFreeHost(m->h_status);
+  scan_ws_free(&m->scan);
+  refine_ws_free(&m->rws);
+  heur_ws_free(&m->hws);
+  if (m->ev0) cudaEventDestroy(m->ev0);
+  if (m->ev1) cudaEventDestroy(m->ev1);
+  if (m->stream) cudaStreamDestroy(m->stream);
+}
+
+/* ---------------- file parsing (io.cpp:25-161) ---------------- */
+struct Reader {
+  std::vector<char> buf;
+  size_t pos = 0;
+  bool open(const char* path) {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return false;
+    std::fseek(f, 0, SEEK_END);
+    long n = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    buf.resize((size_t) n + 1);
+    size_t got = std::fread(buf.data(), 1, (size_t) n, f);
+    std::fclose(f);
+    buf[got] = 0;
+    buf.resize(got + 1);
+    return true;
+  }
+  void skip_ws() {
+    while (pos < buf.size() && (buf[pos] == ' ' || buf[pos] == '\t' || buf[pos] == '\n' || buf[pos] == '\r'))
+      ++pos;
+  }
+  /* io::find: next line whose first token is key; returns the count after it */
+  long find(const char* key) {
+    size_t klen = std::strlen(key);
+    while (pos < buf.size() - 1) {
+      size_t eol = pos;
+      while (eol < buf.size() - 1 && buf[eol] != '\n') ++eol;
+      size_t s = pos;
+      while (s < eol && (buf[s] == ' ' || buf[s] == '\t' || buf[s] == '\r')) ++s;
+      bool hit = (buf[s] != '#' && buf[s] != '%') && eol - s >= klen &&
+                 std::strncmp(&buf[s], key, klen) == 0 &&
+                 (s + klen == eol || buf[s + klen] == ' ' || buf[s + klen] == '\t' || buf[s + klen] == '\r');
+      pos = eol < buf.size() - 1 ? eol + 1 : eol;
+      if (hit) {
+        long c = -1;
+        if (next_long(&c)) return c;
+        return -1;
+      }
+    }
+    return -1;
+  }
+  bool next_long(long* v) {
+    skip_ws();
+    if (pos >= buf.size() - 1) return false;
+    char* end = nullptr;
+    long x = std::strtol(&buf[pos], &end, 10);
+    if (end == &buf[pos]) return false;
+    pos = (size_t) (end - buf.data());
+    *v = x;
+    return true;
+  }
+  bool next_double(double* v) {
+    skip_ws();
+    if (pos >= buf.size() - 1) return false;
+    char* end = nullptr;
+    double x = std::strtod(&buf[pos], &end);
+    if (end == &buf[pos]) return false;
+    pos = (size_t) (end - buf.data());
+    *v = x;
+    return true;
+  }
+  void skip_line() {
+    while (pos < buf.size() - 1 && buf[pos] != '\n') ++pos;
+    if (pos < buf.size() - 1) ++pos;
+  }
+};
+
+}  // namespace
+
+/* ======================================================================== */
+extern "C" {
+
+const char* trn_version(void) { return "trinity_b200 0.1 (sm_100a)"; }
+
+int trn_mesh_create_ex(const int size[2], int bucket, int depth, int verbosity, int rounds,
+                       int capa_scale, trn_mesh** out) {
+  if (!out || !size || size[0] <= 0 || size[1] <= 0 || bucket < 8 || bucket > TRN_MAX_DEG ||
+      depth < 1 || capa_scale < 1)
+    return TRN_ERR_INVALID;
+  *out = nullptr;
+  trn_mesh* m = new trn_mesh();
+  m->size0[0] = size[0];
+  m->size0[1] = size[1];
+  m->bucket = bucket;
+  m->depth = depth;
+  m->verb = verbosity;
+  m->rounds = rounds;
+  m->capa_node = (int) std::min<long long>((long long) size[0] * capa_scale, 1LL << 30);
+  m->capa_elem = (int) std::min<long long>((long long) size[1] * capa_scale, 1LL << 30);
+  const size_t cn = (size_t) m->capa_node, ce = (size_t) m->capa_elem;
+  int rc = TRN_OK;
+  auto bail = [&](int code) {
+    release(m);
+    delete m;
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(TRN_ERR_CUDA);
+  cudaEventCreate(&m->ev0);
+  cudaEventCreate(&m->ev1);
+  DMesh& d = m->d;
+  d.bucket = bucket;
+  d.capa_node = m->capa_node;
+  d.capa_elem = m->capa_elem;
+  if ((rc = dmalloc(m, &d.pts, cn)) || (rc = dmalloc(m, &d.ten, cn)) || (rc = dmalloc(m, &d.tri, ce)) ||
+      (rc = dmalloc(m, &d.stenc, cn * bucket)) || (rc = dmalloc(m, &d.deg, cn)) ||
+      (rc = dmalloc(m, &d.vic, cn * bucket)) || (rc = dmalloc(m, &d.vdeg, cn)) ||
+      (rc = dmalloc(m, &d.tags, cn)) || (rc = dmalloc(m, &d.alive, cn)) ||
+      (rc = dmalloc(m, &d.fixes, cn)) || (rc = dmalloc(m, &d.activ, std::max(cn, ce))) ||
+      (rc = dmalloc(m, &d.qual, ce)) || (rc = dmalloc(m, &m->solut, cn)) ||
+      (rc = dmalloc(m, &m->grad, cn)) || (rc = dmalloc(m, &m->terms, ce + 8192)) ||
+      (rc = dmalloc(m, &m->complexity, 2)) || (rc = dmalloc(m, &m->target, cn)) ||
+      (rc = dmalloc(m, &m->flag, std::max(cn, ce))) || (rc = dmalloc(m, &m->list, std::max(cn, ce))) ||
+      (rc = dmalloc(m, &m->indep, cn)) || (rc = dmalloc(m, &m->map, ce)) ||
+      (rc = dmalloc(m, &m->dual, ce * 4)) || (rc = dmalloc(m, &m->dual_n, ce)) ||
+      (rc = dmalloc(m, &m->pairs, ce * 2)) || (rc = dmalloc(m, &m->parts, cn)) ||
+      (rc = dmalloc(m, &m->status, S_SIZE)))
+    return bail(rc);
+  d.err = m->status + S_ERR;
+  if (cudaMallocHost(&m->h_status, sizeof(int) * H_SIZE) != cudaSuccess) return bail(TRN_ERR_CUDA);
+  scan_ws_alloc(&m->scan, (long long) std::max(cn, ce));
+  refine_ws_alloc(&m->rws, m->capa_node, m->capa_elem);
+  heur_ws_alloc(&m->hws, m->capa_node, m->capa_elem);
+  if (cudaGetLastError() != cudaSuccess) return bail(TRN_ERR_CUDA);
+  *out = m;
+  return TRN_OK;
+}
+
+int trn_mesh_create(const int size[2], int bucket, int depth, int verbosity, int rounds,
+                    trn_mesh** out) {
+  int scale = std::max(3 * (depth - 1), 4);
+  return trn_mesh_create_ex(size, bucket, depth, verbosity, rounds, scale, out);
+}
+
+int trn_mesh_destroy(trn_mesh* m) {
+  if (!m) return TRN_ERR_INVALID;
+  release(m);
+  delete m;
+  return TRN_OK;
+}
+
+int trn_mesh_load_arrays(trn_mesh* m, int nb_nodes, int nb_elems, const double* points,
+                         const int* tris, const uint8_t* tags, const double* solut) {
+  if (!m || !points || !tris || nb_nodes <= 0 || nb_elems <= 0) return fail(m, TRN_ERR_INVALID, "load: bad arguments");
+  if (nb_nodes > m->capa_node || nb_elems > m->capa_elem)
+    return fail(m, TRN_ERR_CAPACITY, "load: mesh larger than the capacity");
+  for (long long i = 0; i < 3LL * nb_elems; ++i)
+    if (tris[i] < 0 || tris[i] >= nb_nodes) return fail(m, TRN_ERR_INVALID, "load: vertex index out of range");
+  DMesh& d = m->d;
+  const size_t cn = (size_t) m->capa_node, ce = (size_t) m->capa_elem, b = (size_t) m->bucket;
+  cudaStream_t s = m->stream;
+  CK(cudaMemsetAsync(d.ten, 0, sizeof(double4) * cn, s));
+  CK(cudaMemsetAsync(d.pts, 0, sizeof(double2) * cn, s));
+  CK(cudaMemsetAsync(d.tri, 0xff, sizeof(int4) * ce, s));
+  CK(cudaMemsetAsync(d.stenc, 0xff, sizeof(int) * cn * b, s));
+  CK(cudaMemsetAsync(d.vic, 0xff, sizeof(int) * cn * b, s));
+  CK(cudaMemsetAsync(d.vdeg, 0, sizeof(int) * cn, s));
+  CK(cudaMemsetAsync(d.tags, 0, cn, s));
+  CK(cudaMemsetAsync(d.alive, 1, cn, s));
+  CK(cudaMemsetAsync(d.fixes, 0, cn, s));
+  CK(cudaMemsetAsync(d.activ, 0, std::max(cn, ce), s));
+  CK(cudaMemsetAsync(d.qual, 0, sizeof(double) * ce, s));
+  CK(cudaMemsetAsync(m->status, 0, sizeof(int) * S_SIZE, s));
+  CK(cudaMemsetAsync(m->map, 0xff, sizeof(int) * ce, s));
+  /* staging: int3 -> int4 triangles; points are already x,y interleaved */
+  std::vector<int4> t4((size_t) nb_elems);
+  for (int i = 0; i < nb_elems; ++i) t4[i] = make_int4(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2], 0);
+  CK(cudaMemcpyAsync(d.pts, points, sizeof(double) * 2 * (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d.tri, t4.data(), sizeof(int4) * (size_t) nb_elems, cudaMemcpyHostToDevice, s));
+  if (tags) CK(cudaMemcpyAsync(d.tags, tags, (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
+  if (solut) CK(cudaMemcpyAsync(m->solut, solut, sizeof(double) * (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
+  else CK(cudaMemsetAsync(m->solut, 0, sizeof(double) * (size_t) nb_nodes, s));
+  m->nb_nodes = nb_nodes;
+  m->nb_elems = nb_elems;
+  m->cursor = 0;
+  build_stencils(d, nb_nodes, nb_elems, s);
+  build_vicin(d, nb_nodes, false, s);
+  return sync_status(m);
+}
+
+int trn_mesh_load(trn_mesh* m, const char* mesh_path, const char* solut_path) {
+  if (!m || !mesh_path) return fail(m, TRN_ERR_INVALID, "load: null path");
+  Reader r;
+  if (!r.open(mesh_path)) return fail(m, TRN_ERR_IO, std::string("cannot open ") + mesh_path);
+  long nv = r.find("Vertices");
+  if (nv <= 0) return fail(m, TRN_ERR_IO, "mesh: no Vertices section");
+  std::vector<double> pts((size_t) nv * 2);
+  std::vector<uint8_t> tags((size_t) nv, 0);
+  for (long i = 0; i < nv; ++i) {
+    long tag;
+    if (!r.next_double(&pts[2 * i]) || !r.next_double(&pts[2 * i + 1]) || !r.next_long(&tag))
+      return fail(m, TRN_ERR_IO, "mesh: truncated Vertices");
+  }
+  size_t after_v = r.pos;
+  long ne = r.find("Edges");
+  if (ne > 0) {
+    for (long i = 0; i < ne; ++i) {
+      long a, b, tag;
+      if (!r.next_long(&a) || !r.next_long(&b) || !r.next_long(&tag))
+        return fail(m, TRN_ERR_IO, "mesh: truncated Edges");
+      if (a < 1 || a > nv || b < 1 || b > nv) return fail(m, TRN_ERR_IO, "mesh: edge index out of range");
+      tags[a - 1] = TRN_TAG_BOUND;
+      tags[b - 1] = TRN_TAG_BOUND;
+    }
+  } else {
+    r.pos = after_v;
+  }
+  long nt = r.find("Triangles");
+  if (nt <= 0) return fail(m, TRN_ERR_IO, "mesh: no Triangles section");
+  std::vector<int> tris((size_t) nt * 3);
+  for (long i = 0; i < nt; ++i) {
+    long a, b, c, tag;
+    if (!r.next_long(&a) || !r.next_long(&b) || !r.next_long(&c) || !r.next_long(&tag))
+      return fail(m, TRN_ERR_IO, "mesh: truncated Triangles");
+    tris[3 * i] = (int) a - 1;
+    tris[3 * i + 1] = (int) b - 1;
+    tris[3 * i + 2] = (int) c - 1;
+  }
+  size_t after_t = r.pos;
+  long nc = r.find("Corners");
+  if (nc > 0) {
+    for (long i = 0; i < nc; ++i) {
+      long v;
+      if (!r.next_long(&v)) return fail(m, TRN_ERR_IO, "mesh: truncated Corners");
+      if (v < 1 || v > nv) return fail(m, TRN_ERR_IO, "mesh: corner index out of range");
+      tags[v - 1] = TRN_TAG_BOUND | TRN_TAG_CORNER;
+    }
+  } else {
+    r.pos = after_t;
+  }
+  if (nv != m->size0[0] || nt != m->size0[1])
+    return fail(m, TRN_ERR_IO, "mesh: sizes differ from the ones the mesh was created with");
+  std::vector<double> u((size_t) nv, 0.0);
+  if (solut_path) {
+    Reader rb;
+    if (!rb.open(solut_path)) return fail(m, TRN_ERR_IO, std::string("cannot open ") + solut_path);
+    long hdr[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 4; ++k)
+      if (!rb.next_long(&hdr[k])) return fail(m, TRN_ERR_IO, "bb: bad header");
+    if (hdr[2] != nv) return fail(m, TRN_ERR_IO, "bb: wrong number of vertices in solution file");
+    rb.pos = 0;
+    rb.skip_line();
+    for (long i = 0; i < nv; ++i)
+      if (!rb.next_double(&u[i])) return fail(m, TRN_ERR_IO, "bb: truncated values");
+  }
+  return trn_mesh_load_arrays(m, (int) nv, (int) nt, pts.data(), tris.data(), tags.data(), u.data());
+}
+
+int trn_mesh_export(trn_mesh* m, double* points, double* tensor, int* tris, uint8_t* alive,
+                    uint8_t* tags) {
+  if (!m) return TRN_ERR_INVALID;
+  const size_t nn = (size_t) m->nb_nodes, ne = (size_t) m->nb_elems;
+  cudaStream_t s = m->stream;
+  if (points) CK(cudaMemcpyAsync(points, m->d.pts, sizeof(double2) * nn, cudaMemcpyDeviceToHost, s));
+  std::vector<double4> t4;
+  std::vector<int4> e4;
+  if (tensor) {
+    t4.resize(nn);
+    CK(cudaMemcpyAsync(t4.data(), m->d.ten, sizeof(double4) * nn, cudaMemcpyDeviceToHost, s));
+  }
+  if (tris) {
+    e4.resize(ne);
+    CK(cudaMemcpyAsync(e4.data(), m->d.tri, sizeof(int4) * ne, cudaMemcpyDeviceToHost, s));
+  }
+  if (alive) CK(cudaMemcpyAsync(alive, m->d.alive, nn, cudaMemcpyDeviceToHost, s));
+  if (tags) CK(cudaMemcpyAsync(tags, m->d.tags, nn, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (size_t i = 0; i < t4.size(); ++i) {
+    tensor[3 * i] = t4[i].x;
+    tensor[3 * i + 1] = t4[i].y;
+    tensor[3 * i + 2] = t4[i].z;
+  }
+  for (size_t i = 0; i < e4.size(); ++i) {
+    tris[3 * i] = e4[i].x;
+    tris[3 * i + 1] = e4[i].y;
+    tris[3 * i + 2] = e4[i].z;
+  }
+  return TRN_OK;
+}
+
+int trn_mesh_counts(trn_mesh* m, int* nb_nodes, int* nb_elems, int* live_nodes, int* live_elems) {
+  if (!m) return TRN_ERR_INVALID;
+  if (nb_nodes) *nb_nodes = m->nb_nodes;
+  if (nb_elems) *nb_elems = m->nb_elems;
+  if (live_nodes || live_elems) {
+    std::vector<uint8_t> alive((size_t) m->nb_nodes);
+    std::vector<int4> e4((size_t) m->nb_elems);
+    CK(cudaMemcpyAsync(alive.data(), m->d.alive, alive.size(), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaMemcpyAsync(e4.data(), m->d.tri, sizeof(int4) * e4.size(), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    if (live_nodes) *live_nodes = (int) std::count(alive.begin(), alive.end(), (uint8_t) 1);
+    if (live_elems) {
+      int c = 0;
+      for (auto& t : e4) c += t.x >= 0;
+      *live_elems = c;
+    }
+  }
+  return TRN_OK;
+}
+
+/* Mesh::store, io.cpp:164-255 */
+int trn_mesh_store(trn_mesh* m, const char* path) {
+  if (!m || !path) return fail(m, TRN_ERR_INVALID, "store: null path");
+  const int nn = m->nb_nodes, ne = m->nb_elems;
+  std::vector<double> pts((size_t) nn * 2);
+  std::vector<int> tri((size_t) ne * 3);
+  std::vector<uint8_t> alive((size_t) nn), tags((size_t) nn);
+  int rc = trn_mesh_export(m, pts.data(), nullptr, tri.data(), alive.data(), tags.data());
+  if (rc) return rc;
+  FILE* f = std::fopen(path, "w");
+  if (!f) return fail(m, TRN_ERR_IO, std::string("cannot write ") + path);
+  int real_nodes = 0, real_elems = 0;
+  for (int i = 0; i < nn; ++i) real_nodes += alive[i] ? 1 : 0;
+  for (int i = 0; i < ne; ++i) real_elems += tri[3 * i] > -1 ? 1 : 0;
+  std::fprintf(f, "MeshVersionFormatted 1\nDimension 2\nVertices\n%d\n", real_nodes);
+  std::vector<int> index((size_t) nn, -1), required;
+  int k = 0;
+  for (int i = 0; i < nn; ++i) {
+    if (!alive[i]) continue;
+    std::fprintf(f, "%.8f\t%.8f\t0\n", pts[2 * i], pts[2 * i + 1]);
+    index[i] = ++k;
+    if (tags[i] & TRN_TAG_BOUND) required.push_back(k);
+  }
+  std::fprintf(f, "\nTriangles\n%d\n", real_elems);
+  for (int i = 0; i < ne; ++i) {
+    const int* n = &tri[3 * i];
+    if (n[0] > -1) std::fprintf(f, "%d\t%d\t%d\t0\n", index[n[0]], index[n[1]], index[n[2]]);
+  }
+  std::fprintf(f, "\nRequiredVertices\n%zu\n", required.size());
+  for (int v : required) std::fprintf(f, "%d\n", v);
+  std::fprintf(f, "\nEnd\n");
+  std::fclose(f);
+  return TRN_OK;
+}
+
+int trn_mesh_store_sol(trn_mesh* m, const char* path) {
+  if (!m || !path) return fail(m, TRN_ERR_INVALID, "store_sol: null path");
+  const int nn = m->nb_nodes;
+  std::vector<double> ten((size_t) nn * 3);
+  std::vector<uint8_t> alive((size_t) nn);
+  int rc = trn_mesh_export(m, nullptr, ten.data(), nullptr, alive.data(), nullptr);
+  if (rc) return rc;
+  FILE* f = std::fopen(path, "w");
+  if (!f) return fail(m, TRN_ERR_IO, std::string("cannot write ") + path);
+  int real = 0;
+  for (int i = 0; i < nn; ++i) real += alive[i] ? 1 : 0;
+  std::fprintf(f, "MeshVersionFormatted 1\nDimension 2\nSolAtVertices\n%d\n1 3\n", real);
+  for (int i = 0; i < nn; ++i)
+    if (alive[i]) std::fprintf(f, "%.17g %.17g %.17g\n", ten[3 * i], ten[3 * i + 1], ten[3 * i + 2]);
+  std::fprintf(f, "\nEnd\n");
+  std::fclose(f);
+  return TRN_OK;
+}
+
+int trn_set_replay(trn_mesh* m, const int32_t* log, size_t n) {
+  if (!m) return TRN_ERR_INVALID;
+  if (m->d_log) {
+    cudaFree(m->d_log);
+    m->d_log = nullptr;
+  }
+  m->log.clear();
+  m->cursor = 0;
+  m->replay = false;
+  if (!log || n == 0) return TRN_OK;
+  m->log.assign(log, log + n);
+  CK(cudaMalloc(&m->d_log, sizeof(int32_t) * n));
+  CK(cudaMemcpy(m->d_log, log, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+  m->replay = true;
+  return TRN_OK;
+}
+
+int trn_set_options(trn_mesh* m, uint64_t seed, int exact_sum) {
+  if (!m) return TRN_ERR_INVALID;
+  m->seed = seed;
+  m->exact_sum = exact_sum != 0;
+  return TRN_OK;
+}
+
+double trn_last_complexity(trn_mesh* m) { return m ? m->last_complexity : 0.0; }
+double trn_last_time_ms(trn_mesh* m) { return m ? m->last_ms : 0.0; }
+void* trn_mesh_stream(trn_mesh* m) { return m ? (void*) m->stream : nullptr; }
+const char* trn_last_error(trn_mesh* m) { return m ? m->err.c_str() : "null mesh"; }
+
+/* Metrics::run, metric.cpp:59-70 */
+int trn_metric_run(trn_mesh* m, double target_factor, int norm, double h_min, double h_max,
+                   trn_stats* st) {
+  if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "metric: no mesh loaded");
+  if (norm < 0 || h_min <= 0 || h_max <= 0) return fail(m, TRN_ERR_INVALID, "metric: bad parameters");
+  m->err.clear();
+  MetricParams p;
+  p.target = (double) (int) std::floor(m->nb_nodes * target_factor);
+  p.scale_exp = norm ? -1. / (2 * norm + 2) : 0.5;
+  p.eig_min = 1 / trn_pow(h_min, 2);
+  p.eig_max = 1 / trn_pow(h_max, 2);
+  begin_timing(m);
+  metric_run(m->d, m->nb_nodes, m->nb_elems, m->solut, m->grad, m->terms, m->complexity,
+             m->exact_sum || m->replay, p, m->stream);
+  CK(cudaMemcpyAsync(m->h_status + H_WIDE, m->complexity, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  int rc = sync_status(m);
+  if (rc) return rc;
+  std::memcpy(&m->last_complexity, m->h_status + H_WIDE, sizeof(double));
+  return end_timing(m, st, m->nb_nodes, m->nb_nodes);
+}
+
+/* Refine::run, refinement.cpp:445-493 */
+int trn_refine_run(trn_mesh* m, int depth, trn_stats* st) {
+  if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "refine: no mesh loaded");
+  if (depth < 1) return fail(m, TRN_ERR_INVALID, "refine: depth < 1");
+  m->err.clear();
+  begin_timing(m);
+  cudaStream_t s = m->stream;
+  refine_reset_hash(m->rws, s);
+  int eval = 0, task = 0;
+  for (int level = 0; level < depth; ++level) {
+    refine_filter(m->d, m->nb_elems, m->rws, s);
+    scan_i64(m->rws.cnt, m->rws.off, m->nb_elems, m->scan, s);
+    long long tot = 0;
+    CK(cudaMemcpyAsync(m->h_status + H_WIDE, m->scan.total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    int rc = sync_status(m);
+    if (rc) return rc;
+    std::memcpy(&tot, m->h_status + H_WIDE, sizeof(long long));
+    const int split = (int) (tot >> 32), adds = (int) (tot & 0xffffffffLL);
+    eval += m->nb_elems;
+    if (adds == 0) break;
+    task += adds;
+    if ((long long) m->nb_nodes + split > m->capa_node || (long long) m->nb_elems + adds > m->capa_elem)
+      return fail(m, TRN_ERR_CAPACITY, "refine: node or element capacity exceeded");
+    refine_apply(m->d, m->nb_nodes, m->nb_elems, m->rws, s);
+    m->nb_nodes += split;
+    m->nb_elems += adds;
+  }
+  flag_all_alive(m->d, m->nb_nodes, s);
+  fix_tagged(m->d, m->nb_nodes, s);
+  int rc = sync_status(m);
+  if (rc) return rc;
+  return end_timing(m, st, eval, task);
+}
+
+/* Coarse::run, coarsening.cpp:463-508 */
+int trn_coarsen_run(trn_mesh* m, int max_colors, trn_stats* st) {
+  if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "coarsen: no mesh loaded");
+  (void) max_colors;
+  m->err.clear();
+  begin_timing(m);
+  cudaStream_t s = m->stream;
+  coarsen_pre(m->d, m->nb_nodes, s);
+  int eval = 0, task = 0, nb_indep = 0, level = 0;
+  do {
+    build_vicin(m->d, m->nb_nodes, true, s);
+    coarsen_filter(m->d, m->nb_nodes, m->target, m->flag, s);
+    compact_u8(m->flag, m->nb_nodes, m->list, m->scan, s);
+    int rc = sync_status(m, m->scan.count);
+    if (rc) return rc;
+    const int ntasks = m->h_status[S_COUNT];
+    if (!ntasks) break;
+    eval += ntasks;
+    const int* indep;
+    const int* count;
+    if (m->replay) {
+      size_t off;
+      int n;
+      if ((rc = replay_take(m, 1, &off, &n))) return rc;
+      indep = m->d_log + off;
+      count = m->d_log + off - 1;
+      nb_indep = n;
+    } else {
+      mis_jp(m->d, m->nb_nodes, m->flag, m->list, ntasks, m->seed ^ (++m->calls * 0x9e37ULL), m->hws,
+             m->indep, m->status + S_NINDEP, m->scan, s);
+      indep = m->indep;
+      count = m->status + S_NINDEP;
+    }
+    collapse(m->d, indep, count, m->target, m->flag, s);
+    fix_tagged(m->d, m->nb_nodes, s);
+    if (!m->replay) {
+      if ((rc = sync_status(m))) return rc;
+      nb_indep = m->h_status[S_NINDEP];
+    }
+    task += nb_indep;
+    if (++level > kLoopCap) return fail(m, TRN_ERR_NO_PROGRESS, "coarsen: level cap reached");
+  } while (nb_indep);
+  int rc = sync_status(m);
+  if (rc) return rc;
+  return end_timing(m, st, eval, task);
+}
+
+/* Swap::run, swapping.cpp:383-428 */
+int trn_swap_run(trn_mesh* m, trn_stats* st) {
+  if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "swap: no mesh loaded");
+  m->err.clear();
+  begin_timing(m);
+  cudaStream_t s = m->stream;
+  swap_init(m->d, m->nb_nodes, m->nb_elems, m->map, s);
+  int eval = 0, task = 0, commit = 0, level = 0;
+  do {
+    swap_filter(m->d, m->nb_elems, m->flag, s);
+    compact_u8(m->flag, m->nb_elems, m->list, m->scan, s);
+    int rc = sync_status(m, m->scan.count);
+    if (rc) return rc;
+    const int ntasks = m->h_status[S_COUNT];
+    if (!ntasks) break;
+    eval += ntasks;
+    swap_dual(m->d, m->list, ntasks, m->dual, m->dual_n, m->map, s);
+    const int* pairs;
+    const int* npairs;
+    if (m->replay) {
+      size_t off;
+      int n;
+      if ((rc = replay_take(m, 2, &off, &n))) return rc;
+      pairs = m->d_log + off;
+      npairs = m->d_log + off - 1;
+    } else {
+      match_handshake(m->d, m->nb_elems, m->dual, m->dual_n, ntasks, m->map,
+                      m->seed ^ (++m->calls * 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s);
+      pairs = m->pairs;
+      npairs = m->status + S_NPAIRS;
+    }
+    CK(cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s));
+    swap_flip(m->d, pairs, npairs, m->map, m->dual, m->dual_n, ntasks, m->status + S_COMMIT, s);
+    fix_tagged(m->d, m->nb_nodes, s);
+    if ((rc = sync_status(m))) return rc;
+    commit = m->h_status[S_COMMIT];
+    task += commit / 2;
+    if (++level > kLoopCap) return fail(m, TRN_ERR_NO_PROGRESS, "swap: level cap reached");
+  } while (commit);
+  return end_timing(m, st, eval, task);
+}
+
+/* Smooth::run, smoothing.cpp:274-302 */
+int trn_smooth_run(trn_mesh* m, int max_colors, int depth, trn_stats* st) {
+  if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "smooth: no mesh loaded");
+  int max_col = std::max(6, max_colors) - 1;  /* Partit: max.part = max(6, n), colors 1..max.part-1 */
+  if (max_col > 30) max_col = 30;
+  m->err.clear();
+  begin_timing(m);
+  cudaStream_t s = m->stream;
+  smooth_pre(m->d, m->nb_nodes, s);
+  build_vicin(m->d, m->nb_nodes, true, s);
+  std::vector<std::pair<const int*, int>> classes;
+  if (m->replay) {
+    size_t off;
+    int parts;
+    int rc = replay_take(m, 3, &off, &parts);
+    if (rc) return rc;
+    size_t p = off;
+    for (int c = 0; c < parts; ++c) {
+      int n = m->log[p];
+      classes.emplace_back(m->d_log + p + 1, n);
+      p += 1 + (size_t) n;
+    }
+  } else {
+    color_jp(m->d, m->nb_nodes, max_col, m->seed ^ (++m->calls * 0xc01dULL), m->hws, m->parts,
+             m->status + S_PARTS, s);
+    int rc = sync_status(m);
+    if (rc) return rc;
+    for (int c = 0; c < max_col && c < 8; ++c) {
+      int a = m->h_status[S_PARTS + c], b = m->h_status[S_PARTS + c + 1];
+      classes.emplace_back(m->parts + a, b - a);
+    }
+  }
+  quality_all(m->d, m->nb_elems, s);
+  CK(cudaMemsetAsync(m->status + S_SMOOTH_TASKS, 0, sizeof(int) * 2, s));
+  for (int level = 0; level < depth; ++level)
+    for (auto& c : classes) smooth_color(m->d, c.first, c.second, m->status + S_SMOOTH_TASKS, s);
+  int rc = sync_status(m);
+  if (rc) return rc;
+  return end_timing(m, st, m->h_status[S_SMOOTH_TASKS], m->h_status[S_SMOOTH_COMMIT]);
+}
+
+int trn_round_run(trn_mesh* m, int depth, trn_stats stats[4]) {
+  int rc;
+  if ((rc = trn_refine_run(m, depth, stats ? stats + 0 : nullptr))) return rc;
+  if ((rc = trn_coarsen_run(m, 8, stats ? stats + 1 : nullptr))) return rc;
+  if ((rc = trn_swap_run(m, stats ? stats + 2 : nullptr))) return rc;
+  return trn_smooth_run(m, 8, depth, stats ? stats + 3 : nullptr);
+}
+
+}  /* extern "C" */

@@ -1,0 +1,150 @@
+/*
+ * trn_common.cuh — device-side mesh layout and helpers shared by all kernels.
+ *
+ * HBM layout of one mesh (capacities fixed at creation; ids are never reused,
+ * deleted entities keep their slot):
+ *   pts   double2[capa_node]        vertex coordinates
+ *   ten   double4[capa_node]        metric tensor (m11, m12, m22, unused):
+ *                                   32-byte records, one sector per gather
+ *   tri   int4[capa_elem]           vertex ids (x,y,z), x = -1 when erased
+ *   stenc int[capa_node * bucket]   vertex -> incident elements (the
+ *                                   reference's "stencil", mesh.h:112), first
+ *                                   deg[v] slots used, appended atomically
+ *   vic   int[capa_node * bucket]   vertex -> adjacent vertices, sorted
+ *                                   (the reference's "vicin", mesh.h:113)
+ *   tags/alive/fixes  uint8 per vertex; activ int8 shared by vertices and
+ *                                   elements exactly like mesh.h:146
+ *   qual  double[capa_elem]         cached element quality
+ */
+#ifndef TRN_COMMON_CUH
+#define TRN_COMMON_CUH
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define TRN_TAG_BOUND 4   /* header.h:58 */
+#define TRN_TAG_CORNER 8  /* header.h:59 */
+#define TRN_MAX_PART 8    /* main.cpp:42, Partit(&mesh, 8) */
+#define TRN_MATCHED (-2)  /* matching.h:27 */
+
+/* device error word values (mirror the C-ABI codes) */
+#define TRN_DERR_CAPACITY 1
+#define TRN_DERR_INVALID 3
+#define TRN_DERR_REPLAY 6
+
+/* per-thread scratch limits (local memory) */
+#define TRN_MAX_PATCH 512   /* 2-ring element patch of the metric */
+#define TRN_MAX_DEG 256     /* stencil entries of one vertex (bucket <= 256) */
+
+#define TRN_THREADS 256
+
+struct DMesh {
+  double2* pts;
+  double4* ten;
+  int4* tri;
+  int* stenc;
+  int* deg;
+  int* vic;
+  int* vdeg;
+  uint8_t* tags;
+  uint8_t* alive;
+  uint8_t* fixes;
+  int8_t* activ;
+  double* qual;
+  int* err;        /* device error word: first error wins */
+  int bucket;
+  int capa_node;
+  int capa_elem;
+};
+
+__device__ __forceinline__ void trn_set_error(int* err, int code) {
+  atomicCAS(err, 0, code);
+}
+
+/* compare-and-swap 0 -> 1 on a byte flag (sync.h:33-38 compareAndSwap) */
+__device__ __forceinline__ void trn_flag_on(uint8_t* f) {
+  if (*(volatile uint8_t*) f == 0) *f = 1;
+}
+
+__device__ __forceinline__ void trn_activ_on(int8_t* a) {
+  /* CAS(activ, 0, 1): corners hold -1 and must keep it */
+  unsigned int* word = (unsigned int*) ((uintptr_t) a & ~(uintptr_t) 3);
+  unsigned int shift = ((uintptr_t) a & 3) * 8;
+  unsigned int old = *word, assumed;
+  do {
+    if (((old >> shift) & 0xffu) != 0u) return;
+    assumed = old;
+    old = atomicCAS(word, assumed, assumed | (1u << shift));
+  } while (old != assumed);
+}
+
+/* once any kernel raised the error word, later kernels of the call do no
+ * work: a failed append may have left unwritten stencil slots behind */
+__device__ __forceinline__ bool trn_failed(const DMesh& m) {
+  return *(volatile int*) m.err != 0;
+}
+
+/* used stencil length of v, never beyond its bucket (an overflowing append
+ * only raises the error word, so the counter itself may exceed it) */
+__device__ __forceinline__ int trn_deg(const DMesh& m, int v) {
+  int d = m.deg[v];
+  return d < m.bucket ? d : m.bucket;
+}
+
+/* append element t to the stencil of v (mesh.cpp:468-494 updateStencil) */
+__device__ __forceinline__ void trn_stenc_append(const DMesh& m, int v, int t) {
+  int k = atomicAdd(m.deg + v, 1);
+  if (k >= m.bucket) {
+    trn_set_error(m.err, TRN_DERR_CAPACITY);
+    return;
+  }
+  m.stenc[(size_t) v * m.bucket + k] = t;
+}
+
+__device__ __forceinline__ void trn_stenc_append_n(const DMesh& m, int v, const int* t, int n) {
+  int k = atomicAdd(m.deg + v, n);
+  if (k + n > m.bucket) {
+    trn_set_error(m.err, TRN_DERR_CAPACITY);
+    return;
+  }
+  int* s = m.stenc + (size_t) v * m.bucket + k;
+  for (int i = 0; i < n; ++i) s[i] = t[i];
+}
+
+__device__ __forceinline__ void trn_isort(int* a, int n) {
+  for (int i = 1; i < n; ++i) {
+    int x = a[i], j = i - 1;
+    while (j >= 0 && a[j] > x) {
+      a[j + 1] = a[j];
+      --j;
+    }
+    a[j + 1] = x;
+  }
+}
+
+__device__ __forceinline__ int trn_iunique(int* a, int n) {
+  if (n == 0) return 0;
+  int k = 1;
+  for (int i = 1; i < n; ++i)
+    if (a[i] != a[k - 1]) a[k++] = a[i];
+  return k;
+}
+
+/* 64-bit mix for seeded hash priorities (splitmix64 finaliser) */
+__device__ __forceinline__ uint64_t trn_hash64(uint64_t x) {
+  x += 0x9e3779b97f4a7c15ULL;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+  return x ^ (x >> 31);
+}
+
+/* priority of id under seed: unique for distinct ids (id in the low bits) */
+__device__ __forceinline__ uint64_t trn_prio(uint64_t seed, int id) {
+  return (trn_hash64(seed ^ ((uint64_t) (uint32_t) id * 0x632be59bd9b4e019ULL)) & ~0xffffffffULL) |
+         (uint32_t) id;
+}
+
+__device__ __forceinline__ int trn_grid_stride() { return gridDim.x * blockDim.x; }
+__device__ __forceinline__ int trn_tid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+
+#endif

@@ -1,0 +1,116 @@
+/*
+ * trn_internal.h — host-side launchers shared between the kernel files and the
+ * C-ABI implementation. Not installed; the public interface is
+ * include/trinity_b200.h.
+ */
+#ifndef TRN_INTERNAL_H
+#define TRN_INTERNAL_H
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "trn_common.cuh"
+
+namespace trn {
+
+/* grid for a grid-stride kernel over n items: a multiple of the SM count */
+int grid_for(long long n, int threads = TRN_THREADS);
+
+/* scratch used by the scans: tile sums of up to max_n items */
+struct ScanWs {
+  long long* tile = nullptr;   /* per-tile sums / offsets */
+  int* count = nullptr;        /* device total (compaction) */
+  long long* total = nullptr;  /* device total (scan) */
+  int max_tiles = 0;
+};
+void scan_ws_alloc(ScanWs* ws, long long max_n);
+void scan_ws_free(ScanWs* ws);
+
+/* exclusive scan of n int64 values; *ws.total receives the sum */
+void scan_i64(const long long* in, long long* out, int n, ScanWs& ws, cudaStream_t s);
+/* ordered compaction: list[k] = i for the k-th i < n with flags[i] != 0;
+ * *ws.count receives the number kept */
+void compact_u8(const uint8_t* flags, int n, int* list, ScanWs& ws, cudaStream_t s);
+
+/* topology (topology.cu) */
+void build_stencils(const DMesh& m, int nb_nodes, int nb_elems, cudaStream_t s);
+void build_vicin(const DMesh& m, int nb_nodes, bool only_flagged, cudaStream_t s);
+void fix_tagged(const DMesh& m, int nb_nodes, cudaStream_t s);
+void flag_all_alive(const DMesh& m, int nb_nodes, cudaStream_t s);
+void quality_all(const DMesh& m, int nb_elems, cudaStream_t s);
+
+/* metric (metric.cu) */
+struct MetricParams {
+  double target;      /* floor(V * target_factor) */
+  double scale_exp;   /* -1/(2p+2) or 0.5 */
+  double eig_min;     /* 1/h_min^2 */
+  double eig_max;     /* 1/h_max^2 */
+};
+void metric_run(const DMesh& m, int nb_nodes, int nb_elems, const double* solut,
+                double2* grad, double* terms, double* complexity, bool exact_sum,
+                const MetricParams& p, cudaStream_t s);
+
+/* refinement (refine.cu) */
+struct RefineWs {
+  int4* info = nullptr;            /* per element: masks, opp[3] */
+  long long* cnt = nullptr;        /* per element: pushes << 32 | pattern */
+  long long* off = nullptr;        /* exclusive scan of cnt */
+  unsigned long long* hkey = nullptr; /* (min,max) -> steiner id */
+  int* hval = nullptr;
+  unsigned long long hcap = 0;     /* power of two */
+};
+void refine_ws_alloc(RefineWs* ws, int capa_node, int capa_elem);
+void refine_ws_free(RefineWs* ws);
+void refine_reset_hash(RefineWs& ws, cudaStream_t s);
+void refine_filter(const DMesh& m, int nb_elems, RefineWs& ws, cudaStream_t s);
+void refine_apply(const DMesh& m, int nb_nodes, int nb_elems, RefineWs& ws, cudaStream_t s);
+
+/* coarsening (coarsen.cu) */
+void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
+void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, cudaStream_t s);
+void collapse(const DMesh& m, const int* indep, const int* count, const int* target,
+              const uint8_t* cand_flag, cudaStream_t s);
+
+/* swapping (swap.cu) */
+void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, cudaStream_t s);
+void swap_filter(const DMesh& m, int nb_elems, uint8_t* flag, cudaStream_t s);
+void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual_n, int* map,
+               cudaStream_t s);
+void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* map,
+               const int* dual, const int* dual_n, int ntasks, int* commit, cudaStream_t s);
+
+/* smoothing (smooth.cu) */
+void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
+void smooth_color(const DMesh& m, const int* list, int n, int* counters, cudaStream_t s);
+
+/* graph heuristics, free mode (heuristics.cu) */
+struct HeurWs {
+  uint8_t* state = nullptr;      /* per vertex / element */
+  unsigned long long* prop = nullptr;
+  int* choice = nullptr;
+  int* color = nullptr;
+  int* mate = nullptr;
+  int* cnt = nullptr;            /* small device counters */
+};
+void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem);
+void heur_ws_free(HeurWs* ws);
+/* Jones-Plassmann MIS over candidates (flag != 0) with adjacency vic;
+ * writes the set to indep[0..*count) */
+void mis_jp(const DMesh& m, int nb_nodes, const uint8_t* cand_flag, const int* cand_list,
+            int ncand, uint64_t seed, HeurWs& ws, int* indep, int* count, ScanWs& scan,
+            cudaStream_t s);
+/* handshake matching on the dual rows; pairs[2k], pairs[2k+1]; *npairs */
+void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n,
+                     int ntasks, const int* map, uint64_t seed, HeurWs& ws, int* pairs,
+                     int* npairs, cudaStream_t s);
+/* Jones-Plassmann first-fit coloring of interior vertices, colors 1..max_col;
+ * parts: vertex ids grouped by color, part_off[c] offsets (c = 0..max_col) */
+void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& ws,
+              int* parts, int* part_off, cudaStream_t s);
+
+void check_launch(const char* what);
+
+}  // namespace trn
+
+#endif
