@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Adaptation-round throughput on B200: adapted triangles per second per full
+round (trinity's refine + coarsen + swap + smooth, graph heuristics and
+topology repairs included), on the 2M-triangle unit-square workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one full adaptation of a fresh copy of the workload: the mesh is
+restored on the device from its resident input (no host transfer), the metric
+is recovered, then 3 rounds run. ``value`` = sum over rounds of the live
+triangles at round start / sum of the rounds' device times (CUDA events on
+the library's stream; the metric stage is excluded, as in the reference's
+per-kernel Stats). ``e2e`` runs the same adaptation through the C ABI from
+host arrays (load, metric, 3 rounds, export) with the transfers inside the
+timed region. Under torchrun each rank adapts its own copy (weak scaling);
+times are the max over ranks.
+
+``--impl reference`` times trinity's own OpenMP implementation (built from its
+sources into oracle/_ref/, all host cores) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+from trinity_b200 import meshgen  # noqa: E402
+
+WORKLOAD = "c2"
+METRIC = "adapted triangles/s per full round"
+UNIT = "triangles/s"
+REF_BIN = os.path.join(REPO, "oracle", "_ref", "trinity_ref")
+
+
+def workload_config():
+    m, u, c = meshgen.make_config(WORKLOAD)
+    cfg = {
+        "workload": "unit square 1000x1000 grid, 1,002,001 vertices / 2,000,000 triangles, "
+                    "interior jitter 0.2h (seed 2), field tanh+gauss+waves, target 0.7, "
+                    "L^2 norm, depth 2, bucket 128, 3 rounds",
+        "mode": "free (GPU heuristics)",
+        "data": "synthetic, generated by trinity_b200/meshgen.py",
+        "l2": "working set larger than L2 (mesh restored every step)",
+    }
+    return m, u, c, cfg
+
+
+def tags_of(m):
+    t = np.zeros(m.nb_nodes, dtype=np.uint8)
+    t[m.edges.ravel()] = 4
+    t[m.corners] = 12
+    return t
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_step(api, g, c, heur, kern):
+    """One adaptation on a mesh already holding the input; returns
+    (sum of live triangles at round starts, sum of round device ms, metric ms)."""
+    api.Metrics(g, c["target"], c["norm"]).run()
+    metric_ms = g.last_time_ms()
+    tin, tms = 0, 0.0
+    for _ in range(c["rounds"]):
+        tin += g.counts()[3]
+        for k in kern:
+            k.run()
+            tms += g.last_time_ms()
+    return tin, tms, metric_ms
+
+
+def b200_arm(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from trinity_b200 import _lib, api
+
+    torch.cuda.set_device(local_rank)
+    dist_on = world > 1
+    m, u, c, cfg = workload_config()
+    tags = tags_of(m)
+    g = api.Mesh((m.nb_nodes, m.nb_elems), c["bucket"], c["depth"], 0, c["rounds"])
+    g.load_arrays(m.points, m.tris, tags, u)
+    g.set_options(seed=0x7472696E697479 + rank)
+    heur = api.Partit(g, 8)
+    kern = [api.Refine(g, c["depth"]), api.Coarse(g, heur), api.Swap(g), api.Smooth(g, heur, c["depth"])]
+
+    def barrier():
+        if dist_on:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        g.reload()
+        run_step(api, g, c, heur, kern)
+    torch.cuda.synchronize()
+
+    # ---- timed region (device-resident input) ----
+    _lib.profile_enable(True)
+    launches0 = _lib.launch_count()
+    tin_sum, tms_sum, metric_ms = 0, 0.0, []
+    barrier()
+    torch.cuda.synchronize()
+    with Clocks(torch.cuda.current_device()) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            g.reload()
+            tin, tms, mms = run_step(api, g, c, heur, kern)
+            tin_sum += tin
+            tms_sum += tms
+            metric_ms.append(mms)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    barrier()
+    launches = _lib.launch_count() - launches0
+    prof = _lib.profile_read()
+    _lib.profile_enable(False)
+    final = g.counts()
+
+    # ---- end-to-end through the C ABI from host buffers ----
+    pts = np.ascontiguousarray(m.points)
+    tris = np.ascontiguousarray(m.tris, dtype=np.int32)
+    e2e_tin, e2e_t, d2h = 0, 0.0, 0
+    h2d = pts.nbytes + tris.nbytes + tags.nbytes + u.nbytes
+    barrier()
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        g.load_arrays(pts, tris, tags, u)
+        tin, _, _ = run_step(api, g, c, heur, kern)
+        out = g.export()
+        e2e_t += time.perf_counter() - t0
+        e2e_tin += tin
+        d2h = sum(a.nbytes for a in out)
+
+    stats = np.array([tin_sum, tms_sum, wall, e2e_tin, e2e_t], dtype=np.float64)
+    if dist_on:
+        t = torch.tensor(stats, device="cuda")
+        sums = t.clone()
+        dist.all_reduce(sums, op=dist.ReduceOp.SUM)
+        maxs = t.clone()
+        dist.all_reduce(maxs, op=dist.ReduceOp.MAX)
+        tin_all, tms_max, wall_max = sums[0].item(), maxs[1].item(), maxs[2].item()
+        e2e_tin_all, e2e_max = sums[3].item(), maxs[4].item()
+    else:
+        tin_all, tms_max, wall_max, e2e_tin_all, e2e_max = stats.tolist()
+    if rank != 0:
+        return None
+
+    value = tin_all / (tms_max / 1e3)
+    dom = max(prof, key=lambda r: r["ms"]) if prof else None
+    roofline = None
+    peaks = {}
+    pk = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    if dom:
+        per_launch_bytes = dom["bytes"] / max(dom["launches"], 1)
+        per_launch_s = dom["ms"] / max(dom["launches"], 1) / 1e3
+        achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
+        roofline = {"kernel": dom["kernel"], "bound": "hbm", "achieved": round(achieved, 2),
+                    "peak": hbm_peak, "peak_source": "measured" if peaks else "fallback",
+                    "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                    "traffic": None, "launches": dom["launches"],
+                    "avg_launch_us": round(per_launch_s * 1e6, 2),
+                    "share_of_kernel_time": round(dom["ms"] / sum(r["ms"] for r in prof), 3)}
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(wall_max / args.steps * 1e3, 3),
+        "round_ms_per_step": round(tms_max / args.steps, 3),
+        "metric_ms_per_step": round(float(np.mean(metric_ms)), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": cfg,
+        "e2e": {"value": round(e2e_tin_all / e2e_max, 1), "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "note": "host arrays -> C ABI load, metric, 3 rounds, export; wall clock"},
+        "gpu_launches": int(launches),
+        "roofline": roofline,
+        "kernels": sorted(({"kernel": r["kernel"], "launches": r["launches"], "ms": round(r["ms"], 3)}
+                           for r in prof), key=lambda r: -r["ms"])[:8],
+        "final_mesh": {"nodes": final[2], "triangles": final[3]},
+        "clocks": clk.summary(),
+    }
+    return line
+
+
+# ------------------------------------------------------------------ reference
+def ensure_files():
+    d = os.path.join(tempfile.gettempdir(), "trinity_b200_bench")
+    mp, bp = os.path.join(d, f"{WORKLOAD}.mesh"), os.path.join(d, f"{WORKLOAD}.bb")
+    if not (os.path.exists(mp) and os.path.exists(bp)):
+        meshgen.write_config(WORKLOAD, d)
+    return mp, bp
+
+
+def reference_once(mp, bp, c, threads):
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close", OMP_PLACES="cores")
+    r = subprocess.run([REF_BIN, mp, bp, str(c["rounds"]), str(c["depth"]), str(c["bucket"]),
+                        str(c["target"]), str(c["norm"]), "--capa-depth", "4", "--time"],
+                       env=env, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference failed: {r.stderr[-400:]}")
+    j = json.loads(r.stdout.strip().splitlines()[-1])
+    return sum(j["tri_in"]), j["rounds_ms"], j
+
+
+def physical_cores():
+    try:
+        import psutil
+        n = psutil.cpu_count(logical=False)
+        if n:
+            return n
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
+def cpu_baseline():
+    """The reference on the host cores, one full adaptation of the workload."""
+    _, _, c = meshgen.make_config(WORKLOAD)
+    if not os.path.exists(REF_BIN):
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/trinity_ref not built"}
+    mp, bp = ensure_files()
+    cores = physical_cores()
+    tin, ms, j = reference_once(mp, bp, c, cores)
+    return {"value": round(tin / (ms / 1e3), 1), "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"one full adaptation of the workload (metric + 3 rounds; rounds timed: "
+                      f"{ms:.0f} ms, metric {j['metric_ms']:.0f} ms)",
+            "final_mesh": {"nodes": j["nodes_out"], "triangles": j["elems_out"]}}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return None
+    _, _, c = meshgen.make_config(WORKLOAD)
+    _, _, _, cfg = workload_config()
+    cfg["mode"] = "reference OpenMP build, its own heuristics"
+    if not os.path.exists(REF_BIN):
+        return {"impl": "reference", "unavailable": "oracle/_ref/trinity_ref was not built "
+                "(needs the reference sources at build time)"}
+    mp, bp = ensure_files()
+    cores = physical_cores()
+    for _ in range(args.warmup):
+        reference_once(mp, bp, c, cores)
+    tin_sum, ms_sum, walls = 0, 0.0, []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        tin, ms, j = reference_once(mp, bp, c, cores)
+        walls.append(time.perf_counter() - t0)
+        tin_sum += tin
+        ms_sum += ms
+    value = tin_sum / (ms_sum / 1e3)
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_sum / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": "full adaptation per step (metric + 3 rounds), rounds timed by "
+                                   "the harness around each kernel run"},
+        "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "final_mesh": {"nodes": j["nodes_out"], "triangles": j["elems_out"]},
+    }
+
+
+def main():
+    p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    args = p.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if "RANK" not in os.environ:
+        world = 1
+
+    if args.impl == "reference":
+        line = reference_arm(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        line = b200_arm(args, rank, world, local_rank)
+        if line is not None:
+            if world == 1 and not args.no_cpu_baseline:
+                line["cpu_baseline"] = cpu_baseline()
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

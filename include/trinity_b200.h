@@ -57,6 +57,9 @@ int trn_mesh_load(trn_mesh* mesh, const char* mesh_path, const char* solut_path)
  * boundary, 12 = boundary|corner, header.h:55-60), solut[V] */
 int trn_mesh_load_arrays(trn_mesh* mesh, int nb_nodes, int nb_elems, const double* points,
                          const int* tris, const uint8_t* tags, const double* solut);
+/* restore the state right after the last load, from device-resident copies
+ * of its input (no host transfer); for repeated runs on one input */
+int trn_mesh_reload(trn_mesh* mesh);
 /* replaces Mesh::store(path) (mesh.h:66, io.cpp:164-255) */
 int trn_mesh_store(trn_mesh* mesh, const char* path);
 /* metric field in medit .sol format (the reference writes none; an addition) */
@@ -103,6 +106,17 @@ double trn_last_time_ms(trn_mesh* mesh);
 void* trn_mesh_stream(trn_mesh* mesh);
 /* message of the last error on this mesh ("" if none) */
 const char* trn_last_error(trn_mesh* mesh);
+/* Per-kernel device timing, process-wide: enable (resets the totals) or
+ * disable; read back per-kernel launches, milliseconds and algorithmic bytes.
+ * No counterpart in the reference (its timers are per-step wall clocks,
+ * timer.h:42-48). */
+int trn_profile_enable(int on);
+int trn_profile_count(void);
+/* kernels launched by this library since the process started */
+unsigned long long trn_launch_count(void);
+int trn_profile_entry(int i, char* name, int name_len, long long* launches, double* ms,
+                      double* bytes);
+
 /* library version string */
 const char* trn_version(void);
 

@@ -72,6 +72,12 @@ def lib():
         L.trn_last_error.argtypes = [pmesh]
         L.trn_last_error.restype = ctypes.c_char_p
         L.trn_version.restype = ctypes.c_char_p
+        L.trn_mesh_reload.argtypes = [pmesh]
+        L.trn_profile_enable.argtypes = [ip]
+        L.trn_profile_count.restype = ip
+        L.trn_profile_entry.argtypes = [ip, ctypes.c_char_p, ip, ctypes.POINTER(ctypes.c_longlong),
+                                        ctypes.POINTER(dp), ctypes.POINTER(dp)]
+        L.trn_launch_count.restype = ctypes.c_ulonglong
         _lib = L
     return _lib
 
@@ -80,3 +86,26 @@ class TrinityError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"{ERRORS.get(code, code)}: {message}")
         self.code = code
+
+
+def profile_enable(on: bool) -> None:
+    """Per-kernel device timing (process-wide); enabling resets the totals."""
+    lib().trn_profile_enable(1 if on else 0)
+
+
+def profile_read() -> list[dict]:
+    L = lib()
+    out = []
+    for i in range(L.trn_profile_count()):
+        name = ctypes.create_string_buffer(64)
+        n = ctypes.c_longlong()
+        ms = ctypes.c_double()
+        by = ctypes.c_double()
+        L.trn_profile_entry(i, name, 64, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(by))
+        out.append({"kernel": name.value.decode(), "launches": n.value, "ms": ms.value,
+                    "bytes": by.value})
+    return out
+
+
+def launch_count() -> int:
+    return int(lib().trn_launch_count())

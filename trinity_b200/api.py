@@ -92,6 +92,10 @@ class Mesh:
         self._check(self._L.trn_mesh_load_arrays(self.h, pts.shape[0], tr.shape[0], _p(pts), _p(tr),
                                                  _p(tg), _p(u)))
 
+    def reload(self) -> None:
+        """Back to the state right after the last load (device-side copy)."""
+        self._check(self._L.trn_mesh_reload(self.h))
+
     def store(self, path: str) -> None:
         self._check(self._L.trn_mesh_store(self.h, path.encode()))
 

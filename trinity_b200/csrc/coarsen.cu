@@ -167,17 +167,22 @@ __global__ void k_collapse(DMesh m, const int* __restrict__ indep, const int* co
 
 void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s) {
   k_coarse_pre<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  note_launch();
   check_launch("coarsen_pre");
 }
 
 void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, cudaStream_t s) {
+  ProfScope ps("coarsen_filter", s, (double) nb_nodes * (1 + 1 + 4 + 1));
   k_coarse_filter<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, flag);
+  note_launch();
   check_launch("coarsen_filter");
 }
 
 void collapse(const DMesh& m, const int* indep, const int* count, const int* target,
               const uint8_t* cand_flag, cudaStream_t s) {
+  ProfScope ps("collapse", s, 0.0);
   k_collapse<<<grid_for(m.capa_node), TRN_THREADS, 0, s>>>(m, indep, count, target, cand_flag);
+  note_launch();
   check_launch("collapse");
 }
 

@@ -71,19 +71,24 @@ void mis_jp(const DMesh& m, int nb_nodes, const uint8_t* cand_flag, const int* c
   (void) nb_nodes;
   (void) cand_flag;
   (void) scan;
+  ProfScope ps("mis_jp", s, 0.0);
   const int g = grid_for(ncand);
   k_mis_init<<<g, TRN_THREADS, 0, s>>>(ws.state, cand_list, ncand);
+  note_launch();
   int host_left = 1;
   for (int batch = 0; batch < 64 && host_left; ++batch) {
     cudaMemsetAsync(ws.cnt, 0, sizeof(int) * 4, s);
     for (int r = 0; r < 4; ++r)
       k_mis_round<<<g, TRN_THREADS, 0, s>>>(m, ws.state, cand_list, ncand, seed, ws.cnt + r);
+      note_launch();
     cudaMemcpyAsync(&host_left, ws.cnt + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
   }
   cudaMemsetAsync(count, 0, sizeof(int), s);
   k_mis_collect<<<g, TRN_THREADS, 0, s>>>(ws.state, cand_list, ncand, indep, count);
+  note_launch();
   k_mis_clear<<<g, TRN_THREADS, 0, s>>>(ws.state, cand_list, ncand);
+  note_launch();
   check_launch("mis_jp");
 }
 
@@ -158,15 +163,20 @@ void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* d
                      cudaStream_t s) {
   (void) nb_elems;
   (void) m;
+  ProfScope ps("match_handshake", s, 0.0);
   const int g = grid_for(ntasks);
   cudaMemsetAsync(npairs, 0, sizeof(int), s);
   k_match_reset<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.mate, ws.prop);
+  note_launch();
   for (int r = 0; r < 6; ++r) {
     k_match_propose<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.mate, ws.prop, ws.choice,
                                                seed, r);
+    note_launch();
     k_match_accept<<<g, TRN_THREADS, 0, s>>>(dual, ntasks, map, ws.mate, ws.prop, ws.choice, seed,
                                               r, pairs, npairs);
+    note_launch();
     k_match_prop_clear<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.prop);
+    note_launch();
   }
   check_launch("match_handshake");
 }
@@ -238,6 +248,7 @@ __global__ void k_color_scatter(int nb_nodes, int* color, int* cursor, int* part
 
 void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& ws, int* parts,
               int* part_off, cudaStream_t s) {
+  ProfScope ps("color_jp", s, 0.0);
   const int g = grid_for(nb_nodes);
   int host_left = 1;
   int round = 0;
@@ -245,6 +256,7 @@ void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& 
     cudaMemsetAsync(ws.cnt, 0, sizeof(int) * 4, s);
     for (int r = 0; r < 4; ++r, ++round)
       k_color_round<<<g, TRN_THREADS, 0, s>>>(m, nb_nodes, ws.color, max_col, seed, round, ws.cnt + r);
+      note_launch();
     cudaMemcpyAsync(&host_left, ws.cnt + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
   }
@@ -252,8 +264,11 @@ void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& 
   int* cursor = ws.cnt + 40;  /* 32 slots */
   cudaMemsetAsync(cnt, 0, sizeof(int) * 32, s);
   k_color_count<<<g, TRN_THREADS, 0, s>>>(m, nb_nodes, ws.color, cnt, max_col);
+  note_launch();
   k_color_offsets<<<1, 32, 0, s>>>(cnt, part_off, cursor, max_col);
+  note_launch();
   k_color_scatter<<<g, TRN_THREADS, 0, s>>>(nb_nodes, ws.color, cursor, parts, max_col);
+  note_launch();
   check_launch("color_jp");
 }
 

@@ -238,19 +238,35 @@ __global__ void k_normalize(DMesh m, int nb_nodes, const double* complexity, dou
 void metric_run(const DMesh& m, int nb_nodes, int nb_elems, const double* solut, double2* grad,
                 double* terms, double* complexity, bool exact_sum, const MetricParams& p,
                 cudaStream_t s) {
+  const double V = nb_nodes, E = nb_elems;
+  {
+  ProfScope ps("metric_gradient", s, V * (2 * kIdx + kAvgDeg * kIdx * 2 + 8 + kPt + 16) + E * kTri);
   k_gradient<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, solut, grad);
+  note_launch();
+  }
+  {
+  ProfScope ps("metric_hessian", s, V * (2 * kIdx + kAvgDeg * kIdx * 2 + 16 + kPt + kTen) + E * kTri);
   k_hessian_local<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, grad, p.scale_exp);
+  note_launch();
+  }
+  ProfScope ps("metric_complexity", s, E * (kTri + 8) + V * (kPt + kTen));
   k_complexity_term<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, terms);
+  note_launch();
   if (exact_sum) {
     k_sum_sequential<<<1, 32, 0, s>>>(terms, nb_elems, complexity);
+    note_launch();
   } else {
     int nb = grid_for(nb_elems);
     /* partials live after the terms (terms has capa_elem + grid slots) */
     k_sum_partial<<<nb, TRN_THREADS, 0, s>>>(terms, nb_elems, terms + m.capa_elem);
+    note_launch();
     k_sum_final<<<1, TRN_THREADS, 0, s>>>(terms + m.capa_elem, nb, complexity);
+    note_launch();
   }
+  ProfScope ps2("metric_normalize", s, V * 2 * kTen);
   k_normalize<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, complexity, p.target,
                                                           p.eig_min, p.eig_max);
+  note_launch();
   check_launch("metric_run");
 }
 

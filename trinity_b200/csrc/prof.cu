@@ -1,0 +1,137 @@
+/*
+ * prof.cu — optional per-launch device timing.
+ *
+ * When enabled, every kernel launcher brackets its launch(es) with a pair of
+ * CUDA events on the launching stream; after the next stream synchronisation
+ * the elapsed times are folded into per-kernel totals together with the
+ * launcher's algorithmic byte count (distinct entries the launch must touch,
+ * each counted once, no cache credit). Disabled, a scope costs one branch.
+ */
+#include "trn_internal.h"
+
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace trn {
+
+namespace {
+
+struct Pending {
+  int id;
+  cudaEvent_t a, b;
+  double bytes;
+};
+
+struct Total {
+  std::string name;
+  long long launches = 0;
+  double ms = 0.0;
+  double bytes = 0.0;
+};
+
+struct Profiler {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  std::vector<Pending> pending;
+  std::vector<Total> totals;
+
+  cudaEvent_t get() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+
+  int id_of(const char* name) {
+    for (size_t i = 0; i < totals.size(); ++i)
+      if (totals[i].name == name) return (int) i;
+    totals.push_back(Total());
+    totals.back().name = name;
+    return (int) totals.size() - 1;
+  }
+};
+
+Profiler& prof() {
+  static Profiler p;
+  return p;
+}
+
+}  // namespace
+
+ProfScope::ProfScope(const char* name, cudaStream_t s, double bytes) : stream_(s) {
+  Profiler& p = prof();
+  if (!p.on) return;
+  id_ = p.id_of(name);
+  bytes_ = bytes;
+  a_ = p.get();
+  cudaEventRecord(a_, s);
+}
+
+ProfScope::~ProfScope() {
+  Profiler& p = prof();
+  if (!p.on || id_ < 0) return;
+  cudaEvent_t b = p.get();
+  cudaEventRecord(b, stream_);
+  p.pending.push_back({id_, a_, b, bytes_});
+}
+
+static unsigned long long g_launches = 0;
+
+void note_launch() { ++g_launches; }
+
+void prof_flush() {
+  Profiler& p = prof();
+  for (auto& q : p.pending) {
+    cudaEventSynchronize(q.b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, q.a, q.b);
+    Total& t = p.totals[q.id];
+    t.launches += 1;
+    t.ms += ms;
+    t.bytes += q.bytes;
+    p.pool.push_back(q.a);
+    p.pool.push_back(q.b);
+  }
+  p.pending.clear();
+}
+
+}  // namespace trn
+
+extern "C" {
+
+int trn_profile_enable(int on) {
+  trn::Profiler& p = trn::prof();
+  trn::prof_flush();
+  p.on = on != 0;
+  if (p.on) p.totals.clear();
+  return 0;
+}
+
+unsigned long long trn_launch_count(void) { return trn::g_launches; }
+
+int trn_profile_count(void) {
+  trn::prof_flush();
+  return (int) trn::prof().totals.size();
+}
+
+int trn_profile_entry(int i, char* name, int name_len, long long* launches, double* ms,
+                      double* bytes) {
+  trn::Profiler& p = trn::prof();
+  if (i < 0 || i >= (int) p.totals.size()) return 3;
+  const trn::Total& t = p.totals[i];
+  if (name && name_len > 0) {
+    std::strncpy(name, t.name.c_str(), (size_t) name_len - 1);
+    name[name_len - 1] = 0;
+  }
+  if (launches) *launches = t.launches;
+  if (ms) *ms = t.ms;
+  if (bytes) *bytes = t.bytes;
+  return 0;
+}
+
+}  // extern "C"

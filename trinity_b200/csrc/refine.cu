@@ -238,15 +238,23 @@ void refine_reset_hash(RefineWs& ws, cudaStream_t s) {
 }
 
 void refine_filter(const DMesh& m, int nb_elems, RefineWs& ws, cudaStream_t s) {
+  ProfScope ps("refine_filter", s, (double) nb_elems * (kTri + 16 + 8) + (double) nb_elems / 2 * (kPt + kTen));
   k_ref_filter<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.cnt);
+  note_launch();
   check_launch("refine_filter");
 }
 
 void refine_apply(const DMesh& m, int nb_nodes, int nb_elems, RefineWs& ws, cudaStream_t s) {
+  {
+  ProfScope ps("refine_steiner", s, (double) nb_elems * (16 + 8));
   k_ref_steiner<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
                                                             ws.hkey, ws.hval, ws.hcap);
+  note_launch();
+  }
+  ProfScope ps("refine_cut", s, (double) nb_elems * (16 + 8 + kTri));
   k_ref_cut<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.off, ws.hkey,
                                                         ws.hval, ws.hcap);
+  note_launch();
   check_launch("refine_apply");
 }
 

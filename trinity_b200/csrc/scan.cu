@@ -164,9 +164,13 @@ void scan_i64(const long long* in, long long* out, int n, ScanWs& ws, cudaStream
     cudaMemsetAsync(ws.total, 0, sizeof(long long), s);
     return;
   }
+  ProfScope ps("scan", s, (double) n * 16);
   k_tile_sum_i64<<<ntiles, TRN_THREADS, 0, s>>>(in, n, ws.tile);
+  note_launch();
   k_scan_tiles<<<1, TRN_THREADS, 0, s>>>(ws.tile, ntiles, ws.total, nullptr);
+  note_launch();
   k_tile_scan_i64<<<ntiles, TRN_THREADS, 0, s>>>(in, out, n, ws.tile);
+  note_launch();
 }
 
 void compact_u8(const uint8_t* flags, int n, int* list, ScanWs& ws, cudaStream_t s) {
@@ -175,9 +179,13 @@ void compact_u8(const uint8_t* flags, int n, int* list, ScanWs& ws, cudaStream_t
     cudaMemsetAsync(ws.count, 0, sizeof(int), s);
     return;
   }
+  ProfScope ps("compact", s, (double) n * 2);
   k_tile_count_u8<<<ntiles, TRN_THREADS, 0, s>>>(flags, n, ws.tile);
+  note_launch();
   k_scan_tiles<<<1, TRN_THREADS, 0, s>>>(ws.tile, ntiles, nullptr, ws.count);
+  note_launch();
   k_tile_compact_u8<<<ntiles, TRN_THREADS, 0, s>>>(flags, n, list, ws.tile);
+  note_launch();
 }
 
 int grid_for(long long n, int threads) {

@@ -17,6 +17,8 @@
 #include "trn_internal.h"
 #include "trn_numeric.cuh"
 
+#include <algorithm>
+
 namespace trn {
 
 __global__ void k_smooth_pre(DMesh m, int nb_nodes) {
@@ -105,12 +107,21 @@ __global__ void k_smooth_move(DMesh m, const int* __restrict__ list, int n, int*
 
 void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s) {
   k_smooth_pre<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  note_launch();
   check_launch("smooth_pre");
 }
 
 void smooth_color(const DMesh& m, const int* list, int n, int* counters, cudaStream_t s) {
   if (n <= 0) return;
+  /* per moved vertex: list id, flag, counts, own point/tensor read+write,
+   * stencil and adjacency rows, its elements and their cached qualities
+   * (read+write); neighbours' points/tensors once each (at most 6 per vertex,
+   * at most every vertex) */
+  const double own = 4 + 1 + 8 + 2 * (kPt + kTen) + kAvgDeg * (2 * kIdx + kTri + 2 * kQ);
+  const double nbr = (double) std::min<long long>((long long) m.capa_node, 6LL * n) * (kPt + kTen);
+  ProfScope ps("smooth_move", s, n * own + nbr);
   k_smooth_move<<<grid_for(n, 128), 128, 0, s>>>(m, list, n, counters);
+  note_launch();
   check_launch("smooth_color");
 }
 

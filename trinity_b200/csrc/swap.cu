@@ -170,26 +170,36 @@ __global__ void k_swap_flip(DMesh m, const int* __restrict__ pairs, const int* n
 }
 
 void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, cudaStream_t s) {
+  ProfScope ps("swap_init", s, (double) nb_nodes + (double) nb_elems * (kTri + kQ + 4 + 1) +
+                                 (double) nb_elems / 2 * (kPt + kTen));
   k_swap_init_nodes<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  note_launch();
   k_swap_init_elems<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, map);
+  note_launch();
   check_launch("swap_init");
 }
 
 void swap_filter(const DMesh& m, int nb_elems, uint8_t* flag, cudaStream_t s) {
+  ProfScope ps("swap_filter", s, (double) nb_elems * 3);
   k_swap_filter<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, flag);
+  note_launch();
   check_launch("swap_filter");
 }
 
 void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual_n, int* map,
                cudaStream_t s) {
+  ProfScope ps("swap_dual", s, (double) ntasks * (4 + kTri + 2 * kAvgDeg * (kIdx + kTri) + 16 + 4 + 4));
   k_swap_dual<<<grid_for(ntasks), TRN_THREADS, 0, s>>>(m, list, ntasks, dual, dual_n, map);
+  note_launch();
   check_launch("swap_dual");
 }
 
 void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* map,
                const int* dual, const int* dual_n, int ntasks, int* commit, cudaStream_t s) {
+  ProfScope ps("swap_flip", s, 0.0);
   k_swap_flip<<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
                                                              ntasks, commit);
+  note_launch();
   check_launch("swap_flip");
 }
 

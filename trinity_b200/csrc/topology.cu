@@ -109,29 +109,59 @@ __global__ void k_quality_all(DMesh m, int nb_elems) {
   }
 }
 
+__global__ void k_count_live(DMesh m, int nb_nodes, int nb_elems, int* out) {
+  int cv = 0, ce = 0;
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) cv += m.alive[v] ? 1 : 0;
+  for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) ce += m.tri[i].x >= 0 ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) {
+    cv += __shfl_down_sync(0xffffffffu, cv, o);
+    ce += __shfl_down_sync(0xffffffffu, ce, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (cv) atomicAdd(out, cv);
+    if (ce) atomicAdd(out + 1, ce);
+  }
+}
+
+void count_live(const DMesh& m, int nb_nodes, int nb_elems, int* out, cudaStream_t s) {
+  cudaMemsetAsync(out, 0, sizeof(int) * 2, s);
+  k_count_live<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_nodes, nb_elems, out);
+  note_launch();
+}
+
 void build_stencils(const DMesh& m, int nb_nodes, int nb_elems, cudaStream_t s) {
+  ProfScope ps("build_stencils", s, 3.0 * nb_elems * (kTri + 2 * kIdx) + 2.0 * nb_nodes * kIdx);
   cudaMemsetAsync(m.deg, 0, sizeof(int) * (size_t) m.capa_node, s);
   k_fill_stencils<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems);
+  note_launch();
   k_sort_stencils<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  note_launch();
   check_launch("build_stencils");
 }
 
 void build_vicin(const DMesh& m, int nb_nodes, bool only_flagged, cudaStream_t s) {
+  ProfScope ps("build_vicin", s, (double) nb_nodes * (1 + 2 * kIdx + kAvgDeg * (kIdx + kTri + kIdx)));
   k_build_vicin<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, only_flagged ? 1 : 0);
+  note_launch();
   check_launch("build_vicin");
 }
 
 void fix_tagged(const DMesh& m, int nb_nodes, cudaStream_t s) {
+  ProfScope ps("fix_tagged", s, (double) nb_nodes);
   k_fix_tagged<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  note_launch();
   check_launch("fix_tagged");
 }
 
 void flag_all_alive(const DMesh& m, int nb_nodes, cudaStream_t s) {
   k_flag_alive<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  note_launch();
 }
 
 void quality_all(const DMesh& m, int nb_elems, cudaStream_t s) {
+  ProfScope ps("quality_all", s, (double) nb_elems * (kTri + kQ) + (double) nb_elems / 2 * (kPt + kTen));
   k_quality_all<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems);
+  note_launch();
   check_launch("quality_all");
 }
 

@@ -33,6 +33,7 @@ enum {
   S_NINDEP = 5,
   S_COUNT = 6,     /* copy of a compaction count */
   S_PARTS = 8,     /* part offsets, 9 slots */
+  S_LIVE = 18,     /* live vertices, live elements */
   S_SIZE = 32,     /* device status block */
   H_WIDE = 40,     /* host-only pinned slot for one 8-byte value */
   H_SIZE = 64,
@@ -64,6 +65,11 @@ struct trn_mesh {
   int* parts = nullptr;
   int* status = nullptr;
   int* h_status = nullptr;
+  /* the last loaded input, kept on the device for trn_mesh_reload */
+  double2* pts0 = nullptr;
+  int4* tri0 = nullptr;
+  uint8_t* tags0 = nullptr;
+  int n0_nodes = 0, n0_elems = 0;
   ScanWs scan;
   RefineWs rws;
   HeurWs hws;
@@ -102,6 +108,7 @@ int sync_status(trn_mesh* m, const int* count = nullptr) {
     CK(cudaMemcpyAsync(m->h_status + S_COUNT, count, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
   CK(cudaStreamSynchronize(m->stream));
   CK(cudaGetLastError());
+  prof_flush();
   int e = m->h_status[S_ERR];
   if (e) {
     const char* what = e == TRN_DERR_CAPACITY ? "capacity exceeded (stencil bucket, hash or patch)"
@@ -165,7 +172,8 @@ void release(trn_mesh* m) {
   void* bufs[] = {m->d.pts, m->d.ten, m->d.tri, m->d.stenc, m->d.deg, m->d.vic, m->d.vdeg,
                   m->d.tags, m->d.alive, m->d.fixes, m->d.activ, m->d.qual, m->solut, m->grad,
                   m->terms, m->complexity, m->target, m->flag, m->list, m->indep, m->map,
-                  m->dual, m->dual_n, m->pairs, m->parts, m->status, m->d_log};
+                  m->dual, m->dual_n, m->pairs, m->parts, m->status, m->d_log, m->pts0,
+                  m->tri0, m->tags0};
   for (void* b : bufs) if (b) cudaFree(b);
   if (m->h_status) cudaFreeHost(m->h_status);
   scan_ws_free(&m->scan);
@@ -316,15 +324,11 @@ int trn_mesh_destroy(trn_mesh* m) {
   return TRN_OK;
 }
 
-int trn_mesh_load_arrays(trn_mesh* m, int nb_nodes, int nb_elems, const double* points,
-                         const int* tris, const uint8_t* tags, const double* solut) {
-  if (!m || !points || !tris || nb_nodes <= 0 || nb_elems <= 0) return fail(m, TRN_ERR_INVALID, "load: bad arguments");
-  if (nb_nodes > m->capa_node || nb_elems > m->capa_elem)
-    return fail(m, TRN_ERR_CAPACITY, "load: mesh larger than the capacity");
-  for (long long i = 0; i < 3LL * nb_elems; ++i)
-    if (tris[i] < 0 || tris[i] >= nb_nodes) return fail(m, TRN_ERR_INVALID, "load: vertex index out of range");
+/* state of a freshly loaded mesh from the device copies pts0/tri0/tags0 */
+static int init_from_device(trn_mesh* m) {
   DMesh& d = m->d;
   const size_t cn = (size_t) m->capa_node, ce = (size_t) m->capa_elem, b = (size_t) m->bucket;
+  const int nb_nodes = m->n0_nodes, nb_elems = m->n0_elems;
   cudaStream_t s = m->stream;
   CK(cudaMemsetAsync(d.ten, 0, sizeof(double4) * cn, s));
   CK(cudaMemsetAsync(d.pts, 0, sizeof(double2) * cn, s));
@@ -339,20 +343,55 @@ int trn_mesh_load_arrays(trn_mesh* m, int nb_nodes, int nb_elems, const double* 
   CK(cudaMemsetAsync(d.qual, 0, sizeof(double) * ce, s));
   CK(cudaMemsetAsync(m->status, 0, sizeof(int) * S_SIZE, s));
   CK(cudaMemsetAsync(m->map, 0xff, sizeof(int) * ce, s));
-  /* staging: int3 -> int4 triangles; points are already x,y interleaved */
-  std::vector<int4> t4((size_t) nb_elems);
-  for (int i = 0; i < nb_elems; ++i) t4[i] = make_int4(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2], 0);
-  CK(cudaMemcpyAsync(d.pts, points, sizeof(double) * 2 * (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(d.tri, t4.data(), sizeof(int4) * (size_t) nb_elems, cudaMemcpyHostToDevice, s));
-  if (tags) CK(cudaMemcpyAsync(d.tags, tags, (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
-  if (solut) CK(cudaMemcpyAsync(m->solut, solut, sizeof(double) * (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
-  else CK(cudaMemsetAsync(m->solut, 0, sizeof(double) * (size_t) nb_nodes, s));
+  CK(cudaMemcpyAsync(d.pts, m->pts0, sizeof(double2) * (size_t) nb_nodes, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(d.tri, m->tri0, sizeof(int4) * (size_t) nb_elems, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(d.tags, m->tags0, (size_t) nb_nodes, cudaMemcpyDeviceToDevice, s));
   m->nb_nodes = nb_nodes;
   m->nb_elems = nb_elems;
   m->cursor = 0;
   build_stencils(d, nb_nodes, nb_elems, s);
   build_vicin(d, nb_nodes, false, s);
   return sync_status(m);
+}
+
+int trn_mesh_load_arrays(trn_mesh* m, int nb_nodes, int nb_elems, const double* points,
+                         const int* tris, const uint8_t* tags, const double* solut) {
+  if (!m || !points || !tris || nb_nodes <= 0 || nb_elems <= 0) return fail(m, TRN_ERR_INVALID, "load: bad arguments");
+  if (nb_nodes > m->capa_node || nb_elems > m->capa_elem)
+    return fail(m, TRN_ERR_CAPACITY, "load: mesh larger than the capacity");
+  for (long long i = 0; i < 3LL * nb_elems; ++i)
+    if (tris[i] < 0 || tris[i] >= nb_nodes) return fail(m, TRN_ERR_INVALID, "load: vertex index out of range");
+  cudaStream_t s = m->stream;
+  if (nb_nodes > m->n0_nodes || nb_elems > m->n0_elems || !m->pts0) {
+    cudaFree(m->pts0);
+    cudaFree(m->tri0);
+    cudaFree(m->tags0);
+    m->pts0 = nullptr;
+    m->tri0 = nullptr;
+    m->tags0 = nullptr;
+    int rc;
+    if ((rc = dmalloc(m, &m->pts0, (size_t) nb_nodes)) || (rc = dmalloc(m, &m->tri0, (size_t) nb_elems)) ||
+        (rc = dmalloc(m, &m->tags0, (size_t) nb_nodes)))
+      return rc;
+  }
+  /* staging: int3 -> int4 triangles; points are already x,y interleaved */
+  std::vector<int4> t4((size_t) nb_elems);
+  for (int i = 0; i < nb_elems; ++i) t4[i] = make_int4(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2], 0);
+  CK(cudaMemcpyAsync(m->pts0, points, sizeof(double) * 2 * (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(m->tri0, t4.data(), sizeof(int4) * (size_t) nb_elems, cudaMemcpyHostToDevice, s));
+  if (tags) CK(cudaMemcpyAsync(m->tags0, tags, (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
+  else CK(cudaMemsetAsync(m->tags0, 0, (size_t) nb_nodes, s));
+  if (solut) CK(cudaMemcpyAsync(m->solut, solut, sizeof(double) * (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
+  else CK(cudaMemsetAsync(m->solut, 0, sizeof(double) * (size_t) nb_nodes, s));
+  m->n0_nodes = nb_nodes;
+  m->n0_elems = nb_elems;
+  return init_from_device(m);
+}
+
+int trn_mesh_reload(trn_mesh* m) {
+  if (!m || !m->pts0) return fail(m, TRN_ERR_INVALID, "reload: nothing loaded");
+  m->err.clear();
+  return init_from_device(m);
 }
 
 int trn_mesh_load(trn_mesh* m, const char* mesh_path, const char* solut_path) {
@@ -460,17 +499,11 @@ int trn_mesh_counts(trn_mesh* m, int* nb_nodes, int* nb_elems, int* live_nodes, 
   if (nb_nodes) *nb_nodes = m->nb_nodes;
   if (nb_elems) *nb_elems = m->nb_elems;
   if (live_nodes || live_elems) {
-    std::vector<uint8_t> alive((size_t) m->nb_nodes);
-    std::vector<int4> e4((size_t) m->nb_elems);
-    CK(cudaMemcpyAsync(alive.data(), m->d.alive, alive.size(), cudaMemcpyDeviceToHost, m->stream));
-    CK(cudaMemcpyAsync(e4.data(), m->d.tri, sizeof(int4) * e4.size(), cudaMemcpyDeviceToHost, m->stream));
-    CK(cudaStreamSynchronize(m->stream));
-    if (live_nodes) *live_nodes = (int) std::count(alive.begin(), alive.end(), (uint8_t) 1);
-    if (live_elems) {
-      int c = 0;
-      for (auto& t : e4) c += t.x >= 0;
-      *live_elems = c;
-    }
+    count_live(m->d, m->nb_nodes, m->nb_elems, m->status + S_LIVE, m->stream);
+    int rc = sync_status(m);
+    if (rc) return rc;
+    if (live_nodes) *live_nodes = m->h_status[S_LIVE];
+    if (live_elems) *live_elems = m->h_status[S_LIVE + 1];
   }
   return TRN_OK;
 }

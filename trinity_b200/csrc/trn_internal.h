@@ -39,6 +39,7 @@ void build_vicin(const DMesh& m, int nb_nodes, bool only_flagged, cudaStream_t s
 void fix_tagged(const DMesh& m, int nb_nodes, cudaStream_t s);
 void flag_all_alive(const DMesh& m, int nb_nodes, cudaStream_t s);
 void quality_all(const DMesh& m, int nb_elems, cudaStream_t s);
+void count_live(const DMesh& m, int nb_nodes, int nb_elems, int* out, cudaStream_t s);
 
 /* metric (metric.cu) */
 struct MetricParams {
@@ -110,6 +111,32 @@ void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& 
               int* parts, int* part_off, cudaStream_t s);
 
 void check_launch(const char* what);
+
+/* per-launch device timing (prof.cu): brackets the launches issued during its
+ * lifetime with events on stream s when profiling is enabled; bytes is the
+ * launcher's algorithmic byte count for them */
+class ProfScope {
+ public:
+  ProfScope(const char* name, cudaStream_t s, double bytes = 0.0);
+  ~ProfScope();
+  ProfScope(const ProfScope&) = delete;
+  ProfScope& operator=(const ProfScope&) = delete;
+
+ private:
+  cudaStream_t stream_;
+  cudaEvent_t a_ = nullptr;
+  int id_ = -1;
+  double bytes_ = 0.0;
+};
+void prof_flush();
+/* count of kernel launches issued by this library (process-wide) */
+void note_launch();
+
+/* algorithmic sizes (bytes per entity) used by the launchers' byte counts:
+ * point 2 x f64, tensor 3 x f64, triangle 3 x i32, quality f64, stencil and
+ * adjacency entries i32; planar triangulations average 6 elements and 6
+ * neighbours per vertex */
+constexpr double kPt = 16, kTen = 24, kTri = 12, kQ = 8, kIdx = 4, kAvgDeg = 6;
 
 }  // namespace trn
 
