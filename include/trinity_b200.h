@@ -117,6 +117,27 @@ unsigned long long trn_launch_count(void);
 int trn_profile_entry(int i, char* name, int name_len, long long* launches, double* ms,
                       double* bytes);
 
+/* Allocation-free metric recovery for one small mesh. No counterpart in the
+ * reference. For callers that own all device memory themselves (a fixed
+ * memory budget, or their own pool allocator) and so cannot let a library
+ * call cudaMalloc/cudaFree: inputs and output are the caller's device
+ * buffers (d_points[2V], d_tris[3T] 0-based CCW, d_solut[V] -> d_tensor[3V],
+ * m11 m12 m22 per vertex), and the working memory is one fixed __device__
+ * array of about 6 MB that every GPU loading this library holds until exit.
+ * Limits: V <= TRN_NOALLOC_MAX_NODES, T <= TRN_NOALLOC_MAX_ELEMS, at most
+ * TRN_NOALLOC_BUCKET triangles around a vertex; larger inputs return
+ * TRN_ERR_CAPACITY. Same tensors as trn_metric_run on the same mesh. The
+ * first call on a device looks up the array's device address, so make it
+ * before any stream capture. Calls share the array: calls that overlap on the
+ * GPU (other streams or host threads) race; serialise them. Runs on `stream`
+ * (a cudaStream_t, NULL = default stream) and returns when done. */
+#define TRN_NOALLOC_MAX_NODES 16384
+#define TRN_NOALLOC_MAX_ELEMS 32768
+#define TRN_NOALLOC_BUCKET 32
+int trn_metric_noalloc(int nb_nodes, int nb_elems, const double* d_points, const int* d_tris,
+                       const double* d_solut, double target_factor, int lp_norm, double h_min,
+                       double h_max, double* d_tensor, void* stream);
+
 /* library version string */
 const char* trn_version(void);
 
