@@ -222,3 +222,14 @@ def run_pipeline(obj, params, stages=None, log_stage=None):
             if log_stage:
                 log_stage(name)
     return names
+
+
+def digest(st: State) -> dict:
+    """SHA-256 per field of a full-precision state (bit-exact fingerprint)."""
+    import hashlib
+    out = {"nodes": int(st.nb_nodes), "elems": int(st.nb_elems),
+           "live_elems": int((st.elems[:, 0] >= 0).sum()), "live_nodes": int(st.alive.sum())}
+    for name in ("points", "tensor", "elems", "alive", "tags"):
+        a = np.ascontiguousarray(getattr(st, name))
+        out[name] = hashlib.sha256(a.tobytes()).hexdigest()
+    return out
