@@ -42,8 +42,8 @@ UNIT = "triangles/s"
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "trinity_ref")
 
 
-def workload_config():
-    m, u, c = meshgen.make_config(WORKLOAD)
+def workload_config(grid=None):
+    m, u, c = meshgen.make_config(WORKLOAD, grid)
     cfg = {
         "workload": "unit square 1000x1000 grid, 1,002,001 vertices / 2,000,000 triangles, "
                     "interior jitter 0.2h (seed 2), field tanh+gauss+waves, target 0.7, "
@@ -52,6 +52,8 @@ def workload_config():
         "data": "synthetic, generated by trinity_b200/meshgen.py",
         "l2": "working set larger than L2 (mesh restored every step)",
     }
+    if grid:
+        cfg["workload"] = f"unit square {grid}x{grid} grid (profiling size), otherwise as the 2M-triangle workload"
     return m, u, c, cfg
 
 
@@ -137,7 +139,7 @@ def b200_arm(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dist_on = world > 1
-    m, u, c, cfg = workload_config()
+    m, u, c, cfg = workload_config(args.grid)
     tags = tags_of(m)
     g = api.Mesh((m.nb_nodes, m.nb_elems), c["bucket"], c["depth"], 0, c["rounds"])
     g.load_arrays(m.points, m.tris, tags, u)
@@ -183,7 +185,7 @@ def b200_arm(args, rank, world, local_rank):
     h2d = pts.nbytes + tris.nbytes + tags.nbytes + u.nbytes
     barrier()
     torch.cuda.synchronize()
-    for _ in range(args.steps):
+    for _ in range(0 if args.no_e2e else args.steps):
         t0 = time.perf_counter()
         g.load_arrays(pts, tris, tags, u)
         tin, _, _ = run_step(api, g, c, heur, kern)
@@ -232,7 +234,7 @@ def b200_arm(args, rank, world, local_rank):
         "metric_ms_per_step": round(float(np.mean(metric_ms)), 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": cfg,
-        "e2e": {"value": round(e2e_tin_all / e2e_max, 1), "unit": UNIT,
+        "e2e": {"value": round(e2e_tin_all / e2e_max, 1) if e2e_max > 0 else None, "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "note": "host arrays -> C ABI load, metric, 3 rounds, export; wall clock"},
         "gpu_launches": int(launches),
@@ -332,6 +334,8 @@ def main():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    p.add_argument("--grid", type=int, default=None, help="grid side override (profiling runs)")
     args = p.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))

@@ -1,0 +1,59 @@
+"""Boundary I/O on the GPU path: loading the .mesh/.bb files gives the same
+state as loading arrays, and after a replayed adaptation Mesh::store writes
+the same bytes as the reference's Mesh::store (digest from the reference)."""
+import hashlib
+import json
+import os
+import subprocess
+
+import pytest
+
+from tests.helpers import gpu_state, oracle_run, run_gpu_stages
+from tests.oracle_lib import tags_of
+from trinity_b200 import meshgen
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = json.load(open(os.path.join(HERE, "golden", "ref_stage_digests.json")))
+
+
+@pytest.mark.gpu
+def test_file_load_equals_array_load(tmp_path):
+    from trinity_b200.api import Mesh
+    m, u, c = meshgen.make_config("c4", 30)
+    mp, bp = str(tmp_path / "a.mesh"), str(tmp_path / "a.bb")
+    meshgen.write_mesh(mp, m)
+    meshgen.write_bb(bp, u)
+    a = Mesh((m.nb_nodes, m.nb_elems), 64, 1, 0, 1)
+    a.load(mp, bp)
+    b = Mesh((m.nb_nodes, m.nb_elems), 64, 1, 0, 1)
+    b.load_arrays(m.points, m.tris, tags_of(m), u)
+    assert not gpu_state(a).diff(gpu_state(b))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c1", "c2_n60"])
+def test_store_after_replay_matches_reference_store(oracle_built, tmp_path, name):
+    g0 = GOLD[name]
+    m, u, c, states, log = oracle_run(g0["config"]["name"], g0["config"]["n"], g0["params"]["rounds"])
+    from tests.helpers import gpu_mesh
+    g = gpu_mesh(m, u, c)
+    g.set_replay(log)
+    run_gpu_stages(g, c, lambda s: None)
+    out = str(tmp_path / "out.mesh")
+    g.store(out)
+    assert hashlib.sha256(open(out, "rb").read()).hexdigest() == g0["store_sha256"]
+
+
+@pytest.mark.gpu
+def test_cli_runs_the_reference_command_line(tmp_path):
+    exe = os.path.join(os.path.dirname(HERE), "trinity_b200", "bin", "trinity")
+    mp, bp, c = meshgen.write_config("c1", str(tmp_path), 50)
+    out = str(tmp_path / "adapted.mesh")
+    r = subprocess.run([exe, "-i", mp, "-s", bp, "-o", out, "-b", "64", "-t", "0.9", "-p", "2",
+                        "-r", "2", "-d", "1", "-v", "1"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "recap" in r.stdout
+    res = meshgen.read_mesh(out) if False else None
+    txt = open(out).read()
+    assert txt.startswith("MeshVersionFormatted 1") and "RequiredVertices" in txt
+    assert os.path.exists(str(tmp_path / "adapted.sol"))
