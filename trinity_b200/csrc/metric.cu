@@ -231,7 +231,9 @@ __global__ void k_normalize(DMesh m, int nb_nodes, const double* complexity, dou
       val[j] = trn_dmin(val[j], eig_min);
       val[j] = trn_dmax(val[j], eig_max);
     }
-    m.ten[v] = trn_recompose(val, vec);
+    double4 t4 = trn_recompose(val, vec);
+    m.ten[v] = t4;
+    if (m.lten) m.lten[v] = trn_log_tensor(t4.x, t4.y, t4.z);
   }
 }
 

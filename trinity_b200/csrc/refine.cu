@@ -127,9 +127,10 @@ __global__ void k_ref_steiner(DMesh m, int nb_elems, int nb_nodes, const int4* _
       int v1 = n[j], v2 = n[(j + 1) % 3];
       double2 rp;
       double rt[3];
-      trn_steiner(m.pts[v1], m.pts[v2], m.ten[v1], m.ten[v2], &rp, rt);
+      trn_steiner(m.pts[v1], m.pts[v2], m.ten[v1], m.ten[v2], m.lten[v1], m.lten[v2], &rp, rt);
       m.pts[id] = rp;
       m.ten[id] = make_double4(rt[0], rt[1], rt[2], 0.0);
+      m.lten[id] = trn_log_tensor(rt[0], rt[1], rt[2]);
       if (opp[j] < 0) m.tags[id] = TRN_TAG_BOUND;
       h_insert(hkey, hval, hcap, edge_key(v1, v2), id, m.err);
       ++id;

@@ -35,6 +35,7 @@ __device__ int move_laplacian(const DMesh& m, int i) {
   for (int a = 0; a < deg; ++a) q_min = trn_dmin(q_min, m.qual[st[a]]);
   const double2 pini = m.pts[i];
   const double4 tini = m.ten[i];
+  const double4 lini = m.lten[i];
   double ox = 0, oy = 0;
   double lm[4] = {0, 0, 0, 0};
   for (int k = 0; k < nb_neigh; ++k) {
@@ -44,14 +45,16 @@ __device__ int move_laplacian(const DMesh& m, int i) {
     const double len = trn_dist2(pini, pb, tini, tb);
     ox += pini.x + ((pb.x - pini.x) / len);
     oy += pini.y + ((pb.y - pini.y) / len);
-    trn_interp_add(lm, tb.x, tb.y, tb.z);
+    trn_interp_addl(lm, m.lten[nb]);
   }
   ox /= nb_neigh;
   oy /= nb_neigh;
   double tn[3];
   trn_interp_finish(lm, nb_neigh, tn);
   const double4 tnew = make_double4(tn[0], tn[1], tn[2], 0.0);
+  const double4 lnew = trn_log_tensor(tn[0], tn[1], tn[2]);
   m.ten[i] = tnew;
+  m.lten[i] = lnew;
   double qual[TRN_MAX_DEG];
   bool valid;
   int retry = 0;
@@ -69,10 +72,10 @@ __device__ int move_laplacian(const DMesh& m, int i) {
       const double2 p2 = (n.z == i) ? pa : m.pts[n.z];
       valid = false;
       if (trn_ccw(p0, p1, p2)) {
-        const double4 t0 = (n.x == i) ? tnew : m.ten[n.x];
-        const double4 t1 = (n.y == i) ? tnew : m.ten[n.y];
-        const double4 t2 = (n.z == i) ? tnew : m.ten[n.z];
-        qual[a] = trn_quality(p0, p1, p2, t0, t1, t2);
+        const double4 l0 = (n.x == i) ? lnew : m.lten[n.x];
+        const double4 l1 = (n.y == i) ? lnew : m.lten[n.y];
+        const double4 l2 = (n.z == i) ? lnew : m.lten[n.z];
+        qual[a] = trn_quality_l(p0, p1, p2, l0, l1, l2);
         valid = (qual[a] > q_min);
       }
     }
@@ -83,6 +86,7 @@ __device__ int move_laplacian(const DMesh& m, int i) {
   } else {
     m.pts[i] = pini;
     m.ten[i] = tini;
+    m.lten[i] = lini;
   }
   return valid ? 1 : 0;
 }

@@ -36,7 +36,7 @@ __global__ void k_swap_init_elems(DMesh m, int nb_elems, int* __restrict__ map) 
       m.activ[i] = 0;
       continue;
     }
-    m.qual[i] = trn_quality(m.pts[t.x], m.pts[t.y], m.pts[t.z], m.ten[t.x], m.ten[t.y], m.ten[t.z]);
+    m.qual[i] = trn_quality_l(m.pts[t.x], m.pts[t.y], m.pts[t.z], m.lten[t.x], m.lten[t.y], m.lten[t.z]);
     m.activ[i] = 1;
   }
 }
@@ -118,10 +118,10 @@ __device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int*
   const double2 p22 = m.pts[c2[2]];
   /* c2 = (c1[2], c1[1], c2[2]) */
   if (!trn_ccw(p10, p11, p12) || !trn_ccw(p12, p11, p22)) return 0;
-  const double4 t10 = m.ten[c1[0]], t11 = m.ten[c1[1]], t12 = m.ten[c1[2]];
-  const double4 t22 = m.ten[c2[2]];
-  const double q0 = trn_quality(p10, p11, p12, t10, t11, t12);
-  const double q1 = trn_quality(p12, p11, p22, t12, t11, t22);
+  const double4 l10 = m.lten[c1[0]], l11 = m.lten[c1[1]], l12 = m.lten[c1[2]];
+  const double4 l22 = m.lten[c2[2]];
+  const double q0 = trn_quality_l(p10, p11, p12, l10, l11, l12);
+  const double q1 = trn_quality_l(p12, p11, p22, l12, l11, l22);
   const double q_old = trn_dmin(m.qual[id1], m.qual[id2]);
   const double q_new = trn_dmin(q0, q1);
   if (q_new < q_old) return 0;

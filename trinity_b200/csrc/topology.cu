@@ -105,7 +105,7 @@ __global__ void k_quality_all(DMesh m, int nb_elems) {
   for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
     int4 t = m.tri[i];
     if (t.x < 0) continue;
-    m.qual[i] = trn_quality(m.pts[t.x], m.pts[t.y], m.pts[t.z], m.ten[t.x], m.ten[t.y], m.ten[t.z]);
+    m.qual[i] = trn_quality_l(m.pts[t.x], m.pts[t.y], m.pts[t.z], m.lten[t.x], m.lten[t.y], m.lten[t.z]);
   }
 }
 

@@ -169,7 +169,7 @@ int dmalloc(trn_mesh* m, T** p, size_t count) {
 void release(trn_mesh* m) {
   if (!m) return;
   if (m->stream) cudaStreamSynchronize(m->stream);
-  void* bufs[] = {m->d.pts, m->d.ten, m->d.tri, m->d.stenc, m->d.deg, m->d.vic, m->d.vdeg,
+  void* bufs[] = {m->d.pts, m->d.ten, m->d.lten, m->d.tri, m->d.stenc, m->d.deg, m->d.vic, m->d.vdeg,
                   m->d.tags, m->d.alive, m->d.fixes, m->d.activ, m->d.qual, m->solut, m->grad,
                   m->terms, m->complexity, m->target, m->flag, m->list, m->indep, m->map,
                   m->dual, m->dual_n, m->pairs, m->parts, m->status, m->d_log, m->pts0,
@@ -287,7 +287,8 @@ int trn_mesh_create_ex(const int size[2], int bucket, int depth, int verbosity, 
   d.bucket = bucket;
   d.capa_node = m->capa_node;
   d.capa_elem = m->capa_elem;
-  if ((rc = dmalloc(m, &d.pts, cn)) || (rc = dmalloc(m, &d.ten, cn)) || (rc = dmalloc(m, &d.tri, ce)) ||
+  if ((rc = dmalloc(m, &d.pts, cn)) || (rc = dmalloc(m, &d.ten, cn)) || (rc = dmalloc(m, &d.lten, cn)) ||
+      (rc = dmalloc(m, &d.tri, ce)) ||
       (rc = dmalloc(m, &d.stenc, cn * bucket)) || (rc = dmalloc(m, &d.deg, cn)) ||
       (rc = dmalloc(m, &d.vic, cn * bucket)) || (rc = dmalloc(m, &d.vdeg, cn)) ||
       (rc = dmalloc(m, &d.tags, cn)) || (rc = dmalloc(m, &d.alive, cn)) ||
@@ -331,6 +332,7 @@ static int init_from_device(trn_mesh* m) {
   const int nb_nodes = m->n0_nodes, nb_elems = m->n0_elems;
   cudaStream_t s = m->stream;
   CK(cudaMemsetAsync(d.ten, 0, sizeof(double4) * cn, s));
+  CK(cudaMemsetAsync(d.lten, 0, sizeof(double4) * cn, s));
   CK(cudaMemsetAsync(d.pts, 0, sizeof(double2) * cn, s));
   CK(cudaMemsetAsync(d.tri, 0xff, sizeof(int4) * ce, s));
   CK(cudaMemsetAsync(d.stenc, 0xff, sizeof(int) * cn * b, s));

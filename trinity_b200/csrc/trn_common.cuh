@@ -41,6 +41,7 @@
 struct DMesh {
   double2* pts;
   double4* ten;
+  double4* lten;   /* per-vertex tensor logarithm P log(D) P^T (4 entries) */
   int4* tri;
   int* stenc;
   int* deg;

@@ -61,9 +61,11 @@ __device__ __forceinline__ void trn_eigen(const double* mat, double* val, double
   vec[3] /= n1;
 }
 
-/* one term of the log-Euclidean sum of numeric::interpolateTensor
- * (numeric.cpp:113-172): log_mat += P log(D) P^T of tensor t */
-__device__ __forceinline__ void trn_interp_add(double* log_mat, double t0, double t1, double t2) {
+/* the logarithm P log(D) P^T of one tensor as numeric::interpolateTensor
+ * forms it (numeric.cpp:115-154), all four entries (not exactly symmetric).
+ * It depends on the tensor alone, so a cached copy summed in the same order
+ * gives the same bits as recomputing it inside every mean. */
+__device__ __forceinline__ double4 trn_log_tensor(double t0, double t1, double t2) {
   double copy[4], cache[4], val[2], vec[4];
   copy[0] = t0;
   copy[1] = t1;
@@ -80,10 +82,20 @@ __device__ __forceinline__ void trn_interp_add(double* log_mat, double t0, doubl
   cache[1] = vec[0] * copy[1] + vec[1] * copy[3];
   cache[2] = vec[2] * copy[0] + vec[3] * copy[2];
   cache[3] = vec[2] * copy[1] + vec[3] * copy[3];
-  log_mat[0] += cache[0];
-  log_mat[1] += cache[1];
-  log_mat[2] += cache[2];
-  log_mat[3] += cache[3];
+  return make_double4(cache[0], cache[1], cache[2], cache[3]);
+}
+
+/* log_mat += a cached tensor logarithm (numeric.cpp:169-171) */
+__device__ __forceinline__ void trn_interp_addl(double* log_mat, double4 l) {
+  log_mat[0] += l.x;
+  log_mat[1] += l.y;
+  log_mat[2] += l.z;
+  log_mat[3] += l.w;
+}
+
+/* one term of the log-Euclidean sum of numeric::interpolateTensor */
+__device__ __forceinline__ void trn_interp_add(double* log_mat, double t0, double t1, double t2) {
+  trn_interp_addl(log_mat, trn_log_tensor(t0, t1, t2));
 }
 
 /* the exponentiation half of numeric::interpolateTensor (numeric.cpp:189-216) */
@@ -105,14 +117,15 @@ __device__ __forceinline__ void trn_interp_finish(double* log_mat, int nb, doubl
   res[2] = cache[3];
 }
 
-/* numeric::computeQuality, numeric.cpp:251-306 */
-__device__ __forceinline__ double trn_quality(double2 pa, double2 pb, double2 pc,
-                                              double4 ta, double4 tb, double4 tc) {
+/* numeric::computeQuality, numeric.cpp:251-306, from the vertices' cached
+ * tensor logarithms */
+__device__ __forceinline__ double trn_quality_l(double2 pa, double2 pb, double2 pc,
+                                                double4 la, double4 lb, double4 lc) {
   double lm[4] = {0, 0, 0, 0};
   double jacob[3];
-  trn_interp_add(lm, ta.x, ta.y, ta.z);
-  trn_interp_add(lm, tb.x, tb.y, tb.z);
-  trn_interp_add(lm, tc.x, tc.y, tc.z);
+  trn_interp_addl(lm, la);
+  trn_interp_addl(lm, lb);
+  trn_interp_addl(lm, lc);
   trn_interp_finish(lm, 3, jacob);
   double det = jacob[0] * jacob[2] - jacob[1] * jacob[1];
   double coef[6];
@@ -137,6 +150,13 @@ __device__ __forceinline__ double trn_quality(double2 pa, double2 pb, double2 pc
   double mean = trn_dmin(perim / 3, 3 / perim);
   double norm = 12 * sqrt(3.0) * trn_pow(mean * (2. - mean), 3);
   return area * norm * sqrt(det) / trn_pow(perim, 2);
+}
+
+/* numeric::computeQuality from the tensors themselves */
+__device__ __forceinline__ double trn_quality(double2 pa, double2 pb, double2 pc,
+                                              double4 ta, double4 tb, double4 tc) {
+  return trn_quality_l(pa, pb, pc, trn_log_tensor(ta.x, ta.y, ta.z),
+                       trn_log_tensor(tb.x, tb.y, tb.z), trn_log_tensor(tc.x, tc.y, tc.z));
 }
 
 /* numeric::approxRiemannDist(a, b, M), numeric.cpp:450-461 */
@@ -165,9 +185,10 @@ __device__ __forceinline__ double trn_dist2(double2 pa, double2 pb, double4 ta, 
   return lmax * (ratio - 1) / (ratio * trn_log(ratio));
 }
 
-/* numeric::computeSteinerPoint, numeric.cpp:387-445 */
+/* numeric::computeSteinerPoint, numeric.cpp:387-445 (la, lb: cached
+ * logarithms of ta, tb) */
 __device__ __forceinline__ void trn_steiner(double2 pa, double2 pb, double4 ta, double4 tb,
-                                            double2* rp, double* rt) {
+                                            double4 la, double4 lb, double2* rp, double* rt) {
   double coef = 1;
   double l0 = trn_dist1(pa, pb, ta);
   double l1 = trn_dist1(pa, pb, tb);
@@ -177,8 +198,8 @@ __device__ __forceinline__ void trn_steiner(double2 pa, double2 pb, double4 ta, 
   rp->x = (1 - weight) * pa.x + (weight * pb.x);
   rp->y = (1 - weight) * pa.y + (weight * pb.y);
   double lm[4] = {0, 0, 0, 0};
-  trn_interp_add(lm, ta.x, ta.y, ta.z);
-  trn_interp_add(lm, tb.x, tb.y, tb.z);
+  trn_interp_addl(lm, la);
+  trn_interp_addl(lm, lb);
   trn_interp_finish(lm, 2, rt);
 }
 
