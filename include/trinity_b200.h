@@ -67,6 +67,12 @@ int trn_mesh_store_sol(trn_mesh* mesh, const char* path);
 /* copy out the raw state: nb_nodes / nb_elems entries (any pointer may be NULL) */
 int trn_mesh_export(trn_mesh* mesh, double* points, double* tensor, int* tris, uint8_t* alive,
                     uint8_t* tags);
+/* The adapted mesh without deleted entities, renumbered in id order as
+ * Mesh::store numbers its output (io.cpp:199-233): points[2V'], tris[3T']
+ * (0-based), tensor[3V'] (may be NULL). Size the arrays with the live counts
+ * of trn_mesh_counts; V' and T' are returned. */
+int trn_mesh_export_compact(trn_mesh* mesh, double* points, int* tris, double* tensor,
+                            int* nb_nodes, int* nb_elems);
 /* slot counts (deleted entities included) and live counts */
 int trn_mesh_counts(trn_mesh* mesh, int* nb_nodes, int* nb_elems, int* live_nodes,
                     int* live_elems);

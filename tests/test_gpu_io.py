@@ -45,6 +45,34 @@ def test_store_after_replay_matches_reference_store(oracle_built, tmp_path, name
 
 
 @pytest.mark.gpu
+def test_export_compact_is_store_numbering(oracle_built):
+    import numpy as np
+    m, u, c, states, log = oracle_run("c1", 40, 2)
+    from tests.helpers import gpu_mesh
+    g = gpu_mesh(m, u, c)
+    run_gpu_stages(g, c, lambda s: None)
+    pts, ten, tri, alive, tags = g.export()
+    newid = np.cumsum(alive.astype(np.int64)) - 1
+    live = tri[tri[:, 0] >= 0]
+    p2, t2, m2 = g.export_compact()
+    assert np.array_equal(p2, pts[alive == 1]) and np.array_equal(m2, ten[alive == 1])
+    assert np.array_equal(t2, newid[live].astype(np.int32))
+
+
+@pytest.mark.gpu
+def test_load_rejects_out_of_range_vertex():
+    import numpy as np
+    from trinity_b200.api import Mesh, TrinityError
+    m, u, c = meshgen.make_config("c1", 10)
+    bad = m.tris.copy()
+    bad[5, 1] = m.nb_nodes + 3
+    g = Mesh((m.nb_nodes, m.nb_elems), 64, 1, 0, 1)
+    with pytest.raises(TrinityError):
+        g.load_arrays(m.points, bad, tags_of(m), u)
+    g.load_arrays(m.points, m.tris, tags_of(m), u)   # and recovers with valid input
+
+
+@pytest.mark.gpu
 def test_cli_runs_the_reference_command_line(tmp_path):
     exe = os.path.join(os.path.dirname(HERE), "trinity_b200", "bin", "trinity")
     mp, bp, c = meshgen.write_config("c1", str(tmp_path), 50)

@@ -115,6 +115,18 @@ class Mesh:
         self._check(self._L.trn_mesh_export(self.h, _p(pts), _p(ten), _p(tri), _p(alive), _p(tags)))
         return pts, ten, tri, alive, tags
 
+    def export_compact(self, with_tensor: bool = True):
+        """The adapted mesh without deleted entities, renumbered like
+        Mesh::store: (points[V',2], tris[T',3] 0-based, tensor[V',3] or None)."""
+        _, _, nv, ne = self.counts()
+        pts = np.empty((nv, 2)); tri = np.empty((ne, 3), np.int32)
+        ten = np.empty((nv, 3)) if with_tensor else None
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._check(self._L.trn_mesh_export_compact(self.h, _p(pts), _p(tri), _p(ten) if with_tensor else None,
+                                                    ctypes.byref(a), ctypes.byref(b)))
+        assert (a.value, b.value) == (nv, ne)
+        return pts, tri, ten
+
     def set_replay(self, log) -> None:
         a = np.ascontiguousarray(log, dtype=np.int32)
         self._check(self._L.trn_set_replay(self.h, _p(a) if a.size else None, a.size))

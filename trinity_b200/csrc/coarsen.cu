@@ -106,13 +106,33 @@ __global__ void k_coarse_filter(DMesh m, int nb_nodes, int* __restrict__ target,
   }
 }
 
+/* free mode: one pass per level rebuilds the adjacency of each active vertex,
+ * finds its target and appends the candidates (in no particular order: the
+ * independent set is chosen by hashed priorities, not by list position),
+ * marking them undecided for the independent-set rounds */
+__global__ void k_coarse_filter_append(DMesh m, int nb_nodes, int* __restrict__ target,
+                                       int* __restrict__ cand, int* count, uint8_t* __restrict__ state) {
+  if (trn_failed(m)) return;
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    if (m.activ[v] <= 0) continue;
+    m.activ[v] = 0;
+    build_one_vicin(m, v);
+    const int t = identify_target(m, v);
+    target[v] = t;
+    if (t > -1) {
+      state[v] = 1;
+      trn_append(cand, count, v);
+    }
+  }
+}
+
 __global__ void k_collapse(DMesh m, const int* __restrict__ indep, const int* count,
                            const int* __restrict__ target, const uint8_t* __restrict__ cand_flag) {
   if (trn_failed(m)) return;
   const int n_indep = *count;
   for (int q = trn_tid(); q < n_indep; q += trn_grid_stride()) {
     const int source = indep[q];
-    if (source < 0 || source >= m.capa_node || !cand_flag[source]) {
+    if (source < 0 || source >= m.capa_node || (cand_flag && !cand_flag[source])) {
       trn_set_error(m.err, TRN_DERR_REPLAY);
       continue;
     }
@@ -176,6 +196,16 @@ void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, cu
   k_coarse_filter<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, flag);
   note_launch();
   check_launch("coarsen_filter");
+}
+
+void coarsen_filter_append(const DMesh& m, int nb_nodes, int* target, int* cand, int* count,
+                           uint8_t* state, cudaStream_t s) {
+  ProfScope ps("coarsen_filter", s, (double) nb_nodes * (1 + 1 + 4 + 1));
+  cudaMemsetAsync(count, 0, sizeof(int), s);
+  k_coarse_filter_append<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, cand, count,
+                                                                     state);
+  note_launch();
+  check_launch("coarsen_filter_append");
 }
 
 void collapse(const DMesh& m, const int* indep, const int* count, const int* target,

@@ -6,10 +6,12 @@
  * greedy matching (matching.cpp:81-135), both sequential in spirit. On the GPU
  * these become round-synchronous algorithms with seeded hash priorities:
  *
- *   mis_jp          Jones-Plassmann maximal independent set on the collapse
- *                   candidates: a candidate joins when it has the highest
- *                   priority among its undecided candidate neighbours, and
- *                   leaves when a neighbour joined.
+ *   mis_jp_rounds   independent set on the collapse candidates, a fixed
+ *                   number of rounds per level: a candidate joins when it has
+ *                   the highest hash priority of the round among its undecided
+ *                   candidate neighbours and leaves when a neighbour joined
+ *                   (Jones-Plassmann / Luby); candidates still undecided after
+ *                   the last round are examined again at the next level.
  *   match_handshake maximal matching on the swap dual rows: every unmatched
  *                   candidate points along its heaviest free edge (symmetric
  *                   hash weight); mutual candidate pairs match, a non-candidate
@@ -25,74 +27,72 @@
 namespace trn {
 
 /* ---------------- independent set ---------------- */
-__global__ void k_mis_init(uint8_t* state, const int* __restrict__ cand, int n) {
-  for (int q = trn_tid(); q < n; q += trn_grid_stride()) state[cand[q]] = 1;
-}
 
-__global__ void k_mis_round(DMesh m, uint8_t* state, const int* __restrict__ cand, int n,
-                            uint64_t seed, int* undecided) {
+
+
+
+/* free-mode round over a device-counted candidate list; states are read
+ * from the previous round's buffer only (0 out / not a candidate,
+ * 1 undecided, 2 in the set), so the outcome does not depend on timing */
+__global__ void k_mis_round_dev(DMesh m, const uint8_t* __restrict__ in, uint8_t* __restrict__ out,
+                                const int* __restrict__ cand, const int* count, uint64_t seed) {
   if (trn_failed(m)) return;
-  int left = 0;
+  const int n = *count;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
     const int v = cand[q];
-    if (state[v] != 1) continue;
+    const uint8_t sv = in[v];
+    if (sv != 1) {
+      out[v] = sv;
+      continue;
+    }
     const uint64_t pv = trn_prio(seed, v);
     const int* vc = m.vic + (size_t) v * m.bucket;
     const int nv = m.vdeg[v];
-    bool is_max = true, out = false;
+    bool is_max = true, leave = false;
     for (int b = 0; b < nv; ++b) {
       const int w = vc[b];
-      const uint8_t sw = *(volatile uint8_t*) (state + w);
-      if (sw == 2) { out = true; break; }
+      const uint8_t sw = in[w];
+      if (sw == 2) { leave = true; break; }
       if (sw == 1 && trn_prio(seed, w) > pv) is_max = false;
     }
-    if (out) state[v] = 0;
-    else if (is_max) state[v] = 2;
-    else ++left;
+    out[v] = leave ? 0 : (is_max ? 2 : 1);
   }
-  if (left) atomicAdd(undecided, left);
 }
 
-__global__ void k_mis_collect(const uint8_t* state, const int* __restrict__ cand, int n, int* indep,
-                              int* count) {
+/* collect the set; candidates still undecided are re-activated so that the
+ * next level examines them again; every candidate's state returns to 0 */
+__global__ void k_mis_finish(DMesh m, uint8_t* state, uint8_t* other, const int* __restrict__ cand,
+                             const int* count, int* indep, int* nindep) {
+  const int n = *count;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
     const int v = cand[q];
-    if (state[v] == 2) indep[atomicAdd(count, 1)] = v;
+    const uint8_t st = state[v];
+    if (st == 2) trn_append(indep, nindep, v);
+    else if (st == 1) m.activ[v] = 1;
+    state[v] = 0;
+    other[v] = 0;
   }
 }
 
-__global__ void k_mis_clear(uint8_t* state, const int* __restrict__ cand, int n) {
-  for (int q = trn_tid(); q < n; q += trn_grid_stride()) state[cand[q]] = 0;
-}
-
-void mis_jp(const DMesh& m, int nb_nodes, const uint8_t* cand_flag, const int* cand_list,
-            int ncand, uint64_t seed, HeurWs& ws, int* indep, int* count, ScanWs& scan,
-            cudaStream_t s) {
-  (void) nb_nodes;
-  (void) cand_flag;
-  (void) scan;
+void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, uint64_t seed,
+                   HeurWs& ws, int* indep, int* nindep, cudaStream_t s) {
   ProfScope ps("mis_jp", s, 0.0);
-  const int g = grid_for(ncand);
-  k_mis_init<<<g, TRN_THREADS, 0, s>>>(ws.state, cand_list, ncand);
-  note_launch();
-  int host_left = 1;
-  for (int batch = 0; batch < 64 && host_left; ++batch) {
-    cudaMemsetAsync(ws.cnt, 0, sizeof(int) * 4, s);
-    for (int r = 0; r < 4; ++r)
-      k_mis_round<<<g, TRN_THREADS, 0, s>>>(m, ws.state, cand_list, ncand, seed, ws.cnt + r);
-      note_launch();
-    cudaMemcpyAsync(&host_left, ws.cnt + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
-    cudaStreamSynchronize(s);
+  const int g = grid_for(m.capa_node);
+  uint8_t* buf[2] = {ws.state, ws.state2};
+  for (int r = 0; r < rounds; ++r) {
+    k_mis_round_dev<<<g, TRN_THREADS, 0, s>>>(m, buf[r & 1], buf[(r + 1) & 1], cand, count,
+                                               seed + 0x9e3779b97f4a7c15ULL * r);
+    note_launch();
   }
-  cudaMemsetAsync(count, 0, sizeof(int), s);
-  k_mis_collect<<<g, TRN_THREADS, 0, s>>>(ws.state, cand_list, ncand, indep, count);
+  cudaMemsetAsync(nindep, 0, sizeof(int), s);
+  k_mis_finish<<<g, TRN_THREADS, 0, s>>>(m, buf[rounds & 1], buf[(rounds + 1) & 1], cand, count, indep,
+                                         nindep);
   note_launch();
-  k_mis_clear<<<g, TRN_THREADS, 0, s>>>(ws.state, cand_list, ncand);
-  note_launch();
-  check_launch("mis_jp");
+  check_launch("mis_jp_rounds");
 }
 
 /* ---------------- matching ---------------- */
+static constexpr int kMatchRounds = 4;
 __device__ __forceinline__ uint32_t edge_weight(uint64_t seed, int a, int b, int round) {
   int lo = a < b ? a : b, hi = a < b ? b : a;
   uint64_t h = trn_hash64(seed ^ ((uint64_t) (uint32_t) lo << 32 | (uint32_t) hi) ^
@@ -101,7 +101,8 @@ __device__ __forceinline__ uint32_t edge_weight(uint64_t seed, int a, int b, int
 }
 
 __global__ void k_match_reset(const int* __restrict__ dual, const int* __restrict__ dual_n,
-                              int ntasks, int* mate, unsigned long long* prop) {
+                              const int* ntasks_dev, int* mate, unsigned long long* prop) {
+  const int ntasks = *ntasks_dev;
   for (int i = trn_tid(); i < ntasks; i += trn_grid_stride())
     for (int q = 0; q < dual_n[i]; ++q) {
       int e = dual[i * 4 + q];
@@ -111,8 +112,9 @@ __global__ void k_match_reset(const int* __restrict__ dual, const int* __restric
 }
 
 __global__ void k_match_propose(const int* __restrict__ dual, const int* __restrict__ dual_n,
-                                int ntasks, const int* mate, unsigned long long* prop, int* choice,
-                                uint64_t seed, int round) {
+                                const int* ntasks_dev, const int* mate, unsigned long long* prop,
+                                int* choice, uint64_t seed, int round) {
+  const int ntasks = *ntasks_dev;
   for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
     const int c = dual[i * 4];
     int best = -1;
@@ -130,9 +132,10 @@ __global__ void k_match_propose(const int* __restrict__ dual, const int* __restr
   }
 }
 
-__global__ void k_match_accept(const int* __restrict__ dual, int ntasks, const int* __restrict__ map,
-                               int* mate, const unsigned long long* prop, const int* choice,
-                               uint64_t seed, int round, int* pairs, int* npairs) {
+__global__ void k_match_accept(const int* __restrict__ dual, const int* ntasks_dev,
+                               const int* __restrict__ map, int* mate, const unsigned long long* prop,
+                               const int* choice, uint64_t seed, int round, int* pairs, int* npairs) {
+  const int ntasks = *ntasks_dev;
   for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
     const int n = choice[i];
     if (n < 0) continue;
@@ -153,22 +156,22 @@ __global__ void k_match_accept(const int* __restrict__ dual, int ntasks, const i
 }
 
 __global__ void k_match_prop_clear(const int* __restrict__ dual, const int* __restrict__ dual_n,
-                                   int ntasks, unsigned long long* prop) {
+                                   const int* ntasks_dev, unsigned long long* prop) {
+  const int ntasks = *ntasks_dev;
   for (int i = trn_tid(); i < ntasks; i += trn_grid_stride())
     for (int q = 1; q < dual_n[i]; ++q) prop[dual[i * 4 + q]] = 0ULL;
 }
 
-void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n, int ntasks,
-                     const int* map, uint64_t seed, HeurWs& ws, int* pairs, int* npairs,
-                     cudaStream_t s) {
-  (void) nb_elems;
+void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n,
+                     const int* ntasks, const int* map, uint64_t seed, HeurWs& ws, int* pairs,
+                     int* npairs, cudaStream_t s) {
   (void) m;
   ProfScope ps("match_handshake", s, 0.0);
-  const int g = grid_for(ntasks);
+  const int g = grid_for(nb_elems);
   cudaMemsetAsync(npairs, 0, sizeof(int), s);
   k_match_reset<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.mate, ws.prop);
   note_launch();
-  for (int r = 0; r < 6; ++r) {
+  for (int r = 0; r < kMatchRounds; ++r) {
     k_match_propose<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.mate, ws.prop, ws.choice,
                                                seed, r);
     note_launch();
@@ -276,6 +279,8 @@ void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {
   size_t big = (size_t) (capa_node > capa_elem ? capa_node : capa_elem);
   cudaMalloc(&ws->state, big);
   cudaMemset(ws->state, 0, big);
+  cudaMalloc(&ws->state2, big);
+  cudaMemset(ws->state2, 0, big);
   cudaMalloc(&ws->prop, sizeof(unsigned long long) * (size_t) capa_elem);
   cudaMalloc(&ws->choice, sizeof(int) * (size_t) capa_elem);
   cudaMalloc(&ws->color, sizeof(int) * (size_t) capa_node);
@@ -286,6 +291,7 @@ void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {
 
 void heur_ws_free(HeurWs* ws) {
   cudaFree(ws->state);
+  cudaFree(ws->state2);
   cudaFree(ws->prop);
   cudaFree(ws->choice);
   cudaFree(ws->color);

@@ -52,11 +52,10 @@ __global__ void k_swap_filter(DMesh m, int nb_elems, uint8_t* __restrict__ flag)
   }
 }
 
-__global__ void k_swap_dual(DMesh m, const int* __restrict__ list, int ntasks, int* __restrict__ dual,
-                            int* __restrict__ dual_n, int* __restrict__ map) {
-  if (trn_failed(m)) return;
-  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
-    const int k = list[i];
+/* the dual row of candidate k at row index i */
+__device__ __forceinline__ void dual_row(const DMesh& m, int k, int i, int* __restrict__ dual,
+                                         int* __restrict__ dual_n, int* __restrict__ map) {
+  {
     const int4 n = m.tri[k];
     int row[4] = {k, -1, -1, -1};
     int dn = 1;
@@ -88,9 +87,32 @@ __global__ void k_swap_dual(DMesh m, const int* __restrict__ list, int ntasks, i
   }
 }
 
+__global__ void k_swap_dual(DMesh m, const int* __restrict__ list, int ntasks, int* __restrict__ dual,
+                            int* __restrict__ dual_n, int* __restrict__ map) {
+  if (trn_failed(m)) return;
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) dual_row(m, list[i], i, dual, dual_n, map);
+}
+
+/* free mode: filter and dual extraction in one pass; rows are numbered in
+ * append order (no use depends on it) */
+__global__ void k_swap_filter_dual(DMesh m, int nb_elems, int* __restrict__ dual,
+                                   int* __restrict__ dual_n, int* __restrict__ map, int* count) {
+  if (trn_failed(m)) return;
+  for (int k = trn_tid(); k < nb_elems; k += trn_grid_stride()) {
+    if (!m.activ[k]) continue;
+    m.activ[k] = 0;
+    if (!(m.qual[k] < TRN_Q_MIN)) continue;
+    unsigned mask = __activemask();
+    int lane = threadIdx.x & 31, leader = __ffs(mask) - 1, base = 0;
+    if (lane == leader) base = atomicAdd(count, __popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    dual_row(m, k, base + __popc(mask & ((1u << lane) - 1)), dual, dual_n, map);
+  }
+}
+
 /* Swap::swap, swapping.cpp:55-149 */
 __device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int* map,
-                         const int* dual, const int* dual_n) {
+                         const int* dual, const int* dual_n, int ntasks, bool strict_map) {
   const int4 a = m.tri[id1], b = m.tri[id2];
   const int o1[3] = {a.x, a.y, a.z};
   const int o2[3] = {b.x, b.y, b.z};
@@ -136,17 +158,23 @@ __device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int*
   m.qual[id1] = q0;
   m.qual[id2] = q1;
   for (int q = 0; q < dual_n[index]; ++q) trn_activ_on(m.activ + dual[index * 4 + q]);
+  /* the reference follows the map even when it points at a row of an earlier
+   * level (the map is reset once per call, swapping.cpp:161-162); replay keeps
+   * that, the free mode (rows numbered in append order) only follows rows of
+   * the current level */
   const int x = map[id2];
-  if (x > -1)
+  if (x > -1 && (!strict_map || (x < ntasks && dual[x * 4] == id2)))
     for (int q = 0; q < dual_n[x]; ++q) trn_activ_on(m.activ + dual[x * 4 + q]);
   return 2;
 }
 
 __global__ void k_swap_flip(DMesh m, const int* __restrict__ pairs, const int* npairs,
                             const int* __restrict__ map, const int* __restrict__ dual,
-                            const int* __restrict__ dual_n, int ntasks, int* commit) {
+                            const int* __restrict__ dual_n, const int* ntasks_dev, int* commit,
+                            int strict_map) {
   if (trn_failed(m)) return;
   const int np = *npairs;
+  const int ntasks = *ntasks_dev;
   int local = 0;
   for (int p = trn_tid(); p < np; p += trn_grid_stride()) {
     const int k1 = pairs[2 * p], k2 = pairs[2 * p + 1];
@@ -164,7 +192,7 @@ __global__ void k_swap_flip(DMesh m, const int* __restrict__ pairs, const int* n
       trn_set_error(m.err, TRN_DERR_REPLAY);
       continue;
     }
-    local += flip_pair(m, k1, k2, index, map, dual, dual_n);
+    local += flip_pair(m, k1, k2, index, map, dual, dual_n, ntasks, strict_map != 0);
   }
   if (local) atomicAdd(commit, local);
 }
@@ -194,11 +222,21 @@ void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual
   check_launch("swap_dual");
 }
 
+void swap_filter_dual(const DMesh& m, int nb_elems, int* dual, int* dual_n, int* map, int* count,
+                      cudaStream_t s) {
+  ProfScope ps("swap_filter", s, (double) nb_elems * 3);
+  cudaMemsetAsync(count, 0, sizeof(int), s);
+  k_swap_filter_dual<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, dual, dual_n, map, count);
+  note_launch();
+  check_launch("swap_filter_dual");
+}
+
 void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* map,
-               const int* dual, const int* dual_n, int ntasks, int* commit, cudaStream_t s) {
+               const int* dual, const int* dual_n, const int* ntasks, int* commit, bool strict_map,
+               cudaStream_t s) {
   ProfScope ps("swap_flip", s, 0.0);
   k_swap_flip<<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
-                                                             ntasks, commit);
+                                                             ntasks, commit, strict_map ? 1 : 0);
   note_launch();
   check_launch("swap_flip");
 }

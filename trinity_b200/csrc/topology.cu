@@ -38,31 +38,6 @@ __global__ void k_sort_stencils(DMesh m, int nb_nodes) {
   }
 }
 
-/* adjacency of v from its (canonical) stencil */
-__device__ __forceinline__ void build_one_vicin(const DMesh& m, int v) {
-  int buf[2 * TRN_MAX_DEG];
-  int k = 0;
-  if (m.alive[v]) {
-    const int* s = m.stenc + (size_t) v * m.bucket;
-    int d = trn_deg(m, v);
-    for (int a = 0; a < d; ++a) {
-      int4 n = m.tri[s[a]];
-      if (v == n.x) { buf[k++] = n.y; buf[k++] = n.z; }
-      else if (v == n.y) { buf[k++] = n.z; buf[k++] = n.x; }
-      else if (v == n.z) { buf[k++] = n.x; buf[k++] = n.y; }
-    }
-  }
-  trn_isort(buf, k);
-  k = trn_iunique(buf, k);
-  if (k > m.bucket) {
-    trn_set_error(m.err, TRN_DERR_CAPACITY);
-    k = m.bucket;
-  }
-  int* out = m.vic + (size_t) v * m.bucket;
-  for (int a = 0; a < k; ++a) out[a] = buf[a];
-  m.vdeg[v] = k;
-}
-
 __global__ void k_build_vicin(DMesh m, int nb_nodes, int only_flagged) {
   if (trn_failed(m)) return;
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
@@ -121,6 +96,76 @@ __global__ void k_count_live(DMesh m, int nb_nodes, int nb_elems, int* out) {
     if (cv) atomicAdd(out, cv);
     if (ce) atomicAdd(out + 1, ce);
   }
+}
+
+/* input triangles (3 x int, 0-based) -> int4 records, checking indices */
+__global__ void k_expand_tris(const int* __restrict__ raw, int nb_elems, int nb_nodes,
+                              int4* __restrict__ out, int* err) {
+  for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
+    int a = raw[3 * i], b = raw[3 * i + 1], c = raw[3 * i + 2];
+    if (a < 0 || a >= nb_nodes || b < 0 || b >= nb_nodes || c < 0 || c >= nb_nodes) {
+      trn_set_error(err, TRN_DERR_INVALID);
+      a = b = c = -1;
+    }
+    out[i] = make_int4(a, b, c, 0);
+  }
+}
+
+void expand_tris(const int* raw, int nb_elems, int nb_nodes, int4* out, int* err, cudaStream_t s) {
+  k_expand_tris<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(raw, nb_elems, nb_nodes, out, err);
+  note_launch();
+}
+
+/* Mesh::store's renumbering (io.cpp:199-233) on the device: live vertex k of
+ * the ordered list gets id k; its point and tensor are packed */
+__global__ void k_pack_nodes(DMesh m, const int* __restrict__ list, const int* count,
+                             int* __restrict__ newid, double* __restrict__ pts, double* __restrict__ ten) {
+  const int n = *count;
+  for (int k = trn_tid(); k < n; k += trn_grid_stride()) {
+    const int v = list[k];
+    newid[v] = k;
+    const double2 p = m.pts[v];
+    const double4 t = m.ten[v];
+    pts[2 * k] = p.x;
+    pts[2 * k + 1] = p.y;
+    if (ten) {
+      ten[3 * k] = t.x;
+      ten[3 * k + 1] = t.y;
+      ten[3 * k + 2] = t.z;
+    }
+  }
+}
+
+__global__ void k_flag_live_tris(DMesh m, int nb_elems, uint8_t* __restrict__ flag) {
+  for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) flag[i] = m.tri[i].x >= 0 ? 1 : 0;
+}
+
+__global__ void k_pack_tris(DMesh m, const int* __restrict__ list, const int* count,
+                            const int* __restrict__ newid, int* __restrict__ out) {
+  const int n = *count;
+  for (int k = trn_tid(); k < n; k += trn_grid_stride()) {
+    const int4 t = m.tri[list[k]];
+    out[3 * k] = newid[t.x];
+    out[3 * k + 1] = newid[t.y];
+    out[3 * k + 2] = newid[t.z];
+  }
+}
+
+void pack_nodes(const DMesh& m, const int* list, const int* count, int* newid, double* pts, double* ten,
+                cudaStream_t s) {
+  k_pack_nodes<<<grid_for(m.capa_node), TRN_THREADS, 0, s>>>(m, list, count, newid, pts, ten);
+  note_launch();
+}
+
+void flag_live_tris(const DMesh& m, int nb_elems, uint8_t* flag, cudaStream_t s) {
+  k_flag_live_tris<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, flag);
+  note_launch();
+}
+
+void pack_tris(const DMesh& m, const int* list, const int* count, const int* newid, int* out,
+               cudaStream_t s) {
+  k_pack_tris<<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, list, count, newid, out);
+  note_launch();
 }
 
 void count_live(const DMesh& m, int nb_nodes, int nb_elems, int* out, cudaStream_t s) {

@@ -34,12 +34,14 @@ enum {
   S_COUNT = 6,     /* copy of a compaction count */
   S_PARTS = 8,     /* part offsets, 9 slots */
   S_LIVE = 18,     /* live vertices, live elements */
+  S_NTASK = 20,    /* device-counted candidates of a level (free mode) */
   S_SIZE = 32,     /* device status block */
   H_WIDE = 40,     /* host-only pinned slot for one 8-byte value */
   H_SIZE = 64,
 };
 
 constexpr int kLoopCap = 100000;
+constexpr int kMisRounds = 8;   /* independent-set rounds per coarsening level (free mode) */
 
 }  // namespace
 
@@ -63,6 +65,7 @@ struct trn_mesh {
   int* dual_n = nullptr;
   int* pairs = nullptr;
   int* parts = nullptr;
+  unsigned char* stage = nullptr;   /* transfer staging: max(24 B/vertex, 12 B/element) */
   int* status = nullptr;
   int* h_status = nullptr;
   /* the last loaded input, kept on the device for trn_mesh_reload */
@@ -172,7 +175,7 @@ void release(trn_mesh* m) {
   void* bufs[] = {m->d.pts, m->d.ten, m->d.lten, m->d.tri, m->d.stenc, m->d.deg, m->d.vic, m->d.vdeg,
                   m->d.tags, m->d.alive, m->d.fixes, m->d.activ, m->d.qual, m->solut, m->grad,
                   m->terms, m->complexity, m->target, m->flag, m->list, m->indep, m->map,
-                  m->dual, m->dual_n, m->pairs, m->parts, m->status, m->d_log, m->pts0,
+                  m->dual, m->dual_n, m->pairs, m->parts, m->stage, m->status, m->d_log, m->pts0,
                   m->tri0, m->tags0};
   for (void* b : bufs) if (b) cudaFree(b);
   if (m->h_status) cudaFreeHost(m->h_status);
@@ -300,6 +303,7 @@ int trn_mesh_create_ex(const int size[2], int bucket, int depth, int verbosity, 
       (rc = dmalloc(m, &m->indep, cn)) || (rc = dmalloc(m, &m->map, ce)) ||
       (rc = dmalloc(m, &m->dual, ce * 4)) || (rc = dmalloc(m, &m->dual_n, ce)) ||
       (rc = dmalloc(m, &m->pairs, ce * 2)) || (rc = dmalloc(m, &m->parts, cn)) ||
+      (rc = dmalloc(m, &m->stage, std::max(24 * cn, 12 * ce))) ||
       (rc = dmalloc(m, &m->status, S_SIZE)))
     return bail(rc);
   d.err = m->status + S_ERR;
@@ -361,8 +365,6 @@ int trn_mesh_load_arrays(trn_mesh* m, int nb_nodes, int nb_elems, const double* 
   if (!m || !points || !tris || nb_nodes <= 0 || nb_elems <= 0) return fail(m, TRN_ERR_INVALID, "load: bad arguments");
   if (nb_nodes > m->capa_node || nb_elems > m->capa_elem)
     return fail(m, TRN_ERR_CAPACITY, "load: mesh larger than the capacity");
-  for (long long i = 0; i < 3LL * nb_elems; ++i)
-    if (tris[i] < 0 || tris[i] >= nb_nodes) return fail(m, TRN_ERR_INVALID, "load: vertex index out of range");
   cudaStream_t s = m->stream;
   if (nb_nodes > m->n0_nodes || nb_elems > m->n0_elems || !m->pts0) {
     cudaFree(m->pts0);
@@ -376,15 +378,21 @@ int trn_mesh_load_arrays(trn_mesh* m, int nb_nodes, int nb_elems, const double* 
         (rc = dmalloc(m, &m->tags0, (size_t) nb_nodes)))
       return rc;
   }
-  /* staging: int3 -> int4 triangles; points are already x,y interleaved */
-  std::vector<int4> t4((size_t) nb_elems);
-  for (int i = 0; i < nb_elems; ++i) t4[i] = make_int4(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2], 0);
+  /* the triangles travel as given (3 ints each) and are checked and widened
+   * to int4 records on the device; points are already x,y interleaved */
+  CK(cudaMemsetAsync(m->status, 0, sizeof(int) * S_SIZE, s));
+  CK(cudaMemcpyAsync(m->stage, tris, sizeof(int) * 3 * (size_t) nb_elems, cudaMemcpyHostToDevice, s));
+  expand_tris(reinterpret_cast<const int*>(m->stage), nb_elems, nb_nodes, m->tri0, m->status + S_ERR, s);
   CK(cudaMemcpyAsync(m->pts0, points, sizeof(double) * 2 * (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(m->tri0, t4.data(), sizeof(int4) * (size_t) nb_elems, cudaMemcpyHostToDevice, s));
   if (tags) CK(cudaMemcpyAsync(m->tags0, tags, (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
   else CK(cudaMemsetAsync(m->tags0, 0, (size_t) nb_nodes, s));
   if (solut) CK(cudaMemcpyAsync(m->solut, solut, sizeof(double) * (size_t) nb_nodes, cudaMemcpyHostToDevice, s));
   else CK(cudaMemsetAsync(m->solut, 0, sizeof(double) * (size_t) nb_nodes, s));
+  int rc = sync_status(m);
+  if (rc) {
+    m->n0_nodes = m->n0_elems = 0;
+    return fail(m, TRN_ERR_INVALID, "load: vertex index out of range");
+  }
   m->n0_nodes = nb_nodes;
   m->n0_elems = nb_elems;
   return init_from_device(m);
@@ -507,6 +515,35 @@ int trn_mesh_counts(trn_mesh* m, int* nb_nodes, int* nb_elems, int* live_nodes, 
     if (live_nodes) *live_nodes = m->h_status[S_LIVE];
     if (live_elems) *live_elems = m->h_status[S_LIVE + 1];
   }
+  return TRN_OK;
+}
+
+/* the adapted mesh in memory, renumbered like Mesh::store (io.cpp:199-233) */
+int trn_mesh_export_compact(trn_mesh* m, double* points, int* tris, double* tensor, int* nb_nodes,
+                            int* nb_elems) {
+  if (!m || !nb_nodes || !nb_elems) return fail(m, TRN_ERR_INVALID, "export_compact: null argument");
+  cudaStream_t s = m->stream;
+  DMesh& d = m->d;
+  compact_u8(d.alive, m->nb_nodes, m->list, m->scan, s);
+  int rc = sync_status(m, m->scan.count);
+  if (rc) return rc;
+  const int nv = m->h_status[S_COUNT];
+  double* st_pts = reinterpret_cast<double*>(m->stage);
+  double* st_ten = reinterpret_cast<double*>(m->stage) + 2 * (size_t) nv;
+  pack_nodes(d, m->list, m->scan.count, m->target, st_pts, tensor ? st_ten : nullptr, s);
+  if (points) CK(cudaMemcpyAsync(points, st_pts, sizeof(double) * 2 * (size_t) nv, cudaMemcpyDeviceToHost, s));
+  if (tensor) CK(cudaMemcpyAsync(tensor, st_ten, sizeof(double) * 3 * (size_t) nv, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  flag_live_tris(d, m->nb_elems, m->flag, s);
+  compact_u8(m->flag, m->nb_elems, m->list, m->scan, s);
+  if ((rc = sync_status(m, m->scan.count))) return rc;
+  const int ne = m->h_status[S_COUNT];
+  int* st_tri = reinterpret_cast<int*>(m->stage);
+  pack_tris(d, m->list, m->scan.count, m->target, st_tri, s);
+  if (tris) CK(cudaMemcpyAsync(tris, st_tri, sizeof(int) * 3 * (size_t) ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *nb_nodes = nv;
+  *nb_elems = ne;
   return TRN_OK;
 }
 
@@ -657,6 +694,25 @@ int trn_coarsen_run(trn_mesh* m, int max_colors, trn_stats* st) {
   cudaStream_t s = m->stream;
   coarsen_pre(m->d, m->nb_nodes, s);
   int eval = 0, task = 0, nb_indep = 0, level = 0;
+  if (!m->replay) {
+    /* free mode: one host synchronisation per level */
+    int ntasks = 0;
+    do {
+      coarsen_filter_append(m->d, m->nb_nodes, m->target, m->list, m->status + S_NTASK, m->hws.state, s);
+      mis_jp_rounds(m->d, m->list, m->status + S_NTASK, kMisRounds, m->seed ^ (++m->calls * 0x9e37ULL),
+                    m->hws, m->indep, m->status + S_NINDEP, s);
+      collapse(m->d, m->indep, m->status + S_NINDEP, m->target, nullptr, s);
+      fix_tagged(m->d, m->nb_nodes, s);
+      int rc = sync_status(m);
+      if (rc) return rc;
+      ntasks = m->h_status[S_NTASK];
+      nb_indep = m->h_status[S_NINDEP];
+      eval += ntasks;
+      task += nb_indep;
+      if (++level > kLoopCap) return fail(m, TRN_ERR_NO_PROGRESS, "coarsen: level cap reached");
+    } while (ntasks && nb_indep);
+    return end_timing(m, st, eval, task);
+  }
   do {
     build_vicin(m->d, m->nb_nodes, true, s);
     coarsen_filter(m->d, m->nb_nodes, m->target, m->flag, s);
@@ -666,27 +722,12 @@ int trn_coarsen_run(trn_mesh* m, int max_colors, trn_stats* st) {
     const int ntasks = m->h_status[S_COUNT];
     if (!ntasks) break;
     eval += ntasks;
-    const int* indep;
-    const int* count;
-    if (m->replay) {
-      size_t off;
-      int n;
-      if ((rc = replay_take(m, 1, &off, &n))) return rc;
-      indep = m->d_log + off;
-      count = m->d_log + off - 1;
-      nb_indep = n;
-    } else {
-      mis_jp(m->d, m->nb_nodes, m->flag, m->list, ntasks, m->seed ^ (++m->calls * 0x9e37ULL), m->hws,
-             m->indep, m->status + S_NINDEP, m->scan, s);
-      indep = m->indep;
-      count = m->status + S_NINDEP;
-    }
-    collapse(m->d, indep, count, m->target, m->flag, s);
+    size_t off;
+    int n;
+    if ((rc = replay_take(m, 1, &off, &n))) return rc;
+    nb_indep = n;
+    collapse(m->d, m->d_log + off, m->d_log + off - 1, m->target, m->flag, s);
     fix_tagged(m->d, m->nb_nodes, s);
-    if (!m->replay) {
-      if ((rc = sync_status(m))) return rc;
-      nb_indep = m->h_status[S_NINDEP];
-    }
     task += nb_indep;
     if (++level > kLoopCap) return fail(m, TRN_ERR_NO_PROGRESS, "coarsen: level cap reached");
   } while (nb_indep);
@@ -704,33 +745,42 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
   swap_init(m->d, m->nb_nodes, m->nb_elems, m->map, s);
   int eval = 0, task = 0, commit = 0, level = 0;
   do {
-    swap_filter(m->d, m->nb_elems, m->flag, s);
-    compact_u8(m->flag, m->nb_elems, m->list, m->scan, s);
-    int rc = sync_status(m, m->scan.count);
-    if (rc) return rc;
-    const int ntasks = m->h_status[S_COUNT];
-    if (!ntasks) break;
-    eval += ntasks;
-    swap_dual(m->d, m->list, ntasks, m->dual, m->dual_n, m->map, s);
+    int ntasks = 0;
     const int* pairs;
     const int* npairs;
+    const int* ntasks_dev;
     if (m->replay) {
+      swap_filter(m->d, m->nb_elems, m->flag, s);
+      compact_u8(m->flag, m->nb_elems, m->list, m->scan, s);
+      int rc = sync_status(m, m->scan.count);
+      if (rc) return rc;
+      ntasks = m->h_status[S_COUNT];
+      if (!ntasks) break;
+      swap_dual(m->d, m->list, ntasks, m->dual, m->dual_n, m->map, s);
       size_t off;
       int n;
       if ((rc = replay_take(m, 2, &off, &n))) return rc;
       pairs = m->d_log + off;
       npairs = m->d_log + off - 1;
+      ntasks_dev = m->scan.count;
     } else {
-      match_handshake(m->d, m->nb_elems, m->dual, m->dual_n, ntasks, m->map,
+      /* free mode: one host synchronisation per level */
+      swap_filter_dual(m->d, m->nb_elems, m->dual, m->dual_n, m->map, m->status + S_NTASK, s);
+      match_handshake(m->d, m->nb_elems, m->dual, m->dual_n, m->status + S_NTASK, m->map,
                       m->seed ^ (++m->calls * 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s);
       pairs = m->pairs;
       npairs = m->status + S_NPAIRS;
+      ntasks_dev = m->status + S_NTASK;
     }
     CK(cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s));
-    swap_flip(m->d, pairs, npairs, m->map, m->dual, m->dual_n, ntasks, m->status + S_COMMIT, s);
+    swap_flip(m->d, pairs, npairs, m->map, m->dual, m->dual_n, ntasks_dev, m->status + S_COMMIT,
+              !m->replay, s);
     fix_tagged(m->d, m->nb_nodes, s);
-    if ((rc = sync_status(m))) return rc;
+    int rc = sync_status(m);
+    if (rc) return rc;
+    if (!m->replay) ntasks = m->h_status[S_NTASK];
     commit = m->h_status[S_COMMIT];
+    eval += ntasks;
     task += commit / 2;
     if (++level > kLoopCap) return fail(m, TRN_ERR_NO_PROGRESS, "swap: level cap reached");
   } while (commit);

@@ -131,6 +131,42 @@ __device__ __forceinline__ int trn_iunique(int* a, int n) {
   return k;
 }
 
+/* adjacency of v from its (canonical) stencil */
+__device__ __forceinline__ void build_one_vicin(const DMesh& m, int v) {
+  int buf[2 * TRN_MAX_DEG];
+  int k = 0;
+  if (m.alive[v]) {
+    const int* s = m.stenc + (size_t) v * m.bucket;
+    int d = trn_deg(m, v);
+    for (int a = 0; a < d; ++a) {
+      int4 n = m.tri[s[a]];
+      if (v == n.x) { buf[k++] = n.y; buf[k++] = n.z; }
+      else if (v == n.y) { buf[k++] = n.z; buf[k++] = n.x; }
+      else if (v == n.z) { buf[k++] = n.x; buf[k++] = n.y; }
+    }
+  }
+  trn_isort(buf, k);
+  k = trn_iunique(buf, k);
+  if (k > m.bucket) {
+    trn_set_error(m.err, TRN_DERR_CAPACITY);
+    k = m.bucket;
+  }
+  int* out = m.vic + (size_t) v * m.bucket;
+  for (int a = 0; a < k; ++a) out[a] = buf[a];
+  m.vdeg[v] = k;
+}
+
+/* warp-aggregated append of id to list[*count] */
+__device__ __forceinline__ void trn_append(int* list, int* count, int id) {
+  unsigned mask = __activemask();
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  list[base + __popc(mask & ((1u << lane) - 1))] = id;
+}
+
 /* 64-bit mix for seeded hash priorities (splitmix64 finaliser) */
 __device__ __forceinline__ uint64_t trn_hash64(uint64_t x) {
   x += 0x9e3779b97f4a7c15ULL;

@@ -40,6 +40,12 @@ void fix_tagged(const DMesh& m, int nb_nodes, cudaStream_t s);
 void flag_all_alive(const DMesh& m, int nb_nodes, cudaStream_t s);
 void quality_all(const DMesh& m, int nb_elems, cudaStream_t s);
 void count_live(const DMesh& m, int nb_nodes, int nb_elems, int* out, cudaStream_t s);
+void expand_tris(const int* raw, int nb_elems, int nb_nodes, int4* out, int* err, cudaStream_t s);
+void pack_nodes(const DMesh& m, const int* list, const int* count, int* newid, double* pts, double* ten,
+                cudaStream_t s);
+void flag_live_tris(const DMesh& m, int nb_elems, uint8_t* flag, cudaStream_t s);
+void pack_tris(const DMesh& m, const int* list, const int* count, const int* newid, int* out,
+               cudaStream_t s);
 
 /* metric (metric.cu) */
 struct MetricParams {
@@ -72,6 +78,9 @@ void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
 void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, cudaStream_t s);
 void collapse(const DMesh& m, const int* indep, const int* count, const int* target,
               const uint8_t* cand_flag, cudaStream_t s);
+/* free mode: adjacency + target + unordered candidate append in one pass */
+void coarsen_filter_append(const DMesh& m, int nb_nodes, int* target, int* cand, int* count,
+                           uint8_t* state, cudaStream_t s);
 
 /* swapping (swap.cu) */
 void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, cudaStream_t s);
@@ -79,7 +88,11 @@ void swap_filter(const DMesh& m, int nb_elems, uint8_t* flag, cudaStream_t s);
 void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual_n, int* map,
                cudaStream_t s);
 void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* map,
-               const int* dual, const int* dual_n, int ntasks, int* commit, cudaStream_t s);
+               const int* dual, const int* dual_n, const int* ntasks, int* commit, bool strict_map,
+               cudaStream_t s);
+/* free mode: filter and dual rows in one pass, *count rows */
+void swap_filter_dual(const DMesh& m, int nb_elems, int* dual, int* dual_n, int* map, int* count,
+                      cudaStream_t s);
 
 /* smoothing (smooth.cu) */
 void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
@@ -88,6 +101,7 @@ void smooth_color(const DMesh& m, const int* list, int n, int* counters, cudaStr
 /* graph heuristics, free mode (heuristics.cu) */
 struct HeurWs {
   uint8_t* state = nullptr;      /* per vertex / element */
+  uint8_t* state2 = nullptr;     /* second buffer of the independent-set rounds */
   unsigned long long* prop = nullptr;
   int* choice = nullptr;
   int* color = nullptr;
@@ -96,15 +110,15 @@ struct HeurWs {
 };
 void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem);
 void heur_ws_free(HeurWs* ws);
-/* Jones-Plassmann MIS over candidates (flag != 0) with adjacency vic;
- * writes the set to indep[0..*count) */
-void mis_jp(const DMesh& m, int nb_nodes, const uint8_t* cand_flag, const int* cand_list,
-            int ncand, uint64_t seed, HeurWs& ws, int* indep, int* count, ScanWs& scan,
-            cudaStream_t s);
-/* handshake matching on the dual rows; pairs[2k], pairs[2k+1]; *npairs */
+/* handshake matching on the dual rows (*ntasks of them); pairs[2k],
+ * pairs[2k+1]; *npairs */
 void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n,
-                     int ntasks, const int* map, uint64_t seed, HeurWs& ws, int* pairs,
+                     const int* ntasks, const int* map, uint64_t seed, HeurWs& ws, int* pairs,
                      int* npairs, cudaStream_t s);
+/* a fixed number of independent-set rounds over a device-counted candidate
+ * list; undecided candidates are re-activated (next level) */
+void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, uint64_t seed,
+                   HeurWs& ws, int* indep, int* nindep, cudaStream_t s);
 /* Jones-Plassmann first-fit coloring of interior vertices, colors 1..max_col;
  * parts: vertex ids grouped by color, part_off[c] offsets (c = 0..max_col) */
 void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& ws,
