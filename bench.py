@@ -194,17 +194,10 @@ def b200_arm(args, rank, world, local_rank):
         e2e_tin += tin
         d2h = sum(a.nbytes for a in out)
 
-    stats = np.array([tin_sum, tms_sum, wall, e2e_tin, e2e_t], dtype=np.float64)
-    if dist_on:
-        t = torch.tensor(stats, device="cuda")
-        sums = t.clone()
-        dist.all_reduce(sums, op=dist.ReduceOp.SUM)
-        maxs = t.clone()
-        dist.all_reduce(maxs, op=dist.ReduceOp.MAX)
-        tin_all, tms_max, wall_max = sums[0].item(), maxs[1].item(), maxs[2].item()
-        e2e_tin_all, e2e_max = sums[3].item(), maxs[4].item()
-    else:
-        tin_all, tms_max, wall_max, e2e_tin_all, e2e_max = stats.tolist()
+    from trinity_b200.dist import reduce_stats
+    agg = reduce_stats([tin_sum, tms_sum, wall, e2e_tin, e2e_t], [0, 3], [1, 2, 4],
+                       device="cuda" if dist_on else "cpu")
+    tin_all, tms_max, wall_max, e2e_tin_all, e2e_max = agg.tolist()
     if rank != 0:
         return None
 
