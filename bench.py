@@ -178,6 +178,29 @@ def b200_arm(args, rank, world, local_rank):
     _lib.profile_enable(False)
     final = g.counts()
 
+    # ---- the mixed-precision form on the same workload (reported beside) ----
+    forms = {}
+    if not args.no_forms:
+        g.set_precision("mixed")
+        for _ in range(args.warmup):
+            g.reload()
+            run_step(api, g, c, heur, kern)
+        m_tin, m_tms = 0, 0.0
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            g.reload()
+            tin, tms, _ = run_step(api, g, c, heur, kern)
+            m_tin += tin
+            m_tms += tms
+        q = g.quality_stats()
+        forms["mixed_fp32"] = {"tri_in": m_tin, "round_ms": m_tms,
+                               "final_mesh": {"nodes": g.counts()[2], "triangles": g.counts()[3]},
+                               "quality_min_max_mean": [round(x, 4) for x in q]}
+        g.set_precision("fp64")
+        g.reload()
+        run_step(api, g, c, heur, kern)
+        forms["fp64_quality_min_max_mean"] = [round(x, 4) for x in g.quality_stats()]
+
     # ---- end-to-end through the C ABI from host buffers ----
     pts = np.ascontiguousarray(m.points)
     tris = np.ascontiguousarray(m.tris, dtype=np.int32)
@@ -238,6 +261,16 @@ def b200_arm(args, rank, world, local_rank):
         "final_mesh": {"nodes": final[2], "triangles": final[3]},
         "clocks": clk.summary(),
     }
+    if "mixed_fp32" in forms:
+        f = forms["mixed_fp32"]
+        mixed = reduce_stats([f["tri_in"], f["round_ms"]], [0], [1], device="cuda" if dist_on else "cpu")
+        line["forms"] = {
+            "mixed_fp32": {"value": round(mixed[0] / (mixed[1] / 1e3), 1), "unit": UNIT,
+                           "round_ms_per_step": round(mixed[1] / args.steps, 3),
+                           "dtype": "f32 metric arithmetic, f64 coordinates/orientation",
+                           "final_mesh": f["final_mesh"], "quality_min_max_mean": f["quality_min_max_mean"]},
+            "fp64_quality_min_max_mean": forms["fp64_quality_min_max_mean"],
+        }
     return line
 
 
@@ -329,6 +362,7 @@ def main():
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    p.add_argument("--no-forms", action="store_true", help="skip the mixed-precision form")
     p.add_argument("--grid", type=int, default=None, help="grid side override (profiling runs)")
     args = p.parse_args()
     rank = int(os.environ.get("RANK", "0"))

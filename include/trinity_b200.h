@@ -73,6 +73,13 @@ int trn_mesh_export(trn_mesh* mesh, double* points, double* tensor, int* tris, u
  * of trn_mesh_counts; V' and T' are returned. */
 int trn_mesh_export_compact(trn_mesh* mesh, double* points, int* tris, double* tensor,
                             int* nb_nodes, int* nb_elems);
+/* per-element quality in the current arithmetic form (nb_elems entries, 0
+ * for deleted elements) */
+int trn_mesh_qualities(trn_mesh* mesh, double* q);
+/* replaces Mesh::computeQuality(double quality[3]) (mesh.cpp:647-681):
+ * quality[0] = min(quality[0], q_min), quality[1] = max(quality[1], q_max),
+ * quality[2] = mean over live elements */
+int trn_mesh_quality_stats(trn_mesh* mesh, double quality[3]);
 /* slot counts (deleted entities included) and live counts */
 int trn_mesh_counts(trn_mesh* mesh, int* nb_nodes, int* nb_elems, int* live_nodes,
                     int* live_elems);
@@ -100,6 +107,15 @@ int trn_round_run(trn_mesh* mesh, int depth, trn_stats stats[4]);
  * replay mode. No counterpart in the reference: it makes the GPU's topology
  * checkable bit for bit against the reference's 1-thread run. */
 int trn_set_replay(trn_mesh* mesh, const int32_t* log, size_t n);
+/* Arithmetic form of the metric computations during the rounds.
+ * TRN_PRECISION_FP64 (default): the drop-in, bit-compatible with the
+ * reference. TRN_PRECISION_MIXED: log-Euclidean means, metric edge lengths,
+ * Steiner weights and element qualities in FP32; coordinates, orientation and
+ * area tests, stored tensors and the Hessian recovery stay FP64. Not
+ * available together with replay. */
+#define TRN_PRECISION_FP64 0
+#define TRN_PRECISION_MIXED 1
+int trn_set_precision(trn_mesh* mesh, int mode);
 /* free-mode options: seed of the hash priorities; exact_sum = 1 takes the
  * metric complexity sum in element order (bit-compatible with the reference) */
 int trn_set_options(trn_mesh* mesh, uint64_t seed, int exact_sum);

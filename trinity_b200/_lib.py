@@ -73,6 +73,9 @@ def lib():
         L.trn_last_error.restype = ctypes.c_char_p
         L.trn_version.restype = ctypes.c_char_p
         L.trn_mesh_reload.argtypes = [pmesh]
+        L.trn_set_precision.argtypes = [pmesh, ip]
+        L.trn_mesh_qualities.argtypes = [pmesh, vp]
+        L.trn_mesh_quality_stats.argtypes = [pmesh, vp]
         L.trn_mesh_export_compact.argtypes = [pmesh, vp, vp, vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
         L.trn_profile_enable.argtypes = [ip]
         L.trn_profile_count.restype = ip

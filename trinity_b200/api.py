@@ -127,6 +127,23 @@ class Mesh:
         assert (a.value, b.value) == (nv, ne)
         return pts, tri, ten
 
+    def set_precision(self, mode: str) -> None:
+        """'fp64' (default, bit-compatible drop-in) or 'mixed' (FP32 metric
+        arithmetic, FP64 coordinates and orientation)."""
+        self._check(self._L.trn_set_precision(self.h, {"fp64": 0, "mixed": 1}[mode]))
+
+    def qualities(self):
+        nn, ne, _, _ = self.counts()
+        q = np.empty(ne)
+        self._check(self._L.trn_mesh_qualities(self.h, _p(q)))
+        return q
+
+    def quality_stats(self):
+        """Mesh::computeQuality(double[3]): (min, max, mean)."""
+        q = np.array([3.0, 0.0, 0.0])
+        self._check(self._L.trn_mesh_quality_stats(self.h, _p(q)))
+        return tuple(q.tolist())
+
     def set_replay(self, log) -> None:
         a = np.ascontiguousarray(log, dtype=np.int32)
         self._check(self._L.trn_set_replay(self.h, _p(a) if a.size else None, a.size))

@@ -17,7 +17,7 @@
  * repair pass sorts them.
  */
 #include "trn_internal.h"
-#include "trn_numeric.cuh"
+#include "trn_mixed.cuh"
 
 namespace trn {
 
@@ -29,6 +29,7 @@ __global__ void k_coarse_pre(DMesh m, int nb_nodes) {
   }
 }
 
+template <bool F32>
 __device__ int identify_target(const DMesh& m, int source) {
   const bool bound_source = (m.tags[source] & TRN_TAG_BOUND) != 0;
   double lens[TRN_MAX_DEG];
@@ -42,7 +43,7 @@ __device__ int identify_target(const DMesh& m, int source) {
     int neigh = vc[b];
     bool bound_destin = (m.tags[neigh] & TRN_TAG_BOUND) != 0;
     if (bound_source && !bound_destin) continue;
-    double len = trn_dist2(ps, m.pts[neigh], ts, m.ten[neigh]);
+    double len = length_x<F32>(ps, m.pts[neigh], ts, m.ten[neigh]);
     if (len < TRN_L_MIN) {
       int p = nc;
       while (p > 0 && lens[p - 1] > len) {
@@ -79,9 +80,9 @@ __device__ int identify_target(const DMesh& m, int source) {
       double2 p0 = m.pts[f0], p1 = m.pts[f1], p2 = m.pts[f2];
       if (trn_ccw(p0, p1, p2)) {
         double4 t0 = m.ten[f0], t1 = m.ten[f1], t2 = m.ten[f2];
-        double l0 = trn_dist2(p0, p1, t0, t1);
-        double l1 = trn_dist2(p1, p2, t1, t2);
-        double l2 = trn_dist2(p2, p0, t2, t0);
+        double l0 = length_x<F32>(p0, p1, t0, t1);
+        double l1 = length_x<F32>(p1, p2, t1, t2);
+        double l2 = length_x<F32>(p2, p0, t2, t0);
         skip = (l0 > TRN_L_MAX || l1 > TRN_L_MAX || l2 > TRN_L_MAX);
         continue;
       }
@@ -91,6 +92,7 @@ __device__ int identify_target(const DMesh& m, int source) {
   return skip ? -1 : destin;
 }
 
+template <bool F32>
 __global__ void k_coarse_filter(DMesh m, int nb_nodes, int* __restrict__ target,
                                 uint8_t* __restrict__ flag) {
   if (trn_failed(m)) return;
@@ -98,7 +100,7 @@ __global__ void k_coarse_filter(DMesh m, int nb_nodes, int* __restrict__ target,
     uint8_t f = 0;
     if (m.activ[v] > 0) {
       m.activ[v] = 0;
-      int t = identify_target(m, v);
+      int t = identify_target<F32>(m, v);
       target[v] = t;
       f = t > -1 ? 1 : 0;
     }
@@ -110,6 +112,7 @@ __global__ void k_coarse_filter(DMesh m, int nb_nodes, int* __restrict__ target,
  * finds its target and appends the candidates (in no particular order: the
  * independent set is chosen by hashed priorities, not by list position),
  * marking them undecided for the independent-set rounds */
+template <bool F32>
 __global__ void k_coarse_filter_append(DMesh m, int nb_nodes, int* __restrict__ target,
                                        int* __restrict__ cand, int* count, uint8_t* __restrict__ state) {
   if (trn_failed(m)) return;
@@ -117,7 +120,7 @@ __global__ void k_coarse_filter_append(DMesh m, int nb_nodes, int* __restrict__ 
     if (m.activ[v] <= 0) continue;
     m.activ[v] = 0;
     build_one_vicin(m, v);
-    const int t = identify_target(m, v);
+    const int t = identify_target<F32>(m, v);
     target[v] = t;
     if (t > -1) {
       state[v] = 1;
@@ -191,19 +194,24 @@ void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s) {
   check_launch("coarsen_pre");
 }
 
-void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, cudaStream_t s) {
+void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, bool fp32, cudaStream_t s) {
   ProfScope ps("coarsen_filter", s, (double) nb_nodes * (1 + 1 + 4 + 1));
-  k_coarse_filter<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, flag);
+  if (fp32) k_coarse_filter<true><<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, flag);
+  else k_coarse_filter<false><<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, flag);
   note_launch();
   check_launch("coarsen_filter");
 }
 
 void coarsen_filter_append(const DMesh& m, int nb_nodes, int* target, int* cand, int* count,
-                           uint8_t* state, cudaStream_t s) {
+                           uint8_t* state, bool fp32, cudaStream_t s) {
   ProfScope ps("coarsen_filter", s, (double) nb_nodes * (1 + 1 + 4 + 1));
   cudaMemsetAsync(count, 0, sizeof(int), s);
-  k_coarse_filter_append<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, cand, count,
-                                                                     state);
+  if (fp32)
+    k_coarse_filter_append<true><<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, cand,
+                                                                           count, state);
+  else
+    k_coarse_filter_append<false><<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, cand,
+                                                                            count, state);
   note_launch();
   check_launch("coarsen_filter_append");
 }

@@ -22,7 +22,7 @@
  * levels of one refinement call and is cleared at its start.
  */
 #include "trn_internal.h"
-#include "trn_numeric.cuh"
+#include "trn_mixed.cuh"
 
 #include <climits>
 
@@ -80,6 +80,7 @@ __device__ __forceinline__ int elem_neigh(const DMesh& m, int id, int i, int j) 
   return -1;
 }
 
+template <bool F32>
 __global__ void k_ref_filter(DMesh m, int nb_elems, int4* __restrict__ info,
                              long long* __restrict__ cnt) {
   if (trn_failed(m)) return;
@@ -97,7 +98,7 @@ __global__ void k_ref_filter(DMesh m, int nb_elems, int4* __restrict__ info,
     int opp[3] = {-1, -1, -1};
     for (int j = 0; j < 3; ++j) {
       int k = (j + 1) % 3;
-      double len = trn_dist2(p[j], p[k], q[j], q[k]);
+      double len = length_x<F32>(p[j], p[k], q[j], q[k]);
       if (len > TRN_L_MAX) {
         lmask |= 1 << j;
         int o = elem_neigh(m, i, n[j], n[k]);
@@ -110,6 +111,7 @@ __global__ void k_ref_filter(DMesh m, int nb_elems, int4* __restrict__ info,
   }
 }
 
+template <bool F32>
 __global__ void k_ref_steiner(DMesh m, int nb_elems, int nb_nodes, const int4* __restrict__ info,
                               const long long* __restrict__ off, unsigned long long* hkey,
                               int* hval, unsigned long long hcap) {
@@ -127,10 +129,11 @@ __global__ void k_ref_steiner(DMesh m, int nb_elems, int nb_nodes, const int4* _
       int v1 = n[j], v2 = n[(j + 1) % 3];
       double2 rp;
       double rt[3];
-      trn_steiner(m.pts[v1], m.pts[v2], m.ten[v1], m.ten[v2], m.lten[v1], m.lten[v2], &rp, rt);
+      steiner_x<F32>(m.pts[v1], m.pts[v2], m.ten[v1], m.ten[v2], log_load<F32>(m, v1),
+                     log_load<F32>(m, v2), &rp, rt);
       m.pts[id] = rp;
       m.ten[id] = make_double4(rt[0], rt[1], rt[2], 0.0);
-      m.lten[id] = trn_log_tensor(rt[0], rt[1], rt[2]);
+      log_store<F32>(m, id, log_of<F32>(rt[0], rt[1], rt[2]));
       if (opp[j] < 0) m.tags[id] = TRN_TAG_BOUND;
       h_insert(hkey, hval, hcap, edge_key(v1, v2), id, m.err);
       ++id;
@@ -142,6 +145,7 @@ __device__ __forceinline__ void put_tri(const DMesh& m, int id, int a, int b, in
   m.tri[id] = make_int4(a, b, c, 0);
 }
 
+template <bool F32>
 __global__ void k_ref_cut(DMesh m, int nb_elems, const int4* __restrict__ info,
                           const long long* __restrict__ off, const unsigned long long* hkey,
                           const int* hval, unsigned long long hcap) {
@@ -177,8 +181,8 @@ __global__ void k_ref_cut(DMesh m, int nb_elems, const int4* __restrict__ info,
            * the two sides of an edge measure it differently) leaves the
            * element uncut instead of reading vertex -1 */
           if (s[j] < 0 || s[k] < 0) break;
-          double diag0 = trn_dist2(m.pts[n[j]], m.pts[s[j]], m.ten[n[j]], m.ten[s[j]]);
-          double diag1 = trn_dist2(m.pts[n[k]], m.pts[s[k]], m.ten[n[k]], m.ten[s[k]]);
+          double diag0 = length_x<F32>(m.pts[n[j]], m.pts[s[j]], m.ten[n[j]], m.ten[s[j]]);
+          double diag1 = length_x<F32>(m.pts[n[k]], m.pts[s[k]], m.ten[n[k]], m.ten[s[k]]);
           int v = (diag0 < diag1 ? j : k);
           int w = (v == j ? k : j);
           const int a3[3] = {t[0], t[1], t[2]};
@@ -238,23 +242,32 @@ void refine_reset_hash(RefineWs& ws, cudaStream_t s) {
   cudaMemsetAsync(ws.hval, 0x7f, sizeof(int) * ws.hcap, s);
 }
 
-void refine_filter(const DMesh& m, int nb_elems, RefineWs& ws, cudaStream_t s) {
+void refine_filter(const DMesh& m, int nb_elems, RefineWs& ws, bool fp32, cudaStream_t s) {
   ProfScope ps("refine_filter", s, (double) nb_elems * (kTri + 16 + 8) + (double) nb_elems / 2 * (kPt + kTen));
-  k_ref_filter<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.cnt);
+  if (fp32) k_ref_filter<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.cnt);
+  else k_ref_filter<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.cnt);
   note_launch();
   check_launch("refine_filter");
 }
 
-void refine_apply(const DMesh& m, int nb_nodes, int nb_elems, RefineWs& ws, cudaStream_t s) {
+void refine_apply(const DMesh& m, int nb_nodes, int nb_elems, RefineWs& ws, bool fp32, cudaStream_t s) {
   {
   ProfScope ps("refine_steiner", s, (double) nb_elems * (16 + 8));
-  k_ref_steiner<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
-                                                            ws.hkey, ws.hval, ws.hcap);
+  if (fp32)
+    k_ref_steiner<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
+                                                                  ws.hkey, ws.hval, ws.hcap);
+  else
+    k_ref_steiner<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
+                                                                   ws.hkey, ws.hval, ws.hcap);
   note_launch();
   }
   ProfScope ps("refine_cut", s, (double) nb_elems * (16 + 8 + kTri));
-  k_ref_cut<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.off, ws.hkey,
-                                                        ws.hval, ws.hcap);
+  if (fp32)
+    k_ref_cut<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.off, ws.hkey,
+                                                              ws.hval, ws.hcap);
+  else
+    k_ref_cut<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.off, ws.hkey,
+                                                               ws.hval, ws.hcap);
   note_launch();
   check_launch("refine_apply");
 }

@@ -15,7 +15,7 @@
  * classes run in order, as in the reference.
  */
 #include "trn_internal.h"
-#include "trn_numeric.cuh"
+#include "trn_mixed.cuh"
 
 #include <algorithm>
 
@@ -26,6 +26,7 @@ __global__ void k_smooth_pre(DMesh m, int nb_nodes) {
     if (m.alive[v]) m.activ[v] = (m.tags[v] & TRN_TAG_BOUND) ? 0 : 1;
 }
 
+template <bool F32>
 __device__ int move_laplacian(const DMesh& m, int i) {
   const int* vc = m.vic + (size_t) i * m.bucket;
   const int* st = m.stenc + (size_t) i * m.bucket;
@@ -35,26 +36,26 @@ __device__ int move_laplacian(const DMesh& m, int i) {
   for (int a = 0; a < deg; ++a) q_min = trn_dmin(q_min, m.qual[st[a]]);
   const double2 pini = m.pts[i];
   const double4 tini = m.ten[i];
-  const double4 lini = m.lten[i];
+  const LogT<F32> lini = log_load<F32>(m, i);
   double ox = 0, oy = 0;
-  double lm[4] = {0, 0, 0, 0};
+  LogSum<F32> lsum;
   for (int k = 0; k < nb_neigh; ++k) {
     const int nb = vc[k];
     const double2 pb = m.pts[nb];
     const double4 tb = m.ten[nb];
-    const double len = trn_dist2(pini, pb, tini, tb);
+    const double len = length_x<F32>(pini, pb, tini, tb);
     ox += pini.x + ((pb.x - pini.x) / len);
     oy += pini.y + ((pb.y - pini.y) / len);
-    trn_interp_addl(lm, m.lten[nb]);
+    lsum.add(log_load<F32>(m, nb));
   }
   ox /= nb_neigh;
   oy /= nb_neigh;
   double tn[3];
-  trn_interp_finish(lm, nb_neigh, tn);
+  lsum.finish(nb_neigh, tn);
   const double4 tnew = make_double4(tn[0], tn[1], tn[2], 0.0);
-  const double4 lnew = trn_log_tensor(tn[0], tn[1], tn[2]);
+  const LogT<F32> lnew = log_of<F32>(tn[0], tn[1], tn[2]);
   m.ten[i] = tnew;
-  m.lten[i] = lnew;
+  log_store<F32>(m, i, lnew);
   double qual[TRN_MAX_DEG];
   bool valid;
   int retry = 0;
@@ -72,10 +73,10 @@ __device__ int move_laplacian(const DMesh& m, int i) {
       const double2 p2 = (n.z == i) ? pa : m.pts[n.z];
       valid = false;
       if (trn_ccw(p0, p1, p2)) {
-        const double4 l0 = (n.x == i) ? lnew : m.lten[n.x];
-        const double4 l1 = (n.y == i) ? lnew : m.lten[n.y];
-        const double4 l2 = (n.z == i) ? lnew : m.lten[n.z];
-        qual[a] = trn_quality_l(p0, p1, p2, l0, l1, l2);
+        const LogT<F32> l0 = (n.x == i) ? lnew : log_load<F32>(m, n.x);
+        const LogT<F32> l1 = (n.y == i) ? lnew : log_load<F32>(m, n.y);
+        const LogT<F32> l2 = (n.z == i) ? lnew : log_load<F32>(m, n.z);
+        qual[a] = quality_x(p0, p1, p2, l0, l1, l2);
         valid = (qual[a] > q_min);
       }
     }
@@ -86,11 +87,12 @@ __device__ int move_laplacian(const DMesh& m, int i) {
   } else {
     m.pts[i] = pini;
     m.ten[i] = tini;
-    m.lten[i] = lini;
+    log_store<F32>(m, i, lini);
   }
   return valid ? 1 : 0;
 }
 
+template <bool F32>
 __global__ void k_smooth_move(DMesh m, const int* __restrict__ list, int n, int* counters) {
   if (trn_failed(m)) return;
   int tasks = 0, commit = 0;
@@ -103,7 +105,7 @@ __global__ void k_smooth_move(DMesh m, const int* __restrict__ list, int n, int*
     if (!m.activ[v]) continue;
     if (m.vdeg[v] == 0) continue;
     tasks++;
-    commit += move_laplacian(m, v);
+    commit += move_laplacian<F32>(m, v);
   }
   if (tasks) atomicAdd(counters, tasks);
   if (commit) atomicAdd(counters + 1, commit);
@@ -115,7 +117,7 @@ void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s) {
   check_launch("smooth_pre");
 }
 
-void smooth_color(const DMesh& m, const int* list, int n, int* counters, cudaStream_t s) {
+void smooth_color(const DMesh& m, const int* list, int n, int* counters, bool fp32, cudaStream_t s) {
   if (n <= 0) return;
   /* per moved vertex: list id, flag, counts, own point/tensor read+write,
    * stencil and adjacency rows, its elements and their cached qualities
@@ -124,7 +126,8 @@ void smooth_color(const DMesh& m, const int* list, int n, int* counters, cudaStr
   const double own = 4 + 1 + 8 + 2 * (kPt + kTen) + kAvgDeg * (2 * kIdx + kTri + 2 * kQ);
   const double nbr = (double) std::min<long long>((long long) m.capa_node, 6LL * n) * (kPt + kTen);
   ProfScope ps("smooth_move", s, n * own + nbr);
-  k_smooth_move<<<grid_for(n, 128), 128, 0, s>>>(m, list, n, counters);
+  if (fp32) k_smooth_move<true><<<grid_for(n, 128), 128, 0, s>>>(m, list, n, counters);
+  else k_smooth_move<false><<<grid_for(n, 128), 128, 0, s>>>(m, list, n, counters);
   note_launch();
   check_launch("smooth_color");
 }

@@ -19,7 +19,7 @@
  * rows therefore persist across levels.
  */
 #include "trn_internal.h"
-#include "trn_numeric.cuh"
+#include "trn_mixed.cuh"
 
 namespace trn {
 
@@ -27,6 +27,7 @@ __global__ void k_swap_init_nodes(DMesh m, int nb_nodes) {
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) m.fixes[v] = 0;
 }
 
+template <bool F32>
 __global__ void k_swap_init_elems(DMesh m, int nb_elems, int* __restrict__ map) {
   if (trn_failed(m)) return;
   for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
@@ -36,7 +37,7 @@ __global__ void k_swap_init_elems(DMesh m, int nb_elems, int* __restrict__ map) 
       m.activ[i] = 0;
       continue;
     }
-    m.qual[i] = trn_quality_l(m.pts[t.x], m.pts[t.y], m.pts[t.z], m.lten[t.x], m.lten[t.y], m.lten[t.z]);
+    m.qual[i] = quality_of<F32>(m, t);
     m.activ[i] = 1;
   }
 }
@@ -111,6 +112,7 @@ __global__ void k_swap_filter_dual(DMesh m, int nb_elems, int* __restrict__ dual
 }
 
 /* Swap::swap, swapping.cpp:55-149 */
+template <bool F32>
 __device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int* map,
                          const int* dual, const int* dual_n, int ntasks, bool strict_map) {
   const int4 a = m.tri[id1], b = m.tri[id2];
@@ -140,10 +142,10 @@ __device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int*
   const double2 p22 = m.pts[c2[2]];
   /* c2 = (c1[2], c1[1], c2[2]) */
   if (!trn_ccw(p10, p11, p12) || !trn_ccw(p12, p11, p22)) return 0;
-  const double4 l10 = m.lten[c1[0]], l11 = m.lten[c1[1]], l12 = m.lten[c1[2]];
-  const double4 l22 = m.lten[c2[2]];
-  const double q0 = trn_quality_l(p10, p11, p12, l10, l11, l12);
-  const double q1 = trn_quality_l(p12, p11, p22, l12, l11, l22);
+  const LogT<F32> l10 = log_load<F32>(m, c1[0]), l11 = log_load<F32>(m, c1[1]);
+  const LogT<F32> l12 = log_load<F32>(m, c1[2]), l22 = log_load<F32>(m, c2[2]);
+  const double q0 = quality_x(p10, p11, p12, l10, l11, l12);
+  const double q1 = quality_x(p12, p11, p22, l12, l11, l22);
   const double q_old = trn_dmin(m.qual[id1], m.qual[id2]);
   const double q_new = trn_dmin(q0, q1);
   if (q_new < q_old) return 0;
@@ -168,6 +170,7 @@ __device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int*
   return 2;
 }
 
+template <bool F32>
 __global__ void k_swap_flip(DMesh m, const int* __restrict__ pairs, const int* npairs,
                             const int* __restrict__ map, const int* __restrict__ dual,
                             const int* __restrict__ dual_n, const int* ntasks_dev, int* commit,
@@ -192,17 +195,18 @@ __global__ void k_swap_flip(DMesh m, const int* __restrict__ pairs, const int* n
       trn_set_error(m.err, TRN_DERR_REPLAY);
       continue;
     }
-    local += flip_pair(m, k1, k2, index, map, dual, dual_n, ntasks, strict_map != 0);
+    local += flip_pair<F32>(m, k1, k2, index, map, dual, dual_n, ntasks, strict_map != 0);
   }
   if (local) atomicAdd(commit, local);
 }
 
-void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, cudaStream_t s) {
+void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, bool fp32, cudaStream_t s) {
   ProfScope ps("swap_init", s, (double) nb_nodes + (double) nb_elems * (kTri + kQ + 4 + 1) +
                                  (double) nb_elems / 2 * (kPt + kTen));
   k_swap_init_nodes<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
   note_launch();
-  k_swap_init_elems<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, map);
+  if (fp32) k_swap_init_elems<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, map);
+  else k_swap_init_elems<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, map);
   note_launch();
   check_launch("swap_init");
 }
@@ -233,10 +237,14 @@ void swap_filter_dual(const DMesh& m, int nb_elems, int* dual, int* dual_n, int*
 
 void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* map,
                const int* dual, const int* dual_n, const int* ntasks, int* commit, bool strict_map,
-               cudaStream_t s) {
+               bool fp32, cudaStream_t s) {
   ProfScope ps("swap_flip", s, 0.0);
-  k_swap_flip<<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
-                                                             ntasks, commit, strict_map ? 1 : 0);
+  if (fp32)
+    k_swap_flip<true><<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
+                                                                   ntasks, commit, strict_map ? 1 : 0);
+  else
+    k_swap_flip<false><<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
+                                                                    ntasks, commit, strict_map ? 1 : 0);
   note_launch();
   check_launch("swap_flip");
 }

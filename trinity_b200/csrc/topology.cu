@@ -12,7 +12,7 @@
  *                    the vertex's bucket held in registers/local memory.
  */
 #include "trn_internal.h"
-#include "trn_numeric.cuh"
+#include "trn_mixed.cuh"
 
 namespace trn {
 
@@ -75,12 +75,13 @@ __global__ void k_flag_alive(DMesh m, int nb_nodes) {
 }
 
 /* cached quality of every live element (swapping.cpp:167-174, smoothing.cpp:145-151) */
+template <bool F32>
 __global__ void k_quality_all(DMesh m, int nb_elems) {
   if (trn_failed(m)) return;
   for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
     int4 t = m.tri[i];
     if (t.x < 0) continue;
-    m.qual[i] = trn_quality_l(m.pts[t.x], m.pts[t.y], m.pts[t.z], m.lten[t.x], m.lten[t.y], m.lten[t.z]);
+    m.qual[i] = quality_of<F32>(m, t);
   }
 }
 
@@ -203,9 +204,31 @@ void flag_all_alive(const DMesh& m, int nb_nodes, cudaStream_t s) {
   note_launch();
 }
 
-void quality_all(const DMesh& m, int nb_elems, cudaStream_t s) {
+/* the per-vertex logarithm cache of the FP32 form, from the stored tensors */
+__global__ void k_log_cache_f32(DMesh m, int nb_nodes) {
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    const double4 t = m.ten[v];
+    log_store<true>(m, v, log_of<true>(t.x, t.y, t.z));
+  }
+}
+
+__global__ void k_log_cache_f64(DMesh m, int nb_nodes) {
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    const double4 t = m.ten[v];
+    m.lten[v] = trn_log_tensor(t.x, t.y, t.z);
+  }
+}
+
+void log_cache(const DMesh& m, int nb_nodes, bool fp32, cudaStream_t s) {
+  if (fp32) k_log_cache_f32<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  else k_log_cache_f64<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  note_launch();
+}
+
+void quality_all(const DMesh& m, int nb_elems, bool fp32, cudaStream_t s) {
   ProfScope ps("quality_all", s, (double) nb_elems * (kTri + kQ) + (double) nb_elems / 2 * (kPt + kTen));
-  k_quality_all<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems);
+  if (fp32) k_quality_all<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems);
+  else k_quality_all<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems);
   note_launch();
   check_launch("quality_all");
 }

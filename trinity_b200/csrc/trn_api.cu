@@ -85,6 +85,7 @@ struct trn_mesh {
   uint64_t seed = 0x7472696e697479ULL;
   uint64_t calls = 0;
   bool exact_sum = false;
+  bool fp32 = false;   /* mixed-precision form of the metric arithmetic */
   double last_complexity = 0.0;
   double last_ms = 0.0;
   std::string err;
@@ -547,6 +548,39 @@ int trn_mesh_export_compact(trn_mesh* m, double* points, int* tris, double* tens
   return TRN_OK;
 }
 
+/* element qualities in the current arithmetic form (dead elements: 0) */
+int trn_mesh_qualities(trn_mesh* m, double* q) {
+  if (!m || !q) return fail(m, TRN_ERR_INVALID, "qualities: null argument");
+  CK(cudaMemsetAsync(m->d.qual, 0, sizeof(double) * (size_t) m->nb_elems, m->stream));
+  quality_all(m->d, m->nb_elems, m->fp32, m->stream);
+  CK(cudaMemcpyAsync(q, m->d.qual, sizeof(double) * (size_t) m->nb_elems, cudaMemcpyDeviceToHost, m->stream));
+  return sync_status(m);
+}
+
+/* Mesh::computeQuality(double quality[3]), mesh.cpp:647-681: min, max and
+ * mean element quality (the min and max are folded into quality[0..1]) */
+int trn_mesh_quality_stats(trn_mesh* m, double quality[3]) {
+  if (!m || !quality) return fail(m, TRN_ERR_INVALID, "quality_stats: null argument");
+  std::vector<double> q((size_t) m->nb_elems);
+  std::vector<int> tri((size_t) m->nb_elems * 3);
+  int rc = trn_mesh_qualities(m, q.data());
+  if (rc) return rc;
+  if ((rc = trn_mesh_export(m, nullptr, nullptr, tri.data(), nullptr, nullptr))) return rc;
+  double qmin = 3., qmax = 0., qtot = 0.;
+  int count = 0;
+  for (int i = 0; i < m->nb_elems; ++i) {
+    if (tri[3 * i] < 0) continue;
+    qmin = std::min(qmin, q[i]);
+    qmax = std::max(qmax, q[i]);
+    qtot += q[i];
+    ++count;
+  }
+  quality[0] = std::min(quality[0], qmin);
+  quality[1] = std::max(quality[1], qmax);
+  quality[2] = count ? qtot / count : 0.0;
+  return TRN_OK;
+}
+
 /* Mesh::store, io.cpp:164-255 */
 int trn_mesh_store(trn_mesh* m, const char* path) {
   if (!m || !path) return fail(m, TRN_ERR_INVALID, "store: null path");
@@ -611,10 +645,25 @@ int trn_set_replay(trn_mesh* m, const int32_t* log, size_t n) {
   m->cursor = 0;
   m->replay = false;
   if (!log || n == 0) return TRN_OK;
+  if (m->fp32) return fail(m, TRN_ERR_INVALID, "set_replay: replay needs the FP64 form");
   m->log.assign(log, log + n);
   CK(cudaMalloc(&m->d_log, sizeof(int32_t) * n));
   CK(cudaMemcpy(m->d_log, log, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
   m->replay = true;
+  return TRN_OK;
+}
+
+int trn_set_precision(trn_mesh* m, int mode) {
+  if (!m || (mode != TRN_PRECISION_FP64 && mode != TRN_PRECISION_MIXED))
+    return fail(m, TRN_ERR_INVALID, "set_precision: unknown mode");
+  const bool f = mode == TRN_PRECISION_MIXED;
+  if (f && m->replay) return fail(m, TRN_ERR_INVALID, "set_precision: replay needs the FP64 form");
+  if (f != m->fp32 && m->nb_nodes > 0) {
+    log_cache(m->d, m->nb_nodes, f, m->stream);
+    int rc = sync_status(m);
+    if (rc) return rc;
+  }
+  m->fp32 = f;
   return TRN_OK;
 }
 
@@ -644,6 +693,7 @@ int trn_metric_run(trn_mesh* m, double target_factor, int norm, double h_min, do
   begin_timing(m);
   metric_run(m->d, m->nb_nodes, m->nb_elems, m->solut, m->grad, m->terms, m->complexity,
              m->exact_sum || m->replay, p, m->stream);
+  if (m->fp32) log_cache(m->d, m->nb_nodes, true, m->stream);
   CK(cudaMemcpyAsync(m->h_status + H_WIDE, m->complexity, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
   int rc = sync_status(m);
   if (rc) return rc;
@@ -661,7 +711,7 @@ int trn_refine_run(trn_mesh* m, int depth, trn_stats* st) {
   refine_reset_hash(m->rws, s);
   int eval = 0, task = 0;
   for (int level = 0; level < depth; ++level) {
-    refine_filter(m->d, m->nb_elems, m->rws, s);
+    refine_filter(m->d, m->nb_elems, m->rws, m->fp32, s);
     scan_i64(m->rws.cnt, m->rws.off, m->nb_elems, m->scan, s);
     long long tot = 0;
     CK(cudaMemcpyAsync(m->h_status + H_WIDE, m->scan.total, sizeof(long long), cudaMemcpyDeviceToHost, s));
@@ -674,7 +724,7 @@ int trn_refine_run(trn_mesh* m, int depth, trn_stats* st) {
     task += adds;
     if ((long long) m->nb_nodes + split > m->capa_node || (long long) m->nb_elems + adds > m->capa_elem)
       return fail(m, TRN_ERR_CAPACITY, "refine: node or element capacity exceeded");
-    refine_apply(m->d, m->nb_nodes, m->nb_elems, m->rws, s);
+    refine_apply(m->d, m->nb_nodes, m->nb_elems, m->rws, m->fp32, s);
     m->nb_nodes += split;
     m->nb_elems += adds;
   }
@@ -698,7 +748,8 @@ int trn_coarsen_run(trn_mesh* m, int max_colors, trn_stats* st) {
     /* free mode: one host synchronisation per level */
     int ntasks = 0;
     do {
-      coarsen_filter_append(m->d, m->nb_nodes, m->target, m->list, m->status + S_NTASK, m->hws.state, s);
+      coarsen_filter_append(m->d, m->nb_nodes, m->target, m->list, m->status + S_NTASK, m->hws.state,
+                            m->fp32, s);
       mis_jp_rounds(m->d, m->list, m->status + S_NTASK, kMisRounds, m->seed ^ (++m->calls * 0x9e37ULL),
                     m->hws, m->indep, m->status + S_NINDEP, s);
       collapse(m->d, m->indep, m->status + S_NINDEP, m->target, nullptr, s);
@@ -715,7 +766,7 @@ int trn_coarsen_run(trn_mesh* m, int max_colors, trn_stats* st) {
   }
   do {
     build_vicin(m->d, m->nb_nodes, true, s);
-    coarsen_filter(m->d, m->nb_nodes, m->target, m->flag, s);
+    coarsen_filter(m->d, m->nb_nodes, m->target, m->flag, m->fp32, s);
     compact_u8(m->flag, m->nb_nodes, m->list, m->scan, s);
     int rc = sync_status(m, m->scan.count);
     if (rc) return rc;
@@ -742,7 +793,7 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
   m->err.clear();
   begin_timing(m);
   cudaStream_t s = m->stream;
-  swap_init(m->d, m->nb_nodes, m->nb_elems, m->map, s);
+  swap_init(m->d, m->nb_nodes, m->nb_elems, m->map, m->fp32, s);
   int eval = 0, task = 0, commit = 0, level = 0;
   do {
     int ntasks = 0;
@@ -774,7 +825,7 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
     }
     CK(cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s));
     swap_flip(m->d, pairs, npairs, m->map, m->dual, m->dual_n, ntasks_dev, m->status + S_COMMIT,
-              !m->replay, s);
+              !m->replay, m->fp32, s);
     fix_tagged(m->d, m->nb_nodes, s);
     int rc = sync_status(m);
     if (rc) return rc;
@@ -819,10 +870,10 @@ int trn_smooth_run(trn_mesh* m, int max_colors, int depth, trn_stats* st) {
       classes.emplace_back(m->parts + a, b - a);
     }
   }
-  quality_all(m->d, m->nb_elems, s);
+  quality_all(m->d, m->nb_elems, m->fp32, s);
   CK(cudaMemsetAsync(m->status + S_SMOOTH_TASKS, 0, sizeof(int) * 2, s));
   for (int level = 0; level < depth; ++level)
-    for (auto& c : classes) smooth_color(m->d, c.first, c.second, m->status + S_SMOOTH_TASKS, s);
+    for (auto& c : classes) smooth_color(m->d, c.first, c.second, m->status + S_SMOOTH_TASKS, m->fp32, s);
   int rc = sync_status(m);
   if (rc) return rc;
   return end_timing(m, st, m->h_status[S_SMOOTH_TASKS], m->h_status[S_SMOOTH_COMMIT]);

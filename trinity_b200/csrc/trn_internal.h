@@ -38,7 +38,9 @@ void build_stencils(const DMesh& m, int nb_nodes, int nb_elems, cudaStream_t s);
 void build_vicin(const DMesh& m, int nb_nodes, bool only_flagged, cudaStream_t s);
 void fix_tagged(const DMesh& m, int nb_nodes, cudaStream_t s);
 void flag_all_alive(const DMesh& m, int nb_nodes, cudaStream_t s);
-void quality_all(const DMesh& m, int nb_elems, cudaStream_t s);
+void quality_all(const DMesh& m, int nb_elems, bool fp32, cudaStream_t s);
+/* recompute the per-vertex tensor-logarithm cache of the FP64 or FP32 form */
+void log_cache(const DMesh& m, int nb_nodes, bool fp32, cudaStream_t s);
 void count_live(const DMesh& m, int nb_nodes, int nb_elems, int* out, cudaStream_t s);
 void expand_tris(const int* raw, int nb_elems, int nb_nodes, int4* out, int* err, cudaStream_t s);
 void pack_nodes(const DMesh& m, const int* list, const int* count, int* newid, double* pts, double* ten,
@@ -70,33 +72,33 @@ struct RefineWs {
 void refine_ws_alloc(RefineWs* ws, int capa_node, int capa_elem);
 void refine_ws_free(RefineWs* ws);
 void refine_reset_hash(RefineWs& ws, cudaStream_t s);
-void refine_filter(const DMesh& m, int nb_elems, RefineWs& ws, cudaStream_t s);
-void refine_apply(const DMesh& m, int nb_nodes, int nb_elems, RefineWs& ws, cudaStream_t s);
+void refine_filter(const DMesh& m, int nb_elems, RefineWs& ws, bool fp32, cudaStream_t s);
+void refine_apply(const DMesh& m, int nb_nodes, int nb_elems, RefineWs& ws, bool fp32, cudaStream_t s);
 
 /* coarsening (coarsen.cu) */
 void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
-void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, cudaStream_t s);
+void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, bool fp32, cudaStream_t s);
 void collapse(const DMesh& m, const int* indep, const int* count, const int* target,
               const uint8_t* cand_flag, cudaStream_t s);
 /* free mode: adjacency + target + unordered candidate append in one pass */
 void coarsen_filter_append(const DMesh& m, int nb_nodes, int* target, int* cand, int* count,
-                           uint8_t* state, cudaStream_t s);
+                           uint8_t* state, bool fp32, cudaStream_t s);
 
 /* swapping (swap.cu) */
-void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, cudaStream_t s);
+void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, bool fp32, cudaStream_t s);
 void swap_filter(const DMesh& m, int nb_elems, uint8_t* flag, cudaStream_t s);
 void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual_n, int* map,
                cudaStream_t s);
 void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* map,
                const int* dual, const int* dual_n, const int* ntasks, int* commit, bool strict_map,
-               cudaStream_t s);
+               bool fp32, cudaStream_t s);
 /* free mode: filter and dual rows in one pass, *count rows */
 void swap_filter_dual(const DMesh& m, int nb_elems, int* dual, int* dual_n, int* map, int* count,
                       cudaStream_t s);
 
 /* smoothing (smooth.cu) */
 void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
-void smooth_color(const DMesh& m, const int* list, int n, int* counters, cudaStream_t s);
+void smooth_color(const DMesh& m, const int* list, int n, int* counters, bool fp32, cudaStream_t s);
 
 /* graph heuristics, free mode (heuristics.cu) */
 struct HeurWs {
