@@ -113,10 +113,13 @@ __global__ void k_coarse_filter(DMesh m, int nb_nodes, int* __restrict__ target,
  * independent set is chosen by hashed priorities, not by list position),
  * marking them undecided for the independent-set rounds */
 template <bool F32>
-__global__ void k_coarse_filter_append(DMesh m, int nb_nodes, int* __restrict__ target,
-                                       int* __restrict__ cand, int* count, uint8_t* __restrict__ state) {
+__global__ void k_coarse_filter_append(DMesh m, const int* __restrict__ act, const int* act_n,
+                                       int* __restrict__ target, int* __restrict__ cand, int* count,
+                                       uint8_t* __restrict__ state) {
   if (trn_failed(m)) return;
-  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+  const int n = *act_n;
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int v = act[q];
     if (m.activ[v] <= 0) continue;
     m.activ[v] = 0;
     build_one_vicin(m, v);
@@ -168,7 +171,7 @@ __global__ void k_collapse(DMesh m, const int* __restrict__ indep, const int* co
       rest[nr++] = e;
     }
     for (int j = 0; j < k; ++j)
-      if (opp[j] >= 0) trn_flag_on(m.fixes + opp[j]);
+      if (opp[j] >= 0) trn_tag_fix(m, opp[j]);
     trn_stenc_append_n(m, destin, rest, nr);
     for (int a = 0; a < nr; ++a) {
       int4 n = m.tri[rest[a]];
@@ -177,10 +180,10 @@ __global__ void k_collapse(DMesh m, const int* __restrict__ indep, const int* co
       else if (n.z == source) n.z = destin;
       m.tri[rest[a]] = n;
     }
-    trn_flag_on(m.fixes + destin);
+    trn_tag_fix(m, destin);
     const int* vc = m.vic + (size_t) source * m.bucket;
     const int nv = m.vdeg[source];
-    for (int b = 0; b < nv; ++b) trn_activ_on(m.activ + vc[b]);
+    for (int b = 0; b < nv; ++b) trn_activate(m, vc[b]);
     m.vdeg[source] = 0;
     m.alive[source] = 0;
     for (int a = 0; a < deg; ++a) st[a] = -1;
@@ -202,16 +205,26 @@ void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, bo
   check_launch("coarsen_filter");
 }
 
-void coarsen_filter_append(const DMesh& m, int nb_nodes, int* target, int* cand, int* count,
-                           uint8_t* state, bool fp32, cudaStream_t s) {
-  ProfScope ps("coarsen_filter", s, (double) nb_nodes * (1 + 1 + 4 + 1));
+__global__ void k_coarse_list_active(DMesh m, int nb_nodes, int* act, int* act_n) {
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride())
+    if (m.activ[v] > 0) trn_append(act, act_n, v);
+}
+
+void coarsen_list_active(const DMesh& m, int nb_nodes, int* act, int* act_n, cudaStream_t s) {
+  cudaMemsetAsync(act_n, 0, sizeof(int), s);
+  k_coarse_list_active<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, act, act_n);
+  note_launch();
+}
+
+void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int* target, int* cand,
+                           int* count, uint8_t* state, bool fp32, cudaStream_t s) {
+  ProfScope ps("coarsen_filter", s, 0.0);
   cudaMemsetAsync(count, 0, sizeof(int), s);
+  const int g = grid_for(m.capa_node);
   if (fp32)
-    k_coarse_filter_append<true><<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, cand,
-                                                                           count, state);
+    k_coarse_filter_append<true><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state);
   else
-    k_coarse_filter_append<false><<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, target, cand,
-                                                                            count, state);
+    k_coarse_filter_append<false><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state);
   note_launch();
   check_launch("coarsen_filter_append");
 }

@@ -68,7 +68,7 @@ __global__ void k_mis_finish(DMesh m, uint8_t* state, uint8_t* other, const int*
     const int v = cand[q];
     const uint8_t st = state[v];
     if (st == 2) trn_append(indep, nindep, v);
-    else if (st == 1) m.activ[v] = 1;
+    else if (st == 1) trn_activate(m, v);
     state[v] = 0;
     other[v] = 0;
   }
@@ -186,12 +186,21 @@ void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* d
 
 /* ---------------- coloring ---------------- */
 /* color word: 0 = uncolored, else (round + 1) << 8 | color, color 0xff = none */
-__global__ void k_color_round(DMesh m, int nb_nodes, int* color, int max_col, uint64_t seed,
-                              int round, int* undecided) {
+__global__ void k_color_init(DMesh m, int nb_nodes, int* list, int* n) {
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride())
+    if (m.activ[v] == 1 && m.vdeg[v] > 0) trn_append(list, n, v);
+}
+
+/* one round over the still-uncolored vertices; those that must wait go to the
+ * next list. A vertex takes the smallest color unused by neighbours colored in
+ * earlier rounds once its priority beats every neighbour still competing
+ * (uncolored, or colored in this very round) */
+__global__ void k_color_round(DMesh m, const int* __restrict__ list, const int* n_in, int* color,
+                              int max_col, uint64_t seed, int round, int* next, int* n_next) {
   if (trn_failed(m)) return;
-  int left = 0;
-  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
-    if (m.activ[v] != 1 || m.vdeg[v] == 0 || color[v] != 0) continue;
+  const int n = *n_in;
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int v = list[q];
     const uint64_t pv = trn_prio(seed, v);
     const int* vc = m.vic + (size_t) v * m.bucket;
     const int nv = m.vdeg[v];
@@ -208,12 +217,14 @@ __global__ void k_color_round(DMesh m, int nb_nodes, int* color, int max_col, ui
         used |= 1u << (cw & 0xff & 31);
       }
     }
-    if (!is_max) { ++left; continue; }
+    if (!is_max) {
+      trn_append(next, n_next, v);
+      continue;
+    }
     int c = 1;
     while (c <= max_col && (used & (1u << c))) ++c;
     color[v] = ((round + 1) << 8) | (c <= max_col ? c : 0xff);
   }
-  if (left) atomicAdd(undecided, left);
 }
 
 __global__ void k_color_count(DMesh m, int nb_nodes, const int* color, int* cnt, int max_col) {
@@ -253,14 +264,20 @@ void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& 
               int* part_off, cudaStream_t s) {
   ProfScope ps("color_jp", s, 0.0);
   const int g = grid_for(nb_nodes);
-  int host_left = 1;
-  int round = 0;
-  for (int batch = 0; batch < 64 && host_left; ++batch) {
-    cudaMemsetAsync(ws.cnt, 0, sizeof(int) * 4, s);
-    for (int r = 0; r < 4; ++r, ++round)
-      k_color_round<<<g, TRN_THREADS, 0, s>>>(m, nb_nodes, ws.color, max_col, seed, round, ws.cnt + r);
+  int* lists[2] = {ws.list_a, ws.list_b};
+  int* counts = ws.cnt + 80;  /* two list counters */
+  cudaMemsetAsync(counts, 0, sizeof(int) * 2, s);
+  k_color_init<<<g, TRN_THREADS, 0, s>>>(m, nb_nodes, lists[0], counts);
+  note_launch();
+  int round = 0, cur = 0, host_left = 1;
+  for (int batch = 0; batch < 8 && host_left; ++batch) {
+    for (int r = 0; r < 8; ++r, ++round, cur ^= 1) {
+      cudaMemsetAsync(counts + (cur ^ 1), 0, sizeof(int), s);
+      k_color_round<<<g, TRN_THREADS, 0, s>>>(m, lists[cur], counts + cur, ws.color, max_col, seed, round,
+                                              lists[cur ^ 1], counts + (cur ^ 1));
       note_launch();
-    cudaMemcpyAsync(&host_left, ws.cnt + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
+    }
+    cudaMemcpyAsync(&host_left, counts + cur, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
   }
   int* cnt = ws.cnt + 4;      /* 32 slots */
@@ -287,6 +304,9 @@ void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {
   cudaMemset(ws->color, 0, sizeof(int) * (size_t) capa_node);
   cudaMalloc(&ws->mate, sizeof(int) * (size_t) capa_elem);
   cudaMalloc(&ws->cnt, sizeof(int) * 128);
+  cudaMalloc(&ws->list_a, sizeof(int) * big);
+  cudaMalloc(&ws->list_b, sizeof(int) * big);
+  cudaMalloc(&ws->fix_list, sizeof(int) * (size_t) capa_node);
 }
 
 void heur_ws_free(HeurWs* ws) {
@@ -297,6 +317,9 @@ void heur_ws_free(HeurWs* ws) {
   cudaFree(ws->color);
   cudaFree(ws->mate);
   cudaFree(ws->cnt);
+  cudaFree(ws->list_a);
+  cudaFree(ws->list_b);
+  cudaFree(ws->fix_list);
   *ws = HeurWs();
 }
 

@@ -96,10 +96,13 @@ __global__ void k_swap_dual(DMesh m, const int* __restrict__ list, int ntasks, i
 
 /* free mode: filter and dual extraction in one pass; rows are numbered in
  * append order (no use depends on it) */
-__global__ void k_swap_filter_dual(DMesh m, int nb_elems, int* __restrict__ dual,
-                                   int* __restrict__ dual_n, int* __restrict__ map, int* count) {
+__global__ void k_swap_filter_dual(DMesh m, const int* __restrict__ act, const int* act_n,
+                                   int* __restrict__ dual, int* __restrict__ dual_n,
+                                   int* __restrict__ map, int* count) {
   if (trn_failed(m)) return;
-  for (int k = trn_tid(); k < nb_elems; k += trn_grid_stride()) {
+  const int na = *act_n;
+  for (int q = trn_tid(); q < na; q += trn_grid_stride()) {
+    const int k = act[q];
     if (!m.activ[k]) continue;
     m.activ[k] = 0;
     if (!(m.qual[k] < TRN_Q_MIN)) continue;
@@ -153,20 +156,20 @@ __device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int*
   m.tri[id2] = make_int4(c2[0], c2[1], c2[2], 0);
   trn_stenc_append(m, c2[0], id2);
   trn_stenc_append(m, c2[1], id1);
-  trn_flag_on(m.fixes + c1[0]);
-  trn_flag_on(m.fixes + c1[1]);
-  trn_flag_on(m.fixes + c1[2]);
-  trn_flag_on(m.fixes + c2[2]);
+  trn_tag_fix(m, c1[0]);
+  trn_tag_fix(m, c1[1]);
+  trn_tag_fix(m, c1[2]);
+  trn_tag_fix(m, c2[2]);
   m.qual[id1] = q0;
   m.qual[id2] = q1;
-  for (int q = 0; q < dual_n[index]; ++q) trn_activ_on(m.activ + dual[index * 4 + q]);
+  for (int q = 0; q < dual_n[index]; ++q) trn_activate(m, dual[index * 4 + q]);
   /* the reference follows the map even when it points at a row of an earlier
    * level (the map is reset once per call, swapping.cpp:161-162); replay keeps
    * that, the free mode (rows numbered in append order) only follows rows of
    * the current level */
   const int x = map[id2];
   if (x > -1 && (!strict_map || (x < ntasks && dual[x * 4] == id2)))
-    for (int q = 0; q < dual_n[x]; ++q) trn_activ_on(m.activ + dual[x * 4 + q]);
+    for (int q = 0; q < dual_n[x]; ++q) trn_activate(m, dual[x * 4 + q]);
   return 2;
 }
 
@@ -226,11 +229,23 @@ void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual
   check_launch("swap_dual");
 }
 
-void swap_filter_dual(const DMesh& m, int nb_elems, int* dual, int* dual_n, int* map, int* count,
-                      cudaStream_t s) {
-  ProfScope ps("swap_filter", s, (double) nb_elems * 3);
+__global__ void k_swap_list_active(DMesh m, int nb_elems, int* act, int* act_n) {
+  for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride())
+    if (m.activ[i]) trn_append(act, act_n, i);
+}
+
+void swap_list_active(const DMesh& m, int nb_elems, int* act, int* act_n, cudaStream_t s) {
+  cudaMemsetAsync(act_n, 0, sizeof(int), s);
+  k_swap_list_active<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, act, act_n);
+  note_launch();
+}
+
+void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,
+                      int* map, int* count, cudaStream_t s) {
+  ProfScope ps("swap_filter", s, 0.0);
   cudaMemsetAsync(count, 0, sizeof(int), s);
-  k_swap_filter_dual<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, dual, dual_n, map, count);
+  k_swap_filter_dual<<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, act, act_n, dual, dual_n, map,
+                                                                    count);
   note_launch();
   check_launch("swap_filter_dual");
 }

@@ -70,6 +70,38 @@ __global__ void k_fix_tagged(DMesh m, int nb_nodes) {
   }
 }
 
+/* the same repair over the listed vertices only */
+__global__ void k_fix_list(DMesh m, const int* __restrict__ list, const int* count) {
+  if (trn_failed(m)) return;
+  int buf[TRN_MAX_DEG];
+  const int n = *count;
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int v = list[q];
+    if (!m.fixes[v]) continue;
+    m.fixes[v] = 0;
+    int* s = m.stenc + (size_t) v * m.bucket;
+    const int d = trn_deg(m, v);
+    int k = 0;
+    for (int a = 0; a < d; ++a) {
+      int t = s[a];
+      if (t < 0) continue;
+      int4 nn = m.tri[t];
+      if (v == nn.x || v == nn.y || v == nn.z) buf[k++] = t;
+    }
+    trn_isort(buf, k);
+    k = trn_iunique(buf, k);
+    for (int a = 0; a < k; ++a) s[a] = buf[a];
+    for (int a = k; a < d; ++a) s[a] = -1;
+    m.deg[v] = k;
+  }
+}
+
+void fix_list(const DMesh& m, const int* list, const int* count, cudaStream_t s) {
+  ProfScope ps("fix_tagged", s, 0.0);
+  k_fix_list<<<grid_for(m.capa_node), TRN_THREADS, 0, s>>>(m, list, count);
+  note_launch();
+}
+
 __global__ void k_flag_alive(DMesh m, int nb_nodes) {
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) m.fixes[v] = m.alive[v] ? 1 : 0;
 }

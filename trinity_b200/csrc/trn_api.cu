@@ -35,6 +35,8 @@ enum {
   S_PARTS = 8,     /* part offsets, 9 slots */
   S_LIVE = 18,     /* live vertices, live elements */
   S_NTASK = 20,    /* device-counted candidates of a level (free mode) */
+  S_ACT = 22,      /* two activity-list counters (free mode) */
+  S_FIX = 24,      /* repair-list counter (free mode) */
   S_SIZE = 32,     /* device status block */
   H_WIDE = 40,     /* host-only pinned slot for one 8-byte value */
   H_SIZE = 64,
@@ -296,7 +298,7 @@ int trn_mesh_create_ex(const int size[2], int bucket, int depth, int verbosity, 
       (rc = dmalloc(m, &d.stenc, cn * bucket)) || (rc = dmalloc(m, &d.deg, cn)) ||
       (rc = dmalloc(m, &d.vic, cn * bucket)) || (rc = dmalloc(m, &d.vdeg, cn)) ||
       (rc = dmalloc(m, &d.tags, cn)) || (rc = dmalloc(m, &d.alive, cn)) ||
-      (rc = dmalloc(m, &d.fixes, cn)) || (rc = dmalloc(m, &d.activ, std::max(cn, ce))) ||
+      (rc = dmalloc(m, &d.fixes, cn + 16)) || (rc = dmalloc(m, &d.activ, std::max(cn, ce) + 16)) ||
       (rc = dmalloc(m, &d.qual, ce)) || (rc = dmalloc(m, &m->solut, cn)) ||
       (rc = dmalloc(m, &m->grad, cn)) || (rc = dmalloc(m, &m->terms, ce + 8192)) ||
       (rc = dmalloc(m, &m->complexity, 2)) || (rc = dmalloc(m, &m->target, cn)) ||
@@ -745,21 +747,32 @@ int trn_coarsen_run(trn_mesh* m, int max_colors, trn_stats* st) {
   coarsen_pre(m->d, m->nb_nodes, s);
   int eval = 0, task = 0, nb_indep = 0, level = 0;
   if (!m->replay) {
-    /* free mode: one host synchronisation per level */
-    int ntasks = 0;
+    /* free mode: one host synchronisation per level; each level works on the
+     * list of vertices the previous one activated, repairs the listed ones */
+    int* act[2] = {m->hws.list_a, m->hws.list_b};
+    coarsen_list_active(m->d, m->nb_nodes, act[0], m->status + S_ACT, s);
+    int ntasks = 0, cur = 0;
     do {
-      coarsen_filter_append(m->d, m->nb_nodes, m->target, m->list, m->status + S_NTASK, m->hws.state,
-                            m->fp32, s);
-      mis_jp_rounds(m->d, m->list, m->status + S_NTASK, kMisRounds, m->seed ^ (++m->calls * 0x9e37ULL),
+      DMesh dl = m->d;
+      dl.act_next = act[cur ^ 1];
+      dl.act_next_n = m->status + S_ACT + (cur ^ 1);
+      dl.fix_list = m->hws.fix_list;
+      dl.fix_n = m->status + S_FIX;
+      CK(cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s));
+      CK(cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s));
+      coarsen_filter_append(dl, act[cur], m->status + S_ACT + cur, m->target, m->list,
+                            m->status + S_NTASK, m->hws.state, m->fp32, s);
+      mis_jp_rounds(dl, m->list, m->status + S_NTASK, kMisRounds, m->seed ^ (++m->calls * 0x9e37ULL),
                     m->hws, m->indep, m->status + S_NINDEP, s);
-      collapse(m->d, m->indep, m->status + S_NINDEP, m->target, nullptr, s);
-      fix_tagged(m->d, m->nb_nodes, s);
+      collapse(dl, m->indep, m->status + S_NINDEP, m->target, nullptr, s);
+      fix_list(dl, dl.fix_list, dl.fix_n, s);
       int rc = sync_status(m);
       if (rc) return rc;
       ntasks = m->h_status[S_NTASK];
       nb_indep = m->h_status[S_NINDEP];
       eval += ntasks;
       task += nb_indep;
+      cur ^= 1;
       if (++level > kLoopCap) return fail(m, TRN_ERR_NO_PROGRESS, "coarsen: level cap reached");
     } while (ntasks && nb_indep);
     return end_timing(m, st, eval, task);
@@ -794,12 +807,15 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
   begin_timing(m);
   cudaStream_t s = m->stream;
   swap_init(m->d, m->nb_nodes, m->nb_elems, m->map, m->fp32, s);
-  int eval = 0, task = 0, commit = 0, level = 0;
+  int eval = 0, task = 0, commit = 0, level = 0, cur = 0;
+  int* act[2] = {m->hws.list_a, m->hws.list_b};
+  if (!m->replay) swap_list_active(m->d, m->nb_elems, act[0], m->status + S_ACT, s);
   do {
     int ntasks = 0;
     const int* pairs;
     const int* npairs;
     const int* ntasks_dev;
+    DMesh dl = m->d;
     if (m->replay) {
       swap_filter(m->d, m->nb_elems, m->flag, s);
       compact_u8(m->flag, m->nb_elems, m->list, m->scan, s);
@@ -815,24 +831,33 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
       npairs = m->d_log + off - 1;
       ntasks_dev = m->scan.count;
     } else {
-      /* free mode: one host synchronisation per level */
-      swap_filter_dual(m->d, m->nb_elems, m->dual, m->dual_n, m->map, m->status + S_NTASK, s);
-      match_handshake(m->d, m->nb_elems, m->dual, m->dual_n, m->status + S_NTASK, m->map,
+      /* free mode: one host synchronisation per level, list-driven */
+      dl.act_next = act[cur ^ 1];
+      dl.act_next_n = m->status + S_ACT + (cur ^ 1);
+      dl.fix_list = m->hws.fix_list;
+      dl.fix_n = m->status + S_FIX;
+      CK(cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s));
+      CK(cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s));
+      swap_filter_dual(dl, act[cur], m->status + S_ACT + cur, m->dual, m->dual_n, m->map,
+                       m->status + S_NTASK, s);
+      match_handshake(dl, m->nb_elems, m->dual, m->dual_n, m->status + S_NTASK, m->map,
                       m->seed ^ (++m->calls * 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s);
       pairs = m->pairs;
       npairs = m->status + S_NPAIRS;
       ntasks_dev = m->status + S_NTASK;
     }
     CK(cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s));
-    swap_flip(m->d, pairs, npairs, m->map, m->dual, m->dual_n, ntasks_dev, m->status + S_COMMIT,
+    swap_flip(dl, pairs, npairs, m->map, m->dual, m->dual_n, ntasks_dev, m->status + S_COMMIT,
               !m->replay, m->fp32, s);
-    fix_tagged(m->d, m->nb_nodes, s);
+    if (m->replay) fix_tagged(m->d, m->nb_nodes, s);
+    else fix_list(dl, dl.fix_list, dl.fix_n, s);
     int rc = sync_status(m);
     if (rc) return rc;
     if (!m->replay) ntasks = m->h_status[S_NTASK];
     commit = m->h_status[S_COMMIT];
     eval += ntasks;
     task += commit / 2;
+    cur ^= 1;
     if (++level > kLoopCap) return fail(m, TRN_ERR_NO_PROGRESS, "swap: level cap reached");
   } while (commit);
   return end_timing(m, st, eval, task);

@@ -53,6 +53,12 @@ struct DMesh {
   int8_t* activ;
   double* qual;
   int* err;        /* device error word: first error wins */
+  /* free-mode worklists (NULL in replay): ids whose activity flag turns
+   * 0 -> 1 are appended to act_next, vertices tagged for repair to fix_list */
+  int* act_next;
+  int* act_next_n;
+  int* fix_list;
+  int* fix_n;
   int bucket;
   int capa_node;
   int capa_elem;
@@ -62,21 +68,33 @@ __device__ __forceinline__ void trn_set_error(int* err, int code) {
   atomicCAS(err, 0, code);
 }
 
-/* compare-and-swap 0 -> 1 on a byte flag (sync.h:33-38 compareAndSwap) */
-__device__ __forceinline__ void trn_flag_on(uint8_t* f) {
-  if (*(volatile uint8_t*) f == 0) *f = 1;
-}
-
-__device__ __forceinline__ void trn_activ_on(int8_t* a) {
-  /* CAS(activ, 0, 1): corners hold -1 and must keep it */
-  unsigned int* word = (unsigned int*) ((uintptr_t) a & ~(uintptr_t) 3);
-  unsigned int shift = ((uintptr_t) a & 3) * 8;
-  unsigned int old = *word, assumed;
+/* compare-and-swap 0 -> 1 on one byte (sync.h:33-38 compareAndSwap);
+ * true for the one caller that made the change */
+__device__ __forceinline__ bool trn_byte_cas01(void* p) {
+  unsigned int* word = (unsigned int*) ((uintptr_t) p & ~(uintptr_t) 3);
+  unsigned int shift = ((uintptr_t) p & 3) * 8;
+  unsigned int old = *(volatile unsigned int*) word, assumed;
   do {
-    if (((old >> shift) & 0xffu) != 0u) return;
+    if (((old >> shift) & 0xffu) != 0u) return false;
     assumed = old;
     old = atomicCAS(word, assumed, assumed | (1u << shift));
   } while (old != assumed);
+  return true;
+}
+
+__device__ __forceinline__ void trn_list_push(int* list, int* n, int id) {
+  list[atomicAdd(n, 1)] = id;
+}
+
+/* tag vertex v for stencil repair (CAS 0 -> 1), listing it once */
+__device__ __forceinline__ void trn_tag_fix(const DMesh& m, int v) {
+  if (trn_byte_cas01(m.fixes + v) && m.fix_list) trn_list_push(m.fix_list, m.fix_n, v);
+}
+
+/* activate vertex or element id (CAS 0 -> 1: corners hold -1 and keep it),
+ * listing it once for the next level */
+__device__ __forceinline__ void trn_activate(const DMesh& m, int id) {
+  if (trn_byte_cas01(m.activ + id) && m.act_next) trn_list_push(m.act_next, m.act_next_n, id);
 }
 
 /* once any kernel raised the error word, later kernels of the call do no

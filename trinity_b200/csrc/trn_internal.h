@@ -37,6 +37,8 @@ void compact_u8(const uint8_t* flags, int n, int* list, ScanWs& ws, cudaStream_t
 void build_stencils(const DMesh& m, int nb_nodes, int nb_elems, cudaStream_t s);
 void build_vicin(const DMesh& m, int nb_nodes, bool only_flagged, cudaStream_t s);
 void fix_tagged(const DMesh& m, int nb_nodes, cudaStream_t s);
+/* repair of the vertices listed in list[0..*count) */
+void fix_list(const DMesh& m, const int* list, const int* count, cudaStream_t s);
 void flag_all_alive(const DMesh& m, int nb_nodes, cudaStream_t s);
 void quality_all(const DMesh& m, int nb_elems, bool fp32, cudaStream_t s);
 /* recompute the per-vertex tensor-logarithm cache of the FP64 or FP32 form */
@@ -80,9 +82,11 @@ void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
 void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, bool fp32, cudaStream_t s);
 void collapse(const DMesh& m, const int* indep, const int* count, const int* target,
               const uint8_t* cand_flag, cudaStream_t s);
-/* free mode: adjacency + target + unordered candidate append in one pass */
-void coarsen_filter_append(const DMesh& m, int nb_nodes, int* target, int* cand, int* count,
-                           uint8_t* state, bool fp32, cudaStream_t s);
+/* free mode: list the active vertices; then per level, over that list,
+ * adjacency + target + unordered candidate append in one pass */
+void coarsen_list_active(const DMesh& m, int nb_nodes, int* act, int* act_n, cudaStream_t s);
+void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int* target, int* cand,
+                           int* count, uint8_t* state, bool fp32, cudaStream_t s);
 
 /* swapping (swap.cu) */
 void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, bool fp32, cudaStream_t s);
@@ -92,9 +96,11 @@ void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual
 void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* map,
                const int* dual, const int* dual_n, const int* ntasks, int* commit, bool strict_map,
                bool fp32, cudaStream_t s);
-/* free mode: filter and dual rows in one pass, *count rows */
-void swap_filter_dual(const DMesh& m, int nb_elems, int* dual, int* dual_n, int* map, int* count,
-                      cudaStream_t s);
+/* free mode: list the active elements; per level, filter and dual rows in
+ * one pass over the list, *count rows */
+void swap_list_active(const DMesh& m, int nb_elems, int* act, int* act_n, cudaStream_t s);
+void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,
+                      int* map, int* count, cudaStream_t s);
 
 /* smoothing (smooth.cu) */
 void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
@@ -109,6 +115,9 @@ struct HeurWs {
   int* color = nullptr;
   int* mate = nullptr;
   int* cnt = nullptr;            /* small device counters */
+  int* list_a = nullptr;         /* two worklists (activity, coloring) */
+  int* list_b = nullptr;
+  int* fix_list = nullptr;       /* vertices tagged for repair */
 };
 void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem);
 void heur_ws_free(HeurWs* ws);
