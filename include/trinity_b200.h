@@ -100,6 +100,17 @@ int trn_smooth_run(trn_mesh* mesh, int max_colors, int depth, trn_stats* stats);
 /* one full round: refine, coarsen, swap, smooth (main.cpp:52-57) */
 int trn_round_run(trn_mesh* mesh, int depth, trn_stats stats[4]);
 
+/* Adapt a batch of independent meshes concurrently on the current GPU: each
+ * mesh (already loaded) gets metric recovery and `rounds` rounds on its own
+ * stream, driven by `threads` host threads, largest meshes first. Per mesh,
+ * round_ms[i] (may be NULL) receives the device time of its rounds and
+ * tri_in[i] (may be NULL) the sum of its live triangles at round starts.
+ * No counterpart in the reference (one mesh per process there); the survey's
+ * batched form. Returns the first error met. */
+int trn_batch_adapt(trn_mesh* const* meshes, int count, double target_factor, int lp_norm,
+                    double h_min, double h_max, int rounds, int depth, int threads,
+                    double* round_ms, long long* tri_in);
+
 /* Replay mode: the independent sets, matchings and colorings are read from a
  * decision log (int32 stream: 1 = set [n, ids], 2 = matching [n, (k1,k2)*n],
  * 3 = coloring [parts, (n, ids)*parts]) instead of being computed; the

@@ -74,6 +74,7 @@ def lib():
         L.trn_version.restype = ctypes.c_char_p
         L.trn_mesh_reload.argtypes = [pmesh]
         L.trn_set_precision.argtypes = [pmesh, ip]
+        L.trn_batch_adapt.argtypes = [vp, ip, dp, ip, dp, dp, ip, ip, ip, vp, vp]
         L.trn_mesh_qualities.argtypes = [pmesh, vp]
         L.trn_mesh_quality_stats.argtypes = [pmesh, vp]
         L.trn_mesh_export_compact.argtypes = [pmesh, vp, vp, vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]

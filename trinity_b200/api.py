@@ -24,7 +24,7 @@ import numpy as np
 from ._lib import Stats, TrinityError, lib
 
 __all__ = ["Mesh", "Metrics", "Partit", "Refine", "Coarse", "Swap", "Smooth", "Stats",
-           "TrinityError", "EPSILON", "H_MAX", "find"]
+           "TrinityError", "EPSILON", "H_MAX", "find", "batch_adapt"]
 
 EPSILON = 1.0e-9   # header.h:50, the h_min the CLI passes (parser.cpp:95)
 H_MAX = 0.4        # parser.cpp:96
@@ -156,6 +156,23 @@ class Mesh:
 
     def stream(self) -> int:
         return self._L.trn_mesh_stream(self.h)
+
+
+def batch_adapt(meshes, target_factor: float, Lp_norm: int = 2, rounds: int = 3, depth: int = 1,
+                threads: int = 8, h_min: float = EPSILON, h_max: float = H_MAX):
+    """Metric recovery + rounds for many loaded meshes at once (one stream per
+    mesh, a pool of host threads). Returns (round_ms[count], tri_in[count])."""
+    L = lib()
+    n = len(meshes)
+    handles = (ctypes.c_void_p * n)(*[m.h.value if hasattr(m.h, "value") else m.h for m in meshes])
+    ms = np.zeros(n)
+    tin = np.zeros(n, dtype=np.int64)
+    rc = L.trn_batch_adapt(ctypes.cast(handles, ctypes.c_void_p), n, target_factor, Lp_norm, h_min, h_max,
+                           rounds, depth, threads, _p(ms), _p(tin))
+    if rc:
+        raise TrinityError(rc, "batch adaptation failed: " + "; ".join(
+            m._L.trn_last_error(m.h).decode() for m in meshes if m._L.trn_last_error(m.h)))
+    return ms, tin
 
 
 class Metrics:

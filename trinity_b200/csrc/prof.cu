@@ -9,7 +9,9 @@
  */
 #include "trn_internal.h"
 
+#include <atomic>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -31,7 +33,8 @@ struct Total {
 };
 
 struct Profiler {
-  bool on = false;
+  std::mutex mu;   /* meshes may run on several host threads */
+  std::atomic<bool> on{false};
   std::vector<cudaEvent_t> pool;
   std::vector<Pending> pending;
   std::vector<Total> totals;
@@ -66,6 +69,7 @@ Profiler& prof() {
 ProfScope::ProfScope(const char* name, cudaStream_t s, double bytes) : stream_(s) {
   Profiler& p = prof();
   if (!p.on) return;
+  std::lock_guard<std::mutex> lock(p.mu);
   id_ = p.id_of(name);
   bytes_ = bytes;
   a_ = p.get();
@@ -75,17 +79,19 @@ ProfScope::ProfScope(const char* name, cudaStream_t s, double bytes) : stream_(s
 ProfScope::~ProfScope() {
   Profiler& p = prof();
   if (!p.on || id_ < 0) return;
+  std::lock_guard<std::mutex> lock(p.mu);
   cudaEvent_t b = p.get();
   cudaEventRecord(b, stream_);
   p.pending.push_back({id_, a_, b, bytes_});
 }
 
-static unsigned long long g_launches = 0;
+static std::atomic<unsigned long long> g_launches{0};
 
-void note_launch() { ++g_launches; }
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void prof_flush() {
   Profiler& p = prof();
+  std::lock_guard<std::mutex> lock(p.mu);
   for (auto& q : p.pending) {
     cudaEventSynchronize(q.b);
     float ms = 0.f;
@@ -107,12 +113,13 @@ extern "C" {
 int trn_profile_enable(int on) {
   trn::Profiler& p = trn::prof();
   trn::prof_flush();
+  std::lock_guard<std::mutex> lock(p.mu);
   p.on = on != 0;
-  if (p.on) p.totals.clear();
+  if (on) p.totals.clear();
   return 0;
 }
 
-unsigned long long trn_launch_count(void) { return trn::g_launches; }
+unsigned long long trn_launch_count(void) { return trn::g_launches.load(); }
 
 int trn_profile_count(void) {
   trn::prof_flush();

@@ -189,13 +189,12 @@ void compact_u8(const uint8_t* flags, int n, int* list, ScanWs& ws, cudaStream_t
 }
 
 int grid_for(long long n, int threads) {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
+  static const int sms = [] {
+    int dev = 0, v = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+  }();
   long long blocks = (n + threads - 1) / threads;
   long long cap = (long long) sms * 8;  /* 8 resident 256-thread blocks per SM */
   if (blocks > cap) blocks = cap;

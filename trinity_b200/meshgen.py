@@ -151,6 +151,19 @@ def batch_specs(count: int = 256, seed: int = 5, lo: int = 32, hi: int = 512):
     return [(int(s), float(x), float(y)) for s, x, y in zip(sides, a, b)]
 
 
+def batch_meshes(count: int = 256, seed: int = 5, lo: int = 32, hi: int = 512):
+    """The batched workload: ``count`` unit-square grids with sides from
+    :func:`batch_specs` and shock fields tanh(a (y - 0.5 - b sin 2 pi x));
+    yields (mesh, field, (side, a, b))."""
+    for side, a, b in batch_specs(count, seed, lo, hi):
+        m = grid_mesh(side)
+        yield m, field_shock(m.points, a, b), (side, a, b)
+
+
+# coarse meshes with sharp shocks grow several-fold in their first refinement
+BATCH_PARAMS = dict(target=0.8, norm=2, rounds=3, depth=1, bucket=64, capa_scale=8)
+
+
 def read_mesh(path: str) -> GridMesh:
     """Read a medit ``.mesh`` (Vertices / Edges / Triangles / Corners)."""
     toks = open(path).read().split()
