@@ -111,6 +111,38 @@ int trn_batch_adapt(trn_mesh* const* meshes, int count, double target_factor, in
                     double h_min, double h_max, int rounds, int depth, int threads,
                     double* round_ms, long long* tri_in);
 
+/* Element-quality functional and its adjoint. No counterpart in the
+ * reference; it differentiates the reference's own arithmetic:
+ *   J = sum over live elements T of q_T, q_T = numeric::computeQuality
+ *       (numeric.cpp:251-306) of T at the coordinates `xy` under the nodal
+ *       metric M.
+ * M is the mesh's current tensors when `solut` is NULL; otherwise it is the
+ * metric that trn_metric_run would recover from the nodal solution `solut`
+ * with (target_factor, lp_norm, h_min, h_max) on the mesh's own coordinates
+ * (hessian.cpp:24-153, metric.cpp:59-238), which the mesh keeps unchanged.
+ * Outputs: *value = J (host pointer, may be NULL); grad_xy[2V] = dJ/dxy at
+ * that fixed nodal metric; grad_solut[V] = dJ/dsolut through the gradient
+ * and Hessian recovery, the local L^p normalisation and the global scale
+ * with its clamp. xy (2V, NULL = the mesh's coordinates), solut, grad_xy and
+ * grad_solut are DEVICE pointers in the mesh's vertex numbering; either
+ * gradient may be NULL (grad_solut needs solut). precision: TRN_PRECISION_FP64
+ * (q bit-identical to the adaptation kernels) or TRN_PRECISION_MIXED (q and
+ * the whole adjoint in FP32; coordinates and areas FP64; the metric recovery
+ * FP64). Deterministic: every sum is a gather in a fixed order. */
+int trn_quality_adjoint(trn_mesh* mesh, const double* xy, const double* solut,
+                        double target_factor, int lp_norm, double h_min, double h_max,
+                        int precision, double* value, double* grad_xy, double* grad_solut);
+/* Gradient-based smoothing, beside Smooth::run's smart Laplacian
+ * (smoothing.cpp:40-126, 274-302): `steps` passes over the color classes of
+ * the interior vertices; each vertex steps along M_v^-1 dJ_v/dx_v (J_v the
+ * summed quality of its elements, M_v its tensor held fixed), at most
+ * `max_len` in metric length, and keeps the move only if its elements stay
+ * CCW, each above the old stencil minimum, with a larger sum; the step backs
+ * off 1, 1/2, .., 1/16. Free mode only (TRN_ERR_INVALID in replay mode).
+ * stats->eval / task: vertices tried / moved. */
+int trn_smooth_gradient_run(trn_mesh* mesh, int max_colors, int steps, double max_len,
+                            trn_stats* stats);
+
 /* Replay mode: the independent sets, matchings and colorings are read from a
  * decision log (int32 stream: 1 = set [n, ids], 2 = matching [n, (k1,k2)*n],
  * 3 = coloring [parts, (n, ids)*parts]) instead of being computed; the

@@ -83,6 +83,8 @@ def lib():
         L.trn_profile_entry.argtypes = [ip, ctypes.c_char_p, ip, ctypes.POINTER(ctypes.c_longlong),
                                         ctypes.POINTER(dp), ctypes.POINTER(dp)]
         L.trn_launch_count.restype = ctypes.c_ulonglong
+        L.trn_quality_adjoint.argtypes = [pmesh, vp, vp, dp, ip, dp, dp, ip, ctypes.POINTER(dp), vp, vp]
+        L.trn_smooth_gradient_run.argtypes = [pmesh, ip, ip, dp, sp]
         _lib = L
     return _lib
 

@@ -157,6 +157,43 @@ class Mesh:
     def stream(self) -> int:
         return self._L.trn_mesh_stream(self.h)
 
+    def quality_adjoint(self, xy=None, solut=None, *, target_factor: float = 1.0, Lp_norm: int = 2,
+                        h_min: float = EPSILON, h_max: float = H_MAX, precision: str = "fp64",
+                        grad_xy: bool = True, grad_solut: bool | None = None):
+        """J = sum of the live elements' qualities, and its adjoint
+        (trn_quality_adjoint). xy: (V, 2) and solut: (V,) float64 CUDA
+        tensors in the mesh's vertex numbering; xy None = the mesh's
+        coordinates; solut None = the mesh's current tensors are the metric,
+        else the metric is recovered from solut with (target_factor, Lp_norm,
+        h_min, h_max) on the mesh's coordinates. Returns (J, dJ/dxy, dJ/dsolut),
+        the gradients as CUDA tensors (None where not asked for)."""
+        import torch
+        nn = self.counts()[0]
+        dev = torch.device("cuda", torch.cuda.current_device())
+
+        def dptr(t, shape, name):
+            if t is None:
+                return None
+            if (t.device.type != "cuda" or t.dtype != torch.float64 or not t.is_contiguous()
+                    or tuple(t.shape) != shape):
+                raise ValueError(f"{name}: want a contiguous float64 CUDA tensor of shape {shape}")
+            return ctypes.c_void_p(t.data_ptr())
+
+        if grad_solut is None:
+            grad_solut = solut is not None
+        if grad_solut and solut is None:
+            raise ValueError("grad_solut needs solut")
+        gxy = torch.empty((nn, 2), dtype=torch.float64, device=dev) if grad_xy else None
+        gu = torch.empty(nn, dtype=torch.float64, device=dev) if grad_solut else None
+        args = (dptr(xy, (nn, 2), "xy"), dptr(solut, (nn,), "solut"))
+        torch.cuda.current_stream().synchronize()
+        J = ctypes.c_double(0.0)
+        self._check(self._L.trn_quality_adjoint(
+            self.h, args[0], args[1], target_factor, Lp_norm, h_min, h_max,
+            {"fp64": 0, "mixed": 1, "fp32": 1}[precision], ctypes.byref(J),
+            dptr(gxy, (nn, 2), "grad_xy"), dptr(gu, (nn,), "grad_solut")))
+        return J.value, gxy, gu
+
 
 def batch_adapt(meshes, target_factor: float, Lp_norm: int = 2, rounds: int = 3, depth: int = 1,
                 threads: int = 8, h_min: float = EPSILON, h_max: float = H_MAX):
@@ -226,6 +263,20 @@ class Swap:
     def run(self, total: Stats | None = None) -> None:
         m = self.mesh
         m._check(m._L.trn_swap_run(m.h, ctypes.byref(total) if total is not None else None))
+
+
+class GradientSmooth:
+    """Gradient-based smoothing beside Smooth (trn_smooth_gradient_run):
+    `steps` passes over the color classes, each interior vertex stepping up
+    the metric-preconditioned gradient of its elements' summed quality."""
+
+    def __init__(self, mesh: Mesh, algo: Partit, steps: int, max_len: float = 0.2):
+        self.mesh, self.algo, self.steps, self.max_len = mesh, algo, steps, max_len
+
+    def run(self, total: Stats | None = None) -> None:
+        m = self.mesh
+        m._check(m._L.trn_smooth_gradient_run(m.h, self.algo.max_part, self.steps, self.max_len,
+                                              ctypes.byref(total) if total is not None else None))
 
 
 class Smooth:

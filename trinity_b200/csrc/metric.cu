@@ -45,35 +45,8 @@ __device__ __forceinline__ int gather_patch(const DMesh& m, int v, int* patch) {
   return trn_iunique(patch, k);
 }
 
-/* P1 basis gradients of one element, times the 4x factor of hessian.cpp:52 */
-struct ElemGrad {
-  double area;
-  double d[6];
-  int4 v;
-};
-
-__device__ __forceinline__ ElemGrad elem_grad(const DMesh& m, int e) {
-  ElemGrad g;
-  g.v = m.tri[e];
-  double2 p0 = m.pts[g.v.x], p1 = m.pts[g.v.y], p2 = m.pts[g.v.z];
-  double point[6] = {p0.x, p0.y, p1.x, p1.y, p2.x, p2.y};
-  double c0 = point[2] - point[0];
-  double c1 = point[4] - point[0];
-  double c2 = point[3] - point[1];
-  double c3 = point[5] - point[1];
-  g.area = 0.5 * (c0 * c3 - c1 * c2);
-  double norm = 2 / g.area;
-  g.d[0] = norm * (point[3] - point[5]);
-  g.d[1] = norm * (point[4] - point[2]);
-  g.d[2] = norm * (point[5] - point[1]);
-  g.d[3] = norm * (point[0] - point[4]);
-  g.d[4] = norm * (point[1] - point[3]);
-  g.d[5] = norm * (point[2] - point[0]);
-  return g;
-}
-
 __global__ void k_gradient(DMesh m, int nb_nodes, const double* __restrict__ solut,
-                           double2* __restrict__ grad) {
+                           double2* __restrict__ grad, double* __restrict__ atot) {
   if (trn_failed(m)) return;
   int patch[TRN_MAX_PATCH];
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
@@ -99,11 +72,13 @@ __global__ void k_gradient(DMesh m, int nb_nodes, const double* __restrict__ sol
     gx /= total_area;
     gy /= total_area;
     grad[v] = make_double2(gx, gy);
+    if (atot) atot[v] = total_area;
   }
 }
 
 __global__ void k_hessian_local(DMesh m, int nb_nodes, const double2* __restrict__ grad,
-                                double scale_exp) {
+                                double scale_exp, double4* __restrict__ hsym,
+                                double4* __restrict__ mloc) {
   if (trn_failed(m)) return;
   int patch[TRN_MAX_PATCH];
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
@@ -134,6 +109,7 @@ __global__ void k_hessian_local(DMesh m, int nb_nodes, const double2* __restrict
     double t0 = h[0];
     double t1 = 0.5 * (h[1] + h[2]);
     double t2 = h[3];
+    if (hsym) hsym[v] = make_double4(t0, t1, t2, 0.0);
     /* normalizeLocally (metric.cpp:107-149) */
     double mm[4] = {t0, t1, t1, t2};
     double val[2] = {0, 0}, vec[4] = {0, 0, 0, 0};
@@ -144,7 +120,9 @@ __global__ void k_hessian_local(DMesh m, int nb_nodes, const double2* __restrict
     double scale_loc = trn_pow(det, scale_exp);
     val[0] *= scale_loc;
     val[1] *= scale_loc;
-    m.ten[v] = trn_recompose(val, vec);
+    const double4 r = trn_recompose(val, vec);
+    m.ten[v] = r;
+    if (mloc) mloc[v] = r;
   }
 }
 
@@ -237,18 +215,30 @@ __global__ void k_normalize(DMesh m, int nb_nodes, const double* complexity, dou
   }
 }
 
+void sum_tree(const double* in, int n, double* partial, double* out, cudaStream_t s) {
+  const int nb = grid_for(n);
+  k_sum_partial<<<nb, TRN_THREADS, 0, s>>>(in, n, partial);
+  note_launch();
+  k_sum_final<<<1, TRN_THREADS, 0, s>>>(partial, nb, out);
+  note_launch();
+}
+
 void metric_run(const DMesh& m, int nb_nodes, int nb_elems, const double* solut, double2* grad,
                 double* terms, double* complexity, bool exact_sum, const MetricParams& p,
-                cudaStream_t s) {
+                cudaStream_t s, const MetricSaves* keep) {
+  double* atot = keep ? keep->atot : nullptr;
+  double4* hsym = keep ? keep->hsym : nullptr;
+  double4* mloc = keep ? keep->mloc : nullptr;
   const double V = nb_nodes, E = nb_elems;
   {
   ProfScope ps("metric_gradient", s, V * (2 * kIdx + kAvgDeg * kIdx * 2 + 8 + kPt + 16) + E * kTri);
-  k_gradient<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, solut, grad);
+  k_gradient<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, solut, grad, atot);
   note_launch();
   }
   {
   ProfScope ps("metric_hessian", s, V * (2 * kIdx + kAvgDeg * kIdx * 2 + 16 + kPt + kTen) + E * kTri);
-  k_hessian_local<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, grad, p.scale_exp);
+  k_hessian_local<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, grad, p.scale_exp,
+                                                                hsym, mloc);
   note_launch();
   }
   ProfScope ps("metric_complexity", s, E * (kTri + 8) + V * (kPt + kTen));
@@ -258,12 +248,8 @@ void metric_run(const DMesh& m, int nb_nodes, int nb_elems, const double* solut,
     k_sum_sequential<<<1, 32, 0, s>>>(terms, nb_elems, complexity);
     note_launch();
   } else {
-    int nb = grid_for(nb_elems);
     /* partials live after the terms (terms has capa_elem + grid slots) */
-    k_sum_partial<<<nb, TRN_THREADS, 0, s>>>(terms, nb_elems, terms + m.capa_elem);
-    note_launch();
-    k_sum_final<<<1, TRN_THREADS, 0, s>>>(terms + m.capa_elem, nb, complexity);
-    note_launch();
+    sum_tree(terms, nb_elems, terms + m.capa_elem, complexity, s);
   }
   ProfScope ps2("metric_normalize", s, V * 2 * kTen);
   k_normalize<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, complexity, p.target,

@@ -42,9 +42,10 @@ __global__ void k_fill_stencils(DMesh m, int nb_elems);
 __global__ void k_sort_stencils(DMesh m, int nb_nodes);
 __global__ void k_build_vicin(DMesh m, int nb_nodes, int only_flagged);
 __global__ void k_gradient(DMesh m, int nb_nodes, const double* __restrict__ solut,
-                           double2* __restrict__ grad);
+                           double2* __restrict__ grad, double* __restrict__ atot);
 __global__ void k_hessian_local(DMesh m, int nb_nodes, const double2* __restrict__ grad,
-                                double scale_exp);
+                                double scale_exp, double4* __restrict__ hsym,
+                                double4* __restrict__ mloc);
 __global__ void k_complexity_term(DMesh m, int nb_elems, double* __restrict__ terms);
 __global__ void k_sum_partial(const double* __restrict__ terms, int n, double* partial);
 __global__ void k_sum_final(const double* __restrict__ partial, int nb, double* out);
@@ -190,8 +191,8 @@ extern "C" int trn_metric_noalloc(int nb_nodes, int nb_elems, const double* d_po
   const double scale_exp = lp_norm ? -1. / (2 * lp_norm + 2) : 0.5;
   const double eig_min = 1 / trn_pow(h_min, 2);
   const double eig_max = 1 / trn_pow(h_max, 2);
-  k_gradient<<<gv, TRN_THREADS, 0, s>>>(d, nb_nodes, d_solut, grad);
-  k_hessian_local<<<gv, TRN_THREADS, 0, s>>>(d, nb_nodes, grad, scale_exp);
+  k_gradient<<<gv, TRN_THREADS, 0, s>>>(d, nb_nodes, d_solut, grad, nullptr);
+  k_hessian_local<<<gv, TRN_THREADS, 0, s>>>(d, nb_nodes, grad, scale_exp, nullptr, nullptr);
   k_complexity_term<<<ge, TRN_THREADS, 0, s>>>(d, nb_elems, terms);
   k_sum_partial<<<ge, TRN_THREADS, 0, s>>>(terms, nb_elems, terms + kMaxE);
   k_sum_final<<<1, TRN_THREADS, 0, s>>>(terms + kMaxE, ge, cplx);

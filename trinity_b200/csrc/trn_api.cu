@@ -78,6 +78,7 @@ struct trn_mesh {
   ScanWs scan;
   RefineWs rws;
   HeurWs hws;
+  AdjWs adj;
   /* replay */
   bool replay = false;
   std::vector<int32_t> log;
@@ -185,6 +186,7 @@ void release(trn_mesh* m) {
   scan_ws_free(&m->scan);
   refine_ws_free(&m->rws);
   heur_ws_free(&m->hws);
+  adj_ws_free(&m->adj);
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
   if (m->stream) cudaStreamDestroy(m->stream);
@@ -901,6 +903,75 @@ int trn_smooth_run(trn_mesh* m, int max_colors, int depth, trn_stats* st) {
     for (auto& c : classes) smooth_color(m->d, c.first, c.second, m->status + S_SMOOTH_TASKS, m->fp32, s);
   int rc = sync_status(m);
   if (rc) return rc;
+  return end_timing(m, st, m->h_status[S_SMOOTH_TASKS], m->h_status[S_SMOOTH_COMMIT]);
+}
+
+/* the element-quality functional J = sum_T q_T and its adjoint */
+int trn_quality_adjoint(trn_mesh* m, const double* xy, const double* solut, double target_factor,
+                        int norm, double h_min, double h_max, int precision, double* value,
+                        double* grad_xy, double* grad_solut) {
+  if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "quality_adjoint: no mesh loaded");
+  if (precision != TRN_PRECISION_FP64 && precision != TRN_PRECISION_MIXED)
+    return fail(m, TRN_ERR_INVALID, "quality_adjoint: unknown precision");
+  if (grad_solut && !solut)
+    return fail(m, TRN_ERR_INVALID, "quality_adjoint: grad_solut needs a solution");
+  if (solut && (norm < 0 || h_min <= 0 || h_max <= 0))
+    return fail(m, TRN_ERR_INVALID, "quality_adjoint: bad metric parameters");
+  m->err.clear();
+  if (adj_ws_ensure(&m->adj, m->nb_nodes, m->nb_elems))
+    return fail(m, TRN_ERR_CUDA, "quality_adjoint: device allocation failed");
+  AdjMetric um;
+  if (solut) {
+    um.solut = solut;
+    um.grad = m->grad;
+    um.terms = m->terms;
+    um.exact_sum = m->exact_sum || m->replay;
+    um.p.target = (double) (int) std::floor(m->nb_nodes * target_factor);
+    um.p.scale_exp = norm ? -1. / (2 * norm + 2) : 0.5;
+    um.p.eig_min = 1 / trn_pow(h_min, 2);
+    um.p.eig_max = 1 / trn_pow(h_max, 2);
+  }
+  begin_timing(m);
+  quality_adjoint(m->d, m->nb_nodes, m->nb_elems, reinterpret_cast<const double2*>(xy),
+                  solut ? &um : nullptr, precision == TRN_PRECISION_MIXED, m->adj, grad_xy,
+                  grad_solut, m->stream);
+  CK(cudaMemcpyAsync(m->h_status + H_WIDE, m->adj.scal + 1, sizeof(double), cudaMemcpyDeviceToHost,
+                     m->stream));
+  int rc = sync_status(m);
+  if (rc) return rc;
+  if (value) std::memcpy(value, m->h_status + H_WIDE, sizeof(double));
+  return end_timing(m, nullptr, m->nb_elems, m->nb_nodes);
+}
+
+/* gradient-based smoothing: steps passes over the color classes of the
+ * interior vertices, each vertex moving up the gradient of its elements'
+ * summed quality (free mode only: the reference has no such pass) */
+int trn_smooth_gradient_run(trn_mesh* m, int max_colors, int steps, double max_len, trn_stats* st) {
+  if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "smooth_gradient: no mesh loaded");
+  if (m->replay) return fail(m, TRN_ERR_INVALID, "smooth_gradient: not available in replay mode");
+  if (steps < 0 || !(max_len > 0)) return fail(m, TRN_ERR_INVALID, "smooth_gradient: bad parameters");
+  int max_col = std::max(6, max_colors) - 1;
+  if (max_col > 30) max_col = 30;
+  m->err.clear();
+  begin_timing(m);
+  cudaStream_t s = m->stream;
+  smooth_pre(m->d, m->nb_nodes, s);
+  build_vicin(m->d, m->nb_nodes, true, s);
+  color_jp(m->d, m->nb_nodes, max_col, m->seed ^ (++m->calls * 0xc01dULL), m->hws, m->parts,
+           m->status + S_PARTS, s);
+  int rc = sync_status(m);
+  if (rc) return rc;
+  std::vector<std::pair<const int*, int>> classes;
+  for (int c = 0; c < max_col && c < 8; ++c) {
+    int a = m->h_status[S_PARTS + c], b = m->h_status[S_PARTS + c + 1];
+    classes.emplace_back(m->parts + a, b - a);
+  }
+  quality_all(m->d, m->nb_elems, m->fp32, s);
+  CK(cudaMemsetAsync(m->status + S_SMOOTH_TASKS, 0, sizeof(int) * 2, s));
+  for (int step = 0; step < steps; ++step)
+    for (auto& c : classes)
+      smooth_gradient_color(m->d, c.first, c.second, max_len, m->status + S_SMOOTH_TASKS, m->fp32, s);
+  if ((rc = sync_status(m))) return rc;
   return end_timing(m, st, m->h_status[S_SMOOTH_TASKS], m->h_status[S_SMOOTH_COMMIT]);
 }
 

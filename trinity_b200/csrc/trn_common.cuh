@@ -174,6 +174,34 @@ __device__ __forceinline__ void build_one_vicin(const DMesh& m, int v) {
   m.vdeg[v] = k;
 }
 
+/* P1 basis gradients of one element, times the 4x factor of hessian.cpp:52
+ * (the gradient and Hessian recovery, hessian.cpp:24-153) */
+struct ElemGrad {
+  double area;
+  double d[6];
+  int4 v;
+};
+
+__device__ __forceinline__ ElemGrad elem_grad(const DMesh& m, int e) {
+  ElemGrad g;
+  g.v = m.tri[e];
+  double2 p0 = m.pts[g.v.x], p1 = m.pts[g.v.y], p2 = m.pts[g.v.z];
+  double point[6] = {p0.x, p0.y, p1.x, p1.y, p2.x, p2.y};
+  double c0 = point[2] - point[0];
+  double c1 = point[4] - point[0];
+  double c2 = point[3] - point[1];
+  double c3 = point[5] - point[1];
+  g.area = 0.5 * (c0 * c3 - c1 * c2);
+  double norm = 2 / g.area;
+  g.d[0] = norm * (point[3] - point[5]);
+  g.d[1] = norm * (point[4] - point[2]);
+  g.d[2] = norm * (point[5] - point[1]);
+  g.d[3] = norm * (point[0] - point[4]);
+  g.d[4] = norm * (point[1] - point[3]);
+  g.d[5] = norm * (point[2] - point[0]);
+  return g;
+}
+
 /* warp-aggregated append of id to list[*count] */
 __device__ __forceinline__ void trn_append(int* list, int* count, int id) {
   unsigned mask = __activemask();

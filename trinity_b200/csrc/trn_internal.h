@@ -58,9 +58,18 @@ struct MetricParams {
   double eig_min;     /* 1/h_min^2 */
   double eig_max;     /* 1/h_max^2 */
 };
+/* optional copies of the recovery's intermediates (any may be null): the
+ * patch areas, the symmetrised Hessians and the locally normalised tensors */
+struct MetricSaves {
+  double* atot = nullptr;
+  double4* hsym = nullptr;
+  double4* mloc = nullptr;
+};
 void metric_run(const DMesh& m, int nb_nodes, int nb_elems, const double* solut,
                 double2* grad, double* terms, double* complexity, bool exact_sum,
-                const MetricParams& p, cudaStream_t s);
+                const MetricParams& p, cudaStream_t s, const MetricSaves* keep = nullptr);
+/* deterministic two-level sum of n doubles; partial holds grid_for(n) slots */
+void sum_tree(const double* in, int n, double* partial, double* out, cudaStream_t s);
 
 /* refinement (refine.cu) */
 struct RefineWs {
@@ -134,6 +143,41 @@ void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds
  * parts: vertex ids grouped by color, part_off[c] offsets (c = 0..max_col) */
 void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& ws,
               int* parts, int* part_off, cudaStream_t s);
+
+/* element-quality functional and its adjoint (adjoint.cu) */
+struct AdjWs {
+  int cap_v = 0, cap_e = 0;
+  double4* ten = nullptr;    /* metric recovered from the solution */
+  double4* lten = nullptr;   /* its logarithms (double4, or float4 in the FP32 form) */
+  double4* mloc = nullptr;   /* locally normalised tensors */
+  double4* hsym = nullptr;   /* symmetrised Hessians */
+  double* atot = nullptr;    /* 2-ring patch areas */
+  double* astar = nullptr;   /* stencil areas */
+  double* q = nullptr;       /* per element quality (+ sum partials) */
+  double* egp = nullptr;     /* per element point partials (6) */
+  double* egl = nullptr;     /* per element log-tensor partials (3) */
+  double* vbuf = nullptr;    /* per vertex scratch (8 doubles) */
+  double* ebuf = nullptr;    /* per element scratch (4 doubles) */
+  double* vfact = nullptr;   /* per vertex share of dJ/d(global scale) (+ partials) */
+  double* scal = nullptr;    /* [0] complexity, [1] J, [2] dJ/d(global scale) */
+};
+int adj_ws_ensure(AdjWs* ws, int nv, int ne);
+void adj_ws_free(AdjWs* ws);
+/* the metric of the functional recovered from a nodal solution */
+struct AdjMetric {
+  const double* solut;
+  double2* grad;       /* recovered-gradient scratch (per vertex) */
+  double* terms;       /* complexity terms (capa_elem + partial slots) */
+  bool exact_sum;
+  MetricParams p;
+};
+/* J -> ws.scal[1]; gxy (2 per vertex) and gu (per vertex) may be null; um
+ * null: the metric is the mesh's own tensors */
+void quality_adjoint(const DMesh& m, int nb_nodes, int nb_elems, const double2* xy,
+                     const AdjMetric* um, bool fp32, AdjWs& ws, double* gxy, double* gu,
+                     cudaStream_t s);
+void smooth_gradient_color(const DMesh& m, const int* list, int n, double max_len, int* counters,
+                           bool fp32, cudaStream_t s);
 
 void check_launch(const char* what);
 
