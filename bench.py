@@ -200,6 +200,8 @@ def b200_arm(args, rank, world, local_rank):
         g.reload()
         run_step(api, g, c, heur, kern)
         forms["fp64_quality_min_max_mean"] = [round(x, 4) for x in g.quality_stats()]
+        if rank == 0:
+            forms["adjoint"] = adjoint_form(args)
 
     # ---- end-to-end through the C ABI from host buffers ----
     pts = np.ascontiguousarray(m.points)
@@ -271,7 +273,63 @@ def b200_arm(args, rank, world, local_rank):
                            "final_mesh": f["final_mesh"], "quality_min_max_mean": f["quality_min_max_mean"]},
             "fp64_quality_min_max_mean": forms["fp64_quality_min_max_mean"],
         }
+        if "adjoint" in forms:
+            line["forms"]["adjoint"] = forms["adjoint"]
     return line
+
+
+# ------------------------------------------------------------------ adjoint
+def adjoint_form(args):
+    """The differentiation form on the 2M-triangle mesh jittered by +-0.3h with
+    the multi-feature field: device time of J = sum of element qualities with
+    dJ/dxy and dJ/du (through the Hessian recovery) in FP64 and FP32, then 20
+    steps of gradient smoothing (log-quality objective, the vertex tensor
+    following the move as in the smart Laplacian) against 20 smart-Laplacian
+    passes: final min / max / mean quality and device time."""
+    import torch
+    from trinity_b200 import _lib, api
+    m, u, c = meshgen.make_config("c4", args.grid)
+    g = api.Mesh((m.nb_nodes, m.nb_elems), 64, 1, 0, 1, capa_scale=2)
+    g.load_arrays(m.points, m.tris, tags_of(m), u)
+    api.Metrics(g, c["target"], c["norm"]).run()
+    ud = torch.tensor(u, dtype=torch.float64, device="cuda")
+    margs = dict(target_factor=c["target"], Lp_norm=c["norm"])
+    out = {"workload": "unit square 1000x1000 grid, 2,000,000 triangles, jitter 0.3h (seed 4), "
+                       "field tanh+gauss+waves, target 0.7, L^2"
+           if not args.grid else f"{args.grid}x{args.grid} grid, jitter 0.3h"}
+    for prec in ("fp64", "mixed"):
+        for _ in range(3):
+            g.quality_adjoint(None, ud, precision=prec, **margs)
+        _lib.profile_enable(True)
+        ms = []
+        for _ in range(max(args.steps, 3)):
+            J, gxy, gu = g.quality_adjoint(None, ud, precision=prec, **margs)
+            ms.append(g.last_time_ms())
+        prof = _lib.profile_read()
+        _lib.profile_enable(False)
+        adj = [r for r in prof if r["kernel"].startswith("adjoint")]
+        by = sum(r["bytes"] for r in adj)
+        kt = sum(r["ms"] for r in adj)
+        out[prec] = {"J": J, "ms_per_gradient": round(float(np.median(ms)), 3),
+                     "triangles_per_s": round(m.nb_elems / (float(np.median(ms)) / 1e3), 1),
+                     "note": "J + dJ/dxy + dJ/du incl. the metric recovery forward",
+                     "adjoint_kernels_gbs": round(by / (kt / 1e3) / 1e9, 1) if kt > 0 else None}
+    heur = api.Partit(g, 8)
+    for kind in ("gradient", "laplacian"):
+        g.reload()
+        api.Metrics(g, c["target"], c["norm"]).run()
+        q0 = g.quality_stats()
+        st = _lib.Stats()
+        if kind == "gradient":
+            api.GradientSmooth(g, heur, 20).run(st)
+        else:
+            api.Smooth(g, heur, 20).run(st)
+        out[f"smooth_{kind}_20"] = {"ms": round(g.last_time_ms(), 3),
+                                    "quality_min_max_mean_before": [round(x, 5) for x in q0],
+                                    "quality_min_max_mean_after": [round(x, 5) for x in g.quality_stats()],
+                                    "moved": st.task, "tried": st.eval}
+    g.close()
+    return out
 
 
 # ------------------------------------------------------------------ batch

@@ -134,13 +134,19 @@ int trn_quality_adjoint(trn_mesh* mesh, const double* xy, const double* solut,
                         int precision, double* value, double* grad_xy, double* grad_solut);
 /* Gradient-based smoothing, beside Smooth::run's smart Laplacian
  * (smoothing.cpp:40-126, 274-302): `steps` passes over the color classes of
- * the interior vertices; each vertex steps along M_v^-1 dJ_v/dx_v (J_v the
- * summed quality of its elements, M_v its tensor held fixed), at most
- * `max_len` in metric length, and keeps the move only if its elements stay
- * CCW, each above the old stencil minimum, with a larger sum; the step backs
- * off 1, 1/2, .., 1/16. Free mode only (TRN_ERR_INVALID in replay mode).
- * stats->eval / task: vertices tried / moved. */
-int trn_smooth_gradient_run(trn_mesh* mesh, int max_colors, int steps, double max_len,
+ * the interior vertices; each vertex v steps along M_v^-1 g_v, g_v the
+ * gradient at v of its elements' summed quality, or summed log-quality with
+ * TRN_SMOOTH_LOG_Q in `mode` (the worst elements weigh most). With
+ * TRN_SMOOTH_TENSOR_FOLLOWS a moved vertex takes the log-Euclidean mean of
+ * its neighbours' tensors, as the smart Laplacian's does (smoothing.cpp:64-81),
+ * and g_v is taken under it; otherwise M_v stays. The step's metric length is
+ * `max_len` times the mean metric length of v's edges (under M_v), and it
+ * backs off 1, 1/2, .., 1/16 until the elements stay CCW, each above the old
+ * stencil minimum, with a larger objective. Free mode only (TRN_ERR_INVALID
+ * in replay mode). stats->eval / task: vertices tried / moved. */
+#define TRN_SMOOTH_LOG_Q 1
+#define TRN_SMOOTH_TENSOR_FOLLOWS 2
+int trn_smooth_gradient_run(trn_mesh* mesh, int max_colors, int steps, double max_len, int mode,
                             trn_stats* stats);
 
 /* Replay mode: the independent sets, matchings and colorings are read from a

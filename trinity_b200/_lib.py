@@ -84,7 +84,7 @@ def lib():
                                         ctypes.POINTER(dp), ctypes.POINTER(dp)]
         L.trn_launch_count.restype = ctypes.c_ulonglong
         L.trn_quality_adjoint.argtypes = [pmesh, vp, vp, dp, ip, dp, dp, ip, ctypes.POINTER(dp), vp, vp]
-        L.trn_smooth_gradient_run.argtypes = [pmesh, ip, ip, dp, sp]
+        L.trn_smooth_gradient_run.argtypes = [pmesh, ip, ip, dp, ip, sp]
         _lib = L
     return _lib
 

@@ -268,14 +268,20 @@ class Swap:
 class GradientSmooth:
     """Gradient-based smoothing beside Smooth (trn_smooth_gradient_run):
     `steps` passes over the color classes, each interior vertex stepping up
-    the metric-preconditioned gradient of its elements' summed quality."""
+    the metric-preconditioned gradient of its elements' summed quality
+    (objective "sum") or summed log-quality ("log"); with tensor_follows the
+    moved vertex takes its neighbours' log-Euclidean mean tensor, as the smart
+    Laplacian's does."""
 
-    def __init__(self, mesh: Mesh, algo: Partit, steps: int, max_len: float = 0.2):
+    def __init__(self, mesh: Mesh, algo: Partit, steps: int, max_len: float = 0.1,
+                 objective: str = "log", tensor_follows: bool = True):
         self.mesh, self.algo, self.steps, self.max_len = mesh, algo, steps, max_len
+        self.mode = {"sum": 0, "log": 1}[objective] | (2 if tensor_follows else 0)
 
     def run(self, total: Stats | None = None) -> None:
         m = self.mesh
         m._check(m._L.trn_smooth_gradient_run(m.h, self.algo.max_part, self.steps, self.max_len,
+                                              self.mode,
                                               ctypes.byref(total) if total is not None else None))
 
 

@@ -579,41 +579,75 @@ void quality_adjoint(const DMesh& m, int nb_nodes, int nb_elems, const double2* 
 }
 
 /* ------------------------------------------------------------------------ */
-/* gradient-based smoothing: one color class of interior vertices; each moves
- * up the metric-preconditioned gradient of the summed quality of its
- * elements, at a fixed nodal tensor, and keeps the move only if every
- * element stays CCW with quality above the old stencil minimum and the
- * summed quality grows (the step backs off 1, 1/2, .., 1/16) */
+/* gradient-based smoothing: one color class of interior vertices. Each
+ * vertex v moves along M_v^-1 g, g the gradient at v of its elements' summed
+ * quality (mode bit 0 clear) or summed log-quality (bit 0 set: each element's
+ * adjoint weighted by 1/q, so the worst elements lead). With mode bit 1 the
+ * vertex's tensor becomes the log-Euclidean mean of its neighbours' tensors
+ * when it moves, as Smooth::moveSmartLaplacian does (smoothing.cpp:64-81),
+ * and the gradient is taken under that tensor; otherwise the tensor stays.
+ * The step's metric length is max_len times the mean metric length of v's
+ * edges, and it backs off 1, 1/2, .., 1/16 until every element stays CCW
+ * with quality above the old stencil minimum and the objective grows. */
 template <bool F32>
-__device__ int move_gradient(const DMesh& m, int i, double max_len) {
+__device__ int move_gradient(const DMesh& m, int i, double max_len, int mode) {
+  const bool use_log = (mode & 1) != 0, follow = (mode & 2) != 0;
   const int* st = m.stenc + (size_t) i * m.bucket;
   const int deg = trn_deg(m, i);
-  double q_min = 1.7976931348623157e308, q_sum = 0;
+  double q_min = 1.7976931348623157e308, obj = 0;
   for (int a = 0; a < deg; ++a) {
     const double q = m.qual[st[a]];
     q_min = trn_dmin(q_min, q);
-    q_sum += q;
+    obj += use_log ? log(q) : q;
   }
   const double2 pini = m.pts[i];
-  const LogT<F32> li = log_load<F32>(m, i);
+  const double4 tini = m.ten[i];
+  const LogT<F32> lini = log_load<F32>(m, i);
+  double4 tnew = tini;
+  LogT<F32> lnew = lini;
+  if (follow) {
+    const int* vc = m.vic + (size_t) i * m.bucket;
+    const int nb_neigh = min(m.vdeg[i], m.bucket);
+    if (nb_neigh == 0) return 0;
+    LogSum<F32> lsum;
+    for (int k = 0; k < nb_neigh; ++k) lsum.add(log_load<F32>(m, vc[k]));
+    double tn[3];
+    lsum.finish(nb_neigh, tn);
+    tnew = make_double4(tn[0], tn[1], tn[2], 0.0);
+    lnew = log_of<F32>(tn[0], tn[1], tn[2]);
+  }
   double gx = 0, gy = 0;
   for (int a = 0; a < deg; ++a) {
     const int4 n = m.tri[st[a]];
     ElemAdj<F32> o;
-    quality_adjoint<F32>(m.pts[n.x], m.pts[n.y], m.pts[n.z], log_load<F32>(m, n.x),
-                         log_load<F32>(m, n.y), log_load<F32>(m, n.z), false, o);
+    quality_adjoint<F32>(m.pts[n.x], m.pts[n.y], m.pts[n.z],
+                         n.x == i ? lnew : log_load<F32>(m, n.x),
+                         n.y == i ? lnew : log_load<F32>(m, n.y),
+                         n.z == i ? lnew : log_load<F32>(m, n.z), false, o);
     const int j = local_index(n, i);
-    gx += (double) o.gp[2 * j];
-    gy += (double) o.gp[2 * j + 1];
+    const double w = use_log ? 1.0 / trn_dmax(o.q, 1e-300) : 1.0;
+    gx += w * (double) o.gp[2 * j];
+    gy += w * (double) o.gp[2 * j + 1];
   }
-  const double4 t = m.ten[i];
+  const double4 t = tnew;
   const double det = t.x * t.z - t.y * t.y;
   if (!(det > 0)) return 0;
   const double dx = (t.z * gx - t.y * gy) / det;
   const double dy = (t.x * gy - t.y * gx) / det;
   const double gn = sqrt(gx * dx + gy * dy);   /* metric length of (dx, dy) */
-  if (!(gn > 0)) return 0;
-  double eta = trn_dmin(0.5, max_len / gn);
+  if (!(gn > 0) || !isfinite(gn)) return 0;
+  /* the step: max_len times the mean metric length (under M_v) of v's edges */
+  double lsum = 0;
+  int lcnt = 0;
+  for (int a = 0; a < deg; ++a) {
+    const int4 n = m.tri[st[a]];
+    const int j = local_index(n, i);
+    const int w = j == 0 ? n.y : (j == 1 ? n.z : n.x);   /* next vertex: each edge once */
+    const double ex = m.pts[w].x - pini.x, ey = m.pts[w].y - pini.y;
+    lsum += sqrt(ex * (t.x * ex + t.y * ey) + ey * (t.y * ex + t.z * ey));
+    ++lcnt;
+  }
+  double eta = max_len * (lsum / lcnt) / gn;
   double qual[TRN_MAX_DEG];
   bool valid = false;
   for (int retry = 0; retry < 5 && !valid; ++retry, eta *= 0.5) {
@@ -627,17 +661,21 @@ __device__ int move_gradient(const DMesh& m, int i, double max_len) {
       const double2 p2 = (n.z == i) ? pa : m.pts[n.z];
       valid = false;
       if (trn_ccw(p0, p1, p2)) {
-        const LogT<F32> l0 = (n.x == i) ? li : log_load<F32>(m, n.x);
-        const LogT<F32> l1 = (n.y == i) ? li : log_load<F32>(m, n.y);
-        const LogT<F32> l2 = (n.z == i) ? li : log_load<F32>(m, n.z);
+        const LogT<F32> l0 = (n.x == i) ? lnew : log_load<F32>(m, n.x);
+        const LogT<F32> l1 = (n.y == i) ? lnew : log_load<F32>(m, n.y);
+        const LogT<F32> l2 = (n.z == i) ? lnew : log_load<F32>(m, n.z);
         qual[a] = quality_x(p0, p1, p2, l0, l1, l2);
         valid = qual[a] > q_min;
-        sum += qual[a];
+        sum += use_log ? log(qual[a]) : qual[a];
       }
     }
-    if (valid && !(sum > q_sum)) valid = false;
+    if (valid && !(sum > obj)) valid = false;
     if (valid) {
       m.pts[i] = pa;
+      if (follow) {
+        m.ten[i] = tnew;
+        log_store<F32>(m, i, lnew);
+      }
       for (int a = 0; a < deg; ++a) m.qual[st[a]] = qual[a];
     }
   }
@@ -646,7 +684,7 @@ __device__ int move_gradient(const DMesh& m, int i, double max_len) {
 
 template <bool F32>
 __global__ void k_smooth_gradient(DMesh m, const int* __restrict__ list, int n, double max_len,
-                                  int* counters) {
+                                  int mode, int* counters) {
   if (trn_failed(m)) return;
   int tasks = 0, commit = 0;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
@@ -657,20 +695,22 @@ __global__ void k_smooth_gradient(DMesh m, const int* __restrict__ list, int n, 
     }
     if (!m.activ[v] || trn_deg(m, v) == 0) continue;
     tasks++;
-    commit += move_gradient<F32>(m, v, max_len);
+    commit += move_gradient<F32>(m, v, max_len, mode);
   }
   if (tasks) atomicAdd(counters, tasks);
   if (commit) atomicAdd(counters + 1, commit);
 }
 
-void smooth_gradient_color(const DMesh& m, const int* list, int n, double max_len, int* counters,
-                           bool fp32, cudaStream_t s) {
+void smooth_gradient_color(const DMesh& m, const int* list, int n, double max_len, int mode,
+                           int* counters, bool fp32, cudaStream_t s) {
   if (n <= 0) return;
   const double own = 4 + 1 + 4 + 2 * kPt + kTen + kAvgDeg * (kIdx + kTri + 2 * kQ);
   const double nbr = (double) std::min<long long>((long long) m.capa_node, 6LL * n) * (kPt + kTen);
   ProfScope ps("smooth_gradient", s, n * own + nbr);
-  if (fp32) k_smooth_gradient<true><<<grid_for(n, 128), 128, 0, s>>>(m, list, n, max_len, counters);
-  else k_smooth_gradient<false><<<grid_for(n, 128), 128, 0, s>>>(m, list, n, max_len, counters);
+  if (fp32)
+    k_smooth_gradient<true><<<grid_for(n, 128), 128, 0, s>>>(m, list, n, max_len, mode, counters);
+  else
+    k_smooth_gradient<false><<<grid_for(n, 128), 128, 0, s>>>(m, list, n, max_len, mode, counters);
   note_launch();
   check_launch("smooth_gradient");
 }

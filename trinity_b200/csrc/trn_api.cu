@@ -945,11 +945,14 @@ int trn_quality_adjoint(trn_mesh* m, const double* xy, const double* solut, doub
 
 /* gradient-based smoothing: steps passes over the color classes of the
  * interior vertices, each vertex moving up the gradient of its elements'
- * summed quality (free mode only: the reference has no such pass) */
-int trn_smooth_gradient_run(trn_mesh* m, int max_colors, int steps, double max_len, trn_stats* st) {
+ * summed quality or log-quality (free mode only: the reference has no such
+ * pass) */
+int trn_smooth_gradient_run(trn_mesh* m, int max_colors, int steps, double max_len, int mode,
+                            trn_stats* st) {
   if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "smooth_gradient: no mesh loaded");
   if (m->replay) return fail(m, TRN_ERR_INVALID, "smooth_gradient: not available in replay mode");
-  if (steps < 0 || !(max_len > 0)) return fail(m, TRN_ERR_INVALID, "smooth_gradient: bad parameters");
+  if (steps < 0 || !(max_len > 0) || (mode & ~(TRN_SMOOTH_LOG_Q | TRN_SMOOTH_TENSOR_FOLLOWS)))
+    return fail(m, TRN_ERR_INVALID, "smooth_gradient: bad parameters");
   int max_col = std::max(6, max_colors) - 1;
   if (max_col > 30) max_col = 30;
   m->err.clear();
@@ -970,7 +973,8 @@ int trn_smooth_gradient_run(trn_mesh* m, int max_colors, int steps, double max_l
   CK(cudaMemsetAsync(m->status + S_SMOOTH_TASKS, 0, sizeof(int) * 2, s));
   for (int step = 0; step < steps; ++step)
     for (auto& c : classes)
-      smooth_gradient_color(m->d, c.first, c.second, max_len, m->status + S_SMOOTH_TASKS, m->fp32, s);
+      smooth_gradient_color(m->d, c.first, c.second, max_len, mode, m->status + S_SMOOTH_TASKS,
+                            m->fp32, s);
   if ((rc = sync_status(m))) return rc;
   return end_timing(m, st, m->h_status[S_SMOOTH_TASKS], m->h_status[S_SMOOTH_COMMIT]);
 }

@@ -176,8 +176,8 @@ struct AdjMetric {
 void quality_adjoint(const DMesh& m, int nb_nodes, int nb_elems, const double2* xy,
                      const AdjMetric* um, bool fp32, AdjWs& ws, double* gxy, double* gu,
                      cudaStream_t s);
-void smooth_gradient_color(const DMesh& m, const int* list, int n, double max_len, int* counters,
-                           bool fp32, cudaStream_t s);
+void smooth_gradient_color(const DMesh& m, const int* list, int n, double max_len, int mode,
+                           int* counters, bool fp32, cudaStream_t s);
 
 void check_launch(const char* what);
 
