@@ -202,6 +202,7 @@ def b200_arm(args, rank, world, local_rank):
         forms["fp64_quality_min_max_mean"] = [round(x, 4) for x in g.quality_stats()]
         if rank == 0:
             forms["adjoint"] = adjoint_form(args)
+            forms["precision"] = precision_form(args)
 
     # ---- end-to-end through the C ABI from host buffers ----
     pts = np.ascontiguousarray(m.points)
@@ -273,9 +274,105 @@ def b200_arm(args, rank, world, local_rank):
                            "final_mesh": f["final_mesh"], "quality_min_max_mean": f["quality_min_max_mean"]},
             "fp64_quality_min_max_mean": forms["fp64_quality_min_max_mean"],
         }
-        if "adjoint" in forms:
-            line["forms"]["adjoint"] = forms["adjoint"]
+        for k in ("adjoint", "precision"):
+            if k in forms:
+                line["forms"][k] = forms[k]
     return line
+
+
+# ------------------------------------------------------------------ precision
+def _metric_lengths(pts, tri, ten):
+    """metric length of every undirected edge (numeric.cpp:469-497), numpy FP64"""
+    e = np.concatenate([tri[:, [0, 1]], tri[:, [1, 2]], tri[:, [2, 0]]])
+    e = np.unique(np.sort(e, axis=1), axis=0)
+    w = pts[e[:, 1]] - pts[e[:, 0]]
+
+    def quad(t):
+        return np.sqrt(w[:, 0] * (t[:, 0] * w[:, 0] + t[:, 1] * w[:, 1])
+                       + w[:, 1] * (t[:, 1] * w[:, 0] + t[:, 2] * w[:, 1]))
+    l0, l1 = quad(ten[e[:, 0]]), quad(ten[e[:, 1]])
+    lo, hi = np.minimum(l0, l1), np.maximum(l0, l1)
+    r = hi / lo
+    with np.errstate(divide="ignore", invalid="ignore"):
+        geo = hi * (r - 1) / (r * np.log(r))
+    return np.where(np.abs(l0 - l1) < 1e-9, l0, geo)
+
+
+def precision_form(args):
+    """The mixed-precision form on the ~4M-triangle mesh (1414x1414 grid,
+    jitter 0.2h, multi-feature field, depth 2): (1) one smoothing pass from
+    the same FP64 state in both forms -> max / RMS relative error of the
+    smoothed coordinates' displacement and of the tensors; (2) full 3-round
+    adaptations in both forms -> throughput, final counts and the histogram
+    of edge lengths in the metric."""
+    import torch
+    from trinity_b200 import api
+    m, u, c = meshgen.make_config("c3", args.grid)
+    tags = tags_of(m)
+    out = {"workload": f"unit square {m.nb_nodes} vertices / {m.nb_elems} triangles, jitter 0.2h "
+                       "(seed 3), field tanh+gauss+waves, target 0.7, L^2, depth 2, bucket 128"}
+    gs = {}
+    for prec in ("fp64", "mixed"):
+        g = api.Mesh((m.nb_nodes, m.nb_elems), c["bucket"], c["depth"], 0, c["rounds"])
+        g.load_arrays(m.points, m.tris, tags, u)
+        heur = api.Partit(g, 8)
+        api.Metrics(g, c["target"], c["norm"]).run()
+        api.Refine(g, c["depth"]).run()
+        api.Coarse(g, heur).run()
+        api.Swap(g).run()
+        gs[prec] = (g, heur)
+    p0 = gs["fp64"][0].export()[0]
+    res = {}
+    for prec, (g, heur) in gs.items():
+        g.set_precision(prec)
+        api.Smooth(g, heur, c["depth"]).run()
+        pts, ten, tri, alive, _ = g.export()
+        res[prec] = (pts, ten, alive)
+    (p64, t64, a64), (p32, t32, a32) = res["fp64"], res["mixed"]
+    live = a64.astype(bool)
+    d64 = np.linalg.norm(p64[live] - p0[live], axis=1)
+    moved = d64 > 0
+    derr = np.linalg.norm(p32[live] - p64[live], axis=1)[moved] / d64[moved]
+    terr = (np.abs(t32[live] - t64[live]) / np.maximum(np.abs(t64[live]).max(axis=1, keepdims=True), 1e-300))
+    flip = derr > 1e-3     # a different accept / back-off decision, not rounding
+    out["same_state_smoothing_pass"] = {
+        "vertices_moved_fp64": int(moved.sum()),
+        "decision_differs_fraction": round(float(flip.mean()), 6) if derr.size else 0.0,
+        "displacement_rel_err_rms_same_decision": float(np.sqrt(np.mean(derr[~flip] ** 2))) if derr.size else 0.0,
+        "displacement_rel_err_max_same_decision": float(derr[~flip].max()) if derr.size else 0.0,
+        "displacement_rel_err_max": float(derr.max()) if derr.size else 0.0,
+        "displacement_rel_err_rms": float(np.sqrt(np.mean(derr ** 2))) if derr.size else 0.0,
+        "displacement_rel_err_median": float(np.median(derr)) if derr.size else 0.0,
+        "tensor_rel_err_max": float(terr.max()), "tensor_rel_err_rms": float(np.sqrt(np.mean(terr ** 2))),
+        "note": "same FP64 state, same coloring; metric recovery itself is FP64 in both forms "
+                "(tensor error 0 after Metrics::run)"}
+    for prec, (g, _) in gs.items():
+        g.close()
+    bins = np.concatenate([np.linspace(0, 3, 31), [np.inf]])
+    hists = {}
+    for prec in ("fp64", "mixed"):
+        g = api.Mesh((m.nb_nodes, m.nb_elems), c["bucket"], c["depth"], 0, c["rounds"])
+        g.load_arrays(m.points, m.tris, tags, u)
+        g.set_precision(prec)
+        heur = api.Partit(g, 8)
+        kern = [api.Refine(g, c["depth"]), api.Coarse(g, heur), api.Swap(g), api.Smooth(g, heur, c["depth"])]
+        run_step(api, g, c, heur, kern)
+        g.reload()
+        torch.cuda.synchronize()
+        tin, tms, _ = run_step(api, g, c, heur, kern)
+        pts, tri, ten = g.export_compact()
+        ln = _metric_lengths(pts, tri, ten)
+        h, _ = np.histogram(ln, bins=bins)
+        hists[prec] = h / h.sum()
+        out[prec] = {"value": round(tin / (tms / 1e3), 1), "unit": UNIT, "round_ms": round(tms, 3),
+                     "final_triangles": int(tri.shape[0]),
+                     "edges_in_unit_range": round(float(np.mean((ln >= 2 ** -0.5) & (ln <= 2 ** 0.5))), 4),
+                     "quality_min_max_mean": [round(x, 4) for x in g.quality_stats()]}
+        g.close()
+    out["histogram_bins"] = "metric edge length, 30 bins on [0, 3] + overflow"
+    out["histogram_l1_fp32_vs_fp64"] = round(float(np.abs(hists["mixed"] - hists["fp64"]).sum()), 5)
+    out["speedup_mixed_vs_fp64"] = round(out["mixed"]["value"] / out["fp64"]["value"], 3)
+    return out
 
 
 # ------------------------------------------------------------------ adjoint
