@@ -31,6 +31,10 @@ import time
 
 import numpy as np
 
+# many meshes adapt concurrently in the batched workload, one stream each:
+# give the device more hardware queues than the default 8 (read at CUDA init)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 

@@ -198,7 +198,9 @@ class Mesh:
 def batch_adapt(meshes, target_factor: float, Lp_norm: int = 2, rounds: int = 3, depth: int = 1,
                 threads: int = 8, h_min: float = EPSILON, h_max: float = H_MAX):
     """Metric recovery + rounds for many loaded meshes at once (one stream per
-    mesh, a pool of host threads). Returns (round_ms[count], tri_in[count])."""
+    mesh, a pool of host threads). Returns (round_ms[count], tri_in[count]).
+    Set CUDA_DEVICE_MAX_CONNECTIONS=32 in the environment before CUDA starts
+    so that the streams do not share the default 8 hardware queues."""
     L = lib()
     n = len(meshes)
     handles = (ctypes.c_void_p * n)(*[m.h.value if hasattr(m.h, "value") else m.h for m in meshes])

@@ -8,6 +8,8 @@
  *                    keeps every surviving element CCW with edges <= sqrt(2)
  *                    (Coarse::identifyTarget, coarsening.cpp:47-133); ties are
  *                    broken in adjacency order, like the reference's multimap
+ *   k_coarse_filter_group  the same search by 8 lanes per vertex, for levels
+ *                    that list few vertices (free mode)
  *   k_collapse       per independent vertex: erase the 1-2 shell elements,
  *                    move the rest of the stencil to the target, relabel,
  *                    tag repairs, re-activate the 1-ring (Coarse::collapseEdge,
@@ -18,6 +20,8 @@
  */
 #include "trn_internal.h"
 #include "trn_mixed.cuh"
+
+#include <algorithm>
 
 namespace trn {
 
@@ -115,9 +119,10 @@ __global__ void k_coarse_filter(DMesh m, int nb_nodes, int* __restrict__ target,
 template <bool F32>
 __global__ void k_coarse_filter_append(DMesh m, const int* __restrict__ act, const int* act_n,
                                        int* __restrict__ target, int* __restrict__ cand, int* count,
-                                       uint8_t* __restrict__ state) {
+                                       uint8_t* __restrict__ state, int min_n) {
   if (trn_failed(m)) return;
   const int n = *act_n;
+  if (n < min_n) return;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
     const int v = act[q];
     if (m.activ[v] <= 0) continue;
@@ -128,6 +133,152 @@ __global__ void k_coarse_filter_append(DMesh m, const int* __restrict__ act, con
     if (t > -1) {
       state[v] = 1;
       trn_append(cand, count, v);
+    }
+  }
+}
+
+/* the same search by a group of kGroup lanes per vertex, for the levels that
+ * list few vertices, where one lane's chain of dependent gathers (adjacency,
+ * stencil, triangles, points, tensors) sets the time. The lanes compute the
+ * neighbours' metric lengths, then check every (candidate, element) pair at
+ * once; the per-candidate verdicts are combined as bit masks, and the pick is
+ * the smallest (length, adjacency index) among the valid candidates, which is
+ * the first valid one in the serial search's stable length order, so the
+ * targets are the same. Vertices with more than 32 neighbours fall back to
+ * the serial search on the group's first lane. */
+constexpr int kGroup = 8;
+/* at most this many listed vertices: the grouped search (measured on B200:
+ * faster below ~16k listed vertices, 2x slower on full-mesh levels) */
+constexpr int kGroupMax = 16384;
+
+template <bool F32>
+__global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, const int* act_n,
+                                      int* __restrict__ target, int* __restrict__ cand, int* count,
+                                      uint8_t* __restrict__ state, int max_n) {
+  if (trn_failed(m)) return;
+  const int n = *act_n;
+  if (n > max_n) return;
+  const int lane = threadIdx.x & 31;
+  const int gl = lane & (kGroup - 1);
+  const int gbase = lane & ~(kGroup - 1);
+  const int per_warp = 32 / kGroup;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int base = warp * per_warp; base < n; base += nwarps * per_warp) {
+    const int q = base + lane / kGroup;
+    int vv = -1;
+    if (gl == 0 && q < n) {
+      const int x = act[q];
+      if (m.activ[x] > 0) {
+        m.activ[x] = 0;
+        build_one_vicin(m, x);
+        vv = x;
+      }
+    }
+    const int v = __shfl_sync(0xffffffffu, vv, gbase);
+    __syncwarp();
+    const int nv = v >= 0 ? m.vdeg[v] : 0;
+    const bool serial = nv > 32;
+    const bool grp = v >= 0 && !serial;
+    const int* vc = m.vic + (size_t) (v >= 0 ? v : 0) * m.bucket;
+    const int* st = m.stenc + (size_t) (v >= 0 ? v : 0) * m.bucket;
+    const bool bsrc = v >= 0 && (m.tags[v] & TRN_TAG_BOUND) != 0;
+    double2 ps = make_double2(0, 0);
+    double4 ts = make_double4(0, 0, 0, 0);
+    if (grp) {
+      ps = m.pts[v];
+      ts = m.ten[v];
+    }
+    /* neighbours b = gl + kGroup * k: candidates closer than 1/sqrt(2) */
+    double lenk[32 / kGroup];
+    unsigned candm = 0, boundm = 0;
+    for (int k = 0; k < 32 / kGroup; ++k) {
+      const int b = gl + kGroup * k;
+      lenk[k] = 0.0;
+      if (grp && b < nv) {
+        const int w = vc[b];
+        const bool bd = (m.tags[w] & TRN_TAG_BOUND) != 0;
+        if (bd) boundm |= 1u << b;
+        if (!(bsrc && !bd)) {
+          const double len = length_x<F32>(ps, m.pts[w], ts, m.ten[w]);
+          if (len < TRN_L_MIN) {
+            candm |= 1u << b;
+            lenk[k] = len;
+          }
+        }
+      }
+    }
+    for (int o = kGroup / 2; o >= 1; o >>= 1) {
+      candm |= __shfl_xor_sync(0xffffffffu, candm, o);
+      boundm |= __shfl_xor_sync(0xffffffffu, boundm, o);
+    }
+    /* every (candidate, element) pair of the simulated collapses */
+    const int deg = grp ? trn_deg(m, v) : 0;
+    const int np = (grp && candm) ? nv * deg : 0;
+    const int iters = __reduce_max_sync(0xffffffffu, (np + kGroup - 1) / kGroup);
+    unsigned failm = 0, once = 0, twice = 0;
+    for (int k = 0; k < iters; ++k) {
+      const int p = gl + kGroup * k;
+      if (p >= np) continue;
+      const int b = p / deg, a = p - b * deg;
+      if (!((candm >> b) & 1u)) continue;
+      const unsigned bit = 1u << b;
+      const int destin = vc[b];
+      const int4 e = m.tri[st[a]];
+      if ((v == e.x && destin == e.y) || (v == e.y && destin == e.x) || (v == e.y && destin == e.z) ||
+          (v == e.z && destin == e.y) || (v == e.z && destin == e.x) || (v == e.x && destin == e.z)) {
+        twice |= once & bit;
+        once |= bit;
+        continue;
+      }
+      const int f0 = (e.x == v ? destin : e.x);
+      const int f1 = (e.y == v ? destin : e.y);
+      const int f2 = (e.z == v ? destin : e.z);
+      const double2 p0 = m.pts[f0], p1 = m.pts[f1], p2 = m.pts[f2];
+      if (trn_ccw(p0, p1, p2)) {
+        const double4 t0 = m.ten[f0], t1 = m.ten[f1], t2 = m.ten[f2];
+        const double l0 = length_x<F32>(p0, p1, t0, t1);
+        const double l1 = length_x<F32>(p1, p2, t1, t2);
+        const double l2 = length_x<F32>(p2, p0, t2, t0);
+        if (l0 > TRN_L_MAX || l1 > TRN_L_MAX || l2 > TRN_L_MAX) failm |= bit;
+      } else {
+        failm |= bit;
+      }
+    }
+    for (int o = kGroup / 2; o >= 1; o >>= 1) {
+      const unsigned fo = __shfl_xor_sync(0xffffffffu, failm, o);
+      const unsigned oo = __shfl_xor_sync(0xffffffffu, once, o);
+      const unsigned to = __shfl_xor_sync(0xffffffffu, twice, o);
+      twice |= to | (once & oo);
+      once |= oo;
+      failm |= fo;
+    }
+    const unsigned valid = candm & ~failm & ~(bsrc ? (twice & boundm) : 0u);
+    /* the smallest (length, adjacency index) among the valid candidates */
+    double best = 0.0;
+    int bestb = -1;
+    for (int k = 0; k < 32 / kGroup; ++k) {
+      const int b = gl + kGroup * k;
+      if (b < 32 && ((valid >> b) & 1u) && (bestb < 0 || lenk[k] < best)) {
+        best = lenk[k];
+        bestb = b;
+      }
+    }
+    for (int o = kGroup / 2; o >= 1; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int obb = __shfl_xor_sync(0xffffffffu, bestb, o);
+      if (obb >= 0 && (bestb < 0 || ob < best || (ob == best && obb < bestb))) {
+        best = ob;
+        bestb = obb;
+      }
+    }
+    if (gl == 0 && v >= 0) {
+      const int t = serial ? identify_target<F32>(m, v) : (bestb >= 0 ? vc[bestb] : -1);
+      target[v] = t;
+      if (t > -1) {
+        state[v] = 1;
+        trn_append(cand, count, v);
+      }
     }
   }
 }
@@ -220,11 +371,23 @@ void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int
                            int* count, uint8_t* state, bool fp32, cudaStream_t s) {
   ProfScope ps("coarsen_filter", s, 0.0);
   cudaMemsetAsync(count, 0, sizeof(int), s);
+  /* a level listing at most kGroupMax vertices runs the grouped search, a
+   * larger one the one-lane search; the count is on the device, so both are
+   * launched and one returns at once */
   const int g = grid_for(m.capa_node);
-  if (fp32)
-    k_coarse_filter_append<true><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state);
-  else
-    k_coarse_filter_append<false><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state);
+  const int gg = grid_for((long long) std::min(m.capa_node, kGroupMax) * kGroup);
+  if (fp32) {
+    k_coarse_filter_group<true><<<gg, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state,
+                                                          kGroupMax);
+    k_coarse_filter_append<true><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state,
+                                                           kGroupMax + 1);
+  } else {
+    k_coarse_filter_group<false><<<gg, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state,
+                                                           kGroupMax);
+    k_coarse_filter_append<false><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state,
+                                                            kGroupMax + 1);
+  }
+  note_launch();
   note_launch();
   check_launch("coarsen_filter_append");
 }
