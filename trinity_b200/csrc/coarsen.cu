@@ -368,14 +368,14 @@ void coarsen_list_active(const DMesh& m, int nb_nodes, int* act, int* act_n, cud
 }
 
 void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int* target, int* cand,
-                           int* count, uint8_t* state, bool fp32, cudaStream_t s) {
+                           int* count, uint8_t* state, bool fp32, cudaStream_t s, long long bound) {
   ProfScope ps("coarsen_filter", s, 0.0);
   cudaMemsetAsync(count, 0, sizeof(int), s);
   /* a level listing at most kGroupMax vertices runs the grouped search, a
    * larger one the one-lane search; the count is on the device, so both are
    * launched and one returns at once */
-  const int g = grid_for(m.capa_node);
-  const int gg = grid_for((long long) std::min(m.capa_node, kGroupMax) * kGroup);
+  const int g = grid_bounded(bound, m.capa_node);
+  const int gg = grid_bounded(bound < 0 ? -1 : bound * kGroup, (long long) kGroupMax * kGroup);
   if (fp32) {
     k_coarse_filter_group<true><<<gg, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state,
                                                           kGroupMax);
@@ -393,9 +393,10 @@ void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int
 }
 
 void collapse(const DMesh& m, const int* indep, const int* count, const int* target,
-              const uint8_t* cand_flag, cudaStream_t s) {
+              const uint8_t* cand_flag, cudaStream_t s, long long bound) {
   ProfScope ps("collapse", s, 0.0);
-  k_collapse<<<grid_for(m.capa_node), TRN_THREADS, 0, s>>>(m, indep, count, target, cand_flag);
+  k_collapse<<<grid_bounded(bound, m.capa_node), TRN_THREADS, 0, s>>>(m, indep, count, target,
+                                                                      cand_flag);
   note_launch();
   check_launch("collapse");
 }

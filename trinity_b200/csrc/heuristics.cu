@@ -75,9 +75,9 @@ __global__ void k_mis_finish(DMesh m, uint8_t* state, uint8_t* other, const int*
 }
 
 void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, uint64_t seed,
-                   HeurWs& ws, int* indep, int* nindep, cudaStream_t s) {
+                   HeurWs& ws, int* indep, int* nindep, cudaStream_t s, long long bound) {
   ProfScope ps("mis_jp", s, 0.0);
-  const int g = grid_for(m.capa_node);
+  const int g = grid_bounded(bound, m.capa_node);
   uint8_t* buf[2] = {ws.state, ws.state2};
   for (int r = 0; r < rounds; ++r) {
     k_mis_round_dev<<<g, TRN_THREADS, 0, s>>>(m, buf[r & 1], buf[(r + 1) & 1], cand, count,
@@ -164,10 +164,10 @@ __global__ void k_match_prop_clear(const int* __restrict__ dual, const int* __re
 
 void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n,
                      const int* ntasks, const int* map, uint64_t seed, HeurWs& ws, int* pairs,
-                     int* npairs, cudaStream_t s) {
+                     int* npairs, cudaStream_t s, long long bound) {
   (void) m;
   ProfScope ps("match_handshake", s, 0.0);
-  const int g = grid_for(nb_elems);
+  const int g = grid_bounded(bound, nb_elems);
   cudaMemsetAsync(npairs, 0, sizeof(int), s);
   k_match_reset<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.mate, ws.prop);
   note_launch();

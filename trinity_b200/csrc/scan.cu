@@ -188,6 +188,10 @@ void compact_u8(const uint8_t* flags, int n, int* list, ScanWs& ws, cudaStream_t
   note_launch();
 }
 
+int grid_bounded(long long bound, long long cap, int threads) {
+  return grid_for(bound < 0 ? cap : (bound < cap ? bound : cap), threads);
+}
+
 int grid_for(long long n, int threads) {
   static const int sms = [] {
     int dev = 0, v = 0;

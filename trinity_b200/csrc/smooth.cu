@@ -93,7 +93,7 @@ __device__ int move_laplacian(const DMesh& m, int i) {
 }
 
 template <bool F32>
-__global__ void k_smooth_move(DMesh m, const int* __restrict__ list, int n, int* counters) {
+__global__ void __launch_bounds__(128, 6) k_smooth_move(DMesh m, const int* __restrict__ list, int n, int* counters) {
   if (trn_failed(m)) return;
   int tasks = 0, commit = 0;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) {

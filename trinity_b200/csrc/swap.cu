@@ -241,10 +241,10 @@ void swap_list_active(const DMesh& m, int nb_elems, int* act, int* act_n, cudaSt
 }
 
 void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,
-                      int* map, int* count, cudaStream_t s) {
+                      int* map, int* count, cudaStream_t s, long long bound) {
   ProfScope ps("swap_filter", s, 0.0);
   cudaMemsetAsync(count, 0, sizeof(int), s);
-  k_swap_filter_dual<<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, act, act_n, dual, dual_n, map,
+  k_swap_filter_dual<<<grid_bounded(bound, m.capa_elem), TRN_THREADS, 0, s>>>(m, act, act_n, dual, dual_n, map,
                                                                     count);
   note_launch();
   check_launch("swap_filter_dual");
@@ -252,13 +252,13 @@ void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dua
 
 void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* map,
                const int* dual, const int* dual_n, const int* ntasks, int* commit, bool strict_map,
-               bool fp32, cudaStream_t s) {
+               bool fp32, cudaStream_t s, long long bound) {
   ProfScope ps("swap_flip", s, 0.0);
   if (fp32)
-    k_swap_flip<true><<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
+    k_swap_flip<true><<<grid_bounded(bound, m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
                                                                    ntasks, commit, strict_map ? 1 : 0);
   else
-    k_swap_flip<false><<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
+    k_swap_flip<false><<<grid_bounded(bound, m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
                                                                     ntasks, commit, strict_map ? 1 : 0);
   note_launch();
   check_launch("swap_flip");

@@ -96,9 +96,9 @@ __global__ void k_fix_list(DMesh m, const int* __restrict__ list, const int* cou
   }
 }
 
-void fix_list(const DMesh& m, const int* list, const int* count, cudaStream_t s) {
+void fix_list(const DMesh& m, const int* list, const int* count, cudaStream_t s, long long bound) {
   ProfScope ps("fix_tagged", s, 0.0);
-  k_fix_list<<<grid_for(m.capa_node), TRN_THREADS, 0, s>>>(m, list, count);
+  k_fix_list<<<grid_bounded(bound, m.capa_node), TRN_THREADS, 0, s>>>(m, list, count);
   note_launch();
 }
 

@@ -754,6 +754,7 @@ int trn_coarsen_run(trn_mesh* m, int max_colors, trn_stats* st) {
     int* act[2] = {m->hws.list_a, m->hws.list_b};
     coarsen_list_active(m->d, m->nb_nodes, act[0], m->status + S_ACT, s);
     int ntasks = 0, cur = 0;
+    long long bound = m->nb_nodes;   /* listed vertices of this level, at most */
     do {
       DMesh dl = m->d;
       dl.act_next = act[cur ^ 1];
@@ -763,15 +764,16 @@ int trn_coarsen_run(trn_mesh* m, int max_colors, trn_stats* st) {
       CK(cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s));
       CK(cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s));
       coarsen_filter_append(dl, act[cur], m->status + S_ACT + cur, m->target, m->list,
-                            m->status + S_NTASK, m->hws.state, m->fp32, s);
+                            m->status + S_NTASK, m->hws.state, m->fp32, s, bound);
       mis_jp_rounds(dl, m->list, m->status + S_NTASK, kMisRounds, m->seed ^ (++m->calls * 0x9e37ULL),
-                    m->hws, m->indep, m->status + S_NINDEP, s);
-      collapse(dl, m->indep, m->status + S_NINDEP, m->target, nullptr, s);
-      fix_list(dl, dl.fix_list, dl.fix_n, s);
+                    m->hws, m->indep, m->status + S_NINDEP, s, bound);
+      collapse(dl, m->indep, m->status + S_NINDEP, m->target, nullptr, s, bound);
+      fix_list(dl, dl.fix_list, dl.fix_n, s, 16 * bound);
       int rc = sync_status(m);
       if (rc) return rc;
       ntasks = m->h_status[S_NTASK];
       nb_indep = m->h_status[S_NINDEP];
+      bound = m->h_status[S_ACT + (cur ^ 1)];
       eval += ntasks;
       task += nb_indep;
       cur ^= 1;
@@ -812,6 +814,8 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
   int eval = 0, task = 0, commit = 0, level = 0, cur = 0;
   int* act[2] = {m->hws.list_a, m->hws.list_b};
   if (!m->replay) swap_list_active(m->d, m->nb_elems, act[0], m->status + S_ACT, s);
+  long long bound = -1;   /* free mode: listed elements of this level, at most */
+  if (!m->replay) bound = m->nb_elems;
   do {
     int ntasks = 0;
     const int* pairs;
@@ -841,21 +845,25 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
       CK(cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s));
       CK(cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s));
       swap_filter_dual(dl, act[cur], m->status + S_ACT + cur, m->dual, m->dual_n, m->map,
-                       m->status + S_NTASK, s);
+                       m->status + S_NTASK, s, bound);
       match_handshake(dl, m->nb_elems, m->dual, m->dual_n, m->status + S_NTASK, m->map,
-                      m->seed ^ (++m->calls * 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s);
+                      m->seed ^ (++m->calls * 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s,
+                      bound);
       pairs = m->pairs;
       npairs = m->status + S_NPAIRS;
       ntasks_dev = m->status + S_NTASK;
     }
     CK(cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s));
     swap_flip(dl, pairs, npairs, m->map, m->dual, m->dual_n, ntasks_dev, m->status + S_COMMIT,
-              !m->replay, m->fp32, s);
+              !m->replay, m->fp32, s, bound);
     if (m->replay) fix_tagged(m->d, m->nb_nodes, s);
-    else fix_list(dl, dl.fix_list, dl.fix_n, s);
+    else fix_list(dl, dl.fix_list, dl.fix_n, s, 4 * bound);
     int rc = sync_status(m);
     if (rc) return rc;
-    if (!m->replay) ntasks = m->h_status[S_NTASK];
+    if (!m->replay) {
+      ntasks = m->h_status[S_NTASK];
+      bound = m->h_status[S_ACT + (cur ^ 1)];
+    }
     commit = m->h_status[S_COMMIT];
     eval += ntasks;
     task += commit / 2;

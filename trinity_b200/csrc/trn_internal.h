@@ -16,6 +16,10 @@ namespace trn {
 
 /* grid for a grid-stride kernel over n items: a multiple of the SM count */
 int grid_for(long long n, int threads = TRN_THREADS);
+/* grid for a kernel over a device-counted list: sized for `bound` items (an
+ * upper bound the host knows, < 0 = unknown) and at most `cap`; the kernels
+ * stride over the true count, so the bound only sizes the launch */
+int grid_bounded(long long bound, long long cap, int threads = TRN_THREADS);
 
 /* scratch used by the scans: tile sums of up to max_n items */
 struct ScanWs {
@@ -38,7 +42,8 @@ void build_stencils(const DMesh& m, int nb_nodes, int nb_elems, cudaStream_t s);
 void build_vicin(const DMesh& m, int nb_nodes, bool only_flagged, cudaStream_t s);
 void fix_tagged(const DMesh& m, int nb_nodes, cudaStream_t s);
 /* repair of the vertices listed in list[0..*count) */
-void fix_list(const DMesh& m, const int* list, const int* count, cudaStream_t s);
+void fix_list(const DMesh& m, const int* list, const int* count, cudaStream_t s,
+              long long bound = -1);
 void flag_all_alive(const DMesh& m, int nb_nodes, cudaStream_t s);
 void quality_all(const DMesh& m, int nb_elems, bool fp32, cudaStream_t s);
 /* recompute the per-vertex tensor-logarithm cache of the FP64 or FP32 form */
@@ -90,12 +95,13 @@ void refine_apply(const DMesh& m, int nb_nodes, int nb_elems, RefineWs& ws, bool
 void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
 void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, bool fp32, cudaStream_t s);
 void collapse(const DMesh& m, const int* indep, const int* count, const int* target,
-              const uint8_t* cand_flag, cudaStream_t s);
+              const uint8_t* cand_flag, cudaStream_t s, long long bound = -1);
 /* free mode: list the active vertices; then per level, over that list,
  * adjacency + target + unordered candidate append in one pass */
 void coarsen_list_active(const DMesh& m, int nb_nodes, int* act, int* act_n, cudaStream_t s);
 void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int* target, int* cand,
-                           int* count, uint8_t* state, bool fp32, cudaStream_t s);
+                           int* count, uint8_t* state, bool fp32, cudaStream_t s,
+                           long long bound = -1);
 
 /* swapping (swap.cu) */
 void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, bool fp32, cudaStream_t s);
@@ -104,12 +110,12 @@ void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual
                cudaStream_t s);
 void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* map,
                const int* dual, const int* dual_n, const int* ntasks, int* commit, bool strict_map,
-               bool fp32, cudaStream_t s);
+               bool fp32, cudaStream_t s, long long bound = -1);
 /* free mode: list the active elements; per level, filter and dual rows in
  * one pass over the list, *count rows */
 void swap_list_active(const DMesh& m, int nb_elems, int* act, int* act_n, cudaStream_t s);
 void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,
-                      int* map, int* count, cudaStream_t s);
+                      int* map, int* count, cudaStream_t s, long long bound = -1);
 
 /* smoothing (smooth.cu) */
 void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
@@ -134,11 +140,11 @@ void heur_ws_free(HeurWs* ws);
  * pairs[2k+1]; *npairs */
 void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n,
                      const int* ntasks, const int* map, uint64_t seed, HeurWs& ws, int* pairs,
-                     int* npairs, cudaStream_t s);
+                     int* npairs, cudaStream_t s, long long bound = -1);
 /* a fixed number of independent-set rounds over a device-counted candidate
  * list; undecided candidates are re-activated (next level) */
 void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, uint64_t seed,
-                   HeurWs& ws, int* indep, int* nindep, cudaStream_t s);
+                   HeurWs& ws, int* indep, int* nindep, cudaStream_t s, long long bound = -1);
 /* Jones-Plassmann first-fit coloring of interior vertices, colors 1..max_col;
  * parts: vertex ids grouped by color, part_off[c] offsets (c = 0..max_col) */
 void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& ws,
