@@ -185,10 +185,17 @@ void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* d
 }
 
 /* ---------------- coloring ---------------- */
-/* color word: 0 = uncolored, else (round + 1) << 8 | color, color 0xff = none */
-__global__ void k_color_init(DMesh m, int nb_nodes, int* list, int* n) {
-  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride())
+/* color word: 0 = uncolored, else (round + 1) << 8 | color, color 0xff =
+ * none. Vertices that take no part get kNotColored: to their neighbours a
+ * vertex colored in no round with a color outside the palette (bit 31 of the
+ * used-color mask, never a color), so a round reads one word per neighbour */
+constexpr int kNotColored = (0x7fffff << 8) | 31;
+
+__global__ void k_color_init(DMesh m, int nb_nodes, int* list, int* n, int* color) {
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
     if (m.activ[v] == 1 && m.vdeg[v] > 0) trn_append(list, n, v);
+    else color[v] = kNotColored;
+  }
 }
 
 /* one round over the still-uncolored vertices; those that must wait go to the
@@ -208,7 +215,6 @@ __global__ void k_color_round(DMesh m, const int* __restrict__ list, const int* 
     unsigned used = 0;
     for (int b = 0; b < nv; ++b) {
       const int w = vc[b];
-      if (m.activ[w] != 1 || m.vdeg[w] == 0) continue;
       const int cw = *(volatile int*) (color + w);
       const int rw = cw >> 8;
       if (cw == 0 || rw == round + 1) {
@@ -251,12 +257,30 @@ __global__ void k_color_offsets(const int* cnt, int* part_off, int* cursor, int 
   part_off[max_col] = acc;
 }
 
+/* vertices into their color's part; per block, the slots are counted in
+ * shared memory and reserved with one global atomic per color (a global
+ * atomic per vertex on at most 31 cursors serialises) */
 __global__ void k_color_scatter(int nb_nodes, int* color, int* cursor, int* parts, int max_col) {
-  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
-    int cw = color[v];
-    int c = cw & 0xff;
-    if (cw != 0 && c >= 1 && c <= max_col) parts[atomicAdd(cursor + c, 1)] = v;
-    color[v] = 0;
+  __shared__ int cnt[32], base[32];
+  for (int v0 = blockIdx.x * blockDim.x; v0 < nb_nodes; v0 += gridDim.x * blockDim.x) {
+    if (threadIdx.x < 32) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int v = v0 + threadIdx.x;
+    int c = 0, slot = 0;
+    if (v < nb_nodes) {
+      const int cw = color[v];
+      if (cw != 0 && (cw & 0xff) >= 1 && (cw & 0xff) <= max_col) {
+        c = cw & 0xff;
+        slot = atomicAdd(cnt + c, 1);
+      }
+      color[v] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x >= 1 && threadIdx.x <= max_col && cnt[threadIdx.x] > 0)
+      base[threadIdx.x] = atomicAdd(cursor + threadIdx.x, cnt[threadIdx.x]);
+    __syncthreads();
+    if (c) parts[base[c] + slot] = v;
+    __syncthreads();
   }
 }
 
@@ -267,7 +291,7 @@ void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& 
   int* lists[2] = {ws.list_a, ws.list_b};
   int* counts = ws.cnt + 80;  /* two list counters */
   cudaMemsetAsync(counts, 0, sizeof(int) * 2, s);
-  k_color_init<<<g, TRN_THREADS, 0, s>>>(m, nb_nodes, lists[0], counts);
+  k_color_init<<<g, TRN_THREADS, 0, s>>>(m, nb_nodes, lists[0], counts, ws.color);
   note_launch();
   int round = 0, cur = 0, host_left = 1;
   for (int batch = 0; batch < 8 && host_left; ++batch) {
