@@ -160,7 +160,20 @@ def b200_arm(args, rank, world, local_rank):
         run_step(api, g, c, heur, kern)
     torch.cuda.synchronize()
 
-    # ---- timed region (device-resident input) ----
+    # ---- per-kernel breakdown: untimed steps with every launch bracketed by
+    # CUDA events (the events cost ~9 % of throughput, so they stay out of
+    # the timed region except around the dominant kernel) ----
+    _lib.profile_enable(True)
+    for _ in range(min(args.steps, 2)):
+        g.reload()
+        run_step(api, g, c, heur, kern)
+    prof_all = _lib.profile_read()
+    _lib.profile_enable(False)
+    dom_name = max(prof_all, key=lambda r: r["ms"])["kernel"] if prof_all else None
+
+    # ---- timed region (device-resident input); CUDA events around the
+    # dominant kernel's launches only ----
+    _lib.profile_only(dom_name)
     _lib.profile_enable(True)
     launches0 = _lib.launch_count()
     tin_sum, tms_sum, metric_ms = 0, 0.0, []
@@ -180,6 +193,7 @@ def b200_arm(args, rank, world, local_rank):
     launches = _lib.launch_count() - launches0
     prof = _lib.profile_read()
     _lib.profile_enable(False)
+    _lib.profile_only(None)
     final = g.counts()
 
     # ---- the mixed-precision form on the same workload (reported beside) ----
@@ -248,7 +262,11 @@ def b200_arm(args, rank, world, local_rank):
                     "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
                     "traffic": None, "launches": dom["launches"],
                     "avg_launch_us": round(per_launch_s * 1e6, 2),
-                    "share_of_kernel_time": round(dom["ms"] / sum(r["ms"] for r in prof), 3)}
+                    "share_of_kernel_time": round(
+                        sum(r["ms"] for r in prof_all if r["kernel"] == dom["kernel"])
+                        / sum(r["ms"] for r in prof_all), 3),
+                    "timing": "CUDA events on the library stream around this kernel's launches "
+                              "during the timed steps; share from the profiled steps before"}
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -264,7 +282,8 @@ def b200_arm(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "roofline": roofline,
         "kernels": sorted(({"kernel": r["kernel"], "launches": r["launches"], "ms": round(r["ms"], 3)}
-                           for r in prof), key=lambda r: -r["ms"])[:8],
+                           for r in prof_all), key=lambda r: -r["ms"])[:10],
+        "kernels_note": f"{min(args.steps, 2)} profiled steps (every launch timed), before the timed region",
         "final_mesh": {"nodes": final[2], "triangles": final[3]},
         "clocks": clk.summary(),
     }

@@ -185,6 +185,9 @@ const char* trn_last_error(trn_mesh* mesh);
  * No counterpart in the reference (its timers are per-step wall clocks,
  * timer.h:42-48). */
 int trn_profile_enable(int on);
+/* time only the launches of the named kernel (NULL or "" = all): each timed
+ * launch adds two events to its stream, which costs throughput */
+int trn_profile_only(const char* name);
 int trn_profile_count(void);
 /* kernels launched by this library since the process started */
 unsigned long long trn_launch_count(void);

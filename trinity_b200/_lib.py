@@ -83,6 +83,7 @@ def lib():
         L.trn_profile_entry.argtypes = [ip, ctypes.c_char_p, ip, ctypes.POINTER(ctypes.c_longlong),
                                         ctypes.POINTER(dp), ctypes.POINTER(dp)]
         L.trn_launch_count.restype = ctypes.c_ulonglong
+        L.trn_profile_only.argtypes = [ctypes.c_char_p]
         L.trn_quality_adjoint.argtypes = [pmesh, vp, vp, dp, ip, dp, dp, ip, ctypes.POINTER(dp), vp, vp]
         L.trn_smooth_gradient_run.argtypes = [pmesh, ip, ip, dp, ip, sp]
         _lib = L
@@ -98,6 +99,11 @@ class TrinityError(RuntimeError):
 def profile_enable(on: bool) -> None:
     """Per-kernel device timing (process-wide); enabling resets the totals."""
     lib().trn_profile_enable(1 if on else 0)
+
+
+def profile_only(name: str | None) -> None:
+    """Time only the named kernel's launches (None = all)."""
+    lib().trn_profile_only(name.encode() if name else None)
 
 
 def profile_read() -> list[dict]:

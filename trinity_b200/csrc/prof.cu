@@ -6,6 +6,9 @@
  * the elapsed times are folded into per-kernel totals together with the
  * launcher's algorithmic byte count (distinct entries the launch must touch,
  * each counted once, no cache credit). Disabled, a scope costs one branch.
+ * Each timed scope records two events on the stream (about 1 us of device
+ * time each between launches), so a throughput measurement can restrict the
+ * timing to one kernel's scopes (trn_profile_only).
  */
 #include "trn_internal.h"
 
@@ -35,6 +38,7 @@ struct Total {
 struct Profiler {
   std::mutex mu;   /* meshes may run on several host threads */
   std::atomic<bool> on{false};
+  std::string only;   /* time only the scopes of this name ("" = all) */
   std::vector<cudaEvent_t> pool;
   std::vector<Pending> pending;
   std::vector<Total> totals;
@@ -70,6 +74,7 @@ ProfScope::ProfScope(const char* name, cudaStream_t s, double bytes) : stream_(s
   Profiler& p = prof();
   if (!p.on) return;
   std::lock_guard<std::mutex> lock(p.mu);
+  if (!p.only.empty() && p.only != name) return;
   id_ = p.id_of(name);
   bytes_ = bytes;
   a_ = p.get();
@@ -86,6 +91,7 @@ ProfScope::~ProfScope() {
 }
 
 static std::atomic<unsigned long long> g_launches{0};
+constexpr size_t kEventPool = 65536;
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
@@ -115,7 +121,24 @@ int trn_profile_enable(int on) {
   trn::prof_flush();
   std::lock_guard<std::mutex> lock(p.mu);
   p.on = on != 0;
-  if (on) p.totals.clear();
+  if (on) {
+    p.totals.clear();
+    /* events are created here, not inside the timed launches: a few
+     * thousand scopes per adaptation step, two events each */
+    while (p.pool.size() < trn::kEventPool) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) break;
+      p.pool.push_back(e);
+    }
+  }
+  return 0;
+}
+
+int trn_profile_only(const char* name) {
+  trn::Profiler& p = trn::prof();
+  trn::prof_flush();
+  std::lock_guard<std::mutex> lock(p.mu);
+  p.only = name ? name : "";
   return 0;
 }
 
