@@ -26,6 +26,7 @@
 namespace trn {
 
 __global__ void k_coarse_pre(DMesh m, int nb_nodes) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
     if (m.tags[v] & TRN_TAG_CORNER) m.activ[v] = -1;
     else m.activ[v] = m.alive[v] ? 1 : 0;
@@ -99,6 +100,7 @@ __device__ int identify_target(const DMesh& m, int source) {
 template <bool F32>
 __global__ void k_coarse_filter(DMesh m, int nb_nodes, int* __restrict__ target,
                                 uint8_t* __restrict__ flag) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   if (trn_failed(m)) return;
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
     uint8_t f = 0;
@@ -357,6 +359,7 @@ void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, bo
 }
 
 __global__ void k_coarse_list_active(DMesh m, int nb_nodes, int* act, int* act_n) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride())
     if (m.activ[v] > 0) trn_append(act, act_n, v);
 }

@@ -35,8 +35,10 @@ namespace trn {
  * from the previous round's buffer only (0 out / not a candidate,
  * 1 undecided, 2 in the set), so the outcome does not depend on timing */
 __global__ void k_mis_round_dev(DMesh m, const uint8_t* __restrict__ in, uint8_t* __restrict__ out,
-                                const int* __restrict__ cand, const int* count, uint64_t seed) {
+                                const int* __restrict__ cand, const int* count, Seed sd,
+                                uint64_t round_mix) {
   if (trn_failed(m)) return;
+  const uint64_t seed = trn_seed(sd) + round_mix;
   const int n = *count;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
     const int v = cand[q];
@@ -74,14 +76,14 @@ __global__ void k_mis_finish(DMesh m, uint8_t* state, uint8_t* other, const int*
   }
 }
 
-void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, uint64_t seed,
+void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, Seed sd,
                    HeurWs& ws, int* indep, int* nindep, cudaStream_t s, long long bound) {
   ProfScope ps("mis_jp", s, 0.0);
   const int g = grid_bounded(bound, m.capa_node);
   uint8_t* buf[2] = {ws.state, ws.state2};
   for (int r = 0; r < rounds; ++r) {
-    k_mis_round_dev<<<g, TRN_THREADS, 0, s>>>(m, buf[r & 1], buf[(r + 1) & 1], cand, count,
-                                               seed + 0x9e3779b97f4a7c15ULL * r);
+    k_mis_round_dev<<<g, TRN_THREADS, 0, s>>>(m, buf[r & 1], buf[(r + 1) & 1], cand, count, sd,
+                                               0x9e3779b97f4a7c15ULL * r);
     note_launch();
   }
   cudaMemsetAsync(nindep, 0, sizeof(int), s);
@@ -113,8 +115,9 @@ __global__ void k_match_reset(const int* __restrict__ dual, const int* __restric
 
 __global__ void k_match_propose(const int* __restrict__ dual, const int* __restrict__ dual_n,
                                 const int* ntasks_dev, const int* mate, unsigned long long* prop,
-                                int* choice, uint64_t seed, int round) {
+                                int* choice, Seed sd, int round) {
   const int ntasks = *ntasks_dev;
+  const uint64_t seed = trn_seed(sd);
   for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
     const int c = dual[i * 4];
     int best = -1;
@@ -134,8 +137,9 @@ __global__ void k_match_propose(const int* __restrict__ dual, const int* __restr
 
 __global__ void k_match_accept(const int* __restrict__ dual, const int* ntasks_dev,
                                const int* __restrict__ map, int* mate, const unsigned long long* prop,
-                               const int* choice, uint64_t seed, int round, int* pairs, int* npairs) {
+                               const int* choice, Seed sd, int round, int* pairs, int* npairs) {
   const int ntasks = *ntasks_dev;
+  const uint64_t seed = trn_seed(sd);
   for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
     const int n = choice[i];
     if (n < 0) continue;
@@ -163,7 +167,7 @@ __global__ void k_match_prop_clear(const int* __restrict__ dual, const int* __re
 }
 
 void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n,
-                     const int* ntasks, const int* map, uint64_t seed, HeurWs& ws, int* pairs,
+                     const int* ntasks, const int* map, Seed seed, HeurWs& ws, int* pairs,
                      int* npairs, cudaStream_t s, long long bound) {
   (void) m;
   ProfScope ps("match_handshake", s, 0.0);
@@ -192,6 +196,7 @@ void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* d
 constexpr int kNotColored = (0x7fffff << 8) | 31;
 
 __global__ void k_color_init(DMesh m, int nb_nodes, int* list, int* n, int* color) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
     if (m.activ[v] == 1 && m.vdeg[v] > 0) trn_append(list, n, v);
     else color[v] = kNotColored;
@@ -203,9 +208,11 @@ __global__ void k_color_init(DMesh m, int nb_nodes, int* list, int* n, int* colo
  * earlier rounds once its priority beats every neighbour still competing
  * (uncolored, or colored in this very round) */
 __global__ void k_color_round(DMesh m, const int* __restrict__ list, const int* n_in, int* color,
-                              int max_col, uint64_t seed, int round, int* next, int* n_next) {
+                              int max_col, Seed sd, const int* round_ctr, int* next, int* n_next) {
   if (trn_failed(m)) return;
   const int n = *n_in;
+  const uint64_t seed = trn_seed(sd);
+  const int round = *round_ctr;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
     const int v = list[q];
     const uint64_t pv = trn_prio(seed, v);
@@ -234,6 +241,7 @@ __global__ void k_color_round(DMesh m, const int* __restrict__ list, const int* 
 }
 
 __global__ void k_color_count(DMesh m, int nb_nodes, const int* color, int* cnt, int max_col) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   __shared__ int sc[32];
   if (threadIdx.x < 32) sc[threadIdx.x] = 0;
   __syncthreads();
@@ -246,8 +254,27 @@ __global__ void k_color_count(DMesh m, int nb_nodes, const int* color, int* cnt,
     atomicAdd(cnt + threadIdx.x, sc[threadIdx.x]);
 }
 
-__global__ void k_color_offsets(const int* cnt, int* part_off, int* cursor, int max_col) {
+/* before a round: its number, and the list it fills starts empty */
+__global__ void k_color_step(int* round_ctr, int* n_next) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  *round_ctr += 1;
+  *n_next = 0;
+}
+
+/* after 8 rounds: another batch while vertices wait and fewer than 8 batches
+ * ran; in a captured round the answer drives the loop node */
+__global__ void k_color_batch_end(const int* left, int* batch, int* cont,
+                                  cudaGraphConditionalHandle h, int use_h) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int c = (*left > 0) && (++*batch < 8);
+  *cont = c;
+  if (use_h) cudaGraphSetConditional(h, c);
+}
+
+__global__ void k_color_offsets(const int* cnt, int* part_off, int* cursor, int max_col,
+                                unsigned* tick) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (tick) ++*tick;
   int acc = 0;
   for (int c = 1; c <= max_col; ++c) {
     part_off[c - 1] = acc;
@@ -260,7 +287,9 @@ __global__ void k_color_offsets(const int* cnt, int* part_off, int* cursor, int 
 /* vertices into their color's part; per block, the slots are counted in
  * shared memory and reserved with one global atomic per color (a global
  * atomic per vertex on at most 31 cursors serialises) */
-__global__ void k_color_scatter(int nb_nodes, int* color, int* cursor, int* parts, int max_col) {
+__global__ void k_color_scatter(int nb_nodes, const int* nbp, int* color, int* cursor, int* parts,
+                                int max_col) {
+  if (nbp) nb_nodes = nbp[0];
   __shared__ int cnt[32], base[32];
   for (int v0 = blockIdx.x * blockDim.x; v0 < nb_nodes; v0 += gridDim.x * blockDim.x) {
     if (threadIdx.x < 32) cnt[threadIdx.x] = 0;
@@ -284,36 +313,67 @@ __global__ void k_color_scatter(int nb_nodes, int* color, int* cursor, int* part
   }
 }
 
-void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& ws, int* parts,
-              int* part_off, cudaStream_t s) {
+/* list counters and loop state of the coloring, in ws.cnt */
+static int* color_counts(HeurWs& ws) { return ws.cnt + 80; }   /* two list counters */
+static int* color_round(HeurWs& ws) { return ws.cnt + 82; }
+static int* color_batch_no(HeurWs& ws) { return ws.cnt + 83; }
+int* color_cont(HeurWs& ws) { return ws.cnt + 84; }
+
+void color_begin(const DMesh& m, int hint, HeurWs& ws, cudaStream_t s) {
   ProfScope ps("color_jp", s, 0.0);
-  const int g = grid_for(nb_nodes);
-  int* lists[2] = {ws.list_a, ws.list_b};
-  int* counts = ws.cnt + 80;  /* two list counters */
+  int* counts = color_counts(ws);
   cudaMemsetAsync(counts, 0, sizeof(int) * 2, s);
-  k_color_init<<<g, TRN_THREADS, 0, s>>>(m, nb_nodes, lists[0], counts, ws.color);
+  cudaMemsetAsync(color_round(ws), 0xff, sizeof(int), s);   /* -1: the first step makes it 0 */
+  cudaMemsetAsync(color_batch_no(ws), 0, sizeof(int), s);
+  k_color_init<<<grid_for(hint), TRN_THREADS, 0, s>>>(m, hint, ws.list_a, counts, ws.color);
   note_launch();
-  int round = 0, cur = 0, host_left = 1;
-  for (int batch = 0; batch < 8 && host_left; ++batch) {
-    for (int r = 0; r < 8; ++r, ++round, cur ^= 1) {
-      cudaMemsetAsync(counts + (cur ^ 1), 0, sizeof(int), s);
-      k_color_round<<<g, TRN_THREADS, 0, s>>>(m, lists[cur], counts + cur, ws.color, max_col, seed, round,
-                                              lists[cur ^ 1], counts + (cur ^ 1));
-      note_launch();
-    }
-    cudaMemcpyAsync(&host_left, counts + cur, sizeof(int), cudaMemcpyDeviceToHost, s);
-    cudaStreamSynchronize(s);
+}
+
+void color_batch(const DMesh& m, int hint, int max_col, Seed sd, HeurWs& ws, cudaStream_t s,
+                 cudaGraphConditionalHandle h, bool use_h) {
+  ProfScope ps("color_jp", s, 0.0);
+  const int g = grid_for(hint);
+  int* lists[2] = {ws.list_a, ws.list_b};
+  int* counts = color_counts(ws);
+  for (int r = 0; r < 8; ++r) {
+    const int cur = r & 1;
+    k_color_step<<<1, 32, 0, s>>>(color_round(ws), counts + (cur ^ 1));
+    note_launch();
+    k_color_round<<<g, TRN_THREADS, 0, s>>>(m, lists[cur], counts + cur, ws.color, max_col, sd,
+                                            color_round(ws), lists[cur ^ 1], counts + (cur ^ 1));
+    note_launch();
   }
+  /* an even number of rounds: the vertices still waiting are in list_a */
+  k_color_batch_end<<<1, 32, 0, s>>>(counts, color_batch_no(ws), color_cont(ws), h, use_h ? 1 : 0);
+  note_launch();
+}
+
+void color_finish(const DMesh& m, int hint, int max_col, HeurWs& ws, int* parts, int* part_off,
+                  unsigned* tick, cudaStream_t s) {
+  ProfScope ps("color_jp", s, 0.0);
+  const int g = grid_for(hint);
   int* cnt = ws.cnt + 4;      /* 32 slots */
   int* cursor = ws.cnt + 40;  /* 32 slots */
   cudaMemsetAsync(cnt, 0, sizeof(int) * 32, s);
-  k_color_count<<<g, TRN_THREADS, 0, s>>>(m, nb_nodes, ws.color, cnt, max_col);
+  k_color_count<<<g, TRN_THREADS, 0, s>>>(m, hint, ws.color, cnt, max_col);
   note_launch();
-  k_color_offsets<<<1, 32, 0, s>>>(cnt, part_off, cursor, max_col);
+  k_color_offsets<<<1, 32, 0, s>>>(cnt, part_off, cursor, max_col, tick);
   note_launch();
-  k_color_scatter<<<g, TRN_THREADS, 0, s>>>(nb_nodes, ws.color, cursor, parts, max_col);
+  k_color_scatter<<<g, TRN_THREADS, 0, s>>>(hint, m.nb, ws.color, cursor, parts, max_col);
   note_launch();
   check_launch("color_jp");
+}
+
+void color_jp(const DMesh& m, int hint, int max_col, Seed sd, HeurWs& ws, int* parts, int* part_off,
+              unsigned* tick, cudaStream_t s) {
+  color_begin(m, hint, ws, s);
+  int cont = 1;
+  while (cont) {
+    color_batch(m, hint, max_col, sd, ws, s, 0, false);
+    cudaMemcpyAsync(&cont, color_cont(ws), sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+  }
+  color_finish(m, hint, max_col, ws, parts, part_off, tick, s);
 }
 
 void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {

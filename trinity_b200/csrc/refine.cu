@@ -83,6 +83,7 @@ __device__ __forceinline__ int elem_neigh(const DMesh& m, int id, int i, int j) 
 template <bool F32>
 __global__ void k_ref_filter(DMesh m, int nb_elems, int4* __restrict__ info,
                              long long* __restrict__ cnt) {
+  nb_elems = trn_elems(m, nb_elems);
   if (trn_failed(m)) return;
   for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
     int4 t = m.tri[i];
@@ -115,6 +116,7 @@ template <bool F32>
 __global__ void k_ref_steiner(DMesh m, int nb_elems, int nb_nodes, const int4* __restrict__ info,
                               const long long* __restrict__ off, unsigned long long* hkey,
                               int* hval, unsigned long long hcap) {
+  nb_elems = trn_elems(m, nb_elems); nb_nodes = trn_nodes(m, nb_nodes);
   if (trn_failed(m)) return;
   for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
     int4 inf = info[i];
@@ -149,6 +151,7 @@ template <bool F32>
 __global__ void k_ref_cut(DMesh m, int nb_elems, const int4* __restrict__ info,
                           const long long* __restrict__ off, const unsigned long long* hkey,
                           const int* hval, unsigned long long hcap) {
+  nb_elems = trn_elems(m, nb_elems);
   if (trn_failed(m)) return;
   for (int id = trn_tid(); id < nb_elems; id += trn_grid_stride()) {
     int4 inf = info[id];
@@ -235,6 +238,46 @@ void refine_ws_free(RefineWs* ws) {
   cudaFree(ws->hkey);
   cudaFree(ws->hval);
   *ws = RefineWs();
+}
+
+/* before a level's splits: a level that would overflow the capacity raises
+ * the error word, and every later kernel of the call does nothing */
+__global__ void k_ref_check(DMesh m, const long long* total) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const long long tot = *total;
+  const long long split = tot >> 32, adds = tot & 0xffffffffLL;
+  if ((long long) m.nb[0] + split > m.capa_node || (long long) m.nb[1] + adds > m.capa_elem)
+    trn_set_error(m.err, TRN_DERR_CAPACITY);
+}
+
+/* after a level's splits: the new slot counts (new vertices and elements are
+ * numbered after the old ones) and the call's statistics in stats[0..2]:
+ * elements examined by each level up to the first that splits nothing,
+ * elements added, and that level's flag */
+__global__ void k_ref_commit(DMesh m, const long long* total, int* stats) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (trn_failed(m)) return;
+  const long long tot = *total;
+  const int split = (int) (tot >> 32), adds = (int) (tot & 0xffffffffLL);
+  if (!stats[2]) {
+    stats[0] += m.nb[1];
+    stats[1] += adds;
+    if (adds == 0) stats[2] = 1;
+  }
+  m.nb[0] += split;
+  m.nb[1] += adds;
+}
+
+void refine_level(const DMesh& m, int hint_nodes, int hint_elems, RefineWs& ws, ScanWs& scan,
+                  int* stats, bool fp32, cudaStream_t s) {
+  refine_filter(m, hint_elems, ws, fp32, s);
+  scan_i64(ws.cnt, ws.off, hint_elems, scan, s, m.nb + 1);
+  k_ref_check<<<1, 32, 0, s>>>(m, scan.total);
+  note_launch();
+  refine_apply(m, hint_nodes, hint_elems, ws, fp32, s);
+  k_ref_commit<<<1, 32, 0, s>>>(m, scan.total, stats);
+  note_launch();
+  check_launch("refine_level");
 }
 
 void refine_reset_hash(RefineWs& ws, cudaStream_t s) {

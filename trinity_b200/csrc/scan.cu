@@ -45,7 +45,9 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T* warp_sums, T* total) {
   return prefix;
 }
 
-__global__ void k_tile_sum_i64(const long long* __restrict__ in, int n, long long* tile) {
+__global__ void k_tile_sum_i64(const long long* __restrict__ in, int n, const int* dn,
+                               long long* tile) {
+  if (dn) n = *dn;
   __shared__ long long sm[kTile];
   __shared__ long long ws[TRN_THREADS / 32];
   const long long base = (long long) blockIdx.x * kTile;
@@ -98,7 +100,8 @@ __global__ void k_scan_tiles(long long* tile, int ntiles, long long* total64, in
 }
 
 __global__ void k_tile_scan_i64(const long long* __restrict__ in, long long* __restrict__ out,
-                                int n, const long long* tile) {
+                                int n, const int* dn, const long long* tile) {
+  if (dn) n = *dn;
   __shared__ long long sm[kTile];
   __shared__ long long ws[TRN_THREADS / 32];
   const long long base = (long long) blockIdx.x * kTile;
@@ -158,18 +161,18 @@ void scan_ws_free(ScanWs* ws) {
   *ws = ScanWs();
 }
 
-void scan_i64(const long long* in, long long* out, int n, ScanWs& ws, cudaStream_t s) {
+void scan_i64(const long long* in, long long* out, int n, ScanWs& ws, cudaStream_t s, const int* dn) {
   int ntiles = (n + kTile - 1) / kTile;
   if (ntiles == 0) {
     cudaMemsetAsync(ws.total, 0, sizeof(long long), s);
     return;
   }
   ProfScope ps("scan", s, (double) n * 16);
-  k_tile_sum_i64<<<ntiles, TRN_THREADS, 0, s>>>(in, n, ws.tile);
+  k_tile_sum_i64<<<ntiles, TRN_THREADS, 0, s>>>(in, n, dn, ws.tile);
   note_launch();
   k_scan_tiles<<<1, TRN_THREADS, 0, s>>>(ws.tile, ntiles, ws.total, nullptr);
   note_launch();
-  k_tile_scan_i64<<<ntiles, TRN_THREADS, 0, s>>>(in, out, n, ws.tile);
+  k_tile_scan_i64<<<ntiles, TRN_THREADS, 0, s>>>(in, out, n, dn, ws.tile);
   note_launch();
 }
 

@@ -22,6 +22,7 @@
 namespace trn {
 
 __global__ void k_smooth_pre(DMesh m, int nb_nodes) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride())
     if (m.alive[v]) m.activ[v] = (m.tags[v] & TRN_TAG_BOUND) ? 0 : 1;
 }
@@ -93,8 +94,13 @@ __device__ int move_laplacian(const DMesh& m, int i) {
 }
 
 template <bool F32>
-__global__ void __launch_bounds__(128, 6) k_smooth_move(DMesh m, const int* __restrict__ list, int n, int* counters) {
+__global__ void __launch_bounds__(128, 6) k_smooth_move(DMesh m, const int* __restrict__ list, int n,
+                                                       const int* off, int c, int* counters) {
   if (trn_failed(m)) return;
+  if (off) {   /* color class c of a device-side partition */
+    list += off[c];
+    n = off[c + 1] - off[c];
+  }
   int tasks = 0, commit = 0;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
     const int v = list[q];
@@ -117,8 +123,8 @@ void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s) {
   check_launch("smooth_pre");
 }
 
-void smooth_color(const DMesh& m, const int* list, int n, int* counters, bool fp32, cudaStream_t s) {
-  if (n <= 0) return;
+static void smooth_launch(const DMesh& m, const int* list, int n, const int* off, int c, int hint,
+                          int* counters, bool fp32, cudaStream_t s) {
   /* per moved vertex: list id, flag, counts, own point/tensor read+write,
    * stencil and adjacency rows, its elements and their cached qualities
    * (read+write); neighbours' points/tensors once each (at most 6 per vertex,
@@ -126,10 +132,20 @@ void smooth_color(const DMesh& m, const int* list, int n, int* counters, bool fp
   const double own = 4 + 1 + 8 + 2 * (kPt + kTen) + kAvgDeg * (2 * kIdx + kTri + 2 * kQ);
   const double nbr = (double) std::min<long long>((long long) m.capa_node, 6LL * n) * (kPt + kTen);
   ProfScope ps("smooth_move", s, n * own + nbr);
-  if (fp32) k_smooth_move<true><<<grid_for(n, 128), 128, 0, s>>>(m, list, n, counters);
-  else k_smooth_move<false><<<grid_for(n, 128), 128, 0, s>>>(m, list, n, counters);
+  if (fp32) k_smooth_move<true><<<grid_for(hint, 128), 128, 0, s>>>(m, list, n, off, c, counters);
+  else k_smooth_move<false><<<grid_for(hint, 128), 128, 0, s>>>(m, list, n, off, c, counters);
   note_launch();
-  check_launch("smooth_color");
+  check_launch("smooth_move");
+}
+
+void smooth_color(const DMesh& m, const int* list, int n, int* counters, bool fp32, cudaStream_t s) {
+  if (n <= 0) return;
+  smooth_launch(m, list, n, nullptr, 0, n, counters, fp32, s);
+}
+
+void smooth_class(const DMesh& m, const int* parts, const int* part_off, int c, int hint, int* counters,
+                  bool fp32, cudaStream_t s) {
+  smooth_launch(m, parts, hint, part_off, c, hint, counters, fp32, s);
 }
 
 }  // namespace trn

@@ -24,11 +24,13 @@
 namespace trn {
 
 __global__ void k_swap_init_nodes(DMesh m, int nb_nodes) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) m.fixes[v] = 0;
 }
 
 template <bool F32>
 __global__ void k_swap_init_elems(DMesh m, int nb_elems, int* __restrict__ map) {
+  nb_elems = trn_elems(m, nb_elems);
   if (trn_failed(m)) return;
   for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
     map[i] = -1;
@@ -43,6 +45,7 @@ __global__ void k_swap_init_elems(DMesh m, int nb_elems, int* __restrict__ map) 
 }
 
 __global__ void k_swap_filter(DMesh m, int nb_elems, uint8_t* __restrict__ flag) {
+  nb_elems = trn_elems(m, nb_elems);
   for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
     uint8_t f = 0;
     if (m.activ[i]) {
@@ -230,6 +233,7 @@ void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual
 }
 
 __global__ void k_swap_list_active(DMesh m, int nb_elems, int* act, int* act_n) {
+  nb_elems = trn_elems(m, nb_elems);
   for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride())
     if (m.activ[i]) trn_append(act, act_n, i);
 }

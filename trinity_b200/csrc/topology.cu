@@ -39,6 +39,7 @@ __global__ void k_sort_stencils(DMesh m, int nb_nodes) {
 }
 
 __global__ void k_build_vicin(DMesh m, int nb_nodes, int only_flagged) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   if (trn_failed(m)) return;
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
     if (only_flagged && m.activ[v] == 0) continue;
@@ -47,6 +48,7 @@ __global__ void k_build_vicin(DMesh m, int nb_nodes, int only_flagged) {
 }
 
 __global__ void k_fix_tagged(DMesh m, int nb_nodes) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   if (trn_failed(m)) return;
   int buf[TRN_MAX_DEG];
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
@@ -103,12 +105,14 @@ void fix_list(const DMesh& m, const int* list, const int* count, cudaStream_t s,
 }
 
 __global__ void k_flag_alive(DMesh m, int nb_nodes) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) m.fixes[v] = m.alive[v] ? 1 : 0;
 }
 
 /* cached quality of every live element (swapping.cpp:167-174, smoothing.cpp:145-151) */
 template <bool F32>
 __global__ void k_quality_all(DMesh m, int nb_elems) {
+  nb_elems = trn_elems(m, nb_elems);
   if (trn_failed(m)) return;
   for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
     int4 t = m.tri[i];
@@ -238,6 +242,7 @@ void flag_all_alive(const DMesh& m, int nb_nodes, cudaStream_t s) {
 
 /* the per-vertex logarithm cache of the FP32 form, from the stored tensors */
 __global__ void k_log_cache_f32(DMesh m, int nb_nodes) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
     const double4 t = m.ten[v];
     log_store<true>(m, v, log_of<true>(t.x, t.y, t.z));
@@ -245,6 +250,7 @@ __global__ void k_log_cache_f32(DMesh m, int nb_nodes) {
 }
 
 __global__ void k_log_cache_f64(DMesh m, int nb_nodes) {
+  nb_nodes = trn_nodes(m, nb_nodes);
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
     const double4 t = m.ten[v];
     m.lten[v] = trn_log_tensor(t.x, t.y, t.z);

@@ -23,26 +23,13 @@ using namespace trn;
 
 namespace {
 
-/* status block layout (device and pinned host mirror) */
+/* host-only part of the pinned status mirror (after the device block) */
 enum {
-  S_ERR = 0,
-  S_COMMIT = 1,
-  S_SMOOTH_TASKS = 2,
-  S_SMOOTH_COMMIT = 3,
-  S_NPAIRS = 4,
-  S_NINDEP = 5,
-  S_COUNT = 6,     /* copy of a compaction count */
-  S_PARTS = 8,     /* part offsets, 9 slots */
-  S_LIVE = 18,     /* live vertices, live elements */
-  S_NTASK = 20,    /* device-counted candidates of a level (free mode) */
-  S_ACT = 22,      /* two activity-list counters (free mode) */
-  S_FIX = 24,      /* repair-list counter (free mode) */
-  S_SIZE = 32,     /* device status block */
   H_WIDE = 40,     /* host-only pinned slot for one 8-byte value */
   H_SIZE = 64,
 };
 
-constexpr int kLoopCap = 100000;
+constexpr int kLoopCap = kLevelCap;
 constexpr int kMisRounds = 8;   /* independent-set rounds per coarsening level (free mode) */
 
 }  // namespace
@@ -86,7 +73,6 @@ struct trn_mesh {
   size_t cursor = 0;
   /* options */
   uint64_t seed = 0x7472696e697479ULL;
-  uint64_t calls = 0;
   bool exact_sum = false;
   bool fp32 = false;   /* mixed-precision form of the metric arithmetic */
   double last_complexity = 0.0;
@@ -118,11 +104,13 @@ int sync_status(trn_mesh* m, const int* count = nullptr) {
   prof_flush();
   int e = m->h_status[S_ERR];
   if (e) {
-    const char* what = e == TRN_DERR_CAPACITY ? "capacity exceeded (stencil bucket, hash or patch)"
-                       : e == TRN_DERR_REPLAY  ? "replay log does not match the mesh"
-                                               : "invalid state";
-    return fail(m, e == TRN_DERR_CAPACITY ? TRN_ERR_CAPACITY
-                   : e == TRN_DERR_REPLAY ? TRN_ERR_REPLAY : TRN_ERR_INVALID,
+    const char* what = e == TRN_DERR_CAPACITY      ? "capacity exceeded (nodes, elements, stencil bucket, hash or patch)"
+                       : e == TRN_DERR_REPLAY      ? "replay log does not match the mesh"
+                       : e == TRN_DERR_NO_PROGRESS ? "level cap reached"
+                                                   : "invalid state";
+    return fail(m, e == TRN_DERR_CAPACITY      ? TRN_ERR_CAPACITY
+                   : e == TRN_DERR_REPLAY      ? TRN_ERR_REPLAY
+                   : e == TRN_DERR_NO_PROGRESS ? TRN_ERR_NO_PROGRESS : TRN_ERR_INVALID,
                 std::string("device: ") + what);
   }
   return TRN_OK;
@@ -312,6 +300,7 @@ int trn_mesh_create_ex(const int size[2], int bucket, int depth, int verbosity, 
       (rc = dmalloc(m, &m->status, S_SIZE)))
     return bail(rc);
   d.err = m->status + S_ERR;
+  d.nb = m->status + S_NB;
   if (cudaMallocHost(&m->h_status, sizeof(int) * H_SIZE) != cudaSuccess) return bail(TRN_ERR_CUDA);
   scan_ws_alloc(&m->scan, (long long) std::max(cn, ce));
   refine_ws_alloc(&m->rws, m->capa_node, m->capa_elem);
@@ -353,6 +342,8 @@ static int init_from_device(trn_mesh* m) {
   CK(cudaMemsetAsync(d.activ, 0, std::max(cn, ce), s));
   CK(cudaMemsetAsync(d.qual, 0, sizeof(double) * ce, s));
   CK(cudaMemsetAsync(m->status, 0, sizeof(int) * S_SIZE, s));
+  const int counts[2] = {nb_nodes, nb_elems};
+  CK(cudaMemcpyAsync(m->status + S_NB, counts, sizeof(counts), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(m->map, 0xff, sizeof(int) * ce, s));
   CK(cudaMemcpyAsync(d.pts, m->pts0, sizeof(double2) * (size_t) nb_nodes, cudaMemcpyDeviceToDevice, s));
   CK(cudaMemcpyAsync(d.tri, m->tri0, sizeof(int4) * (size_t) nb_elems, cudaMemcpyDeviceToDevice, s));
@@ -705,38 +696,115 @@ int trn_metric_run(trn_mesh* m, double target_factor, int norm, double h_min, do
   return end_timing(m, st, m->nb_nodes, m->nb_nodes);
 }
 
+/* ---------------- stage enqueuers ----------------
+ * The same kernels serve the per-stage calls below (the host reads the status
+ * block back once per coarsening / swapping level, or per coloring batch) and
+ * a captured round (trn_round_capture: loop nodes decide on the device).
+ * Every count a kernel needs is on the device (S_NB, list counters); the host
+ * only sizes grids: by its own copy of a count, or, in a captured round, by
+ * the capacity. */
+namespace {
+
+int hint_nodes(const trn_mesh* m, bool capture) { return capture ? m->capa_node : m->nb_nodes; }
+int hint_elems(const trn_mesh* m, bool capture) { return capture ? m->capa_elem : m->nb_elems; }
+
+Seed seed_of(trn_mesh* m, uint64_t mix) {
+  return Seed{m->seed, reinterpret_cast<const unsigned*>(m->status + S_TICK), mix};
+}
+
+void stats_reset(trn_mesh* m, cudaStream_t s) {
+  cudaMemsetAsync(m->status + S_EVAL, 0, sizeof(int) * 3, s);
+  cudaMemsetAsync(m->status + S_LEVEL, 0, sizeof(int), s);
+}
+
+int* act_list(trn_mesh* m, int k) { return k ? m->hws.list_b : m->hws.list_a; }
+
+DMesh level_mesh(trn_mesh* m) {
+  DMesh dl = m->d;
+  dl.act_next = act_list(m, 1);
+  dl.act_next_n = m->status + S_ACT + 1;
+  dl.fix_list = m->hws.fix_list;
+  dl.fix_n = m->status + S_FIX;
+  return dl;
+}
+
+/* Refine::run: depth levels, every count on the device (refine.cu) */
+void enq_refine(trn_mesh* m, int depth, cudaStream_t s) {
+  stats_reset(m, s);
+  refine_reset_hash(m->rws, s);
+  for (int level = 0; level < depth; ++level)
+    refine_level(m->d, m->capa_node, m->capa_elem, m->rws, m->scan, m->status + S_EVAL, m->fp32, s);
+  flag_all_alive(m->d, m->capa_node, s);
+  fix_tagged(m->d, m->capa_node, s);
+}
+
+void enq_coarsen_begin(trn_mesh* m, cudaStream_t s, bool capture) {
+  stats_reset(m, s);
+  coarsen_pre(m->d, hint_nodes(m, capture), s);
+  coarsen_list_active(m->d, hint_nodes(m, capture), act_list(m, 0), m->status + S_ACT, s);
+}
+
+/* one free-mode coarsening level over list 0 (bound: its length, < 0 unknown) */
+void enq_coarsen_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphConditionalHandle h,
+                       bool use_h) {
+  DMesh dl = level_mesh(m);
+  cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s);
+  cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s);
+  coarsen_filter_append(dl, act_list(m, 0), m->status + S_ACT, m->target, m->list, m->status + S_NTASK,
+                        m->hws.state, m->fp32, s, bound);
+  mis_jp_rounds(dl, m->list, m->status + S_NTASK, kMisRounds, seed_of(m, 0x9e37ULL), m->hws, m->indep,
+                m->status + S_NINDEP, s, bound);
+  collapse(dl, m->indep, m->status + S_NINDEP, m->target, nullptr, s, bound);
+  fix_list(dl, dl.fix_list, dl.fix_n, s, bound < 0 ? -1 : 16 * bound);
+  level_end(m->status, kLevelCoarsen, kLoopCap, act_list(m, 1), act_list(m, 0),
+            bound < 0 ? m->capa_node : (int) std::max(bound, 1LL), s, h, use_h);
+}
+
+void enq_swap_begin(trn_mesh* m, cudaStream_t s, bool capture) {
+  stats_reset(m, s);
+  swap_init(m->d, hint_nodes(m, capture), hint_elems(m, capture), m->map, m->fp32, s);
+  swap_list_active(m->d, hint_elems(m, capture), act_list(m, 0), m->status + S_ACT, s);
+}
+
+void enq_swap_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphConditionalHandle h,
+                    bool use_h) {
+  DMesh dl = level_mesh(m);
+  cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s);
+  cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s);
+  swap_filter_dual(dl, act_list(m, 0), m->status + S_ACT, m->dual, m->dual_n, m->map,
+                   m->status + S_NTASK, s, bound);
+  match_handshake(dl, m->capa_elem, m->dual, m->dual_n, m->status + S_NTASK, m->map,
+                  seed_of(m, 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s, bound);
+  cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s);
+  swap_flip(dl, m->pairs, m->status + S_NPAIRS, m->map, m->dual, m->dual_n, m->status + S_NTASK,
+            m->status + S_COMMIT, true, m->fp32, s, bound);
+  fix_list(dl, dl.fix_list, dl.fix_n, s, bound < 0 ? -1 : 4 * bound);
+  level_end(m->status, kLevelSwap, kLoopCap, act_list(m, 1), act_list(m, 0),
+            bound < 0 ? m->capa_elem : (int) std::max(bound, 1LL), s, h, use_h);
+}
+
+int max_colors_of(int max_colors) {
+  int max_col = std::max(6, max_colors) - 1;  /* Partit: max.part = max(6, n), colors 1..max.part-1 */
+  return std::min(max_col, 30);
+}
+
+}  // namespace
+
 /* Refine::run, refinement.cpp:445-493 */
 int trn_refine_run(trn_mesh* m, int depth, trn_stats* st) {
   if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "refine: no mesh loaded");
   if (depth < 1) return fail(m, TRN_ERR_INVALID, "refine: depth < 1");
   m->err.clear();
   begin_timing(m);
-  cudaStream_t s = m->stream;
-  refine_reset_hash(m->rws, s);
-  int eval = 0, task = 0;
-  for (int level = 0; level < depth; ++level) {
-    refine_filter(m->d, m->nb_elems, m->rws, m->fp32, s);
-    scan_i64(m->rws.cnt, m->rws.off, m->nb_elems, m->scan, s);
-    long long tot = 0;
-    CK(cudaMemcpyAsync(m->h_status + H_WIDE, m->scan.total, sizeof(long long), cudaMemcpyDeviceToHost, s));
-    int rc = sync_status(m);
-    if (rc) return rc;
-    std::memcpy(&tot, m->h_status + H_WIDE, sizeof(long long));
-    const int split = (int) (tot >> 32), adds = (int) (tot & 0xffffffffLL);
-    eval += m->nb_elems;
-    if (adds == 0) break;
-    task += adds;
-    if ((long long) m->nb_nodes + split > m->capa_node || (long long) m->nb_elems + adds > m->capa_elem)
-      return fail(m, TRN_ERR_CAPACITY, "refine: node or element capacity exceeded");
-    refine_apply(m->d, m->nb_nodes, m->nb_elems, m->rws, m->fp32, s);
-    m->nb_nodes += split;
-    m->nb_elems += adds;
-  }
-  flag_all_alive(m->d, m->nb_nodes, s);
-  fix_tagged(m->d, m->nb_nodes, s);
+  enq_refine(m, depth, m->stream);
   int rc = sync_status(m);
-  if (rc) return rc;
-  return end_timing(m, st, eval, task);
+  if (rc) {
+    if (rc == TRN_ERR_CAPACITY) m->err = "refine: node or element capacity exceeded";
+    return rc;
+  }
+  m->nb_nodes = m->h_status[S_NB];
+  m->nb_elems = m->h_status[S_NB + 1];
+  return end_timing(m, st, m->h_status[S_EVAL], m->h_status[S_TASK]);
 }
 
 /* Coarse::run, coarsening.cpp:463-508 */
@@ -746,41 +814,21 @@ int trn_coarsen_run(trn_mesh* m, int max_colors, trn_stats* st) {
   m->err.clear();
   begin_timing(m);
   cudaStream_t s = m->stream;
-  coarsen_pre(m->d, m->nb_nodes, s);
-  int eval = 0, task = 0, nb_indep = 0, level = 0;
   if (!m->replay) {
-    /* free mode: one host synchronisation per level; each level works on the
-     * list of vertices the previous one activated, repairs the listed ones */
-    int* act[2] = {m->hws.list_a, m->hws.list_b};
-    coarsen_list_active(m->d, m->nb_nodes, act[0], m->status + S_ACT, s);
-    int ntasks = 0, cur = 0;
-    long long bound = m->nb_nodes;   /* listed vertices of this level, at most */
+    /* free mode: one read back per level; each level works on the list of
+     * vertices the previous one activated and repairs the listed ones */
+    enq_coarsen_begin(m, s, false);
+    long long bound = m->nb_nodes;
     do {
-      DMesh dl = m->d;
-      dl.act_next = act[cur ^ 1];
-      dl.act_next_n = m->status + S_ACT + (cur ^ 1);
-      dl.fix_list = m->hws.fix_list;
-      dl.fix_n = m->status + S_FIX;
-      CK(cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s));
-      CK(cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s));
-      coarsen_filter_append(dl, act[cur], m->status + S_ACT + cur, m->target, m->list,
-                            m->status + S_NTASK, m->hws.state, m->fp32, s, bound);
-      mis_jp_rounds(dl, m->list, m->status + S_NTASK, kMisRounds, m->seed ^ (++m->calls * 0x9e37ULL),
-                    m->hws, m->indep, m->status + S_NINDEP, s, bound);
-      collapse(dl, m->indep, m->status + S_NINDEP, m->target, nullptr, s, bound);
-      fix_list(dl, dl.fix_list, dl.fix_n, s, 16 * bound);
+      enq_coarsen_level(m, s, bound, 0, false);
       int rc = sync_status(m);
       if (rc) return rc;
-      ntasks = m->h_status[S_NTASK];
-      nb_indep = m->h_status[S_NINDEP];
-      bound = m->h_status[S_ACT + (cur ^ 1)];
-      eval += ntasks;
-      task += nb_indep;
-      cur ^= 1;
-      if (++level > kLoopCap) return fail(m, TRN_ERR_NO_PROGRESS, "coarsen: level cap reached");
-    } while (ntasks && nb_indep);
-    return end_timing(m, st, eval, task);
+      bound = m->h_status[S_ACT];
+    } while (m->h_status[S_CONT]);
+    return end_timing(m, st, m->h_status[S_EVAL], m->h_status[S_TASK]);
   }
+  coarsen_pre(m->d, m->nb_nodes, s);
+  int eval = 0, task = 0, nb_indep = 0, level = 0;
   do {
     build_vicin(m->d, m->nb_nodes, true, s);
     coarsen_filter(m->d, m->nb_nodes, m->target, m->flag, m->fp32, s);
@@ -810,64 +858,38 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
   m->err.clear();
   begin_timing(m);
   cudaStream_t s = m->stream;
-  swap_init(m->d, m->nb_nodes, m->nb_elems, m->map, m->fp32, s);
-  int eval = 0, task = 0, commit = 0, level = 0, cur = 0;
-  int* act[2] = {m->hws.list_a, m->hws.list_b};
-  if (!m->replay) swap_list_active(m->d, m->nb_elems, act[0], m->status + S_ACT, s);
-  long long bound = -1;   /* free mode: listed elements of this level, at most */
-  if (!m->replay) bound = m->nb_elems;
-  do {
-    int ntasks = 0;
-    const int* pairs;
-    const int* npairs;
-    const int* ntasks_dev;
-    DMesh dl = m->d;
-    if (m->replay) {
-      swap_filter(m->d, m->nb_elems, m->flag, s);
-      compact_u8(m->flag, m->nb_elems, m->list, m->scan, s);
-      int rc = sync_status(m, m->scan.count);
+  if (!m->replay) {
+    enq_swap_begin(m, s, false);
+    long long bound = m->nb_elems;
+    do {
+      enq_swap_level(m, s, bound, 0, false);
+      int rc = sync_status(m);
       if (rc) return rc;
-      ntasks = m->h_status[S_COUNT];
-      if (!ntasks) break;
-      swap_dual(m->d, m->list, ntasks, m->dual, m->dual_n, m->map, s);
-      size_t off;
-      int n;
-      if ((rc = replay_take(m, 2, &off, &n))) return rc;
-      pairs = m->d_log + off;
-      npairs = m->d_log + off - 1;
-      ntasks_dev = m->scan.count;
-    } else {
-      /* free mode: one host synchronisation per level, list-driven */
-      dl.act_next = act[cur ^ 1];
-      dl.act_next_n = m->status + S_ACT + (cur ^ 1);
-      dl.fix_list = m->hws.fix_list;
-      dl.fix_n = m->status + S_FIX;
-      CK(cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s));
-      CK(cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s));
-      swap_filter_dual(dl, act[cur], m->status + S_ACT + cur, m->dual, m->dual_n, m->map,
-                       m->status + S_NTASK, s, bound);
-      match_handshake(dl, m->nb_elems, m->dual, m->dual_n, m->status + S_NTASK, m->map,
-                      m->seed ^ (++m->calls * 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s,
-                      bound);
-      pairs = m->pairs;
-      npairs = m->status + S_NPAIRS;
-      ntasks_dev = m->status + S_NTASK;
-    }
-    CK(cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s));
-    swap_flip(dl, pairs, npairs, m->map, m->dual, m->dual_n, ntasks_dev, m->status + S_COMMIT,
-              !m->replay, m->fp32, s, bound);
-    if (m->replay) fix_tagged(m->d, m->nb_nodes, s);
-    else fix_list(dl, dl.fix_list, dl.fix_n, s, 4 * bound);
-    int rc = sync_status(m);
+      bound = m->h_status[S_ACT];
+    } while (m->h_status[S_CONT]);
+    return end_timing(m, st, m->h_status[S_EVAL], m->h_status[S_TASK]);
+  }
+  swap_init(m->d, m->nb_nodes, m->nb_elems, m->map, m->fp32, s);
+  int eval = 0, task = 0, commit = 0, level = 0;
+  do {
+    swap_filter(m->d, m->nb_elems, m->flag, s);
+    compact_u8(m->flag, m->nb_elems, m->list, m->scan, s);
+    int rc = sync_status(m, m->scan.count);
     if (rc) return rc;
-    if (!m->replay) {
-      ntasks = m->h_status[S_NTASK];
-      bound = m->h_status[S_ACT + (cur ^ 1)];
-    }
+    const int ntasks = m->h_status[S_COUNT];
+    if (!ntasks) break;
+    swap_dual(m->d, m->list, ntasks, m->dual, m->dual_n, m->map, s);
+    size_t off;
+    int n;
+    if ((rc = replay_take(m, 2, &off, &n))) return rc;
+    CK(cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s));
+    swap_flip(m->d, m->d_log + off, m->d_log + off - 1, m->map, m->dual, m->dual_n, m->scan.count,
+              m->status + S_COMMIT, false, m->fp32, s);
+    fix_tagged(m->d, m->nb_nodes, s);
+    if ((rc = sync_status(m))) return rc;
     commit = m->h_status[S_COMMIT];
     eval += ntasks;
     task += commit / 2;
-    cur ^= 1;
     if (++level > kLoopCap) return fail(m, TRN_ERR_NO_PROGRESS, "swap: level cap reached");
   } while (commit);
   return end_timing(m, st, eval, task);
@@ -876,8 +898,7 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
 /* Smooth::run, smoothing.cpp:274-302 */
 int trn_smooth_run(trn_mesh* m, int max_colors, int depth, trn_stats* st) {
   if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "smooth: no mesh loaded");
-  int max_col = std::max(6, max_colors) - 1;  /* Partit: max.part = max(6, n), colors 1..max.part-1 */
-  if (max_col > 30) max_col = 30;
+  const int max_col = max_colors_of(max_colors);
   m->err.clear();
   begin_timing(m);
   cudaStream_t s = m->stream;
@@ -896,8 +917,8 @@ int trn_smooth_run(trn_mesh* m, int max_colors, int depth, trn_stats* st) {
       p += 1 + (size_t) n;
     }
   } else {
-    color_jp(m->d, m->nb_nodes, max_col, m->seed ^ (++m->calls * 0xc01dULL), m->hws, m->parts,
-             m->status + S_PARTS, s);
+    color_jp(m->d, m->nb_nodes, max_col, seed_of(m, 0xc01dULL), m->hws, m->parts, m->status + S_PARTS,
+             reinterpret_cast<unsigned*>(m->status + S_TICK), s);
     int rc = sync_status(m);
     if (rc) return rc;
     for (int c = 0; c < max_col && c < 8; ++c) {
@@ -968,8 +989,8 @@ int trn_smooth_gradient_run(trn_mesh* m, int max_colors, int steps, double max_l
   cudaStream_t s = m->stream;
   smooth_pre(m->d, m->nb_nodes, s);
   build_vicin(m->d, m->nb_nodes, true, s);
-  color_jp(m->d, m->nb_nodes, max_col, m->seed ^ (++m->calls * 0xc01dULL), m->hws, m->parts,
-           m->status + S_PARTS, s);
+  color_jp(m->d, m->nb_nodes, max_col, seed_of(m, 0xc01dULL), m->hws, m->parts, m->status + S_PARTS,
+           reinterpret_cast<unsigned*>(m->status + S_TICK), s);
   int rc = sync_status(m);
   if (rc) return rc;
   std::vector<std::pair<const int*, int>> classes;

@@ -30,6 +30,7 @@
 /* device error word values (mirror the C-ABI codes) */
 #define TRN_DERR_CAPACITY 1
 #define TRN_DERR_INVALID 3
+#define TRN_DERR_NO_PROGRESS 4
 #define TRN_DERR_REPLAY 6
 
 /* per-thread scratch limits (local memory) */
@@ -53,6 +54,8 @@ struct DMesh {
   int8_t* activ;
   double* qual;
   int* err;        /* device error word: first error wins */
+  int* nb;         /* device slot counts {vertices, elements}, NULL = the
+                      launch arguments are the counts */
   /* free-mode worklists (NULL in replay): ids whose activity flag turns
    * 0 -> 1 are appended to act_next, vertices tagged for repair to fix_list */
   int* act_next;
@@ -102,6 +105,11 @@ __device__ __forceinline__ void trn_activate(const DMesh& m, int id) {
 __device__ __forceinline__ bool trn_failed(const DMesh& m) {
   return *(volatile int*) m.err != 0;
 }
+
+/* slot counts: the device copy when the mesh keeps one (it changes on the
+ * device during a round), else the count the launch was given */
+__device__ __forceinline__ int trn_nodes(const DMesh& m, int given) { return m.nb ? m.nb[0] : given; }
+__device__ __forceinline__ int trn_elems(const DMesh& m, int given) { return m.nb ? m.nb[1] : given; }
 
 /* used stencil length of v, never beyond its bucket (an overflowing append
  * only raises the error word, so the counter itself may exceed it) */
@@ -211,6 +219,18 @@ __device__ __forceinline__ void trn_append(int* list, int* count, int id) {
   if (lane == leader) base = atomicAdd(count, __popc(mask));
   base = __shfl_sync(mask, base, leader);
   list[base + __popc(mask & ((1u << lane) - 1))] = id;
+}
+
+/* seed of a level's hashed priorities: base ^ (tick * mix), tick a device
+ * counter that each coarsening / swapping level and each coloring advances,
+ * so the seed sequence lives on the device (a captured round replays it) */
+struct Seed {
+  uint64_t base;
+  const unsigned* tick;
+  uint64_t mix;
+};
+__device__ __forceinline__ uint64_t trn_seed(const Seed& s) {
+  return s.base ^ ((uint64_t) (s.tick ? *s.tick : 0u) * s.mix);
 }
 
 /* 64-bit mix for seeded hash priorities (splitmix64 finaliser) */

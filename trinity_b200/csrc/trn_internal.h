@@ -14,6 +14,39 @@
 
 namespace trn {
 
+/* the per-mesh status block: device words the kernels count into, mirrored
+ * to pinned host memory at each synchronisation */
+enum StatusSlot {
+  S_ERR = 0,
+  S_COMMIT = 1,
+  S_SMOOTH_TASKS = 2,
+  S_SMOOTH_COMMIT = 3,
+  S_NPAIRS = 4,
+  S_NINDEP = 5,
+  S_COUNT = 6,     /* copy of a compaction count */
+  S_PARTS = 8,     /* part offsets, 9 slots */
+  S_LIVE = 18,     /* live vertices, live elements */
+  S_NTASK = 20,    /* device-counted candidates of a level (free mode) */
+  S_LEVEL = 21,    /* levels run by the current call */
+  S_ACT = 22,      /* two activity-list counters (free mode) */
+  S_FIX = 24,      /* repair-list counter (free mode) */
+  S_CONT = 25,     /* 1 while another level should run */
+  S_NB = 26,       /* slot counts: vertices, elements */
+  S_TICK = 28,     /* seed counter */
+  S_EVAL = 29,     /* statistics of the current call: examined, changed, */
+  S_TASK = 30,
+  S_RDONE = 31,    /* and refinement's "a level split nothing" */
+  S_SIZE = 32,
+};
+constexpr int kLevelCoarsen = 0, kLevelSwap = 1;
+constexpr int kLevelCap = 100000;
+
+/* end of a coarsening / swapping level (round.cu): next list into place,
+ * statistics, level cap, seed counter, and the decision in S_CONT (also
+ * handed to the loop node h when use_h) */
+void level_end(int* status, int kind, int cap, const int* next, int* cur, int hint, cudaStream_t s,
+               cudaGraphConditionalHandle h, bool use_h);
+
 /* grid for a grid-stride kernel over n items: a multiple of the SM count */
 int grid_for(long long n, int threads = TRN_THREADS);
 /* grid for a kernel over a device-counted list: sized for `bound` items (an
@@ -31,8 +64,10 @@ struct ScanWs {
 void scan_ws_alloc(ScanWs* ws, long long max_n);
 void scan_ws_free(ScanWs* ws);
 
-/* exclusive scan of n int64 values; *ws.total receives the sum */
-void scan_i64(const long long* in, long long* out, int n, ScanWs& ws, cudaStream_t s);
+/* exclusive scan of n int64 values; *ws.total receives the sum. With dn,
+ * the count is *dn (read on the device, at most n) */
+void scan_i64(const long long* in, long long* out, int n, ScanWs& ws, cudaStream_t s,
+              const int* dn = nullptr);
 /* ordered compaction: list[k] = i for the k-th i < n with flags[i] != 0;
  * *ws.count receives the number kept */
 void compact_u8(const uint8_t* flags, int n, int* list, ScanWs& ws, cudaStream_t s);
@@ -90,6 +125,11 @@ void refine_ws_free(RefineWs* ws);
 void refine_reset_hash(RefineWs& ws, cudaStream_t s);
 void refine_filter(const DMesh& m, int nb_elems, RefineWs& ws, bool fp32, cudaStream_t s);
 void refine_apply(const DMesh& m, int nb_nodes, int nb_elems, RefineWs& ws, bool fp32, cudaStream_t s);
+/* one refinement level driven by the device counts (m.nb): filter, scan,
+ * capacity check, splits, new counts; hints size the grids (at least the
+ * counts); stats: examined, added, done */
+void refine_level(const DMesh& m, int hint_nodes, int hint_elems, RefineWs& ws, ScanWs& scan,
+                  int* stats, bool fp32, cudaStream_t s);
 
 /* coarsening (coarsen.cu) */
 void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
@@ -120,6 +160,10 @@ void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dua
 /* smoothing (smooth.cu) */
 void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
 void smooth_color(const DMesh& m, const int* list, int n, int* counters, bool fp32, cudaStream_t s);
+/* the same over color class c of a device-side partition (parts, part_off);
+ * hint: grid size, at least the class size */
+void smooth_class(const DMesh& m, const int* parts, const int* part_off, int c, int hint, int* counters,
+                  bool fp32, cudaStream_t s);
 
 /* graph heuristics, free mode (heuristics.cu) */
 struct HeurWs {
@@ -139,16 +183,26 @@ void heur_ws_free(HeurWs* ws);
 /* handshake matching on the dual rows (*ntasks of them); pairs[2k],
  * pairs[2k+1]; *npairs */
 void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n,
-                     const int* ntasks, const int* map, uint64_t seed, HeurWs& ws, int* pairs,
+                     const int* ntasks, const int* map, Seed seed, HeurWs& ws, int* pairs,
                      int* npairs, cudaStream_t s, long long bound = -1);
 /* a fixed number of independent-set rounds over a device-counted candidate
  * list; undecided candidates are re-activated (next level) */
-void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, uint64_t seed,
+void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, Seed seed,
                    HeurWs& ws, int* indep, int* nindep, cudaStream_t s, long long bound = -1);
 /* Jones-Plassmann first-fit coloring of interior vertices, colors 1..max_col;
- * parts: vertex ids grouped by color, part_off[c] offsets (c = 0..max_col) */
-void color_jp(const DMesh& m, int nb_nodes, int max_col, uint64_t seed, HeurWs& ws,
-              int* parts, int* part_off, cudaStream_t s);
+ * parts: vertex ids grouped by color, part_off[c] offsets (c = 0..max_col).
+ * hint: grid size (at least the vertex count). color_jp runs batches of 8
+ * rounds while vertices wait (at most 8 batches), reading the decision back
+ * after each; a captured round runs color_batch inside a loop node instead.
+ * color_finish advances *tick (the seeds' counter). */
+void color_jp(const DMesh& m, int hint, int max_col, Seed seed, HeurWs& ws, int* parts,
+              int* part_off, unsigned* tick, cudaStream_t s);
+void color_begin(const DMesh& m, int hint, HeurWs& ws, cudaStream_t s);
+void color_batch(const DMesh& m, int hint, int max_col, Seed seed, HeurWs& ws, cudaStream_t s,
+                 cudaGraphConditionalHandle h, bool use_h);
+void color_finish(const DMesh& m, int hint, int max_col, HeurWs& ws, int* parts, int* part_off,
+                  unsigned* tick, cudaStream_t s);
+int* color_cont(HeurWs& ws);
 
 /* element-quality functional and its adjoint (adjoint.cu) */
 struct AdjWs {
