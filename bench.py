@@ -122,14 +122,19 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def run_step(api, g, c, heur, kern):
+def run_step(api, g, c, heur, kern, graph=False):
     """One adaptation on a mesh already holding the input; returns
-    (sum of live triangles at round starts, sum of round device ms, metric ms)."""
+    (sum of live triangles at round starts, sum of round device ms, metric ms).
+    graph: each round as the mesh's captured CUDA graph."""
     api.Metrics(g, c["target"], c["norm"]).run()
     metric_ms = g.last_time_ms()
     tin, tms = 0, 0.0
     for _ in range(c["rounds"]):
         tin += g.counts()[3]
+        if graph:
+            g.round_graph(c["depth"])
+            tms += g.last_time_ms()
+            continue
         for k in kern:
             k.run()
             tms += g.last_time_ms()
@@ -218,6 +223,19 @@ def b200_arm(args, rank, world, local_rank):
         g.reload()
         run_step(api, g, c, heur, kern)
         forms["fp64_quality_min_max_mean"] = [round(x, 4) for x in g.quality_stats()]
+        for prec in ("fp64", "mixed"):
+            g.set_precision(prec)
+            g.reload()
+            run_step(api, g, c, heur, kern, graph=True)       # captures the round
+            gt, gm = 0, 0.0
+            for _ in range(args.steps):
+                g.reload()
+                tin, tms, _ = run_step(api, g, c, heur, kern, graph=True)
+                gt += tin
+                gm += tms
+            forms[f"graph_{prec}"] = {"tri_in": gt, "round_ms": gm,
+                                      "quality_min_max_mean": [round(x, 4) for x in g.quality_stats()]}
+        g.set_precision("fp64")
         if rank == 0:
             forms["adjoint"] = adjoint_form(args)
             forms["precision"] = precision_form(args)
@@ -297,6 +315,14 @@ def b200_arm(args, rank, world, local_rank):
                            "final_mesh": f["final_mesh"], "quality_min_max_mean": f["quality_min_max_mean"]},
             "fp64_quality_min_max_mean": forms["fp64_quality_min_max_mean"],
         }
+        for prec in ("fp64", "mixed"):
+            f = forms[f"graph_{prec}"]
+            gg = reduce_stats([f["tri_in"], f["round_ms"]], [0], [1], device="cuda" if dist_on else "cpu")
+            line["forms"][f"graph_{prec}"] = {
+                "value": round(gg[0] / (gg[1] / 1e3), 1), "unit": UNIT,
+                "round_ms_per_step": round(gg[1] / args.steps, 3),
+                "note": "each round one captured CUDA graph (loops as device-decided loop nodes)",
+                "quality_min_max_mean": f["quality_min_max_mean"]}
         for k in ("adjoint", "precision"):
             if k in forms:
                 line["forms"][k] = forms[k]
@@ -457,8 +483,9 @@ def batch_arm(args, rank, world, local_rank):
     """The batched workload: 256 unit-square meshes of sides log-uniform in
     [32, 512] (2k-520k triangles), shock fields with random (a, b), target 0.8,
     3 rounds, depth 1; adapted concurrently (one stream per mesh, a pool of
-    host threads), sharded by size across ranks. Compared with adapting the
-    same meshes one at a time."""
+    host threads), each round one captured CUDA graph per mesh, sharded by size
+    across ranks. Compared with the same concurrency without graphs and with
+    adapting the meshes one at a time with the per-stage calls."""
     import torch
     from trinity_b200 import api
     from trinity_b200.dist import reduce_stats, shard_meshes
@@ -476,27 +503,32 @@ def batch_arm(args, rank, world, local_rank):
         meshes.append(g)
     threads = args.threads or min(16, os.cpu_count() or 8)
 
-    def run(nthreads):
+    def run(nthreads, graph):
         for g in meshes:
             g.reload()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ms, tin = api.batch_adapt(meshes, p["target"], p["norm"], p["rounds"], p["depth"], threads=nthreads)
+        ms, tin = api.batch_adapt(meshes, p["target"], p["norm"], p["rounds"], p["depth"], threads=nthreads,
+                                  graph=graph)
         torch.cuda.synchronize()
         return time.perf_counter() - t0, ms, tin
 
-    for _ in range(args.warmup):
-        run(threads)
+    for _ in range(args.warmup):          # the first graph round of each mesh captures it
+        run(threads, True)
+    l0 = _lib_launches()
     wall, tins, mss = 0.0, 0, []
     with Clocks(torch.cuda.current_device()) as clk:
         for _ in range(args.steps):
-            w, ms, tin = run(threads)
+            w, ms, tin = run(threads, True)
             wall += w
             tins += int(tin.sum())
             mss.append(ms)
-    seq_w, seq_ms, seq_tin = run(1)
+    launches = _lib_launches() - l0
+    run(threads, False)
+    pw, _, ptin = run(threads, False)
+    seq_w, seq_ms, seq_tin = run(1, False)
     dist_on = world > 1
-    agg = reduce_stats([tins, wall, int(seq_tin.sum()), seq_w], [0, 2], [1, 3],
+    agg = reduce_stats([tins, wall, int(seq_tin.sum()), seq_w, int(ptin.sum()), pw], [0, 2, 4], [1, 3, 5],
                        device="cuda" if dist_on else "cpu")
     if rank != 0:
         return None
@@ -508,16 +540,25 @@ def batch_arm(args, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "256 unit-square meshes, side log-uniform in [32, 512] (seed 5), "
                                "shock field tanh(a (y - 0.5 - b sin 2 pi x)), a ~ U[10, 100], b ~ U[0, 0.3], "
-                               "target 0.8, L^2, 3 rounds, depth 1, bucket 64, capacity 8x input",
-                   "mode": f"concurrent: one stream per mesh, {threads} host threads; wall time of metric + rounds",
+                               "target 0.8, L^2, 3 rounds, depth 1, bucket 128, capacity 8x input",
+                   "mode": f"concurrent: one stream per mesh, {threads} host threads, each round one captured "
+                           "CUDA graph per mesh; wall time of metric + rounds",
                    "meshes_on_rank0": len(meshes)},
+        "gpu_launches": int(launches),
+        "concurrent_without_graphs": {"value": round(agg[4] / agg[5], 1), "unit": UNIT},
         "one_at_a_time": {"value": round(agg[2] / agg[3], 1), "unit": UNIT,
+                          "note": "per-stage calls, no graphs, one mesh after the other",
                           "round_ms_p50": round(float(np.percentile(seq_ms, 50)), 3),
                           "round_ms_p99": round(float(np.percentile(seq_ms, 99)), 3)},
         "per_mesh_round_ms": {"p50": round(float(np.percentile(conc, 50)), 3),
                               "p99": round(float(np.percentile(conc, 99)), 3)},
         "clocks": clk.summary(),
     }
+
+
+def _lib_launches():
+    from trinity_b200 import _lib
+    return _lib.launch_count()
 
 
 # ------------------------------------------------------------------ reference

@@ -99,6 +99,14 @@ int trn_swap_run(trn_mesh* mesh, trn_stats* stats);
 int trn_smooth_run(trn_mesh* mesh, int max_colors, int depth, trn_stats* stats);
 /* one full round: refine, coarsen, swap, smooth (main.cpp:52-57) */
 int trn_round_run(trn_mesh* mesh, int depth, trn_stats stats[4]);
+/* The same round, free mode only, as one CUDA graph: captured on the mesh's
+ * first call (and again when depth, precision or seed change), replayed by
+ * later calls with no host round trip inside the round (the coarsening,
+ * swapping and coloring loops are device-decided loop nodes). Ends where
+ * trn_round_run ends. stats[k].eval / task per stage as trn_round_run;
+ * stats[0].elap holds the whole round's device time. TRN_ERR_INVALID in
+ * replay mode. No counterpart in the reference. */
+int trn_round_graph_run(trn_mesh* mesh, int depth, trn_stats stats[4]);
 
 /* Adapt a batch of independent meshes concurrently on the current GPU: each
  * mesh (already loaded) gets metric recovery and `rounds` rounds on its own
@@ -113,6 +121,12 @@ int trn_round_run(trn_mesh* mesh, int depth, trn_stats stats[4]);
 int trn_batch_adapt(trn_mesh* const* meshes, int count, double target_factor, int lp_norm,
                     double h_min, double h_max, int rounds, int depth, int threads,
                     double* round_ms, long long* tri_in);
+/* as trn_batch_adapt; flags TRN_BATCH_GRAPH runs each round as the mesh's
+ * captured round (trn_round_graph_run; free mode) */
+#define TRN_BATCH_GRAPH 1
+int trn_batch_adapt_ex(trn_mesh* const* meshes, int count, double target_factor, int lp_norm,
+                       double h_min, double h_max, int rounds, int depth, int threads, int flags,
+                       double* round_ms, long long* tri_in);
 
 /* Element-quality functional and its adjoint. No counterpart in the
  * reference; it differentiates the reference's own arithmetic:

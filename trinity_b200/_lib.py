@@ -75,6 +75,8 @@ def lib():
         L.trn_mesh_reload.argtypes = [pmesh]
         L.trn_set_precision.argtypes = [pmesh, ip]
         L.trn_batch_adapt.argtypes = [vp, ip, dp, ip, dp, dp, ip, ip, ip, vp, vp]
+        L.trn_batch_adapt_ex.argtypes = [vp, ip, dp, ip, dp, dp, ip, ip, ip, ip, vp, vp]
+        L.trn_round_graph_run.argtypes = [pmesh, ip, sp]
         L.trn_mesh_qualities.argtypes = [pmesh, vp]
         L.trn_mesh_quality_stats.argtypes = [pmesh, vp]
         L.trn_mesh_export_compact.argtypes = [pmesh, vp, vp, vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]

@@ -157,6 +157,11 @@ class Mesh:
     def stream(self) -> int:
         return self._L.trn_mesh_stream(self.h)
 
+    def round_graph(self, depth: int, stats=None) -> None:
+        """One free-mode round as the mesh's captured CUDA graph
+        (trn_round_graph_run); stats: a ctypes array of 4 Stats or None."""
+        self._check(self._L.trn_round_graph_run(self.h, depth, stats))
+
     def quality_adjoint(self, xy=None, solut=None, *, target_factor: float = 1.0, Lp_norm: int = 2,
                         h_min: float = EPSILON, h_max: float = H_MAX, precision: str = "fp64",
                         grad_xy: bool = True, grad_solut: bool | None = None):
@@ -196,18 +201,19 @@ class Mesh:
 
 
 def batch_adapt(meshes, target_factor: float, Lp_norm: int = 2, rounds: int = 3, depth: int = 1,
-                threads: int = 8, h_min: float = EPSILON, h_max: float = H_MAX):
+                threads: int = 8, h_min: float = EPSILON, h_max: float = H_MAX, graph: bool = False):
     """Metric recovery + rounds for many loaded meshes at once (one stream per
     mesh, a pool of host threads). Returns (round_ms[count], tri_in[count]).
     Set CUDA_DEVICE_MAX_CONNECTIONS=32 in the environment before CUDA starts
-    so that the streams do not share the default 8 hardware queues."""
+    so that the streams do not share the default 8 hardware queues. graph:
+    each round as the mesh's captured CUDA graph (free mode)."""
     L = lib()
     n = len(meshes)
     handles = (ctypes.c_void_p * n)(*[m.h.value if hasattr(m.h, "value") else m.h for m in meshes])
     ms = np.zeros(n)
     tin = np.zeros(n, dtype=np.int64)
-    rc = L.trn_batch_adapt(ctypes.cast(handles, ctypes.c_void_p), n, target_factor, Lp_norm, h_min, h_max,
-                           rounds, depth, threads, _p(ms), _p(tin))
+    rc = L.trn_batch_adapt_ex(ctypes.cast(handles, ctypes.c_void_p), n, target_factor, Lp_norm, h_min, h_max,
+                              rounds, depth, threads, 1 if graph else 0, _p(ms), _p(tin))
     if rc:
         raise TrinityError(rc, "batch adaptation failed: " + "; ".join(
             m._L.trn_last_error(m.h).decode() for m in meshes if m._L.trn_last_error(m.h)))

@@ -370,7 +370,7 @@ __device__ __forceinline__ int patch_owners(const DMesh& m, int4 n, int* ids) {
     const int* vc = m.vic + (size_t) c[j] * m.bucket;
     const int nv = min(m.vdeg[c[j]], m.bucket);
     if (k + 1 + nv > TRN_MAX_PATCH) {
-      trn_set_error(m.err, TRN_DERR_CAPACITY);
+      trn_set_error(m.err, TRN_DERR_BUCKET);
       break;
     }
     ids[k++] = c[j];

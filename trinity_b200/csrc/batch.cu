@@ -5,8 +5,10 @@
  * adapted here concurrently on one GPU: every mesh has its own CUDA stream,
  * and a pool of host threads drives the meshes (largest first) through metric
  * recovery and the rounds, so that the launch- and synchronisation-bound
- * phases of small meshes overlap with the compute of large ones. Meshes share
- * nothing on the device; no host lock is held while a mesh runs.
+ * phases of small meshes overlap with the compute of large ones. With
+ * TRN_BATCH_GRAPH each round is the mesh's captured round (one graph launch,
+ * no host round trip inside). Meshes share nothing on the device; no host
+ * lock is held while a mesh runs.
  */
 #include "../../include/trinity_b200.h"
 
@@ -21,6 +23,14 @@
 extern "C" int trn_batch_adapt(trn_mesh* const* meshes, int count, double target_factor, int lp_norm,
                                double h_min, double h_max, int rounds, int depth, int threads,
                                double* round_ms, long long* tri_in) {
+  return trn_batch_adapt_ex(meshes, count, target_factor, lp_norm, h_min, h_max, rounds, depth, threads,
+                            0, round_ms, tri_in);
+}
+
+extern "C" int trn_batch_adapt_ex(trn_mesh* const* meshes, int count, double target_factor, int lp_norm,
+                                  double h_min, double h_max, int rounds, int depth, int threads,
+                                  int flags, double* round_ms, long long* tri_in) {
+  const bool graph = (flags & TRN_BATCH_GRAPH) != 0;
   if (!meshes || count <= 0 || rounds < 0 || depth < 1) return TRN_ERR_INVALID;
   for (int i = 0; i < count; ++i)
     if (!meshes[i]) return TRN_ERR_INVALID;
@@ -50,6 +60,11 @@ extern "C" int trn_batch_adapt(trn_mesh* const* meshes, int count, double target
         int live = 0;
         rc = trn_mesh_counts(m, nullptr, nullptr, nullptr, &live);
         tin += live;
+        if (graph) {
+          if (rc == TRN_OK) rc = trn_round_graph_run(m, depth, nullptr);
+          if (rc == TRN_OK) ms += trn_last_time_ms(m);
+          continue;
+        }
         if (rc == TRN_OK) rc = trn_refine_run(m, depth, nullptr);
         if (rc == TRN_OK) ms += trn_last_time_ms(m), rc = trn_coarsen_run(m, 8, nullptr);
         if (rc == TRN_OK) ms += trn_last_time_ms(m), rc = trn_swap_run(m, nullptr);

@@ -35,7 +35,7 @@ __device__ __forceinline__ int gather_patch(const DMesh& m, int v, int* patch) {
     int dw = trn_deg(m, w);
     for (int a = 0; a < dw; ++a) {
       if (k == TRN_MAX_PATCH) {
-        trn_set_error(m.err, TRN_DERR_CAPACITY);
+        trn_set_error(m.err, TRN_DERR_BUCKET);
         break;
       }
       patch[k++] = sw[a];

@@ -204,7 +204,7 @@ extern "C" int trn_metric_noalloc(int nb_nodes, int nb_elems, const double* d_po
   if (cudaMemcpyAsync(&err, d.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return TRN_ERR_CUDA;
-  if (err == TRN_DERR_CAPACITY) {
+  if (err == TRN_DERR_CAPACITY || err == TRN_DERR_BUCKET) {
     std::fprintf(stderr, "trn_metric_noalloc: a vertex has more than %d incident triangles\n",
                  TRN_NOALLOC_BUCKET);
     return TRN_ERR_CAPACITY;

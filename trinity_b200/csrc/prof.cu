@@ -73,6 +73,8 @@ Profiler& prof() {
 ProfScope::ProfScope(const char* name, cudaStream_t s, double bytes) : stream_(s) {
   Profiler& p = prof();
   if (!p.on) return;
+  cudaStreamCaptureStatus cs;
+  if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) return;
   std::lock_guard<std::mutex> lock(p.mu);
   if (!p.only.empty() && p.only != name) return;
   id_ = p.id_of(name);
@@ -93,7 +95,18 @@ ProfScope::~ProfScope() {
 static std::atomic<unsigned long long> g_launches{0};
 constexpr size_t kEventPool = 65536;
 
-void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+/* per host thread as well: a round captured on one thread counts only its own launches */
+static thread_local unsigned long long t_launches = 0;
+
+void note_launch() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  ++t_launches;
+}
+void note_launches(unsigned long long n) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  t_launches += n;
+}
+unsigned long long thread_launches() { return t_launches; }
 
 void prof_flush() {
   Profiler& p = prof();

@@ -50,7 +50,7 @@ __device__ void h_insert(unsigned long long* hkey, int* hval, unsigned long long
     }
     s = (s + 1) & mask;
   }
-  trn_set_error(err, TRN_DERR_CAPACITY);
+  trn_set_error(err, TRN_DERR_HASH);
 }
 
 __device__ int h_get(const unsigned long long* hkey, const int* hval, unsigned long long cap,

@@ -26,6 +26,7 @@ namespace {
 /* host-only part of the pinned status mirror (after the device block) */
 enum {
   H_WIDE = 40,     /* host-only pinned slot for one 8-byte value */
+  H_STATS = 48,    /* a captured round's statistics, 8 slots */
   H_SIZE = 64,
 };
 
@@ -66,6 +67,14 @@ struct trn_mesh {
   RefineWs rws;
   HeurWs hws;
   AdjWs adj;
+  /* a captured free-mode round (trn_round_graph_run) and what it was captured for */
+  cudaGraphExec_t round_exec = nullptr;
+  cudaStream_t body_stream = nullptr;   /* captures the loop bodies */
+  int* rstats = nullptr;                /* device: examined / changed per stage */
+  int round_depth = 0;
+  bool round_fp32 = false;
+  uint64_t round_seed = 0;
+  unsigned long long round_launches = 0;
   /* replay */
   bool replay = false;
   std::vector<int32_t> log;
@@ -104,11 +113,13 @@ int sync_status(trn_mesh* m, const int* count = nullptr) {
   prof_flush();
   int e = m->h_status[S_ERR];
   if (e) {
-    const char* what = e == TRN_DERR_CAPACITY      ? "capacity exceeded (nodes, elements, stencil bucket, hash or patch)"
+    const char* what = e == TRN_DERR_CAPACITY      ? "vertex or element capacity exceeded"
+                       : e == TRN_DERR_BUCKET      ? "a vertex has more triangles than the stencil bucket"
+                       : e == TRN_DERR_HASH        ? "refinement edge table full"
                        : e == TRN_DERR_REPLAY      ? "replay log does not match the mesh"
                        : e == TRN_DERR_NO_PROGRESS ? "level cap reached"
                                                    : "invalid state";
-    return fail(m, e == TRN_DERR_CAPACITY      ? TRN_ERR_CAPACITY
+    return fail(m, (e == TRN_DERR_CAPACITY || e == TRN_DERR_BUCKET || e == TRN_DERR_HASH) ? TRN_ERR_CAPACITY
                    : e == TRN_DERR_REPLAY      ? TRN_ERR_REPLAY
                    : e == TRN_DERR_NO_PROGRESS ? TRN_ERR_NO_PROGRESS : TRN_ERR_INVALID,
                 std::string("device: ") + what);
@@ -175,6 +186,9 @@ void release(trn_mesh* m) {
   refine_ws_free(&m->rws);
   heur_ws_free(&m->hws);
   adj_ws_free(&m->adj);
+  if (m->round_exec) cudaGraphExecDestroy(m->round_exec);
+  if (m->body_stream) cudaStreamDestroy(m->body_stream);
+  if (m->rstats) cudaFree(m->rstats);
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
   if (m->stream) cudaStreamDestroy(m->stream);
@@ -798,10 +812,7 @@ int trn_refine_run(trn_mesh* m, int depth, trn_stats* st) {
   begin_timing(m);
   enq_refine(m, depth, m->stream);
   int rc = sync_status(m);
-  if (rc) {
-    if (rc == TRN_ERR_CAPACITY) m->err = "refine: node or element capacity exceeded";
-    return rc;
-  }
+  if (rc) return rc;
   m->nb_nodes = m->h_status[S_NB];
   m->nb_elems = m->h_status[S_NB + 1];
   return end_timing(m, st, m->h_status[S_EVAL], m->h_status[S_TASK]);
@@ -1006,6 +1017,139 @@ int trn_smooth_gradient_run(trn_mesh* m, int max_colors, int steps, double max_l
                             m->fp32, s);
   if ((rc = sync_status(m))) return rc;
   return end_timing(m, st, m->h_status[S_SMOOTH_TASKS], m->h_status[S_SMOOTH_COMMIT]);
+}
+
+/* ---------------- a captured round ----------------
+ * The whole free-mode round as one CUDA graph: the refinement levels, then
+ * coarsening, swapping and the coloring's batches as loop nodes whose body
+ * is one level (the device decides, in k_level_end / k_color_batch_end,
+ * whether it runs again), then the smoothing passes over the device-side
+ * color classes. Grids are sized by the capacities; every count is read on
+ * the device. The kernels and seeds are those of the per-stage calls, so a
+ * captured round ends where trn_round_run ends. */
+}  /* extern "C" */
+
+namespace {
+
+template <class F>
+cudaError_t capture_loop(cudaStream_t s, cudaStream_t bs, F&& body) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd);
+  if (e != cudaSuccess) return e;
+  if (st != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureInvalidated;
+  cudaGraphConditionalHandle h;
+  if ((e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  if ((e = cudaGraphAddNode(&node, g, deps, nd, &p)) != cudaSuccess) return e;
+  cudaGraph_t bodyg = p.conditional.phGraph_out[0];
+  if ((e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+    return e;
+  if ((e = cudaStreamBeginCaptureToGraph(bs, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+      cudaSuccess)
+    return e;
+  body(bs, h);
+  return cudaStreamEndCapture(bs, &bodyg);
+}
+
+int capture_round(trn_mesh* m, int depth) {
+  if (m->round_exec) {
+    cudaGraphExecDestroy(m->round_exec);
+    m->round_exec = nullptr;
+  }
+  if (!m->body_stream) CK(cudaStreamCreateWithFlags(&m->body_stream, cudaStreamNonBlocking));
+  if (!m->rstats) CK(cudaMalloc(&m->rstats, sizeof(int) * 8));
+  cudaStream_t s = m->stream, bs = m->body_stream;
+  const int max_col = max_colors_of(8);
+  unsigned* tick = reinterpret_cast<unsigned*>(m->status + S_TICK);
+  const unsigned long long l0 = thread_launches();
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  auto stage_stats = [&](int k) {
+    cudaMemcpyAsync(m->rstats + 2 * k, m->status + S_EVAL, sizeof(int) * 2, cudaMemcpyDeviceToDevice, s);
+  };
+  cudaError_t e = cudaSuccess;
+  enq_refine(m, depth, s);
+  stage_stats(0);
+  enq_coarsen_begin(m, s, true);
+  if (e == cudaSuccess)
+    e = capture_loop(s, bs, [&](cudaStream_t b, cudaGraphConditionalHandle h) {
+      enq_coarsen_level(m, b, -1, h, true);
+    });
+  stage_stats(1);
+  enq_swap_begin(m, s, true);
+  if (e == cudaSuccess)
+    e = capture_loop(s, bs, [&](cudaStream_t b, cudaGraphConditionalHandle h) {
+      enq_swap_level(m, b, -1, h, true);
+    });
+  stage_stats(2);
+  smooth_pre(m->d, m->capa_node, s);
+  build_vicin(m->d, m->capa_node, true, s);
+  color_begin(m->d, m->capa_node, m->hws, s);
+  if (e == cudaSuccess)
+    e = capture_loop(s, bs, [&](cudaStream_t b, cudaGraphConditionalHandle h) {
+      color_batch(m->d, m->capa_node, max_col, seed_of(m, 0xc01dULL), m->hws, b, h, true);
+    });
+  color_finish(m->d, m->capa_node, max_col, m->hws, m->parts, m->status + S_PARTS, tick, s);
+  quality_all(m->d, m->capa_elem, m->fp32, s);
+  cudaMemsetAsync(m->status + S_SMOOTH_TASKS, 0, sizeof(int) * 2, s);
+  for (int level = 0; level < depth; ++level)
+    for (int c = 0; c < max_col && c < 8; ++c)
+      smooth_class(m->d, m->parts, m->status + S_PARTS, c, m->capa_node, m->status + S_SMOOTH_TASKS,
+                   m->fp32, s);
+  cudaMemcpyAsync(m->rstats + 6, m->status + S_SMOOTH_TASKS, sizeof(int) * 2, cudaMemcpyDeviceToDevice, s);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(s, &g);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&m->round_exec, g, 0);
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  if (e != cudaSuccess) {
+    m->round_exec = nullptr;
+    return fail(m, TRN_ERR_CUDA, std::string("round capture: ") + cudaGetErrorString(e));
+  }
+  m->round_depth = depth;
+  m->round_fp32 = m->fp32;
+  m->round_seed = m->seed;
+  m->round_launches = thread_launches() - l0;
+  return TRN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trn_round_graph_run(trn_mesh* m, int depth, trn_stats stats[4]) {
+  if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "round: no mesh loaded");
+  if (depth < 1) return fail(m, TRN_ERR_INVALID, "round: depth < 1");
+  if (m->replay) return fail(m, TRN_ERR_INVALID, "round: a captured round runs the free mode only");
+  m->err.clear();
+  if (!m->round_exec || m->round_depth != depth || m->round_fp32 != m->fp32 || m->round_seed != m->seed) {
+    int rc = capture_round(m, depth);
+    if (rc) return rc;
+  }
+  begin_timing(m);
+  CK(cudaGraphLaunch(m->round_exec, m->stream));
+  note_launches(m->round_launches);
+  CK(cudaMemcpyAsync(m->h_status + H_STATS, m->rstats, sizeof(int) * 8, cudaMemcpyDeviceToHost, m->stream));
+  int rc = sync_status(m);
+  if (rc) return rc;
+  m->nb_nodes = m->h_status[S_NB];
+  m->nb_elems = m->h_status[S_NB + 1];
+  rc = end_timing(m, nullptr, 0, 0);
+  if (stats)
+    for (int k = 0; k < 4; ++k) {
+      stats[k].eval += m->h_status[H_STATS + 2 * k];
+      stats[k].task += m->h_status[H_STATS + 2 * k + 1];
+      if (k == 0) stats[k].elap += (int) m->last_ms;
+    }
+  return rc;
 }
 
 int trn_round_run(trn_mesh* m, int depth, trn_stats stats[4]) {

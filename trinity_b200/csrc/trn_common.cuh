@@ -28,7 +28,9 @@
 #define TRN_MATCHED (-2)  /* matching.h:27 */
 
 /* device error word values (mirror the C-ABI codes) */
-#define TRN_DERR_CAPACITY 1
+#define TRN_DERR_CAPACITY 1    /* vertex or element slots */
+#define TRN_DERR_BUCKET 2      /* a stencil, adjacency row or patch longer than its bucket */
+#define TRN_DERR_HASH 5        /* the refinement's edge table is full */
 #define TRN_DERR_INVALID 3
 #define TRN_DERR_NO_PROGRESS 4
 #define TRN_DERR_REPLAY 6
@@ -122,7 +124,7 @@ __device__ __forceinline__ int trn_deg(const DMesh& m, int v) {
 __device__ __forceinline__ void trn_stenc_append(const DMesh& m, int v, int t) {
   int k = atomicAdd(m.deg + v, 1);
   if (k >= m.bucket) {
-    trn_set_error(m.err, TRN_DERR_CAPACITY);
+    trn_set_error(m.err, TRN_DERR_BUCKET);
     return;
   }
   m.stenc[(size_t) v * m.bucket + k] = t;
@@ -131,7 +133,7 @@ __device__ __forceinline__ void trn_stenc_append(const DMesh& m, int v, int t) {
 __device__ __forceinline__ void trn_stenc_append_n(const DMesh& m, int v, const int* t, int n) {
   int k = atomicAdd(m.deg + v, n);
   if (k + n > m.bucket) {
-    trn_set_error(m.err, TRN_DERR_CAPACITY);
+    trn_set_error(m.err, TRN_DERR_BUCKET);
     return;
   }
   int* s = m.stenc + (size_t) v * m.bucket + k;
@@ -174,7 +176,7 @@ __device__ __forceinline__ void build_one_vicin(const DMesh& m, int v) {
   trn_isort(buf, k);
   k = trn_iunique(buf, k);
   if (k > m.bucket) {
-    trn_set_error(m.err, TRN_DERR_CAPACITY);
+    trn_set_error(m.err, TRN_DERR_BUCKET);
     k = m.bucket;
   }
   int* out = m.vic + (size_t) v * m.bucket;

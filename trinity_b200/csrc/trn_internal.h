@@ -260,6 +260,9 @@ class ProfScope {
 void prof_flush();
 /* count of kernel launches issued by this library (process-wide) */
 void note_launch();
+void note_launches(unsigned long long n);
+/* launches issued by the calling host thread */
+unsigned long long thread_launches();
 
 /* algorithmic sizes (bytes per entity) used by the launchers' byte counts:
  * point 2 x f64, tensor 3 x f64, triangle 3 x i32, quality f64, stencil and
