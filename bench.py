@@ -155,6 +155,7 @@ def b200_arm(args, rank, world, local_rank):
     g.set_options(seed=0x7472696E697479 + rank)
     heur = api.Partit(g, 8)
     kern = [api.Refine(g, c["depth"]), api.Coarse(g, heur), api.Swap(g), api.Smooth(g, heur, c["depth"])]
+    tuned = g.autotune(c["target"], c["norm"], depth=c["depth"], rounds=1)   # launch shapes only
 
     def barrier():
         if dist_on:
@@ -303,6 +304,7 @@ def b200_arm(args, rank, world, local_rank):
                            for r in prof_all), key=lambda r: -r["ms"])[:10],
         "kernels_note": f"{min(args.steps, 2)} profiled steps (every launch timed), before the timed region",
         "final_mesh": {"nodes": final[2], "triangles": final[3]},
+        "launch_shapes": dict(tuned, chosen_by="trn_autotune on this mesh (changes no result)"),
         "clocks": clk.summary(),
     }
     if "mixed_fp32" in forms:
@@ -502,6 +504,10 @@ def batch_arm(args, rank, world, local_rank):
         g.load_arrays(m.points, m.tris, tags_of(m), u)
         meshes.append(g)
     threads = args.threads or min(16, os.cpu_count() or 8)
+    # launch shapes: one table for the whole batch, chosen by timing the
+    # concurrent batch itself (api.batch_autotune: coordinate descent)
+    tuned, trials = api.batch_autotune(meshes, p["target"], p["norm"], p["rounds"], p["depth"],
+                                       threads=threads, graph=True)
 
     def run(nthreads, graph):
         for g in meshes:
@@ -545,6 +551,8 @@ def batch_arm(args, rank, world, local_rank):
                            "CUDA graph per mesh; wall time of metric + rounds",
                    "meshes_on_rank0": len(meshes)},
         "gpu_launches": int(launches),
+        "launch_shapes": dict(tuned, chosen_by="api.batch_autotune (whole-batch timing, "
+                                                "changes no result)", trials_s=trials),
         "concurrent_without_graphs": {"value": round(agg[4] / agg[5], 1), "unit": UNIT},
         "one_at_a_time": {"value": round(agg[2] / agg[3], 1), "unit": UNIT,
                           "note": "per-stage calls, no graphs, one mesh after the other",

@@ -93,3 +93,38 @@ def test_graph_batch_equals_plain_batch():
         sa, sb = gpu_state(a), gpu_state(b)
         assert not sb.diff(sa)
         check_invariants(sb)
+
+
+ODD_TUNE = dict(smooth_threads=64, filter_threads=512, group_lanes=4, group_max=65536, flip_threads=128)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_launch_shapes_change_no_result(graph):
+    m, u, c = meshgen.make_config("c2", 100)
+    states = []
+    for cfg in (None, ODD_TUNE, dict(ODD_TUNE, group_lanes=16, group_max=0, smooth_threads=256)):
+        g = gpu_mesh(m, u, c)
+        if cfg:
+            g.set_tune(cfg)
+            assert g.get_tune() == cfg
+        _rounds(g, c, graph)
+        states.append(gpu_state(g))
+        g.close()
+    assert not states[1].diff(states[0])
+    assert not states[2].diff(states[0])
+
+
+def test_autotune_picks_valid_shapes_and_reloads():
+    from trinity_b200.api import TrinityError
+    m, u, c = meshgen.make_config("c2", 80)
+    g = gpu_mesh(m, u, c)
+    cfg = g.autotune(c["target"], c["norm"], depth=c["depth"], rounds=1)
+    assert cfg["smooth_threads"] in (64, 128, 256) and cfg["group_lanes"] in (4, 8, 16)
+    assert g.get_tune() == cfg
+    assert g.counts()[:2] == (m.nb_nodes, m.nb_elems)
+    ref = gpu_mesh(m, u, c)
+    _rounds(g, c, True)
+    _rounds(ref, c, False)
+    assert not gpu_state(g).diff(gpu_state(ref))
+    with pytest.raises(TrinityError):
+        g.set_tune(dict(ODD_TUNE, group_lanes=6))

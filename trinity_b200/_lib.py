@@ -77,6 +77,9 @@ def lib():
         L.trn_batch_adapt.argtypes = [vp, ip, dp, ip, dp, dp, ip, ip, ip, vp, vp]
         L.trn_batch_adapt_ex.argtypes = [vp, ip, dp, ip, dp, dp, ip, ip, ip, ip, vp, vp]
         L.trn_round_graph_run.argtypes = [pmesh, ip, sp]
+        L.trn_get_tune.argtypes = [pmesh, vp]
+        L.trn_set_tune.argtypes = [pmesh, vp]
+        L.trn_autotune.argtypes = [pmesh, dp, ip, dp, dp, ip, ip, vp]
         L.trn_mesh_qualities.argtypes = [pmesh, vp]
         L.trn_mesh_quality_stats.argtypes = [pmesh, vp]
         L.trn_mesh_export_compact.argtypes = [pmesh, vp, vp, vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]

@@ -157,6 +157,25 @@ class Mesh:
     def stream(self) -> int:
         return self._L.trn_mesh_stream(self.h)
 
+    TUNE_KEYS = ("smooth_threads", "filter_threads", "group_lanes", "group_max", "flip_threads")
+
+    def get_tune(self) -> dict:
+        a = np.zeros(len(self.TUNE_KEYS), dtype=np.int32)
+        self._check(self._L.trn_get_tune(self.h, _p(a)))
+        return dict(zip(self.TUNE_KEYS, a.tolist()))
+
+    def set_tune(self, cfg: dict) -> None:
+        a = np.array([cfg[k] for k in self.TUNE_KEYS], dtype=np.int32)
+        self._check(self._L.trn_set_tune(self.h, _p(a)))
+
+    def autotune(self, target_factor: float, Lp_norm: int = 2, depth: int = 1, rounds: int = 1,
+                 h_min: float = EPSILON, h_max: float = H_MAX) -> dict:
+        """Launch shapes chosen on this mesh (trn_autotune); the mesh is
+        reloaded afterwards."""
+        a = np.zeros(len(self.TUNE_KEYS), dtype=np.int32)
+        self._check(self._L.trn_autotune(self.h, target_factor, Lp_norm, h_min, h_max, depth, rounds, _p(a)))
+        return dict(zip(self.TUNE_KEYS, a.tolist()))
+
     def round_graph(self, depth: int, stats=None) -> None:
         """One free-mode round as the mesh's captured CUDA graph
         (trn_round_graph_run); stats: a ctypes array of 4 Stats or None."""
@@ -218,6 +237,44 @@ def batch_adapt(meshes, target_factor: float, Lp_norm: int = 2, rounds: int = 3,
         raise TrinityError(rc, "batch adaptation failed: " + "; ".join(
             m._L.trn_last_error(m.h).decode() for m in meshes if m._L.trn_last_error(m.h)))
     return ms, tin
+
+
+def batch_autotune(meshes, target_factor: float, Lp_norm: int = 2, rounds: int = 3, depth: int = 1,
+                   threads: int = 8, graph: bool = True, candidates: dict | None = None):
+    """Launch shapes for a batch adapted concurrently: coordinate descent
+    over one table shared by all meshes, each candidate timed by running the
+    whole batch (wall clock, best of two); shapes that suit a mesh alone need
+    not suit it among many. Leaves the chosen table set on every mesh and the
+    meshes reloaded. Returns (table, {trial: seconds})."""
+    import time
+    cand = candidates or {"group_lanes": [4, 8, 16], "group_max": [4096, 16384, 65536],
+                          "smooth_threads": [64, 128, 256], "filter_threads": [128, 256, 512],
+                          "flip_threads": [128, 256, 512]}
+    best = meshes[0].get_tune()
+
+    def timed(cfg):
+        t = 1e300
+        for _ in range(2):
+            for g in meshes:
+                g.set_tune(cfg)
+                g.reload()
+            t0 = time.perf_counter()
+            batch_adapt(meshes, target_factor, Lp_norm, rounds, depth, threads=threads, graph=graph)
+            t = min(t, time.perf_counter() - t0)
+        return t
+
+    trials = {}
+    for key, values in cand.items():
+        scores = {}
+        for v in values:
+            cfg = dict(best, **{key: v})
+            scores[v] = timed(cfg)
+            trials[f"{key}={v}"] = round(scores[v], 4)
+        best[key] = min(scores, key=scores.get)
+    for g in meshes:
+        g.set_tune(best)
+        g.reload()
+    return best, trials
 
 
 class Metrics:

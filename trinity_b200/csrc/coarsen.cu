@@ -8,8 +8,8 @@
  *                    keeps every surviving element CCW with edges <= sqrt(2)
  *                    (Coarse::identifyTarget, coarsening.cpp:47-133); ties are
  *                    broken in adjacency order, like the reference's multimap
- *   k_coarse_filter_group  the same search by 8 lanes per vertex, for levels
- *                    that list few vertices (free mode)
+ *   k_coarse_filter_group  the same search by 4, 8 or 16 lanes per vertex, for
+ *                    levels that list few vertices (free mode)
  *   k_collapse       per independent vertex: erase the 1-2 shell elements,
  *                    move the rest of the stencil to the target, relabel,
  *                    tag repairs, re-activate the 1-ring (Coarse::collapseEdge,
@@ -139,7 +139,7 @@ __global__ void k_coarse_filter_append(DMesh m, const int* __restrict__ act, con
   }
 }
 
-/* the same search by a group of kGroup lanes per vertex, for the levels that
+/* the same search by a group of G lanes per vertex, for the levels that
  * list few vertices, where one lane's chain of dependent gathers (adjacency,
  * stencil, triangles, points, tensors) sets the time. The lanes compute the
  * neighbours' metric lengths, then check every (candidate, element) pair at
@@ -148,12 +148,8 @@ __global__ void k_coarse_filter_append(DMesh m, const int* __restrict__ act, con
  * the first valid one in the serial search's stable length order, so the
  * targets are the same. Vertices with more than 32 neighbours fall back to
  * the serial search on the group's first lane. */
-constexpr int kGroup = 8;
-/* at most this many listed vertices: the grouped search (measured on B200:
- * faster below ~16k listed vertices, 2x slower on full-mesh levels) */
-constexpr int kGroupMax = 16384;
 
-template <bool F32>
+template <bool F32, int G>
 __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, const int* act_n,
                                       int* __restrict__ target, int* __restrict__ cand, int* count,
                                       uint8_t* __restrict__ state, int max_n) {
@@ -161,13 +157,13 @@ __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, cons
   const int n = *act_n;
   if (n > max_n) return;
   const int lane = threadIdx.x & 31;
-  const int gl = lane & (kGroup - 1);
-  const int gbase = lane & ~(kGroup - 1);
-  const int per_warp = 32 / kGroup;
+  const int gl = lane & (G - 1);
+  const int gbase = lane & ~(G - 1);
+  const int per_warp = 32 / G;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int base = warp * per_warp; base < n; base += nwarps * per_warp) {
-    const int q = base + lane / kGroup;
+    const int q = base + lane / G;
     int vv = -1;
     if (gl == 0 && q < n) {
       const int x = act[q];
@@ -191,11 +187,11 @@ __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, cons
       ps = m.pts[v];
       ts = m.ten[v];
     }
-    /* neighbours b = gl + kGroup * k: candidates closer than 1/sqrt(2) */
-    double lenk[32 / kGroup];
+    /* neighbours b = gl + G * k: candidates closer than 1/sqrt(2) */
+    double lenk[32 / G];
     unsigned candm = 0, boundm = 0;
-    for (int k = 0; k < 32 / kGroup; ++k) {
-      const int b = gl + kGroup * k;
+    for (int k = 0; k < 32 / G; ++k) {
+      const int b = gl + G * k;
       lenk[k] = 0.0;
       if (grp && b < nv) {
         const int w = vc[b];
@@ -210,17 +206,17 @@ __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, cons
         }
       }
     }
-    for (int o = kGroup / 2; o >= 1; o >>= 1) {
+    for (int o = G / 2; o >= 1; o >>= 1) {
       candm |= __shfl_xor_sync(0xffffffffu, candm, o);
       boundm |= __shfl_xor_sync(0xffffffffu, boundm, o);
     }
     /* every (candidate, element) pair of the simulated collapses */
     const int deg = grp ? trn_deg(m, v) : 0;
     const int np = (grp && candm) ? nv * deg : 0;
-    const int iters = __reduce_max_sync(0xffffffffu, (np + kGroup - 1) / kGroup);
+    const int iters = __reduce_max_sync(0xffffffffu, (np + G - 1) / G);
     unsigned failm = 0, once = 0, twice = 0;
     for (int k = 0; k < iters; ++k) {
-      const int p = gl + kGroup * k;
+      const int p = gl + G * k;
       if (p >= np) continue;
       const int b = p / deg, a = p - b * deg;
       if (!((candm >> b) & 1u)) continue;
@@ -247,7 +243,7 @@ __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, cons
         failm |= bit;
       }
     }
-    for (int o = kGroup / 2; o >= 1; o >>= 1) {
+    for (int o = G / 2; o >= 1; o >>= 1) {
       const unsigned fo = __shfl_xor_sync(0xffffffffu, failm, o);
       const unsigned oo = __shfl_xor_sync(0xffffffffu, once, o);
       const unsigned to = __shfl_xor_sync(0xffffffffu, twice, o);
@@ -259,14 +255,14 @@ __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, cons
     /* the smallest (length, adjacency index) among the valid candidates */
     double best = 0.0;
     int bestb = -1;
-    for (int k = 0; k < 32 / kGroup; ++k) {
-      const int b = gl + kGroup * k;
+    for (int k = 0; k < 32 / G; ++k) {
+      const int b = gl + G * k;
       if (b < 32 && ((valid >> b) & 1u) && (bestb < 0 || lenk[k] < best)) {
         best = lenk[k];
         bestb = b;
       }
     }
-    for (int o = kGroup / 2; o >= 1; o >>= 1) {
+    for (int o = G / 2; o >= 1; o >>= 1) {
       const double ob = __shfl_xor_sync(0xffffffffu, best, o);
       const int obb = __shfl_xor_sync(0xffffffffu, bestb, o);
       if (obb >= 0 && (bestb < 0 || ob < best || (ob == best && obb < bestb))) {
@@ -374,22 +370,30 @@ void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int
                            int* count, uint8_t* state, bool fp32, cudaStream_t s, long long bound) {
   ProfScope ps("coarsen_filter", s, 0.0);
   cudaMemsetAsync(count, 0, sizeof(int), s);
-  /* a level listing at most kGroupMax vertices runs the grouped search, a
-   * larger one the one-lane search; the count is on the device, so both are
-   * launched and one returns at once */
-  const int g = grid_bounded(bound, m.capa_node);
-  const int gg = grid_bounded(bound < 0 ? -1 : bound * kGroup, (long long) kGroupMax * kGroup);
+  /* a level listing at most group_max vertices runs the grouped search
+   * (measured on B200 with 8 lanes: faster below ~16k listed vertices, 2x
+   * slower on full-mesh levels), a larger one the one-lane search; the count
+   * is on the device, so both are launched and one returns at once */
+  const Tune& t = tune();
+  const int g = grid_bounded(bound, m.capa_node, t.filter_threads);
+  const int gg = grid_bounded(bound < 0 ? -1 : bound * t.group_lanes, (long long) t.group_max * t.group_lanes);
+  const int gm = t.group_max;
+#define TRN_GROUP(F, G)                                                                              \
+  k_coarse_filter_group<F, G><<<gg, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state, gm)
   if (fp32) {
-    k_coarse_filter_group<true><<<gg, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state,
-                                                          kGroupMax);
-    k_coarse_filter_append<true><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state,
-                                                           kGroupMax + 1);
+    if (t.group_lanes == 4) TRN_GROUP(true, 4);
+    else if (t.group_lanes == 16) TRN_GROUP(true, 16);
+    else TRN_GROUP(true, 8);
+    k_coarse_filter_append<true><<<g, t.filter_threads, 0, s>>>(m, act, act_n, target, cand, count, state,
+                                                                 gm + 1);
   } else {
-    k_coarse_filter_group<false><<<gg, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state,
-                                                           kGroupMax);
-    k_coarse_filter_append<false><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state,
-                                                            kGroupMax + 1);
+    if (t.group_lanes == 4) TRN_GROUP(false, 4);
+    else if (t.group_lanes == 16) TRN_GROUP(false, 16);
+    else TRN_GROUP(false, 8);
+    k_coarse_filter_append<false><<<g, t.filter_threads, 0, s>>>(m, act, act_n, target, cand, count, state,
+                                                                  gm + 1);
   }
+#undef TRN_GROUP
   note_launch();
   note_launch();
   check_launch("coarsen_filter_append");

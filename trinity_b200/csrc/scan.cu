@@ -191,6 +191,11 @@ void compact_u8(const uint8_t* flags, int n, int* list, ScanWs& ws, cudaStream_t
   note_launch();
 }
 
+static const Tune kDefaultTune;
+static thread_local const Tune* t_tune = nullptr;
+const Tune& tune() { return t_tune ? *t_tune : kDefaultTune; }
+void set_thread_tune(const Tune* t) { t_tune = t; }
+
 int grid_bounded(long long bound, long long cap, int threads) {
   return grid_for(bound < 0 ? cap : (bound < cap ? bound : cap), threads);
 }

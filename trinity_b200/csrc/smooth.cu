@@ -94,7 +94,7 @@ __device__ int move_laplacian(const DMesh& m, int i) {
 }
 
 template <bool F32>
-__global__ void __launch_bounds__(128, 6) k_smooth_move(DMesh m, const int* __restrict__ list, int n,
+__global__ void __launch_bounds__(256, 3) k_smooth_move(DMesh m, const int* __restrict__ list, int n,
                                                        const int* off, int c, int* counters) {
   if (trn_failed(m)) return;
   if (off) {   /* color class c of a device-side partition */
@@ -132,8 +132,9 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
   const double own = 4 + 1 + 8 + 2 * (kPt + kTen) + kAvgDeg * (2 * kIdx + kTri + 2 * kQ);
   const double nbr = (double) std::min<long long>((long long) m.capa_node, 6LL * n) * (kPt + kTen);
   ProfScope ps("smooth_move", s, n * own + nbr);
-  if (fp32) k_smooth_move<true><<<grid_for(hint, 128), 128, 0, s>>>(m, list, n, off, c, counters);
-  else k_smooth_move<false><<<grid_for(hint, 128), 128, 0, s>>>(m, list, n, off, c, counters);
+  const int t = tune().smooth_threads;
+  if (fp32) k_smooth_move<true><<<grid_for(hint, t), t, 0, s>>>(m, list, n, off, c, counters);
+  else k_smooth_move<false><<<grid_for(hint, t), t, 0, s>>>(m, list, n, off, c, counters);
   note_launch();
   check_launch("smooth_move");
 }

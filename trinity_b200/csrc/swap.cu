@@ -258,11 +258,12 @@ void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* m
                const int* dual, const int* dual_n, const int* ntasks, int* commit, bool strict_map,
                bool fp32, cudaStream_t s, long long bound) {
   ProfScope ps("swap_flip", s, 0.0);
+  const int ft = tune().flip_threads;
   if (fp32)
-    k_swap_flip<true><<<grid_bounded(bound, m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
+    k_swap_flip<true><<<grid_bounded(bound, m.capa_elem, ft), ft, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
                                                                    ntasks, commit, strict_map ? 1 : 0);
   else
-    k_swap_flip<false><<<grid_bounded(bound, m.capa_elem), TRN_THREADS, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
+    k_swap_flip<false><<<grid_bounded(bound, m.capa_elem, ft), ft, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
                                                                     ntasks, commit, strict_map ? 1 : 0);
   note_launch();
   check_launch("swap_flip");

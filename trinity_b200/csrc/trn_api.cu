@@ -72,6 +72,8 @@ struct trn_mesh {
   cudaStream_t body_stream = nullptr;   /* captures the loop bodies */
   int* rstats = nullptr;                /* device: examined / changed per stage */
   int round_depth = 0;
+  Tune tune;                /* launch shapes (trn_autotune) */
+  Tune round_tune;
   bool round_fp32 = false;
   uint64_t round_seed = 0;
   unsigned long long round_launches = 0;
@@ -127,7 +129,10 @@ int sync_status(trn_mesh* m, const int* count = nullptr) {
   return TRN_OK;
 }
 
-void begin_timing(trn_mesh* m) { cudaEventRecord(m->ev0, m->stream); }
+void begin_timing(trn_mesh* m) {
+  set_thread_tune(&m->tune);
+  cudaEventRecord(m->ev0, m->stream);
+}
 
 int end_timing(trn_mesh* m, trn_stats* st, int eval, int task) {
   cudaEventRecord(m->ev1, m->stream);
@@ -1069,6 +1074,7 @@ int capture_round(trn_mesh* m, int depth) {
   cudaStream_t s = m->stream, bs = m->body_stream;
   const int max_col = max_colors_of(8);
   unsigned* tick = reinterpret_cast<unsigned*>(m->status + S_TICK);
+  set_thread_tune(&m->tune);
   const unsigned long long l0 = thread_launches();
   CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   auto stage_stats = [&](int k) {
@@ -1115,6 +1121,7 @@ int capture_round(trn_mesh* m, int depth) {
     return fail(m, TRN_ERR_CUDA, std::string("round capture: ") + cudaGetErrorString(e));
   }
   m->round_depth = depth;
+  m->round_tune = m->tune;
   m->round_fp32 = m->fp32;
   m->round_seed = m->seed;
   m->round_launches = thread_launches() - l0;
@@ -1130,7 +1137,8 @@ int trn_round_graph_run(trn_mesh* m, int depth, trn_stats stats[4]) {
   if (depth < 1) return fail(m, TRN_ERR_INVALID, "round: depth < 1");
   if (m->replay) return fail(m, TRN_ERR_INVALID, "round: a captured round runs the free mode only");
   m->err.clear();
-  if (!m->round_exec || m->round_depth != depth || m->round_fp32 != m->fp32 || m->round_seed != m->seed) {
+  if (!m->round_exec || m->round_depth != depth || m->round_fp32 != m->fp32 || m->round_seed != m->seed ||
+      !(m->round_tune == m->tune)) {
     int rc = capture_round(m, depth);
     if (rc) return rc;
   }
@@ -1149,6 +1157,88 @@ int trn_round_graph_run(trn_mesh* m, int depth, trn_stats stats[4]) {
       stats[k].task += m->h_status[H_STATS + 2 * k + 1];
       if (k == 0) stats[k].elap += (int) m->last_ms;
     }
+  return rc;
+}
+
+/* ---------------- launch-shape autotuner ---------------- */
+int trn_get_tune(trn_mesh* m, int cfg[TRN_TUNE_N]) {
+  if (!m || !cfg) return TRN_ERR_INVALID;
+  const Tune& t = m->tune;
+  cfg[0] = t.smooth_threads;
+  cfg[1] = t.filter_threads;
+  cfg[2] = t.group_lanes;
+  cfg[3] = t.group_max;
+  cfg[4] = t.flip_threads;
+  return TRN_OK;
+}
+
+int trn_set_tune(trn_mesh* m, const int cfg[TRN_TUNE_N]) {
+  if (!m || !cfg) return TRN_ERR_INVALID;
+  auto pow2_in = [](int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; };
+  if (!pow2_in(cfg[0], 32, 256) || !pow2_in(cfg[1], 32, 1024) || (cfg[2] != 4 && cfg[2] != 8 && cfg[2] != 16) ||
+      cfg[3] < 0 || !pow2_in(cfg[4], 32, 1024))
+    return fail(m, TRN_ERR_INVALID, "set_tune: value out of range");
+  m->tune.smooth_threads = cfg[0];
+  m->tune.filter_threads = cfg[1];
+  m->tune.group_lanes = cfg[2];
+  m->tune.group_max = cfg[3];
+  m->tune.flip_threads = cfg[4];
+  return TRN_OK;
+}
+
+/* Coordinate descent over the launch shapes on this mesh: for each parameter
+ * in turn, every candidate is timed (the best of two runs of metric + rounds
+ * from the loaded input, device time of the rounds) with the others at their
+ * best so far. The shapes change no result, only the time. The mesh is
+ * reloaded at the end. */
+int trn_autotune(trn_mesh* m, double target_factor, int norm, double h_min, double h_max, int depth,
+                 int rounds, int cfg[TRN_TUNE_N]) {
+  if (!m || !m->pts0) return fail(m, TRN_ERR_INVALID, "autotune: nothing loaded");
+  if (m->replay) return fail(m, TRN_ERR_INVALID, "autotune: free mode only");
+  if (depth < 1 || rounds < 1) return fail(m, TRN_ERR_INVALID, "autotune: bad depth or rounds");
+  int rc = TRN_OK;
+  auto measure = [&](double* out) -> int {
+    double best = 1e300;
+    for (int rep = 0; rep < 2; ++rep) {
+      int r;
+      if ((r = trn_mesh_reload(m)) || (r = trn_metric_run(m, target_factor, norm, h_min, h_max, nullptr)))
+        return r;
+      double ms = 0;
+      for (int k = 0; k < rounds; ++k) {
+        if ((r = trn_refine_run(m, depth, nullptr))) return r;
+        ms += m->last_ms;
+        if ((r = trn_coarsen_run(m, 8, nullptr))) return r;
+        ms += m->last_ms;
+        if ((r = trn_swap_run(m, nullptr))) return r;
+        ms += m->last_ms;
+        if ((r = trn_smooth_run(m, 8, depth, nullptr))) return r;
+        ms += m->last_ms;
+      }
+      best = std::min(best, ms);
+    }
+    *out = best;
+    return TRN_OK;
+  };
+  int* fields[5] = {&m->tune.smooth_threads, &m->tune.filter_threads, &m->tune.group_lanes,
+                    &m->tune.group_max, &m->tune.flip_threads};
+  const std::vector<std::vector<int>> cands = {
+      {64, 128, 256}, {128, 256, 512}, {4, 8, 16}, {4096, 16384, 65536}, {128, 256, 512}};
+  for (int f = 0; f < 5 && rc == TRN_OK; ++f) {
+    int best_v = *fields[f];
+    double best_ms = 1e300;
+    for (int v : cands[f]) {
+      *fields[f] = v;
+      double ms;
+      if ((rc = measure(&ms))) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_v = v;
+      }
+    }
+    *fields[f] = best_v;
+  }
+  if (rc == TRN_OK) rc = trn_mesh_reload(m);
+  if (rc == TRN_OK && cfg) trn_get_tune(m, cfg);
   return rc;
 }
 

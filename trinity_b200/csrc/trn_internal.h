@@ -47,6 +47,23 @@ constexpr int kLevelCap = 100000;
 void level_end(int* status, int kind, int cap, const int* next, int* cur, int hint, cudaStream_t s,
                cudaGraphConditionalHandle h, bool use_h);
 
+/* launch shapes the autotuner (trn_autotune) chooses; none of them changes
+ * a result. Each mesh keeps its own table; the C-ABI entry that drives a
+ * mesh makes it the calling thread's table for the launchers. */
+struct Tune {
+  int smooth_threads = 128;   /* k_smooth_move block: 64, 128, 256 */
+  int filter_threads = 256;   /* one-lane collapse-target search block: 128, 256, 512 */
+  int group_lanes = 8;        /* lanes per vertex of the grouped search: 4, 8, 16 */
+  int group_max = 16384;      /* longest level list the grouped search takes */
+  int flip_threads = 256;     /* k_swap_flip block: 128, 256, 512 */
+  bool operator==(const Tune& o) const {
+    return smooth_threads == o.smooth_threads && filter_threads == o.filter_threads &&
+           group_lanes == o.group_lanes && group_max == o.group_max && flip_threads == o.flip_threads;
+  }
+};
+const Tune& tune();
+void set_thread_tune(const Tune* t);
+
 /* grid for a grid-stride kernel over n items: a multiple of the SM count */
 int grid_for(long long n, int threads = TRN_THREADS);
 /* grid for a kernel over a device-counted list: sized for `bound` items (an
