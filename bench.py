@@ -155,7 +155,7 @@ def b200_arm(args, rank, world, local_rank):
     g.set_options(seed=0x7472696E697479 + rank)
     heur = api.Partit(g, 8)
     kern = [api.Refine(g, c["depth"]), api.Coarse(g, heur), api.Swap(g), api.Smooth(g, heur, c["depth"])]
-    tuned = g.autotune(c["target"], c["norm"], depth=c["depth"], rounds=1)   # launch shapes only
+    tuned = g.get_tune() if args.no_tune else g.autotune(c["target"], c["norm"], depth=c["depth"], rounds=1)
 
     def barrier():
         if dist_on:
@@ -304,7 +304,8 @@ def b200_arm(args, rank, world, local_rank):
                            for r in prof_all), key=lambda r: -r["ms"])[:10],
         "kernels_note": f"{min(args.steps, 2)} profiled steps (every launch timed), before the timed region",
         "final_mesh": {"nodes": final[2], "triangles": final[3]},
-        "launch_shapes": dict(tuned, chosen_by="trn_autotune on this mesh (changes no result)"),
+        "launch_shapes": dict(tuned, chosen_by="defaults (--no-tune)" if args.no_tune
+                              else "trn_autotune on this mesh (changes no result)"),
         "clocks": clk.summary(),
     }
     if "mixed_fp32" in forms:
@@ -662,6 +663,7 @@ def main():
     p.add_argument("--workload", choices=["adapt", "batch"], default="adapt",
                    help="adapt: the 2M-triangle mesh (headline); batch: 256 meshes of uneven size")
     p.add_argument("--threads", type=int, default=0, help="host threads of the batched run")
+    p.add_argument("--no-tune", action="store_true", help="default launch shapes (no autotuning)")
     args = p.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
