@@ -48,8 +48,8 @@ __device__ int identify_target(const DMesh& m, int source) {
     int neigh = vc[b];
     bool bound_destin = (m.tags[neigh] & TRN_TAG_BOUND) != 0;
     if (bound_source && !bound_destin) continue;
-    double len = length_x<F32>(ps, m.pts[neigh], ts, m.ten[neigh]);
-    if (len < TRN_L_MIN) {
+    double len;
+    if (length_lt<F32>(ps, m.pts[neigh], ts, m.ten[neigh], TRN_L_MIN, &len)) {
       int p = nc;
       while (p > 0 && lens[p - 1] > len) {
         lens[p] = lens[p - 1];
@@ -85,10 +85,8 @@ __device__ int identify_target(const DMesh& m, int source) {
       double2 p0 = m.pts[f0], p1 = m.pts[f1], p2 = m.pts[f2];
       if (trn_ccw(p0, p1, p2)) {
         double4 t0 = m.ten[f0], t1 = m.ten[f1], t2 = m.ten[f2];
-        double l0 = length_x<F32>(p0, p1, t0, t1);
-        double l1 = length_x<F32>(p1, p2, t1, t2);
-        double l2 = length_x<F32>(p2, p0, t2, t0);
-        skip = (l0 > TRN_L_MAX || l1 > TRN_L_MAX || l2 > TRN_L_MAX);
+        skip = length_gt<F32>(p0, p1, t0, t1, TRN_L_MAX) || length_gt<F32>(p1, p2, t1, t2, TRN_L_MAX) ||
+               length_gt<F32>(p2, p0, t2, t0, TRN_L_MAX);
         continue;
       }
       skip = true;
@@ -198,8 +196,8 @@ __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, cons
         const bool bd = (m.tags[w] & TRN_TAG_BOUND) != 0;
         if (bd) boundm |= 1u << b;
         if (!(bsrc && !bd)) {
-          const double len = length_x<F32>(ps, m.pts[w], ts, m.ten[w]);
-          if (len < TRN_L_MIN) {
+          double len;
+          if (length_lt<F32>(ps, m.pts[w], ts, m.ten[w], TRN_L_MIN, &len)) {
             candm |= 1u << b;
             lenk[k] = len;
           }
@@ -235,10 +233,9 @@ __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, cons
       const double2 p0 = m.pts[f0], p1 = m.pts[f1], p2 = m.pts[f2];
       if (trn_ccw(p0, p1, p2)) {
         const double4 t0 = m.ten[f0], t1 = m.ten[f1], t2 = m.ten[f2];
-        const double l0 = length_x<F32>(p0, p1, t0, t1);
-        const double l1 = length_x<F32>(p1, p2, t1, t2);
-        const double l2 = length_x<F32>(p2, p0, t2, t0);
-        if (l0 > TRN_L_MAX || l1 > TRN_L_MAX || l2 > TRN_L_MAX) failm |= bit;
+        if (length_gt<F32>(p0, p1, t0, t1, TRN_L_MAX) || length_gt<F32>(p1, p2, t1, t2, TRN_L_MAX) ||
+            length_gt<F32>(p2, p0, t2, t0, TRN_L_MAX))
+          failm |= bit;
       } else {
         failm |= bit;
       }

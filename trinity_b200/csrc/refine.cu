@@ -99,8 +99,7 @@ __global__ void k_ref_filter(DMesh m, int nb_elems, int4* __restrict__ info,
     int opp[3] = {-1, -1, -1};
     for (int j = 0; j < 3; ++j) {
       int k = (j + 1) % 3;
-      double len = length_x<F32>(p[j], p[k], q[j], q[k]);
-      if (len > TRN_L_MAX) {
+      if (length_gt<F32>(p[j], p[k], q[j], q[k], TRN_L_MAX)) {
         lmask |= 1 << j;
         int o = elem_neigh(m, i, n[j], n[k]);
         opp[j] = o;

@@ -115,17 +115,27 @@ __device__ __forceinline__ double trnf_quality_l(double2 pa, double2 pb, double2
   return (double) ((float) area * norm * sqrtf(det) / (perim * perim));
 }
 
-/* metric edge length (numeric.cpp:469-497) in FP32 */
-__device__ __forceinline__ float trnf_dist2(double2 pa, double2 pb, double4 ta, double4 tb) {
+/* metric edge length (numeric.cpp:469-497) in FP32, in the same two halves */
+__device__ __forceinline__ void trnf_dist2_ends(double2 pa, double2 pb, double4 ta, double4 tb,
+                                                float* l0, float* l1) {
   const float w0 = (float) (pb.x - pa.x), w1 = (float) (pb.y - pa.y);
   const float a0 = (float) ta.x, a1 = (float) ta.y, a2 = (float) ta.z;
   const float b0 = (float) tb.x, b1 = (float) tb.y, b2 = (float) tb.z;
-  const float l0 = sqrtf(w0 * (a0 * w0 + a1 * w1) + w1 * (a1 * w0 + a2 * w1));
-  const float l1 = sqrtf(w0 * (b0 * w0 + b1 * w1) + w1 * (b1 * w0 + b2 * w1));
+  *l0 = sqrtf(w0 * (a0 * w0 + a1 * w1) + w1 * (a1 * w0 + a2 * w1));
+  *l1 = sqrtf(w0 * (b0 * w0 + b1 * w1) + w1 * (b1 * w0 + b2 * w1));
+}
+
+__device__ __forceinline__ float trnf_dist2_finish(float l0, float l1) {
   if (fabsf(l0 - l1) < 1.e-9f) return l0;
   const float lmin = trnf_min(l0, l1), lmax = trnf_max(l0, l1);
   const float ratio = lmax / lmin;
   return lmax * (ratio - 1.f) / (ratio * logf(ratio));
+}
+
+__device__ __forceinline__ float trnf_dist2(double2 pa, double2 pb, double4 ta, double4 tb) {
+  float l0, l1;
+  trnf_dist2_ends(pa, pb, ta, tb, &l0, &l1);
+  return trnf_dist2_finish(l0, l1);
 }
 
 __device__ __forceinline__ float trnf_dist1(double2 pa, double2 pb, double4 t) {
@@ -176,6 +186,52 @@ template <bool F32>
 __device__ __forceinline__ double length_x(double2 pa, double2 pb, double4 ta, double4 tb) {
   if constexpr (F32) return (double) trnf_dist2(pa, pb, ta, tb);
   else return trn_dist2(pa, pb, ta, tb);
+}
+
+/* Comparisons of a metric edge length with a threshold, with the answer of
+ * comparing length_x itself. That length interpolates the edge's lengths
+ * under its two endpoint tensors geometrically, so it lies between them: up
+ * to a few units in the last place as computed, far inside the margins below
+ * (1e-12 relative in FP64, 1e-5 in FP32). When the threshold lies outside
+ * that range, with the margin, the answer is known without the logarithm. */
+template <bool F32>
+__device__ __forceinline__ bool length_gt(double2 pa, double2 pb, double4 ta, double4 tb, double thresh) {
+  if constexpr (F32) {
+    float l0, l1;
+    trnf_dist2_ends(pa, pb, ta, tb, &l0, &l1);
+    const float t = (float) thresh;
+    if (l0 == l0 && l1 == l1) {
+      if (trnf_max(l0, l1) < t * (1.f - 1.e-5f)) return false;
+      if (trnf_min(l0, l1) > t * (1.f + 1.e-5f)) return true;
+    }
+    return (double) trnf_dist2_finish(l0, l1) > thresh;
+  } else {
+    double l0, l1;
+    trn_dist2_ends(pa, pb, ta, tb, &l0, &l1);
+    if (l0 == l0 && l1 == l1) {
+      if (trn_dmax(l0, l1) < thresh * (1 - 1.e-12)) return false;
+      if (trn_dmin(l0, l1) > thresh * (1 + 1.e-12)) return true;
+    }
+    return trn_dist2_finish(l0, l1) > thresh;
+  }
+}
+
+/* length_x < thresh; *len receives length_x whenever the answer is true */
+template <bool F32>
+__device__ __forceinline__ bool length_lt(double2 pa, double2 pb, double4 ta, double4 tb, double thresh,
+                                          double* len) {
+  if constexpr (F32) {
+    float l0, l1;
+    trnf_dist2_ends(pa, pb, ta, tb, &l0, &l1);
+    if (l0 == l0 && l1 == l1 && trnf_min(l0, l1) > (float) thresh * (1.f + 1.e-5f)) return false;
+    *len = (double) trnf_dist2_finish(l0, l1);
+  } else {
+    double l0, l1;
+    trn_dist2_ends(pa, pb, ta, tb, &l0, &l1);
+    if (l0 == l0 && l1 == l1 && trn_dmin(l0, l1) > thresh * (1 + 1.e-12)) return false;
+    *len = trn_dist2_finish(l0, l1);
+  }
+  return *len < thresh;
 }
 
 /* mean of a run of cached logarithms, then exponentiated: the new tensor */

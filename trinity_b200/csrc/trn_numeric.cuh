@@ -168,21 +168,33 @@ __device__ __forceinline__ double trn_dist1(double2 pa, double2 pb, double4 t) {
   return sqrt(u0 * v0 + u1 * v1);
 }
 
-/* numeric::approxRiemannDist(a, b, Ma, Mb), numeric.cpp:469-497 */
-__device__ __forceinline__ double trn_dist2(double2 pa, double2 pb, double4 ta, double4 tb) {
+/* numeric::approxRiemannDist(a, b, Ma, Mb), numeric.cpp:469-497, in two
+ * halves: the edge's length under each endpoint tensor, then their
+ * geometric interpolation */
+__device__ __forceinline__ void trn_dist2_ends(double2 pa, double2 pb, double4 ta, double4 tb,
+                                               double* l0, double* l1) {
   double w0 = pb.x - pa.x;
   double w1 = pb.y - pa.y;
   double m0 = ta.x * w0 + ta.y * w1;
   double m1 = ta.y * w0 + ta.z * w1;
   double m2 = tb.x * w0 + tb.y * w1;
   double m3 = tb.y * w0 + tb.z * w1;
-  double l0 = sqrt(w0 * m0 + w1 * m1);
-  double l1 = sqrt(w0 * m2 + w1 * m3);
+  *l0 = sqrt(w0 * m0 + w1 * m1);
+  *l1 = sqrt(w0 * m2 + w1 * m3);
+}
+
+__device__ __forceinline__ double trn_dist2_finish(double l0, double l1) {
   if (fabs(l0 - l1) < TRN_EPS) return l0;
   double lmin = trn_dmin(l0, l1);
   double lmax = trn_dmax(l0, l1);
   double ratio = lmax / lmin;
   return lmax * (ratio - 1) / (ratio * trn_log(ratio));
+}
+
+__device__ __forceinline__ double trn_dist2(double2 pa, double2 pb, double4 ta, double4 tb) {
+  double l0, l1;
+  trn_dist2_ends(pa, pb, ta, tb, &l0, &l1);
+  return trn_dist2_finish(l0, l1);
 }
 
 /* numeric::computeSteinerPoint, numeric.cpp:387-445 (la, lb: cached
