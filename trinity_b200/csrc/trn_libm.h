@@ -17,10 +17,12 @@
  * Methods (textbook, Cody & Waite, "Software Manual for the Elementary
  * Functions", 1980):
  *   exp(x): x = k ln2 + r with ln2 split in a 32-bit head (k*head exact) and
- *           a tail; exp(r), |r| <= ln2/2, by its Taylor series to degree 14 in
- *           Horner form; scale by 2^k built from the exponent bits.
+ *           a tail; exp(r), |r| <= ln2/2, by its Taylor series to degree 14,
+ *           evaluated by Estrin's scheme (short dependency chains: the GPU
+ *           kernels that call it are latency-bound); scale by 2^k built from
+ *           the exponent bits.
  *   log(x): x = 2^e m with m in [sqrt(1/2), sqrt(2)); log(m) = 2 atanh(s),
- *           s = (m-1)/(m+1), |s| <= 0.1716, odd series to s^25;
+ *           s = (m-1)/(m+1), |s| <= 0.1716, odd series to s^25 (Estrin);
  *           log(x) = e*ln2_head + (e*ln2_tail + log(m)).
  *   pow(x,y): y == 2 -> x*x, y == 3 -> (x*x)*x (the reference only raises to
  *           these integer powers and to one fractional exponent, -1/(2p+2));
@@ -78,22 +80,21 @@ TRN_HD double trn_exp(double x) {
   int k = (int)(t + (t >= 0.0 ? 0.5 : -0.5)); /* round half away from zero */
   double kd = (double)k;
   double r = (x - kd * TRN_LN2_HI) - kd * TRN_LN2_LO;
-  /* Taylor coefficients 1/n!, n = 0..14 (correctly rounded) */
-  double p = 0x1.93974a8c07c9dp-37;
-  p = 0x1.6124613a86d09p-33 + r * p;
-  p = 0x1.1eed8eff8d898p-29 + r * p;
-  p = 0x1.ae64567f544e4p-26 + r * p;
-  p = 0x1.27e4fb7789f5cp-22 + r * p;
-  p = 0x1.71de3a556c734p-19 + r * p;
-  p = 0x1.a01a01a01a01ap-16 + r * p;
-  p = 0x1.a01a01a01a01ap-13 + r * p;
-  p = 0x1.6c16c16c16c17p-10 + r * p;
-  p = 0x1.1111111111111p-7 + r * p;
-  p = 0x1.5555555555555p-5 + r * p;
-  p = 0x1.5555555555555p-3 + r * p;
-  p = 0x1.0000000000000p-1 + r * p;
-  p = 1.0 + r * p;
-  p = 1.0 + r * p;
+  /* Taylor coefficients 1/n!, n = 0..14 (correctly rounded), evaluated by
+   * Estrin's scheme: pairs, then pairs of pairs in r^2, r^4, r^8, so that the
+   * chain of dependent operations is 8 long instead of Horner's 28 */
+  const double r2 = r * r, r4 = r2 * r2, r8 = r4 * r4;
+  const double a0 = 1.0 + r;
+  const double a1 = 0x1.0000000000000p-1 + 0x1.5555555555555p-3 * r;
+  const double a2 = 0x1.5555555555555p-5 + 0x1.1111111111111p-7 * r;
+  const double a3 = 0x1.6c16c16c16c17p-10 + 0x1.a01a01a01a01ap-13 * r;
+  const double a4 = 0x1.a01a01a01a01ap-16 + 0x1.71de3a556c734p-19 * r;
+  const double a5 = 0x1.27e4fb7789f5cp-22 + 0x1.ae64567f544e4p-26 * r;
+  const double a6 = 0x1.1eed8eff8d898p-29 + 0x1.6124613a86d09p-33 * r;
+  const double a7 = 0x1.93974a8c07c9dp-37;
+  const double b0 = a0 + a1 * r2, b1 = a2 + a3 * r2, b2 = a4 + a5 * r2, b3 = a6 + a7 * r2;
+  const double d0 = b0 + b1 * r4, d1 = b2 + b3 * r4;
+  const double p = d0 + d1 * r8;
   /* scale by 2^k, in two steps when 2^k alone is not a normal number */
   if (k > 1023) return (p * trn_pow2i(1023)) * trn_pow2i(k - 1023);
   if (k < -1022) return (p * trn_pow2i(-1022)) * trn_pow2i(k + 1022 < -1022 ? -1022 : k + 1022);
@@ -121,19 +122,17 @@ TRN_HD double trn_log(double x) {
   double f = m - 1.0;
   double s = f / (2.0 + f);
   double z = s * s;
-  /* 1/(2n+1), n = 1..12 */
-  double q = 0x1.47ae147ae147bp-5;
-  q = 0x1.642c8590b2164p-5 + z * q;
-  q = 0x1.8618618618618p-5 + z * q;
-  q = 0x1.af286bca1af28p-5 + z * q;
-  q = 0x1.e1e1e1e1e1e1ep-5 + z * q;
-  q = 0x1.1111111111111p-4 + z * q;
-  q = 0x1.3b13b13b13b14p-4 + z * q;
-  q = 0x1.745d1745d1746p-4 + z * q;
-  q = 0x1.c71c71c71c71cp-4 + z * q;
-  q = 0x1.2492492492492p-3 + z * q;
-  q = 0x1.999999999999ap-3 + z * q;
-  q = 0x1.5555555555555p-2 + z * q;
+  /* 1/(2n+1), n = 1..12, as a polynomial in z, by Estrin's scheme (a chain
+   * of 8 dependent operations instead of 22) */
+  const double z2 = z * z, z4 = z2 * z2, z8 = z4 * z4;
+  const double a0 = 0x1.5555555555555p-2 + 0x1.999999999999ap-3 * z;
+  const double a1 = 0x1.2492492492492p-3 + 0x1.c71c71c71c71cp-4 * z;
+  const double a2 = 0x1.745d1745d1746p-4 + 0x1.3b13b13b13b14p-4 * z;
+  const double a3 = 0x1.1111111111111p-4 + 0x1.e1e1e1e1e1e1ep-5 * z;
+  const double a4 = 0x1.af286bca1af28p-5 + 0x1.8618618618618p-5 * z;
+  const double a5 = 0x1.642c8590b2164p-5 + 0x1.47ae147ae147bp-5 * z;
+  const double b0 = a0 + a1 * z2, b1 = a2 + a3 * z2, b2 = a4 + a5 * z2;
+  const double q = (b0 + b1 * z4) + b2 * z8;
   double two_s = s + s;
   double logm = two_s + two_s * (z * q);
   double ed = (double)e;
