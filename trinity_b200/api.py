@@ -115,12 +115,20 @@ class Mesh:
         self._check(self._L.trn_mesh_export(self.h, _p(pts), _p(ten), _p(tri), _p(alive), _p(tags)))
         return pts, ten, tri, alive, tags
 
-    def export_compact(self, with_tensor: bool = True):
+    def export_compact(self, with_tensor: bool = True, out=None):
         """The adapted mesh without deleted entities, renumbered like
-        Mesh::store: (points[V',2], tris[T',3] 0-based, tensor[V',3] or None)."""
+        Mesh::store: (points[V',2], tris[T',3] 0-based, tensor[V',3] or None).
+        out: optional (points, tris, tensor) arrays with at least V' / T' rows
+        (e.g. views of pinned host memory); the results are their leading rows."""
         _, _, nv, ne = self.counts()
-        pts = np.empty((nv, 2)); tri = np.empty((ne, 3), np.int32)
-        ten = np.empty((nv, 3)) if with_tensor else None
+        if out is not None:
+            if out[0].shape[0] < nv or out[1].shape[0] < ne or (with_tensor and out[2].shape[0] < nv):
+                raise ValueError("export_compact: output arrays too small")
+            pts, tri = out[0][:nv], out[1][:ne]
+            ten = out[2][:nv] if with_tensor else None
+        else:
+            pts = np.empty((nv, 2)); tri = np.empty((ne, 3), np.int32)
+            ten = np.empty((nv, 3)) if with_tensor else None
         a, b = ctypes.c_int(), ctypes.c_int()
         self._check(self._L.trn_mesh_export_compact(self.h, _p(pts), _p(tri), _p(ten) if with_tensor else None,
                                                     ctypes.byref(a), ctypes.byref(b)))
