@@ -40,17 +40,33 @@ __device__ int move_laplacian(const DMesh& m, int i) {
   const LogT<F32> lini = log_load<F32>(m, i);
   double ox = 0, oy = 0;
   LogSum<F32> lsum;
-  for (int k = 0; k < nb_neigh; ++k) {
-    const int nb = vc[k];
-    const double2 pb = m.pts[nb];
-    const double4 tb = m.ten[nb];
-    const double len = length_x<F32>(pini, pb, tini, tb);
-    ox += pini.x + ((pb.x - pini.x) / len);
-    oy += pini.y + ((pb.y - pini.y) / len);
-    lsum.add(log_load<F32>(m, nb));
+  if constexpr (F32) {
+    /* the mean displacement in single precision, added to the FP64 point */
+    float dx = 0.f, dy = 0.f;
+    for (int k = 0; k < nb_neigh; ++k) {
+      const int nb = vc[k];
+      const double2 pb = m.pts[nb];
+      const float il = __frcp_rn(trnf_dist2(pini, pb, tini, m.ten[nb]));
+      dx += (float) (pb.x - pini.x) * il;
+      dy += (float) (pb.y - pini.y) * il;
+      lsum.add(log_load<F32>(m, nb));
+    }
+    const float inv = __frcp_rn((float) nb_neigh);
+    ox = pini.x + (double) (dx * inv);
+    oy = pini.y + (double) (dy * inv);
+  } else {
+    for (int k = 0; k < nb_neigh; ++k) {
+      const int nb = vc[k];
+      const double2 pb = m.pts[nb];
+      const double4 tb = m.ten[nb];
+      const double len = length_x<F32>(pini, pb, tini, tb);
+      ox += pini.x + ((pb.x - pini.x) / len);
+      oy += pini.y + ((pb.y - pini.y) / len);
+      lsum.add(log_load<F32>(m, nb));
+    }
+    ox /= nb_neigh;
+    oy /= nb_neigh;
   }
-  ox /= nb_neigh;
-  oy /= nb_neigh;
   double tn[3];
   lsum.finish(nb_neigh, tn);
   const double4 tnew = make_double4(tn[0], tn[1], tn[2], 0.0);

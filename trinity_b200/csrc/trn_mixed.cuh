@@ -10,6 +10,10 @@
  * the metric values. The log cache holds a float4 per vertex in the same
  * buffer as the FP64 form's double4.
  *
+ * Divisions become reciprocal multiplications here (FP32 results within a
+ * few ulp of the divided forms; the FP64 form keeps the reference's
+ * divisions for its bit-exactness).
+ *
  * Templates at the end (LogT<F32>, log_of<F32>, quality_x, length_x, ...)
  * let one kernel source serve both forms; the FP64 instantiation calls the
  * bit-exact functions unchanged.
@@ -60,12 +64,14 @@ __device__ __forceinline__ void trnf_eigen(const float* mat, float* val, float* 
     vec[2] = -0.5f * dm - root;
     vec[3] = mat[1];
   }
-  float n0 = sqrtf(vec[0] * vec[0] + vec[1] * vec[1]);
-  float n1 = sqrtf(vec[2] * vec[2] + vec[3] * vec[3]);
-  vec[0] /= n0;
-  vec[2] /= n1;
-  vec[1] /= n0;
-  vec[3] /= n1;
+  /* the reference divides by the norms; single precision multiplies by
+   * reciprocal square roots (within a few ulp) */
+  const float r0 = rsqrtf(vec[0] * vec[0] + vec[1] * vec[1]);
+  const float r1 = rsqrtf(vec[2] * vec[2] + vec[3] * vec[3]);
+  vec[0] *= r0;
+  vec[2] *= r1;
+  vec[1] *= r0;
+  vec[3] *= r1;
 }
 
 /* P log(D) P^T of one tensor, FP32 */
@@ -83,8 +89,8 @@ __device__ __forceinline__ float4 trnf_log_tensor(float t0, float t1, float t2) 
  * (exact in exact arithmetic, free of the cancellation of m11 m22 - m12^2) */
 __device__ __forceinline__ void trnf_interp_finish(float* lm, int nb, float* res, float* det = nullptr) {
   float val[2], vec[4];
-  const float inv = (float) nb;
-  for (int i = 0; i < 4; ++i) lm[i] /= inv;
+  const float inv = nb == 3 ? 0.333333343f : __frcp_rn((float) nb);
+  for (int i = 0; i < 4; ++i) lm[i] *= inv;
   trnf_eigen(lm, val, vec);
   val[0] = expf(val[0]);
   val[1] = expf(val[1]);
@@ -109,10 +115,11 @@ __device__ __forceinline__ double trnf_quality_l(double2 pa, double2 pb, double2
     perim += sqrtf(u * (j[0] * u + j[1] * v) + v * (j[1] * u + j[2] * v));
   }
   const double area = 0.5 * fabs((pb.x - pa.x) * (pc.y - pa.y) - (pc.x - pa.x) * (pb.y - pa.y));
-  const float mean = trnf_min(perim / 3.f, 3.f / perim);
+  const float ip = __frcp_rn(perim);
+  const float mean = trnf_min(perim * 0.333333343f, 3.f * ip);
   const float mm = mean * (2.f - mean);
   const float norm = 20.78460969082653f * (mm * mm * mm);  /* 12 sqrt(3) */
-  return (double) ((float) area * norm * sqrtf(det) / (perim * perim));
+  return (double) ((float) area * norm * sqrtf(det) * (ip * ip));
 }
 
 /* metric edge length (numeric.cpp:469-497) in FP32, in the same two halves */
@@ -128,8 +135,8 @@ __device__ __forceinline__ void trnf_dist2_ends(double2 pa, double2 pb, double4 
 __device__ __forceinline__ float trnf_dist2_finish(float l0, float l1) {
   if (fabsf(l0 - l1) < 1.e-9f) return l0;
   const float lmin = trnf_min(l0, l1), lmax = trnf_max(l0, l1);
-  const float ratio = lmax / lmin;
-  return lmax * (ratio - 1.f) / (ratio * logf(ratio));
+  const float ratio = lmax * __frcp_rn(lmin);
+  return lmax * (ratio - 1.f) * __frcp_rn(ratio * logf(ratio));
 }
 
 __device__ __forceinline__ float trnf_dist2(double2 pa, double2 pb, double4 ta, double4 tb) {
