@@ -673,7 +673,7 @@ __device__ int move_gradient(const DMesh& m, int i, double max_len, int mode) {
     if (valid) {
       m.pts[i] = pa;
       if (follow) {
-        m.ten[i] = tnew;
+        ten_store<F32>(m, i, tnew);
         log_store<F32>(m, i, lnew);
       }
       for (int a = 0; a < deg; ++a) m.qual[st[a]] = qual[a];

@@ -43,13 +43,13 @@ __device__ int identify_target(const DMesh& m, int source) {
   const int* vc = m.vic + (size_t) source * m.bucket;
   const int nv = m.vdeg[source];
   const double2 ps = m.pts[source];
-  const double4 ts = m.ten[source];
+  const TenT<F32> ts = ten_load<F32>(m, source);
   for (int b = 0; b < nv; ++b) {
     int neigh = vc[b];
     bool bound_destin = (m.tags[neigh] & TRN_TAG_BOUND) != 0;
     if (bound_source && !bound_destin) continue;
     double len;
-    if (length_lt<F32>(ps, m.pts[neigh], ts, m.ten[neigh], TRN_L_MIN, &len)) {
+    if (length_lt<F32>(ps, m.pts[neigh], ts, ten_load<F32>(m, neigh), TRN_L_MIN, &len)) {
       int p = nc;
       while (p > 0 && lens[p - 1] > len) {
         lens[p] = lens[p - 1];
@@ -84,7 +84,7 @@ __device__ int identify_target(const DMesh& m, int source) {
       int f2 = (n.z == source ? destin : n.z);
       double2 p0 = m.pts[f0], p1 = m.pts[f1], p2 = m.pts[f2];
       if (trn_ccw(p0, p1, p2)) {
-        double4 t0 = m.ten[f0], t1 = m.ten[f1], t2 = m.ten[f2];
+        const TenT<F32> t0 = ten_load<F32>(m, f0), t1 = ten_load<F32>(m, f1), t2 = ten_load<F32>(m, f2);
         skip = length_gt<F32>(p0, p1, t0, t1, TRN_L_MAX) || length_gt<F32>(p1, p2, t1, t2, TRN_L_MAX) ||
                length_gt<F32>(p2, p0, t2, t0, TRN_L_MAX);
         continue;
@@ -180,10 +180,10 @@ __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, cons
     const int* st = m.stenc + (size_t) (v >= 0 ? v : 0) * m.bucket;
     const bool bsrc = v >= 0 && (m.tags[v] & TRN_TAG_BOUND) != 0;
     double2 ps = make_double2(0, 0);
-    double4 ts = make_double4(0, 0, 0, 0);
+    TenT<F32> ts{};
     if (grp) {
       ps = m.pts[v];
-      ts = m.ten[v];
+      ts = ten_load<F32>(m, v);
     }
     /* neighbours b = gl + G * k: candidates closer than 1/sqrt(2) */
     double lenk[32 / G];
@@ -197,7 +197,7 @@ __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, cons
         if (bd) boundm |= 1u << b;
         if (!(bsrc && !bd)) {
           double len;
-          if (length_lt<F32>(ps, m.pts[w], ts, m.ten[w], TRN_L_MIN, &len)) {
+          if (length_lt<F32>(ps, m.pts[w], ts, ten_load<F32>(m, w), TRN_L_MIN, &len)) {
             candm |= 1u << b;
             lenk[k] = len;
           }
@@ -232,7 +232,7 @@ __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, cons
       const int f2 = (e.z == v ? destin : e.z);
       const double2 p0 = m.pts[f0], p1 = m.pts[f1], p2 = m.pts[f2];
       if (trn_ccw(p0, p1, p2)) {
-        const double4 t0 = m.ten[f0], t1 = m.ten[f1], t2 = m.ten[f2];
+        const TenT<F32> t0 = ten_load<F32>(m, f0), t1 = ten_load<F32>(m, f1), t2 = ten_load<F32>(m, f2);
         if (length_gt<F32>(p0, p1, t0, t1, TRN_L_MAX) || length_gt<F32>(p1, p2, t1, t2, TRN_L_MAX) ||
             length_gt<F32>(p2, p0, t2, t0, TRN_L_MAX))
           failm |= bit;

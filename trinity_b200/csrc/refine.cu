@@ -94,7 +94,7 @@ __global__ void k_ref_filter(DMesh m, int nb_elems, int4* __restrict__ info,
     }
     int n[3] = {t.x, t.y, t.z};
     double2 p[3] = {m.pts[n[0]], m.pts[n[1]], m.pts[n[2]]};
-    double4 q[3] = {m.ten[n[0]], m.ten[n[1]], m.ten[n[2]]};
+    const TenT<F32> q[3] = {ten_load<F32>(m, n[0]), ten_load<F32>(m, n[1]), ten_load<F32>(m, n[2])};
     int lmask = 0, pmask = 0;
     int opp[3] = {-1, -1, -1};
     for (int j = 0; j < 3; ++j) {
@@ -130,10 +130,10 @@ __global__ void k_ref_steiner(DMesh m, int nb_elems, int nb_nodes, const int4* _
       int v1 = n[j], v2 = n[(j + 1) % 3];
       double2 rp;
       double rt[3];
-      steiner_x<F32>(m.pts[v1], m.pts[v2], m.ten[v1], m.ten[v2], log_load<F32>(m, v1),
+      steiner_x<F32>(m.pts[v1], m.pts[v2], ten_load<F32>(m, v1), ten_load<F32>(m, v2), log_load<F32>(m, v1),
                      log_load<F32>(m, v2), &rp, rt);
       m.pts[id] = rp;
-      m.ten[id] = make_double4(rt[0], rt[1], rt[2], 0.0);
+      ten_store<F32>(m, id, make_double4(rt[0], rt[1], rt[2], 0.0));
       log_store<F32>(m, id, log_of<F32>(rt[0], rt[1], rt[2]));
       if (opp[j] < 0) m.tags[id] = TRN_TAG_BOUND;
       h_insert(hkey, hval, hcap, edge_key(v1, v2), id, m.err);
@@ -183,8 +183,8 @@ __global__ void k_ref_cut(DMesh m, int nb_elems, const int4* __restrict__ info,
            * the two sides of an edge measure it differently) leaves the
            * element uncut instead of reading vertex -1 */
           if (s[j] < 0 || s[k] < 0) break;
-          double diag0 = length_x<F32>(m.pts[n[j]], m.pts[s[j]], m.ten[n[j]], m.ten[s[j]]);
-          double diag1 = length_x<F32>(m.pts[n[k]], m.pts[s[k]], m.ten[n[k]], m.ten[s[k]]);
+          double diag0 = length_x<F32>(m.pts[n[j]], m.pts[s[j]], ten_load<F32>(m, n[j]), ten_load<F32>(m, s[j]));
+          double diag1 = length_x<F32>(m.pts[n[k]], m.pts[s[k]], ten_load<F32>(m, n[k]), ten_load<F32>(m, s[k]));
           int v = (diag0 < diag1 ? j : k);
           int w = (v == j ? k : j);
           const int a3[3] = {t[0], t[1], t[2]};

@@ -37,6 +37,7 @@ __device__ int move_laplacian(const DMesh& m, int i) {
   for (int a = 0; a < deg; ++a) q_min = trn_dmin(q_min, m.qual[st[a]]);
   const double2 pini = m.pts[i];
   const double4 tini = m.ten[i];
+  const TenT<F32> tinf = ten_load<F32>(m, i);
   const LogT<F32> lini = log_load<F32>(m, i);
   double ox = 0, oy = 0;
   LogSum<F32> lsum;
@@ -46,7 +47,7 @@ __device__ int move_laplacian(const DMesh& m, int i) {
     for (int k = 0; k < nb_neigh; ++k) {
       const int nb = vc[k];
       const double2 pb = m.pts[nb];
-      const float il = __frcp_rn(trnf_dist2(pini, pb, tini, m.ten[nb]));
+      const float il = __frcp_rn(trnf_dist2(pini, pb, tenf_of(tinf), tenf_of(ten_load<F32>(m, nb))));
       dx += (float) (pb.x - pini.x) * il;
       dy += (float) (pb.y - pini.y) * il;
       lsum.add(log_load<F32>(m, nb));
@@ -71,7 +72,7 @@ __device__ int move_laplacian(const DMesh& m, int i) {
   lsum.finish(nb_neigh, tn);
   const double4 tnew = make_double4(tn[0], tn[1], tn[2], 0.0);
   const LogT<F32> lnew = log_of<F32>(tn[0], tn[1], tn[2]);
-  m.ten[i] = tnew;
+  ten_store<F32>(m, i, tnew);
   log_store<F32>(m, i, lnew);
   double qual[TRN_MAX_DEG];
   bool valid;
@@ -103,7 +104,7 @@ __device__ int move_laplacian(const DMesh& m, int i) {
     for (int a = 0; a < deg; ++a) m.qual[st[a]] = qual[a];
   } else {
     m.pts[i] = pini;
-    m.ten[i] = tini;
+    ten_store<F32>(m, i, tini);
     log_store<F32>(m, i, lini);
   }
   return valid ? 1 : 0;

@@ -246,6 +246,7 @@ __global__ void k_log_cache_f32(DMesh m, int nb_nodes) {
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
     const double4 t = m.ten[v];
     log_store<true>(m, v, log_of<true>(t.x, t.y, t.z));
+    m.tenf[v] = tenf_of(t);
   }
 }
 

@@ -180,7 +180,7 @@ int dmalloc(trn_mesh* m, T** p, size_t count) {
 void release(trn_mesh* m) {
   if (!m) return;
   if (m->stream) cudaStreamSynchronize(m->stream);
-  void* bufs[] = {m->d.pts, m->d.ten, m->d.lten, m->d.tri, m->d.stenc, m->d.deg, m->d.vic, m->d.vdeg,
+  void* bufs[] = {m->d.pts, m->d.ten, m->d.lten, m->d.tenf, m->d.tri, m->d.stenc, m->d.deg, m->d.vic, m->d.vdeg,
                   m->d.tags, m->d.alive, m->d.fixes, m->d.activ, m->d.qual, m->solut, m->grad,
                   m->terms, m->complexity, m->target, m->flag, m->list, m->indep, m->map,
                   m->dual, m->dual_n, m->pairs, m->parts, m->stage, m->status, m->d_log, m->pts0,
@@ -303,6 +303,7 @@ int trn_mesh_create_ex(const int size[2], int bucket, int depth, int verbosity, 
   d.capa_node = m->capa_node;
   d.capa_elem = m->capa_elem;
   if ((rc = dmalloc(m, &d.pts, cn)) || (rc = dmalloc(m, &d.ten, cn)) || (rc = dmalloc(m, &d.lten, cn)) ||
+      (rc = dmalloc(m, &d.tenf, cn)) ||
       (rc = dmalloc(m, &d.tri, ce)) ||
       (rc = dmalloc(m, &d.stenc, cn * bucket)) || (rc = dmalloc(m, &d.deg, cn)) ||
       (rc = dmalloc(m, &d.vic, cn * bucket)) || (rc = dmalloc(m, &d.vdeg, cn)) ||

@@ -45,6 +45,7 @@ struct DMesh {
   double2* pts;
   double4* ten;
   double4* lten;   /* per-vertex tensor logarithm P log(D) P^T (4 entries) */
+  float4* tenf;    /* single-precision copy of ten, kept in the mixed form */
   int4* tri;
   int* stenc;
   int* deg;

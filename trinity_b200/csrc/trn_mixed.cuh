@@ -122,12 +122,17 @@ __device__ __forceinline__ double trnf_quality_l(double2 pa, double2 pb, double2
   return (double) ((float) area * norm * sqrtf(det) * (ip * ip));
 }
 
+__device__ __forceinline__ float4 tenf_of(double4 t) {
+  return make_float4((float) t.x, (float) t.y, (float) t.z, 0.f);
+}
+__device__ __forceinline__ float4 tenf_of(float4 t) { return t; }
+
 /* metric edge length (numeric.cpp:469-497) in FP32, in the same two halves */
-__device__ __forceinline__ void trnf_dist2_ends(double2 pa, double2 pb, double4 ta, double4 tb,
+__device__ __forceinline__ void trnf_dist2_ends(double2 pa, double2 pb, float4 ta, float4 tb,
                                                 float* l0, float* l1) {
   const float w0 = (float) (pb.x - pa.x), w1 = (float) (pb.y - pa.y);
-  const float a0 = (float) ta.x, a1 = (float) ta.y, a2 = (float) ta.z;
-  const float b0 = (float) tb.x, b1 = (float) tb.y, b2 = (float) tb.z;
+  const float a0 = ta.x, a1 = ta.y, a2 = ta.z;
+  const float b0 = tb.x, b1 = tb.y, b2 = tb.z;
   *l0 = sqrtf(w0 * (a0 * w0 + a1 * w1) + w1 * (a1 * w0 + a2 * w1));
   *l1 = sqrtf(w0 * (b0 * w0 + b1 * w1) + w1 * (b1 * w0 + b2 * w1));
 }
@@ -139,16 +144,15 @@ __device__ __forceinline__ float trnf_dist2_finish(float l0, float l1) {
   return lmax * (ratio - 1.f) * __frcp_rn(ratio * logf(ratio));
 }
 
-__device__ __forceinline__ float trnf_dist2(double2 pa, double2 pb, double4 ta, double4 tb) {
+__device__ __forceinline__ float trnf_dist2(double2 pa, double2 pb, float4 ta, float4 tb) {
   float l0, l1;
   trnf_dist2_ends(pa, pb, ta, tb, &l0, &l1);
   return trnf_dist2_finish(l0, l1);
 }
 
-__device__ __forceinline__ float trnf_dist1(double2 pa, double2 pb, double4 t) {
+__device__ __forceinline__ float trnf_dist1(double2 pa, double2 pb, float4 t) {
   const float u0 = (float) (pb.x - pa.x), u1 = (float) (pb.y - pa.y);
-  const float t0 = (float) t.x, t1 = (float) t.y, t2 = (float) t.z;
-  return sqrtf(u0 * (t0 * u0 + t1 * u1) + u1 * (t1 * u0 + t2 * u1));
+  return sqrtf(u0 * (t.x * u0 + t.y * u1) + u1 * (t.y * u0 + t.z * u1));
 }
 
 /* ---------------- dispatch between the two forms ---------------- */
@@ -189,9 +193,26 @@ __device__ __forceinline__ double quality_of(const DMesh& m, int4 t) {
                    log_load<F32>(m, t.z));
 }
 
+/* the stored tensors as each form reads them: FP64, or the FP32 copy */
 template <bool F32>
-__device__ __forceinline__ double length_x(double2 pa, double2 pb, double4 ta, double4 tb) {
-  if constexpr (F32) return (double) trnf_dist2(pa, pb, ta, tb);
+using TenT = typename std::conditional<F32, float4, double4>::type;
+
+template <bool F32>
+__device__ __forceinline__ TenT<F32> ten_load(const DMesh& m, int v) {
+  if constexpr (F32) return m.tenf[v];
+  else return m.ten[v];
+}
+
+/* a new stored tensor (and its FP32 copy in the mixed form) */
+template <bool F32>
+__device__ __forceinline__ void ten_store(const DMesh& m, int v, double4 t) {
+  m.ten[v] = t;
+  if constexpr (F32) m.tenf[v] = tenf_of(t);
+}
+
+template <bool F32, class T>
+__device__ __forceinline__ double length_x(double2 pa, double2 pb, T ta, T tb) {
+  if constexpr (F32) return (double) trnf_dist2(pa, pb, tenf_of(ta), tenf_of(tb));
   else return trn_dist2(pa, pb, ta, tb);
 }
 
@@ -201,11 +222,11 @@ __device__ __forceinline__ double length_x(double2 pa, double2 pb, double4 ta, d
  * to a few units in the last place as computed, far inside the margins below
  * (1e-12 relative in FP64, 1e-5 in FP32). When the threshold lies outside
  * that range, with the margin, the answer is known without the logarithm. */
-template <bool F32>
-__device__ __forceinline__ bool length_gt(double2 pa, double2 pb, double4 ta, double4 tb, double thresh) {
+template <bool F32, class T>
+__device__ __forceinline__ bool length_gt(double2 pa, double2 pb, T ta, T tb, double thresh) {
   if constexpr (F32) {
     float l0, l1;
-    trnf_dist2_ends(pa, pb, ta, tb, &l0, &l1);
+    trnf_dist2_ends(pa, pb, tenf_of(ta), tenf_of(tb), &l0, &l1);
     const float t = (float) thresh;
     if (l0 == l0 && l1 == l1) {
       if (trnf_max(l0, l1) < t * (1.f - 1.e-5f)) return false;
@@ -224,12 +245,12 @@ __device__ __forceinline__ bool length_gt(double2 pa, double2 pb, double4 ta, do
 }
 
 /* length_x < thresh; *len receives length_x whenever the answer is true */
-template <bool F32>
-__device__ __forceinline__ bool length_lt(double2 pa, double2 pb, double4 ta, double4 tb, double thresh,
+template <bool F32, class T>
+__device__ __forceinline__ bool length_lt(double2 pa, double2 pb, T ta, T tb, double thresh,
                                           double* len) {
   if constexpr (F32) {
     float l0, l1;
-    trnf_dist2_ends(pa, pb, ta, tb, &l0, &l1);
+    trnf_dist2_ends(pa, pb, tenf_of(ta), tenf_of(tb), &l0, &l1);
     if (l0 == l0 && l1 == l1 && trnf_min(l0, l1) > (float) thresh * (1.f + 1.e-5f)) return false;
     *len = (double) trnf_dist2_finish(l0, l1);
   } else {
@@ -266,11 +287,11 @@ struct LogSum {
 };
 
 /* numeric::computeSteinerPoint in either form (point in FP64) */
-template <bool F32>
-__device__ __forceinline__ void steiner_x(double2 pa, double2 pb, double4 ta, double4 tb,
+template <bool F32, class T>
+__device__ __forceinline__ void steiner_x(double2 pa, double2 pb, T ta, T tb,
                                           LogT<F32> la, LogT<F32> lb, double2* rp, double* rt) {
   if constexpr (F32) {
-    const float l0 = trnf_dist1(pa, pb, ta), l1 = trnf_dist1(pa, pb, tb);
+    const float l0 = trnf_dist1(pa, pb, tenf_of(ta)), l1 = trnf_dist1(pa, pb, tenf_of(tb));
     const float w = (fabsf(l0 - l1) < 1.e-9f) ? 0.5f : (sqrtf(l0 * l1) - l1) / (l0 - l1);
     const double wd = (double) w;
     rp->x = (1 - wd) * pa.x + (wd * pb.x);
