@@ -34,62 +34,111 @@ namespace trn {
 /* free-mode round over a device-counted candidate list; states are read
  * from the previous round's buffer only (0 out / not a candidate,
  * 1 undecided, 2 in the set), so the outcome does not depend on timing */
-__global__ void k_mis_round_dev(DMesh m, const uint8_t* __restrict__ in, uint8_t* __restrict__ out,
-                                const int* __restrict__ cand, const int* count, Seed sd,
-                                uint64_t round_mix) {
-  if (trn_failed(m)) return;
-  const uint64_t seed = trn_seed(sd) + round_mix;
-  const int n = *count;
-  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
-    const int v = cand[q];
-    const uint8_t sv = in[v];
-    if (sv != 1) {
-      out[v] = sv;
-      continue;
-    }
-    const uint64_t pv = trn_prio(seed, v);
-    const int* vc = m.vic + (size_t) v * m.bucket;
-    const int nv = m.vdeg[v];
-    bool is_max = true, leave = false;
-    for (int b = 0; b < nv; ++b) {
-      const int w = vc[b];
-      const uint8_t sw = in[w];
-      if (sw == 2) { leave = true; break; }
-      if (sw == 1 && trn_prio(seed, w) > pv) is_max = false;
-    }
-    out[v] = leave ? 0 : (is_max ? 2 : 1);
+__device__ __forceinline__ void mis_item(const DMesh& m, const uint8_t* __restrict__ in,
+                                         uint8_t* __restrict__ out, int v, uint64_t seed) {
+  const uint8_t sv = in[v];
+  if (sv != 1) {
+    out[v] = sv;
+    return;
   }
+  const uint64_t pv = trn_prio(seed, v);
+  const int* vc = m.vic + (size_t) v * m.bucket;
+  const int nv = m.vdeg[v];
+  bool is_max = true, leave = false;
+  for (int b = 0; b < nv; ++b) {
+    const int w = vc[b];
+    const uint8_t sw = in[w];
+    if (sw == 2) { leave = true; break; }
+    if (sw == 1 && trn_prio(seed, w) > pv) is_max = false;
+  }
+  out[v] = leave ? 0 : (is_max ? 2 : 1);
 }
 
 /* collect the set; candidates still undecided are re-activated so that the
  * next level examines them again; every candidate's state returns to 0 */
-__global__ void k_mis_finish(DMesh m, uint8_t* state, uint8_t* other, const int* __restrict__ cand,
-                             const int* count, int* indep, int* nindep) {
+__device__ __forceinline__ void mis_finish_item(const DMesh& m, uint8_t* state, uint8_t* other, int v,
+                                                int* indep, int* nindep) {
+  const uint8_t st = state[v];
+  if (st == 2) trn_append(indep, nindep, v);
+  else if (st == 1) trn_activate(m, v);
+  state[v] = 0;
+  other[v] = 0;
+}
+
+__global__ void k_mis_round_dev(DMesh m, const uint8_t* __restrict__ in, uint8_t* __restrict__ out,
+                                const int* __restrict__ cand, const int* count, Seed sd,
+                                uint64_t round_mix, int min_n) {
+  if (trn_failed(m)) return;
+  const uint64_t seed = trn_seed(sd) + round_mix;
   const int n = *count;
-  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
-    const int v = cand[q];
-    const uint8_t st = state[v];
-    if (st == 2) trn_append(indep, nindep, v);
-    else if (st == 1) trn_activate(m, v);
-    state[v] = 0;
-    other[v] = 0;
+  if (n < min_n) return;
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) mis_item(m, in, out, cand[q], seed);
+}
+
+__global__ void k_mis_finish(DMesh m, uint8_t* state, uint8_t* other, const int* __restrict__ cand,
+                             const int* count, int* indep, int* nindep, int min_n) {
+  const int n = *count;
+  if (n < min_n) return;
+  for (int q = trn_tid(); q < n; q += trn_grid_stride())
+    mis_finish_item(m, state, other, cand[q], indep, nindep);
+}
+
+/* all the rounds and the collection in one block, the rounds separated by
+ * block barriers: for a level whose list the host knows to be short, where
+ * one launch per round would cost more than the round */
+constexpr int kFusedThreads = 1024;
+
+__global__ void __launch_bounds__(kFusedThreads) k_mis_fused(DMesh m, uint8_t* s0, uint8_t* s1,
+                                                             const int* __restrict__ cand,
+                                                             const int* count, Seed sd, int rounds,
+                                                             int* indep, int* nindep, int max_n) {
+  if (trn_failed(m)) return;
+  const int n = *count;
+  if (n > max_n) return;
+  if (threadIdx.x == 0) *nindep = 0;
+  const uint64_t base = trn_seed(sd);
+  for (int r = 0; r < rounds; ++r) {
+    const uint8_t* in = (r & 1) ? s1 : s0;
+    uint8_t* out = (r & 1) ? s0 : s1;
+    const uint64_t seed = base + 0x9e3779b97f4a7c15ULL * r;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) mis_item(m, in, out, cand[q], seed);
+    __syncthreads();
   }
+  uint8_t* state = (rounds & 1) ? s1 : s0;
+  uint8_t* other = (rounds & 1) ? s0 : s1;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) mis_finish_item(m, state, other, cand[q], indep, nindep);
 }
 
 void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, Seed sd,
                    HeurWs& ws, int* indep, int* nindep, cudaStream_t s, long long bound) {
   ProfScope ps("mis_jp", s, 0.0);
-  const int g = grid_bounded(bound, m.capa_node);
   uint8_t* buf[2] = {ws.state, ws.state2};
+  if (bound >= 0 && bound <= kFusedThreads) {   /* known short: the one-block form only */
+    k_mis_fused<<<1, kFusedThreads, 0, s>>>(m, buf[0], buf[1], cand, count, sd, rounds, indep, nindep,
+                                            kFusedThreads);
+    note_launch();
+    check_launch("mis_jp_rounds");
+    return;
+  }
+  /* known long: the per-round launches only; unknown (a captured round):
+   * both, each form returning at once when the device count is not its case
+   * (the one-block form last, as it clears the count it fills) */
+  const int g = grid_bounded(bound, m.capa_node);
+  const int min_n = bound < 0 ? kFusedThreads + 1 : 0;
   for (int r = 0; r < rounds; ++r) {
     k_mis_round_dev<<<g, TRN_THREADS, 0, s>>>(m, buf[r & 1], buf[(r + 1) & 1], cand, count, sd,
-                                               0x9e3779b97f4a7c15ULL * r);
+                                               0x9e3779b97f4a7c15ULL * r, min_n);
     note_launch();
   }
   cudaMemsetAsync(nindep, 0, sizeof(int), s);
   k_mis_finish<<<g, TRN_THREADS, 0, s>>>(m, buf[rounds & 1], buf[(rounds + 1) & 1], cand, count, indep,
-                                         nindep);
+                                         nindep, min_n);
   note_launch();
+  if (bound < 0) {
+    k_mis_fused<<<1, kFusedThreads, 0, s>>>(m, buf[0], buf[1], cand, count, sd, rounds, indep, nindep,
+                                            kFusedThreads);
+    note_launch();
+  }
   check_launch("mis_jp_rounds");
 }
 
@@ -102,68 +151,119 @@ __device__ __forceinline__ uint32_t edge_weight(uint64_t seed, int a, int b, int
   return (uint32_t) (h >> 32) | 1u;
 }
 
-__global__ void k_match_reset(const int* __restrict__ dual, const int* __restrict__ dual_n,
-                              const int* ntasks_dev, int* mate, unsigned long long* prop) {
-  const int ntasks = *ntasks_dev;
-  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride())
-    for (int q = 0; q < dual_n[i]; ++q) {
-      int e = dual[i * 4 + q];
-      mate[e] = -1;
-      prop[e] = 0ULL;
+__device__ __forceinline__ void match_reset_item(const int* __restrict__ dual, const int* __restrict__ dual_n,
+                                                 int i, int* mate, unsigned long long* prop) {
+  for (int q = 0; q < dual_n[i]; ++q) {
+    int e = dual[i * 4 + q];
+    mate[e] = -1;
+    prop[e] = 0ULL;
+  }
+}
+
+__device__ __forceinline__ void match_propose_item(const int* __restrict__ dual, const int* __restrict__ dual_n,
+                                                   int i, const int* mate, unsigned long long* prop,
+                                                   int* choice, uint64_t seed, int round) {
+  const int c = dual[i * 4];
+  int best = -1;
+  uint32_t bw = 0;
+  if (mate[c] == -1) {
+    for (int q = 1; q < dual_n[i]; ++q) {
+      const int n = dual[i * 4 + q];
+      if (mate[n] != -1) continue;
+      uint32_t w = edge_weight(seed, c, n, round);
+      if (w > bw) { bw = w; best = n; }
     }
+    if (best >= 0) atomicMax(prop + best, ((unsigned long long) bw << 32) | (uint32_t) c);
+  }
+  choice[i] = best;
+}
+
+__device__ __forceinline__ void match_accept_item(const int* __restrict__ dual, int ntasks, int i,
+                                                  const int* __restrict__ map, int* mate,
+                                                  const unsigned long long* prop, const int* choice,
+                                                  uint64_t seed, int round, int* pairs, int* npairs) {
+  const int n = choice[i];
+  if (n < 0) return;
+  const int c = dual[i * 4];
+  const int x = map[n];
+  const bool n_cand = x >= 0 && x < ntasks && dual[x * 4] == n;
+  bool ok;
+  if (n_cand) ok = (choice[x] == c) && (c < n);
+  else ok = prop[n] == (((unsigned long long) edge_weight(seed, c, n, round) << 32) | (uint32_t) c);
+  if (ok) {
+    mate[c] = n;
+    mate[n] = c;
+    int p = atomicAdd(npairs, 1);
+    pairs[2 * p] = c;
+    pairs[2 * p + 1] = n;
+  }
+}
+
+__device__ __forceinline__ void match_clear_item(const int* __restrict__ dual, const int* __restrict__ dual_n,
+                                                 int i, unsigned long long* prop) {
+  for (int q = 1; q < dual_n[i]; ++q) prop[dual[i * 4 + q]] = 0ULL;
+}
+
+__global__ void k_match_reset(const int* __restrict__ dual, const int* __restrict__ dual_n,
+                              const int* ntasks_dev, int* mate, unsigned long long* prop, int min_n) {
+  const int ntasks = *ntasks_dev;
+  if (ntasks < min_n) return;
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) match_reset_item(dual, dual_n, i, mate, prop);
 }
 
 __global__ void k_match_propose(const int* __restrict__ dual, const int* __restrict__ dual_n,
                                 const int* ntasks_dev, const int* mate, unsigned long long* prop,
-                                int* choice, Seed sd, int round) {
+                                int* choice, Seed sd, int round, int min_n) {
   const int ntasks = *ntasks_dev;
+  if (ntasks < min_n) return;
   const uint64_t seed = trn_seed(sd);
-  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
-    const int c = dual[i * 4];
-    int best = -1;
-    uint32_t bw = 0;
-    if (mate[c] == -1) {
-      for (int q = 1; q < dual_n[i]; ++q) {
-        const int n = dual[i * 4 + q];
-        if (mate[n] != -1) continue;
-        uint32_t w = edge_weight(seed, c, n, round);
-        if (w > bw) { bw = w; best = n; }
-      }
-      if (best >= 0) atomicMax(prop + best, ((unsigned long long) bw << 32) | (uint32_t) c);
-    }
-    choice[i] = best;
-  }
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride())
+    match_propose_item(dual, dual_n, i, mate, prop, choice, seed, round);
 }
 
 __global__ void k_match_accept(const int* __restrict__ dual, const int* ntasks_dev,
                                const int* __restrict__ map, int* mate, const unsigned long long* prop,
-                               const int* choice, Seed sd, int round, int* pairs, int* npairs) {
+                               const int* choice, Seed sd, int round, int* pairs, int* npairs,
+                               int min_n) {
   const int ntasks = *ntasks_dev;
+  if (ntasks < min_n) return;
   const uint64_t seed = trn_seed(sd);
-  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
-    const int n = choice[i];
-    if (n < 0) continue;
-    const int c = dual[i * 4];
-    const int x = map[n];
-    const bool n_cand = x >= 0 && x < ntasks && dual[x * 4] == n;
-    bool ok;
-    if (n_cand) ok = (choice[x] == c) && (c < n);
-    else ok = prop[n] == (((unsigned long long) edge_weight(seed, c, n, round) << 32) | (uint32_t) c);
-    if (ok) {
-      mate[c] = n;
-      mate[n] = c;
-      int p = atomicAdd(npairs, 1);
-      pairs[2 * p] = c;
-      pairs[2 * p + 1] = n;
-    }
-  }
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride())
+    match_accept_item(dual, ntasks, i, map, mate, prop, choice, seed, round, pairs, npairs);
 }
 
 __global__ void k_match_prop_clear(const int* __restrict__ dual, const int* __restrict__ dual_n,
-                                   const int* ntasks_dev, unsigned long long* prop) {
+                                   const int* ntasks_dev, unsigned long long* prop, int min_n) {
   const int ntasks = *ntasks_dev;
-  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride())
-    for (int q = 1; q < dual_n[i]; ++q) prop[dual[i * 4 + q]] = 0ULL;
+  if (ntasks < min_n) return;
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) match_clear_item(dual, dual_n, i, prop);
+}
+
+/* the whole handshake in one block (reset, then propose / accept / clear per
+ * round, separated by block barriers), for levels the host knows to be short */
+__global__ void __launch_bounds__(kFusedThreads) k_match_fused(const int* __restrict__ dual,
+                                                               const int* __restrict__ dual_n,
+                                                               const int* ntasks_dev,
+                                                               const int* __restrict__ map, int* mate,
+                                                               unsigned long long* prop, int* choice,
+                                                               Seed sd, int* pairs, int* npairs,
+                                                               int max_n) {
+  const int ntasks = *ntasks_dev;
+  if (ntasks > max_n) return;
+  const uint64_t seed = trn_seed(sd);
+  if (threadIdx.x == 0) *npairs = 0;
+  for (int i = threadIdx.x; i < ntasks; i += blockDim.x) match_reset_item(dual, dual_n, i, mate, prop);
+  __syncthreads();
+  for (int r = 0; r < kMatchRounds; ++r) {
+    for (int i = threadIdx.x; i < ntasks; i += blockDim.x)
+      match_propose_item(dual, dual_n, i, mate, prop, choice, seed, r);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ntasks; i += blockDim.x)
+      match_accept_item(dual, ntasks, i, map, mate, prop, choice, seed, r, pairs, npairs);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ntasks; i += blockDim.x) match_clear_item(dual, dual_n, i, prop);
+    __syncthreads();
+  }
 }
 
 void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n,
@@ -171,18 +271,32 @@ void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* d
                      int* npairs, cudaStream_t s, long long bound) {
   (void) m;
   ProfScope ps("match_handshake", s, 0.0);
+  if (bound >= 0 && bound <= kFusedThreads) {   /* known short: the one-block form only */
+    k_match_fused<<<1, kFusedThreads, 0, s>>>(dual, dual_n, ntasks, map, ws.mate, ws.prop, ws.choice, seed,
+                                              pairs, npairs, kFusedThreads);
+    note_launch();
+    check_launch("match_handshake");
+    return;
+  }
+  /* as in mis_jp_rounds: both forms when the length is unknown */
   const int g = grid_bounded(bound, nb_elems);
+  const int min_n = bound < 0 ? kFusedThreads + 1 : 0;
   cudaMemsetAsync(npairs, 0, sizeof(int), s);
-  k_match_reset<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.mate, ws.prop);
+  k_match_reset<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.mate, ws.prop, min_n);
   note_launch();
   for (int r = 0; r < kMatchRounds; ++r) {
     k_match_propose<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.mate, ws.prop, ws.choice,
-                                               seed, r);
+                                               seed, r, min_n);
     note_launch();
     k_match_accept<<<g, TRN_THREADS, 0, s>>>(dual, ntasks, map, ws.mate, ws.prop, ws.choice, seed,
-                                              r, pairs, npairs);
+                                              r, pairs, npairs, min_n);
     note_launch();
-    k_match_prop_clear<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.prop);
+    k_match_prop_clear<<<g, TRN_THREADS, 0, s>>>(dual, dual_n, ntasks, ws.prop, min_n);
+    note_launch();
+  }
+  if (bound < 0) {
+    k_match_fused<<<1, kFusedThreads, 0, s>>>(dual, dual_n, ntasks, map, ws.mate, ws.prop, ws.choice, seed,
+                                              pairs, npairs, kFusedThreads);
     note_launch();
   }
   check_launch("match_handshake");
