@@ -200,6 +200,14 @@ int trn_set_precision(trn_mesh* mesh, int mode);
 /* free-mode options: seed of the hash priorities; exact_sum = 1 takes the
  * metric complexity sum in element order (bit-compatible with the reference) */
 int trn_set_options(trn_mesh* mesh, uint64_t seed, int exact_sum);
+/* free-mode swap matching: which flip a candidate element prefers.
+ * TRN_SWAP_ROW_ORDER (default) ranks its edges by their slot in its dual row,
+ * the order in which the reference's greedy matching (matching.cpp:103-135)
+ * takes them; TRN_SWAP_GAIN ranks them by the quality their flip gains and
+ * makes better meshes than the reference. No counterpart in the reference. */
+#define TRN_SWAP_ROW_ORDER 0
+#define TRN_SWAP_GAIN 1
+int trn_set_swap_match(trn_mesh* mesh, int policy);
 
 /* last metric complexity (Metrics::field.complexity) */
 double trn_last_complexity(trn_mesh* mesh);

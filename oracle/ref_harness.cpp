@@ -20,9 +20,11 @@
  *                   PREFIX.<stage>.bin of the full-precision mesh state (the
  *                   class internals are reached by compiling with
  *                   -Dprivate=public; no reference source is edited).
+ *   --final PATH  : the same snapshot, after the last round only.
  *   --time        : one JSON line with per-kernel wall times (std::chrono),
- *                   the active triangle count at the start of every round and
- *                   the final counts.
+ *                   the active triangle count at the start of every round,
+ *                   the final counts and each kernel's statistics summed over
+ *                   the rounds ([eval, task] for refine, coarse, swap, smooth).
  */
 #include "trinity.h"
 
@@ -73,7 +75,7 @@ int main(int argc, char* argv[]) {
   if (argc < 8) {
     std::fprintf(stderr,
       "usage: %s mesh bb rounds depth bucket target norm "
-      "[--capa-depth D] [--dump PREFIX] [--time] [--out result.mesh]\n", argv[0]);
+      "[--capa-depth D] [--dump PREFIX] [--final PATH] [--time] [--out result.mesh]\n", argv[0]);
     return 1;
   }
   std::string input = argv[1], solut = argv[2];
@@ -83,12 +85,13 @@ int main(int argc, char* argv[]) {
   double target = std::atof(argv[6]);
   int norm = std::atoi(argv[7]);
   int capa_depth = 4;
-  std::string prefix, out;
+  std::string prefix, out, final_path;
   bool timing = false;
   for (int i = 8; i < argc; ++i) {
     if (!std::strcmp(argv[i], "--capa-depth") && i + 1 < argc) capa_depth = std::atoi(argv[++i]);
     else if (!std::strcmp(argv[i], "--dump") && i + 1 < argc) prefix = argv[++i];
     else if (!std::strcmp(argv[i], "--out") && i + 1 < argc) out = argv[++i];
+    else if (!std::strcmp(argv[i], "--final") && i + 1 < argc) final_path = argv[++i];
     else if (!std::strcmp(argv[i], "--time")) timing = true;
   }
 
@@ -136,6 +139,7 @@ int main(int argc, char* argv[]) {
     t_k[3] += ms_since(t);
     if (!prefix.empty()) dump(mesh, prefix + ".r" + std::to_string(r) + ".smooth.bin");
   }
+  if (!final_path.empty()) dump(mesh, final_path);
   if (!out.empty()) mesh.store(out);
 
   if (timing) {
@@ -148,7 +152,11 @@ int main(int argc, char* argv[]) {
                 t_k[0] + t_k[1] + t_k[2] + t_k[3]);
     for (size_t i = 0; i < t_in.size(); ++i)
       std::printf("%s%d", i ? ", " : "", t_in[i]);
-    std::printf("], \"nodes_out\": %d, \"elems_out\": %d}\n", nodes, count_active_elems(mesh));
+    std::printf("], \"nodes_out\": %d, \"elems_out\": %d, \"stats\": [", nodes,
+                count_active_elems(mesh));
+    for (int k = 1; k < 5; ++k)
+      std::printf("%s[%d, %d]", k > 1 ? ", " : "", stat[k].eval, stat[k].task);
+    std::printf("]}\n");
   }
   return 0;
 }

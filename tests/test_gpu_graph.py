@@ -28,13 +28,15 @@ def _rounds(g, c, graph):
     return per_round
 
 
-@pytest.mark.parametrize("name,n,prec", [("c2", 120, "fp64"), ("c2", 120, "mixed"), ("c1", 40, "fp64")])
-def test_graph_round_equals_stage_calls(name, n, prec):
+@pytest.mark.parametrize("name,n,prec,policy", [("c2", 120, "fp64", "row_order"), ("c2", 120, "mixed", "row_order"),
+                                               ("c1", 40, "fp64", "row_order"), ("c2", 120, "fp64", "gain")])
+def test_graph_round_equals_stage_calls(name, n, prec, policy):
     m, u, c = meshgen.make_config(name, n)
     out = {}
     for graph in (False, True):
         g = gpu_mesh(m, u, c)
         g.set_precision(prec)
+        g.set_swap_match(policy)
         stats = _rounds(g, c, graph)
         out[graph] = (gpu_state(g), stats)
         g.close()

@@ -63,6 +63,7 @@ def lib():
         L.trn_round_run.argtypes = [pmesh, ip, sp]
         L.trn_set_replay.argtypes = [pmesh, vp, sz]
         L.trn_set_options.argtypes = [pmesh, ctypes.c_uint64, ip]
+        L.trn_set_swap_match.argtypes = [pmesh, ip]
         L.trn_last_complexity.argtypes = [pmesh]
         L.trn_last_complexity.restype = dp
         L.trn_last_time_ms.argtypes = [pmesh]

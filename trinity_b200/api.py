@@ -159,6 +159,15 @@ class Mesh:
     def set_options(self, seed: int = 0x7472696E697479, exact_sum: bool = False) -> None:
         self._check(self._L.trn_set_options(self.h, seed, 1 if exact_sum else 0))
 
+    SWAP_MATCH = {"row_order": 0, "gain": 1}
+
+    def set_swap_match(self, policy: str = "row_order") -> None:
+        """Free-mode swap matching: "row_order" (the reference's preference,
+        the default) or "gain" (each candidate prefers its best flip)."""
+        if policy not in self.SWAP_MATCH:
+            raise ValueError(f"swap matching policy {policy!r}: one of {sorted(self.SWAP_MATCH)}")
+        self._check(self._L.trn_set_swap_match(self.h, self.SWAP_MATCH[policy]))
+
     def last_time_ms(self) -> float:
         return self._L.trn_last_time_ms(self.h)
 

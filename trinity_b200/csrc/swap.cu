@@ -10,6 +10,9 @@
  *                  its first vertex found in that vertex's stencil order, then
  *                  the one across the opposite edge (extractDualGraph,
  *                  swapping.cpp:204-248); records element -> row index
+ *   k_swap_filter_dual  free mode: the filter and the rows in one pass, with
+ *                  the quality change of each row's flips when the matching
+ *                  ranks its edges by gain
  *   k_swap_flip    per matched pair: flip the shared edge when both new
  *                  elements are CCW and the smaller quality does not drop;
  *                  stencil appends, repair tags, cached qualities and
@@ -56,9 +59,9 @@ __global__ void k_swap_filter(DMesh m, int nb_elems, uint8_t* __restrict__ flag)
   }
 }
 
-/* the dual row of candidate k at row index i */
-__device__ __forceinline__ void dual_row(const DMesh& m, int k, int i, int* __restrict__ dual,
-                                         int* __restrict__ dual_n, int* __restrict__ map) {
+/* the dual row of candidate k at row index i; returns its length */
+__device__ __forceinline__ int dual_row(const DMesh& m, int k, int i, int* __restrict__ dual,
+                                        int* __restrict__ dual_n, int* __restrict__ map) {
   {
     const int4 n = m.tri[k];
     int row[4] = {k, -1, -1, -1};
@@ -88,6 +91,7 @@ __device__ __forceinline__ void dual_row(const DMesh& m, int k, int i, int* __re
     reinterpret_cast<int4*>(dual)[i] = make_int4(row[0], row[1], row[2], row[3]);
     dual_n[i] = dn;
     map[k] = i;
+    return dn;
   }
 }
 
@@ -97,34 +101,16 @@ __global__ void k_swap_dual(DMesh m, const int* __restrict__ list, int ntasks, i
   for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) dual_row(m, list[i], i, dual, dual_n, map);
 }
 
-/* free mode: filter and dual extraction in one pass; rows are numbered in
- * append order (no use depends on it) */
-__global__ void k_swap_filter_dual(DMesh m, const int* __restrict__ act, const int* act_n,
-                                   int* __restrict__ dual, int* __restrict__ dual_n,
-                                   int* __restrict__ map, int* count) {
-  if (trn_failed(m)) return;
-  const int na = *act_n;
-  for (int q = trn_tid(); q < na; q += trn_grid_stride()) {
-    const int k = act[q];
-    if (!m.activ[k]) continue;
-    m.activ[k] = 0;
-    if (!(m.qual[k] < TRN_Q_MIN)) continue;
-    unsigned mask = __activemask();
-    int lane = threadIdx.x & 31, leader = __ffs(mask) - 1, base = 0;
-    if (lane == leader) base = atomicAdd(count, __popc(mask));
-    base = __shfl_sync(mask, base, leader);
-    dual_row(m, k, base + __popc(mask & ((1u << lane) - 1)), dual, dual_n, map);
-  }
-}
-
-/* Swap::swap, swapping.cpp:55-149 */
+/* the two elements that replace id1 and id2 when their shared edge flips
+ * (Swap::swap, swapping.cpp:59-106): false when they share no edge or a new
+ * element is not CCW; else c1, c2 and their qualities q0, q1 */
 template <bool F32>
-__device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int* map,
-                         const int* dual, const int* dual_n, int ntasks, bool strict_map) {
+__device__ __forceinline__ bool flip_eval(const DMesh& m, int id1, int id2, int c1[3], int c2[3],
+                                          double* q0, double* q1) {
   const int4 a = m.tri[id1], b = m.tri[id2];
   const int o1[3] = {a.x, a.y, a.z};
   const int o2[3] = {b.x, b.y, b.z};
-  int c1[3] = {-1, -1, -1}, c2[3] = {-1, -1, -1};
+  c1[0] = c1[1] = c1[2] = c2[0] = c2[1] = c2[2] = -1;
   for (int i = 0; i < 3; ++i) {
     int j = (i + 1) % 3, k = (i + 2) % 3;
     if (o1[i] == o2[1] && o1[j] == o2[0]) {
@@ -143,15 +129,70 @@ __device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int*
       break;
     }
   }
-  if (c1[0] < 0) return 0;
+  if (c1[0] < 0) return false;
   const double2 p10 = m.pts[c1[0]], p11 = m.pts[c1[1]], p12 = m.pts[c1[2]];
   const double2 p22 = m.pts[c2[2]];
   /* c2 = (c1[2], c1[1], c2[2]) */
-  if (!trn_ccw(p10, p11, p12) || !trn_ccw(p12, p11, p22)) return 0;
+  if (!trn_ccw(p10, p11, p12) || !trn_ccw(p12, p11, p22)) return false;
   const LogT<F32> l10 = log_load<F32>(m, c1[0]), l11 = log_load<F32>(m, c1[1]);
   const LogT<F32> l12 = log_load<F32>(m, c1[2]), l22 = log_load<F32>(m, c2[2]);
-  const double q0 = quality_x(p10, p11, p12, l10, l11, l12);
-  const double q1 = quality_x(p12, p11, p22, l12, l11, l22);
+  *q0 = quality_x(p10, p11, p12, l10, l11, l12);
+  *q1 = quality_x(p12, p11, p22, l12, l11, l22);
+  return true;
+}
+
+/* the matching rank of the flip of the edge shared by elements a and b: the
+ * change of the smaller quality, min(q_new) - min(q_old), in [-1, 1], or
+ * -1.5 when the flip is impossible, quantized to the upper 22 bits of a
+ * word. Both rows of a candidate pair evaluate the flip with the smaller id
+ * first, so the two ranks agree bit for bit */
+template <bool F32>
+__device__ __forceinline__ uint32_t flip_rank(const DMesh& m, int a, int b) {
+  const int id1 = a < b ? a : b, id2 = a < b ? b : a;
+  int c1[3], c2[3];
+  double q0, q1, gain = -1.5;
+  if (flip_eval<F32>(m, id1, id2, c1, c2, &q0, &q1))
+    gain = trn_dmin(q0, q1) - trn_dmin(m.qual[id1], m.qual[id2]);
+  if (!(gain >= -1.5)) gain = -1.5;
+  if (gain > 1.0) gain = 1.0;
+  return ((uint32_t) ((gain + 2.0) * 1048576.0)) << 10;
+}
+
+/* free mode: filter, dual extraction and (when rank is given) the ranks of
+ * each row's flips in one pass; rows are numbered in append order (no use
+ * depends on it) */
+template <bool F32>
+__global__ void k_swap_filter_dual(DMesh m, const int* __restrict__ act, const int* act_n,
+                                   int* __restrict__ dual, int* __restrict__ dual_n,
+                                   int* __restrict__ map, uint32_t* __restrict__ rank, int* count) {
+  if (trn_failed(m)) return;
+  const int na = *act_n;
+  for (int q = trn_tid(); q < na; q += trn_grid_stride()) {
+    const int k = act[q];
+    if (!m.activ[k]) continue;
+    m.activ[k] = 0;
+    if (!(m.qual[k] < TRN_Q_MIN)) continue;
+    unsigned mask = __activemask();
+    int lane = threadIdx.x & 31, leader = __ffs(mask) - 1, base = 0;
+    if (lane == leader) base = atomicAdd(count, __popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    const int r = base + __popc(mask & ((1u << lane) - 1));
+    const int dn = dual_row(m, k, r, dual, dual_n, map);
+    if (rank) {
+      uint32_t w[4] = {0u, 0u, 0u, 0u};
+      for (int e = 1; e < dn; ++e) w[e] = flip_rank<F32>(m, k, dual[r * 4 + e]);
+      reinterpret_cast<uint4*>(rank)[r] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+}
+
+/* Swap::swap, swapping.cpp:55-149 */
+template <bool F32>
+__device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int* map,
+                         const int* dual, const int* dual_n, int ntasks, bool strict_map) {
+  int c1[3], c2[3];
+  double q0, q1;
+  if (!flip_eval<F32>(m, id1, id2, c1, c2, &q0, &q1)) return 0;
   const double q_old = trn_dmin(m.qual[id1], m.qual[id2]);
   const double q_new = trn_dmin(q0, q1);
   if (q_new < q_old) return 0;
@@ -245,11 +286,14 @@ void swap_list_active(const DMesh& m, int nb_elems, int* act, int* act_n, cudaSt
 }
 
 void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,
-                      int* map, int* count, cudaStream_t s, long long bound) {
+                      int* map, uint32_t* rank, int* count, bool fp32, cudaStream_t s, long long bound) {
   ProfScope ps("swap_filter", s, 0.0);
   cudaMemsetAsync(count, 0, sizeof(int), s);
-  k_swap_filter_dual<<<grid_bounded(bound, m.capa_elem), TRN_THREADS, 0, s>>>(m, act, act_n, dual, dual_n, map,
-                                                                    count);
+  const int g = grid_bounded(bound, m.capa_elem);
+  if (fp32)
+    k_swap_filter_dual<true><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, dual, dual_n, map, rank, count);
+  else
+    k_swap_filter_dual<false><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, dual, dual_n, map, rank, count);
   note_launch();
   check_launch("swap_filter_dual");
 }

@@ -76,6 +76,7 @@ struct trn_mesh {
   Tune round_tune;
   bool round_fp32 = false;
   uint64_t round_seed = 0;
+  int round_swap_match = 0;
   unsigned long long round_launches = 0;
   /* replay */
   bool replay = false;
@@ -85,6 +86,7 @@ struct trn_mesh {
   /* options */
   uint64_t seed = 0x7472696e697479ULL;
   bool exact_sum = false;
+  int swap_match = TRN_SWAP_ROW_ORDER;
   bool fp32 = false;   /* mixed-precision form of the metric arithmetic */
   double last_complexity = 0.0;
   double last_ms = 0.0;
@@ -689,6 +691,14 @@ int trn_set_options(trn_mesh* m, uint64_t seed, int exact_sum) {
   return TRN_OK;
 }
 
+int trn_set_swap_match(trn_mesh* m, int policy) {
+  if (!m) return TRN_ERR_INVALID;
+  if (policy != TRN_SWAP_ROW_ORDER && policy != TRN_SWAP_GAIN)
+    return fail(m, TRN_ERR_INVALID, "swap matching: unknown policy");
+  m->swap_match = policy;
+  return TRN_OK;
+}
+
 double trn_last_complexity(trn_mesh* m) { return m ? m->last_complexity : 0.0; }
 double trn_last_time_ms(trn_mesh* m) { return m ? m->last_ms : 0.0; }
 void* trn_mesh_stream(trn_mesh* m) { return m ? (void*) m->stream : nullptr; }
@@ -791,9 +801,10 @@ void enq_swap_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphCondi
   DMesh dl = level_mesh(m);
   cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s);
   cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s);
-  swap_filter_dual(dl, act_list(m, 0), m->status + S_ACT, m->dual, m->dual_n, m->map,
-                   m->status + S_NTASK, s, bound);
-  match_handshake(dl, m->capa_elem, m->dual, m->dual_n, m->status + S_NTASK, m->map,
+  uint32_t* rank = m->swap_match == TRN_SWAP_GAIN ? m->hws.rank : nullptr;
+  swap_filter_dual(dl, act_list(m, 0), m->status + S_ACT, m->dual, m->dual_n, m->map, rank,
+                   m->status + S_NTASK, m->fp32, s, bound);
+  match_handshake(dl, m->capa_elem, m->dual, m->dual_n, m->status + S_NTASK, m->map, rank,
                   seed_of(m, 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s, bound);
   cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s);
   swap_flip(dl, m->pairs, m->status + S_NPAIRS, m->map, m->dual, m->dual_n, m->status + S_NTASK,
@@ -1125,6 +1136,7 @@ int capture_round(trn_mesh* m, int depth) {
   m->round_tune = m->tune;
   m->round_fp32 = m->fp32;
   m->round_seed = m->seed;
+  m->round_swap_match = m->swap_match;
   m->round_launches = thread_launches() - l0;
   return TRN_OK;
 }
@@ -1139,7 +1151,7 @@ int trn_round_graph_run(trn_mesh* m, int depth, trn_stats stats[4]) {
   if (m->replay) return fail(m, TRN_ERR_INVALID, "round: a captured round runs the free mode only");
   m->err.clear();
   if (!m->round_exec || m->round_depth != depth || m->round_fp32 != m->fp32 || m->round_seed != m->seed ||
-      !(m->round_tune == m->tune)) {
+      m->round_swap_match != m->swap_match || !(m->round_tune == m->tune)) {
     int rc = capture_round(m, depth);
     if (rc) return rc;
   }

@@ -169,10 +169,12 @@ void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* m
                const int* dual, const int* dual_n, const int* ntasks, int* commit, bool strict_map,
                bool fp32, cudaStream_t s, long long bound = -1);
 /* free mode: list the active elements; per level, filter and dual rows in
- * one pass over the list, *count rows */
+ * one pass over the list, *count rows; when rank is given, rank[4 r + e]:
+ * the gain rank of the flip between row r's candidate and its neighbour e */
 void swap_list_active(const DMesh& m, int nb_elems, int* act, int* act_n, cudaStream_t s);
 void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,
-                      int* map, int* count, cudaStream_t s, long long bound = -1);
+                      int* map, uint32_t* rank, int* count, bool fp32, cudaStream_t s,
+                      long long bound = -1);
 
 /* smoothing (smooth.cu) */
 void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
@@ -190,6 +192,7 @@ struct HeurWs {
   int* choice = nullptr;
   int* color = nullptr;
   int* mate = nullptr;
+  uint32_t* rank = nullptr;      /* four flip ranks per swap dual row */
   int* cnt = nullptr;            /* small device counters */
   int* list_a = nullptr;         /* two worklists (activity, coloring) */
   int* list_b = nullptr;
@@ -197,11 +200,12 @@ struct HeurWs {
 };
 void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem);
 void heur_ws_free(HeurWs* ws);
-/* handshake matching on the dual rows (*ntasks of them); pairs[2k],
- * pairs[2k+1]; *npairs */
+/* handshake matching on the dual rows (*ntasks of them), edges ranked by
+ * their slot in the row (rank == nullptr) or by rank[4 i + slot] (the flip
+ * gains of swap_filter_dual); pairs[2k], pairs[2k+1]; *npairs */
 void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n,
-                     const int* ntasks, const int* map, Seed seed, HeurWs& ws, int* pairs,
-                     int* npairs, cudaStream_t s, long long bound = -1);
+                     const int* ntasks, const int* map, const uint32_t* rank, Seed seed, HeurWs& ws,
+                     int* pairs, int* npairs, cudaStream_t s, long long bound = -1);
 /* a fixed number of independent-set rounds over a device-counted candidate
  * list; undecided candidates are re-activated (next level) */
 void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, Seed seed,
