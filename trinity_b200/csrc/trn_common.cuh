@@ -88,8 +88,18 @@ __device__ __forceinline__ bool trn_byte_cas01(void* p) {
   return true;
 }
 
+/* append id to list[*n]; the lanes of a warp that push to the same counter
+ * at once share one atomic (a flip pushes up to a dozen ids onto two
+ * counters, which one-atomic-per-push serializes in L2) */
 __device__ __forceinline__ void trn_list_push(int* list, int* n, int id) {
-  list[atomicAdd(n, 1)] = id;
+  const unsigned mask = __activemask();
+  const unsigned peers = __match_any_sync(mask, (unsigned long long) (uintptr_t) n);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(n, __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  list[base + __popc(peers & ((1u << lane) - 1))] = id;
 }
 
 /* tag vertex v for stencil repair (CAS 0 -> 1), listing it once */
