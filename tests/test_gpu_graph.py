@@ -97,14 +97,15 @@ def test_graph_batch_equals_plain_batch():
         check_invariants(sb)
 
 
-ODD_TUNE = dict(smooth_threads=64, filter_threads=512, group_lanes=4, group_max=65536, flip_threads=128)
+ODD_TUNE = dict(smooth_threads=64, filter_threads=512, group_lanes=4, group_max=65536, flip_threads=128,
+                smooth_lanes=4)
 
 
 @pytest.mark.parametrize("graph", [False, True])
 def test_launch_shapes_change_no_result(graph):
     m, u, c = meshgen.make_config("c2", 100)
     states = []
-    for cfg in (None, ODD_TUNE, dict(ODD_TUNE, group_lanes=16, group_max=0, smooth_threads=256)):
+    for cfg in (None, ODD_TUNE, dict(ODD_TUNE, group_lanes=16, group_max=0, smooth_threads=256, smooth_lanes=8)):
         g = gpu_mesh(m, u, c)
         if cfg:
             g.set_tune(cfg)
@@ -122,6 +123,7 @@ def test_autotune_picks_valid_shapes_and_reloads():
     g = gpu_mesh(m, u, c)
     cfg = g.autotune(c["target"], c["norm"], depth=c["depth"], rounds=1)
     assert cfg["smooth_threads"] in (64, 128, 256) and cfg["group_lanes"] in (4, 8, 16)
+    assert cfg["smooth_lanes"] in (1, 4, 8)
     assert g.get_tune() == cfg
     assert g.counts()[:2] == (m.nb_nodes, m.nb_elems)
     ref = gpu_mesh(m, u, c)

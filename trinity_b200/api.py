@@ -174,7 +174,7 @@ class Mesh:
     def stream(self) -> int:
         return self._L.trn_mesh_stream(self.h)
 
-    TUNE_KEYS = ("smooth_threads", "filter_threads", "group_lanes", "group_max", "flip_threads")
+    TUNE_KEYS = ("smooth_threads", "filter_threads", "group_lanes", "group_max", "flip_threads", "smooth_lanes")
 
     def get_tune(self) -> dict:
         a = np.zeros(len(self.TUNE_KEYS), dtype=np.int32)

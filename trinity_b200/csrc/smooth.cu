@@ -11,6 +11,8 @@
  *                  incident element stays CCW with quality above the old
  *                  stencil minimum, backing off the step 1, 1/2, .., 1/16
  *                  (Smooth::moveSmartLaplacian, smoothing.cpp:40-126).
+ *   k_smooth_move_grp  the same with 4 or 8 lanes per vertex (launch shape
+ *                  smooth_lanes; the same results)
  * Vertices of one color share no element, so a class moves in parallel; the
  * classes run in order, as in the reference.
  */
@@ -134,6 +136,171 @@ __global__ void __launch_bounds__(256, 3) k_smooth_move(DMesh m, const int* __re
   if (commit) atomicAdd(counters + 1, commit);
 }
 
+/* The same move with G lanes per vertex: lane j gathers the neighbours
+ * j, j+G, ... and evaluates the elements j, j+G, ... of the stencil. The
+ * displacement and the tensor-logarithm sums are accumulated in neighbour
+ * order by every lane from the lanes' terms (shuffles), the stencil minimum
+ * is a min-reduction and validity an all-vote, so the results are the bits
+ * of move_laplacian. More loads in flight per vertex and no per-thread
+ * quality array: the one-lane form is bound by gather latency, divergence
+ * and registers. */
+template <class T>
+__device__ __forceinline__ T grp_shfl(unsigned mask, T v, int src, int width);
+template <>
+__device__ __forceinline__ double grp_shfl(unsigned mask, double v, int src, int width) {
+  return __shfl_sync(mask, v, src, width);
+}
+template <>
+__device__ __forceinline__ float grp_shfl(unsigned mask, float v, int src, int width) {
+  return __shfl_sync(mask, v, src, width);
+}
+template <>
+__device__ __forceinline__ double4 grp_shfl(unsigned mask, double4 v, int src, int width) {
+  return make_double4(__shfl_sync(mask, v.x, src, width), __shfl_sync(mask, v.y, src, width),
+                      __shfl_sync(mask, v.z, src, width), __shfl_sync(mask, v.w, src, width));
+}
+template <>
+__device__ __forceinline__ float4 grp_shfl(unsigned mask, float4 v, int src, int width) {
+  return make_float4(__shfl_sync(mask, v.x, src, width), __shfl_sync(mask, v.y, src, width),
+                     __shfl_sync(mask, v.z, src, width), __shfl_sync(mask, v.w, src, width));
+}
+
+/* quality of stencil element t of vertex i with i at pa (log lnew); false
+ * when it is not CCW */
+template <bool F32>
+__device__ __forceinline__ bool elem_quality_at(const DMesh& m, int i, int4 n, double2 pa, LogT<F32> lnew,
+                                                double* q) {
+  const double2 p0 = (n.x == i) ? pa : m.pts[n.x];
+  const double2 p1 = (n.y == i) ? pa : m.pts[n.y];
+  const double2 p2 = (n.z == i) ? pa : m.pts[n.z];
+  if (!trn_ccw(p0, p1, p2)) return false;
+  const LogT<F32> l0 = (n.x == i) ? lnew : log_load<F32>(m, n.x);
+  const LogT<F32> l1 = (n.y == i) ? lnew : log_load<F32>(m, n.y);
+  const LogT<F32> l2 = (n.z == i) ? lnew : log_load<F32>(m, n.z);
+  *q = quality_x(p0, p1, p2, l0, l1, l2);
+  return true;
+}
+
+template <bool F32, int G>
+__device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmask) {
+  const int* vc = m.vic + (size_t) i * m.bucket;
+  const int* st = m.stenc + (size_t) i * m.bucket;
+  const int deg = trn_deg(m, i);
+  const int nb_neigh = m.vdeg[i];
+  double q_min = 1.7976931348623157e308;
+  for (int a = lane; a < deg; a += G) q_min = trn_dmin(q_min, m.qual[st[a]]);
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) q_min = trn_dmin(q_min, __shfl_xor_sync(gmask, q_min, o, G));
+  const double2 pini = m.pts[i];
+  const double4 tini = m.ten[i];
+  const TenT<F32> tinf = ten_load<F32>(m, i);
+  using R = typename std::conditional<F32, float, double>::type;
+  R sx = 0, sy = 0;
+  LogSum<F32> lsum;
+  for (int b = 0; b < nb_neigh; b += G) {
+    const int k = b + lane;
+    R tx = 0, ty = 0;
+    LogT<F32> l{};
+    if (k < nb_neigh) {
+      const int nb = vc[k];
+      const double2 pb = m.pts[nb];
+      if constexpr (F32) {
+        const float il = __frcp_rn(trnf_dist2(pini, pb, tenf_of(tinf), tenf_of(ten_load<F32>(m, nb))));
+        tx = (float) (pb.x - pini.x) * il;
+        ty = (float) (pb.y - pini.y) * il;
+      } else {
+        const double len = length_x<F32>(pini, pb, tini, m.ten[nb]);
+        tx = pini.x + ((pb.x - pini.x) / len);
+        ty = pini.y + ((pb.y - pini.y) / len);
+      }
+      l = log_load<F32>(m, nb);
+    }
+    const int cnt = min(G, nb_neigh - b);
+    for (int j = 0; j < cnt; ++j) {
+      sx += grp_shfl(gmask, tx, j, G);
+      sy += grp_shfl(gmask, ty, j, G);
+      lsum.add(grp_shfl(gmask, l, j, G));
+    }
+  }
+  double ox, oy;
+  if constexpr (F32) {
+    const float inv = __frcp_rn((float) nb_neigh);
+    ox = pini.x + (double) (sx * inv);
+    oy = pini.y + (double) (sy * inv);
+  } else {
+    ox = sx / nb_neigh;
+    oy = sy / nb_neigh;
+  }
+  double tn[3];
+  lsum.finish(nb_neigh, tn);
+  const double4 tnew = make_double4(tn[0], tn[1], tn[2], 0.0);
+  const LogT<F32> lnew = log_of<F32>(tn[0], tn[1], tn[2]);
+  constexpr int KQ = 2;   /* qualities kept per lane; later ones are recomputed */
+  double qv[KQ];
+  bool valid;
+  int retry = 0;
+  double weight = 1;
+  double2 pa;
+  do {
+    pa.x = (1 - weight) * pini.x + weight * ox;
+    pa.y = (1 - weight) * pini.y + weight * oy;
+    bool ok = true;
+    int j = 0;
+    for (int a = lane; ok && a < deg; a += G, ++j) {
+      double q = 0;
+      ok = elem_quality_at<F32>(m, i, m.tri[st[a]], pa, lnew, &q) && (q > q_min);
+      if (j < KQ) qv[j] = q;
+    }
+    valid = __all_sync(gmask, ok);
+    weight *= 0.5;
+  } while (!valid && ++retry < 5);
+  if (valid) {
+    int j = 0;
+    for (int a = lane; a < deg; a += G, ++j) {
+      double q = 0;
+      if (j < KQ) q = qv[j];
+      else elem_quality_at<F32>(m, i, m.tri[st[a]], pa, lnew, &q);
+      m.qual[st[a]] = q;
+    }
+    if (lane == 0) {
+      m.pts[i] = pa;
+      ten_store<F32>(m, i, tnew);
+      log_store<F32>(m, i, lnew);
+    }
+  }
+  return valid ? 1 : 0;
+}
+
+template <bool F32, int G>
+__global__ void __launch_bounds__(256) k_smooth_move_grp(DMesh m, const int* __restrict__ list, int n,
+                                                         const int* off, int c, int* counters) {
+  if (trn_failed(m)) return;
+  if (off) {
+    list += off[c];
+    n = off[c + 1] - off[c];
+  }
+  const int lane = threadIdx.x % G;
+  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) - lane));
+  const long long g0 = ((long long) blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const long long gs = ((long long) gridDim.x * blockDim.x) / G;
+  int tasks = 0, commit = 0;
+  for (long long q = g0; q < n; q += gs) {
+    const int v = list[q];
+    if (v < 0 || v >= m.capa_node) {
+      if (lane == 0) trn_set_error(m.err, TRN_DERR_REPLAY);
+      continue;
+    }
+    if (!m.activ[v]) continue;
+    if (m.vdeg[v] == 0) continue;
+    tasks++;
+    commit += move_laplacian_grp<F32, G>(m, v, lane, gmask);
+  }
+  if (lane == 0) {
+    if (tasks) atomicAdd(counters, tasks);
+    if (commit) atomicAdd(counters + 1, commit);
+  }
+}
+
 void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s) {
   k_smooth_pre<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
   note_launch();
@@ -150,8 +317,18 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
   const double nbr = (double) std::min<long long>((long long) m.capa_node, 6LL * n) * (kPt + kTen);
   ProfScope ps("smooth_move", s, n * own + nbr);
   const int t = tune().smooth_threads;
-  if (fp32) k_smooth_move<true><<<grid_for(hint, t), t, 0, s>>>(m, list, n, off, c, counters);
-  else k_smooth_move<false><<<grid_for(hint, t), t, 0, s>>>(m, list, n, off, c, counters);
+  const int lanes = tune().smooth_lanes;
+  const int g = grid_for((long long) hint * lanes, t);
+  if (lanes == 8) {
+    if (fp32) k_smooth_move_grp<true, 8><<<g, t, 0, s>>>(m, list, n, off, c, counters);
+    else k_smooth_move_grp<false, 8><<<g, t, 0, s>>>(m, list, n, off, c, counters);
+  } else if (lanes == 4) {
+    if (fp32) k_smooth_move_grp<true, 4><<<g, t, 0, s>>>(m, list, n, off, c, counters);
+    else k_smooth_move_grp<false, 4><<<g, t, 0, s>>>(m, list, n, off, c, counters);
+  } else {
+    if (fp32) k_smooth_move<true><<<g, t, 0, s>>>(m, list, n, off, c, counters);
+    else k_smooth_move<false><<<g, t, 0, s>>>(m, list, n, off, c, counters);
+  }
   note_launch();
   check_launch("smooth_move");
 }

@@ -1182,6 +1182,7 @@ int trn_get_tune(trn_mesh* m, int cfg[TRN_TUNE_N]) {
   cfg[2] = t.group_lanes;
   cfg[3] = t.group_max;
   cfg[4] = t.flip_threads;
+  cfg[5] = t.smooth_lanes;
   return TRN_OK;
 }
 
@@ -1189,13 +1190,14 @@ int trn_set_tune(trn_mesh* m, const int cfg[TRN_TUNE_N]) {
   if (!m || !cfg) return TRN_ERR_INVALID;
   auto pow2_in = [](int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; };
   if (!pow2_in(cfg[0], 32, 256) || !pow2_in(cfg[1], 32, 1024) || (cfg[2] != 4 && cfg[2] != 8 && cfg[2] != 16) ||
-      cfg[3] < 0 || !pow2_in(cfg[4], 32, 1024))
+      cfg[3] < 0 || !pow2_in(cfg[4], 32, 1024) || (cfg[5] != 1 && cfg[5] != 4 && cfg[5] != 8))
     return fail(m, TRN_ERR_INVALID, "set_tune: value out of range");
   m->tune.smooth_threads = cfg[0];
   m->tune.filter_threads = cfg[1];
   m->tune.group_lanes = cfg[2];
   m->tune.group_max = cfg[3];
   m->tune.flip_threads = cfg[4];
+  m->tune.smooth_lanes = cfg[5];
   return TRN_OK;
 }
 
@@ -1232,11 +1234,11 @@ int trn_autotune(trn_mesh* m, double target_factor, int norm, double h_min, doub
     *out = best;
     return TRN_OK;
   };
-  int* fields[5] = {&m->tune.smooth_threads, &m->tune.filter_threads, &m->tune.group_lanes,
-                    &m->tune.group_max, &m->tune.flip_threads};
+  int* fields[TRN_TUNE_N] = {&m->tune.smooth_lanes, &m->tune.smooth_threads, &m->tune.filter_threads,
+                             &m->tune.group_lanes, &m->tune.group_max, &m->tune.flip_threads};
   const std::vector<std::vector<int>> cands = {
-      {64, 128, 256}, {128, 256, 512}, {4, 8, 16}, {4096, 16384, 65536}, {128, 256, 512}};
-  for (int f = 0; f < 5 && rc == TRN_OK; ++f) {
+      {1, 4, 8}, {64, 128, 256}, {128, 256, 512}, {4, 8, 16}, {4096, 16384, 65536}, {128, 256, 512}};
+  for (int f = 0; f < TRN_TUNE_N && rc == TRN_OK; ++f) {
     int best_v = *fields[f];
     double best_ms = 1e300;
     for (int v : cands[f]) {
