@@ -211,6 +211,8 @@ def b200_arm(args, rank, world, local_rank):
     forms = {}
     if not args.no_forms:
         g.set_precision("mixed")
+        # launch shapes chosen again for the FP32 arithmetic (same results)
+        mixed_tune = tuned if args.no_tune else g.autotune(c["target"], c["norm"], depth=c["depth"], rounds=1)
         for _ in range(args.warmup):
             g.reload()
             run_step(api, g, c, heur, kern)
@@ -224,13 +226,16 @@ def b200_arm(args, rank, world, local_rank):
         q = g.quality_stats()
         forms["mixed_fp32"] = {"tri_in": m_tin, "round_ms": m_tms,
                                "final_mesh": {"nodes": g.counts()[2], "triangles": g.counts()[3]},
-                               "quality_min_max_mean": [round(x, 4) for x in q]}
+                               "quality_min_max_mean": [round(x, 4) for x in q],
+                               "launch_shapes": mixed_tune}
         g.set_precision("fp64")
+        g.set_tune(tuned)
         g.reload()
         run_step(api, g, c, heur, kern)
         forms["fp64_quality_min_max_mean"] = [round(x, 4) for x in g.quality_stats()]
         for prec in ("fp64", "mixed"):
             g.set_precision(prec)
+            g.set_tune(tuned if prec == "fp64" else mixed_tune)
             g.reload()
             run_step(api, g, c, heur, kern, graph=True)       # captures the round
             gt, gm = 0, 0.0
@@ -242,6 +247,7 @@ def b200_arm(args, rank, world, local_rank):
             forms[f"graph_{prec}"] = {"tri_in": gt, "round_ms": gm,
                                       "quality_min_max_mean": [round(x, 4) for x in g.quality_stats()]}
         g.set_precision("fp64")
+        g.set_tune(tuned)
         if rank == 0:
             forms["adjoint"] = adjoint_form(args)
             forms["precision"] = precision_form(args)
