@@ -329,7 +329,18 @@ __global__ void k_collapse(DMesh m, const int* __restrict__ indep, const int* co
     trn_tag_fix(m, destin);
     const int* vc = m.vic + (size_t) source * m.bucket;
     const int nv = m.vdeg[source];
-    for (int b = 0; b < nv; ++b) trn_activate(m, vc[b]);
+    /* re-activate the 1-ring: independent flag atomics, newly set ids listed
+     * in batches of 16 with one atomic each */
+    int ids[16], na = 0;
+    for (int b = 0; b < nv; ++b) {
+      const int t = vc[b];
+      if (trn_byte_cas01(m.activ + t)) ids[na++] = t;
+      if (na == 16) {
+        if (m.act_next) trn_list_push_n(m.act_next, m.act_next_n, ids, na);
+        na = 0;
+      }
+    }
+    if (m.act_next) trn_list_push_n(m.act_next, m.act_next_n, ids, na);
     m.vdeg[source] = 0;
     m.alive[source] = 0;
     for (int a = 0; a < deg; ++a) st[a] = -1;

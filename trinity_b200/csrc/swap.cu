@@ -200,20 +200,32 @@ __device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int*
   m.tri[id2] = make_int4(c2[0], c2[1], c2[2], 0);
   trn_stenc_append(m, c2[0], id2);
   trn_stenc_append(m, c2[1], id1);
-  trn_tag_fix(m, c1[0]);
-  trn_tag_fix(m, c1[1]);
-  trn_tag_fix(m, c1[2]);
-  trn_tag_fix(m, c2[2]);
   m.qual[id1] = q0;
   m.qual[id2] = q1;
-  for (int q = 0; q < dual_n[index]; ++q) trn_activate(m, dual[index * 4 + q]);
+  /* repair tags and re-activations: the flag atomics are independent of one
+   * another, and the newly set ones go onto their lists with one atomic
+   * each, which keeps a flip's chain of dependent L2 round trips short */
+  const int fv[4] = {c1[0], c1[1], c1[2], c2[2]};
+  int fx[4], nf = 0;
+  for (int j = 0; j < 4; ++j)
+    if (trn_byte_cas01(m.fixes + fv[j])) fx[nf++] = fv[j];
+  if (m.fix_list) trn_list_push_n(m.fix_list, m.fix_n, fx, nf);
+  int act[8], na = 0;
+  for (int q = 0; q < dual_n[index]; ++q) {
+    const int t = dual[index * 4 + q];
+    if (trn_byte_cas01(m.activ + t)) act[na++] = t;
+  }
   /* the reference follows the map even when it points at a row of an earlier
    * level (the map is reset once per call, swapping.cpp:161-162); replay keeps
    * that, the free mode (rows numbered in append order) only follows rows of
    * the current level */
   const int x = map[id2];
   if (x > -1 && (!strict_map || (x < ntasks && dual[x * 4] == id2)))
-    for (int q = 0; q < dual_n[x]; ++q) trn_activate(m, dual[x * 4 + q]);
+    for (int q = 0; q < dual_n[x]; ++q) {
+      const int t = dual[x * 4 + q];
+      if (trn_byte_cas01(m.activ + t)) act[na++] = t;
+    }
+  if (m.act_next) trn_list_push_n(m.act_next, m.act_next_n, act, na);
   return 2;
 }
 

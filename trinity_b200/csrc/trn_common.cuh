@@ -75,17 +75,14 @@ __device__ __forceinline__ void trn_set_error(int* err, int code) {
 }
 
 /* compare-and-swap 0 -> 1 on one byte (sync.h:33-38 compareAndSwap);
- * true for the one caller that made the change */
+ * true for the one caller that made the change. The flags hold 0, 1 or -1
+ * (corners), so one atomic OR of bit 0 does it: a byte at 1 or -1 keeps its
+ * value, and only the caller that saw 0 returns true */
 __device__ __forceinline__ bool trn_byte_cas01(void* p) {
   unsigned int* word = (unsigned int*) ((uintptr_t) p & ~(uintptr_t) 3);
-  unsigned int shift = ((uintptr_t) p & 3) * 8;
-  unsigned int old = *(volatile unsigned int*) word, assumed;
-  do {
-    if (((old >> shift) & 0xffu) != 0u) return false;
-    assumed = old;
-    old = atomicCAS(word, assumed, assumed | (1u << shift));
-  } while (old != assumed);
-  return true;
+  const unsigned int shift = ((uintptr_t) p & 3) * 8;
+  const unsigned int old = atomicOr(word, 1u << shift);
+  return ((old >> shift) & 0xffu) == 0u;
 }
 
 /* append id to list[*n]; the lanes of a warp that push to the same counter
@@ -111,6 +108,13 @@ __device__ __forceinline__ void trn_tag_fix(const DMesh& m, int v) {
  * listing it once for the next level */
 __device__ __forceinline__ void trn_activate(const DMesh& m, int id) {
   if (trn_byte_cas01(m.activ + id) && m.act_next) trn_list_push(m.act_next, m.act_next_n, id);
+}
+
+/* append ids[0..k) to list[*n] with one atomic */
+__device__ __forceinline__ void trn_list_push_n(int* list, int* n, const int* ids, int k) {
+  if (k <= 0) return;
+  const int base = atomicAdd(n, k);
+  for (int j = 0; j < k; ++j) list[base + j] = ids[j];
 }
 
 /* once any kernel raised the error word, later kernels of the call do no
