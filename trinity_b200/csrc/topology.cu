@@ -47,6 +47,56 @@ __global__ void k_build_vicin(DMesh m, int nb_nodes, int only_flagged) {
   }
 }
 
+/* repair of one tagged stencil (Mesh::fixTagged, mesh.cpp:716-760): keep the
+ * entries whose element still holds v, sorted, without duplicates. Stencils
+ * of up to 16 entries stay in registers (the element loads all in flight at
+ * once, a sorting network, no local memory); longer ones take the scratch
+ * array. Both give the same entries in the same order. */
+constexpr int kFixRegs = 16;
+
+__device__ __forceinline__ void fix_stencil(const DMesh& m, int v, int* buf) {
+  int* s = m.stenc + (size_t) v * m.bucket;
+  const int d = trn_deg(m, v);
+  int k = 0;
+  if (d <= kFixRegs) {
+    int r[kFixRegs];
+#pragma unroll
+    for (int a = 0; a < kFixRegs; ++a) r[a] = (a < d) ? s[a] : -1;
+#pragma unroll
+    for (int a = 0; a < kFixRegs; ++a) {
+      int keep = 0x7fffffff;
+      if (r[a] >= 0) {
+        const int4 nn = m.tri[r[a]];
+        if (v == nn.x || v == nn.y || v == nn.z) keep = r[a];
+      }
+      r[a] = keep;
+    }
+#pragma unroll
+    for (int p = 0; p < kFixRegs; ++p)
+#pragma unroll
+      for (int a = p & 1; a + 1 < kFixRegs; a += 2) {
+        const int lo = min(r[a], r[a + 1]), hi = max(r[a], r[a + 1]);
+        r[a] = lo;
+        r[a + 1] = hi;
+      }
+#pragma unroll
+    for (int a = 0; a < kFixRegs; ++a)
+      if (r[a] != 0x7fffffff && (a == 0 || r[a] != r[a - 1])) s[k++] = r[a];
+  } else {
+    for (int a = 0; a < d; ++a) {
+      const int t = s[a];
+      if (t < 0) continue;
+      const int4 nn = m.tri[t];
+      if (v == nn.x || v == nn.y || v == nn.z) buf[k++] = t;
+    }
+    trn_isort(buf, k);
+    k = trn_iunique(buf, k);
+    for (int a = 0; a < k; ++a) s[a] = buf[a];
+  }
+  for (int a = k; a < d; ++a) s[a] = -1;
+  m.deg[v] = k;
+}
+
 __global__ void k_fix_tagged(DMesh m, int nb_nodes) {
   nb_nodes = trn_nodes(m, nb_nodes);
   if (trn_failed(m)) return;
@@ -54,21 +104,7 @@ __global__ void k_fix_tagged(DMesh m, int nb_nodes) {
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
     if (!m.fixes[v]) continue;
     m.fixes[v] = 0;
-    int* s = m.stenc + (size_t) v * m.bucket;
-    int d = trn_deg(m, v);
-    if (d > m.bucket) d = m.bucket;
-    int k = 0;
-    for (int a = 0; a < d; ++a) {
-      int t = s[a];
-      if (t < 0) continue;
-      int4 n = m.tri[t];
-      if (v == n.x || v == n.y || v == n.z) buf[k++] = t;
-    }
-    trn_isort(buf, k);
-    k = trn_iunique(buf, k);
-    for (int a = 0; a < k; ++a) s[a] = buf[a];
-    for (int a = k; a < d; ++a) s[a] = -1;
-    m.deg[v] = k;
+    fix_stencil(m, v, buf);
   }
 }
 
@@ -81,20 +117,7 @@ __global__ void k_fix_list(DMesh m, const int* __restrict__ list, const int* cou
     const int v = list[q];
     if (!m.fixes[v]) continue;
     m.fixes[v] = 0;
-    int* s = m.stenc + (size_t) v * m.bucket;
-    const int d = trn_deg(m, v);
-    int k = 0;
-    for (int a = 0; a < d; ++a) {
-      int t = s[a];
-      if (t < 0) continue;
-      int4 nn = m.tri[t];
-      if (v == nn.x || v == nn.y || v == nn.z) buf[k++] = t;
-    }
-    trn_isort(buf, k);
-    k = trn_iunique(buf, k);
-    for (int a = 0; a < k; ++a) s[a] = buf[a];
-    for (int a = k; a < d; ++a) s[a] = -1;
-    m.deg[v] = k;
+    fix_stencil(m, v, buf);
   }
 }
 
