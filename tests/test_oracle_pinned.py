@@ -7,6 +7,7 @@ import os
 
 import pytest
 
+from tests.oracle_lib import REF_EXACT as REF_EXACT_BIN
 from tests.oracle_lib import Oracle, digest, run_pipeline
 from trinity_b200 import meshgen
 
@@ -43,3 +44,29 @@ def test_oracle_matches_reference_on_grid4_fixture(oracle_built):
     m = meshgen.read_mesh(os.path.join(REF_SRC, g["fixture"]["mesh"]))
     u = meshgen.read_bb(os.path.join(REF_SRC, g["fixture"]["bb"]), m.nb_nodes)
     _check("grid4_shock4", m, u, g["params"], g["params"]["bucket"])
+
+
+@pytest.mark.skipif(not os.path.exists(REF_EXACT_BIN), reason="reference build (oracle/_ref) absent")
+def test_harness_final_snapshot_is_last_stage(oracle_built, tmp_path):
+    """The harness's --final snapshot (read by the reference-build comparison
+    of the free mode) is the state after the last kernel of the last round,
+    the same as the oracle's."""
+    import subprocess
+    from tests.oracle_lib import read_snapshot
+    m, u, c = meshgen.make_config("c2", 40)
+    mp, bp = str(tmp_path / "m.mesh"), str(tmp_path / "m.bb")
+    meshgen.write_mesh(mp, m)
+    meshgen.write_bb(bp, u)
+    pre, fin = str(tmp_path / "d"), str(tmp_path / "final.bin")
+    subprocess.run([REF_EXACT_BIN, mp, bp, "2", str(c["depth"]), str(c["bucket"]), str(c["target"]),
+                    str(c["norm"]), "--capa-depth", "4", "--dump", pre, "--final", fin],
+                   check=True, capture_output=True, timeout=300,
+                   env=dict(os.environ, OMP_NUM_THREADS="1"))
+    last = read_snapshot(pre + ".r1.smooth.bin")
+    final = read_snapshot(fin)
+    assert not final.diff(last)
+    params = dict(c)
+    params["rounds"] = 2
+    o = Oracle(m, u, capa_scale=9, bucket=c["bucket"])
+    run_pipeline(o, params)
+    assert digest(o.state()) == digest(final)
