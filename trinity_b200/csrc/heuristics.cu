@@ -391,18 +391,32 @@ __global__ void k_color_round(DMesh m, const int* __restrict__ list, const int* 
   }
 }
 
+/* Within a color class the vertices are ordered by stencil length (bins of
+ * 3, 4, .., 10 and more): the smoothing of a class then runs warps of equal
+ * degree, whose quality loops do not wait for one long stencil. A class is
+ * an independent set, so the order inside it changes no result. Keys are
+ * color * kDegBins + bin. */
+constexpr int kDegBins = 8;
+constexpr int kColorKeys = 32 * kDegBins;
+
+__device__ __forceinline__ int color_key(const DMesh& m, int v, int c) {
+  int b = trn_deg(m, v) - 3;
+  b = b < 0 ? 0 : (b >= kDegBins ? kDegBins - 1 : b);
+  return c * kDegBins + b;
+}
+
 __global__ void k_color_count(DMesh m, int nb_nodes, const int* color, int* cnt, int max_col) {
   nb_nodes = trn_nodes(m, nb_nodes);
-  __shared__ int sc[32];
-  if (threadIdx.x < 32) sc[threadIdx.x] = 0;
+  __shared__ int sc[kColorKeys];
+  for (int k = threadIdx.x; k < kColorKeys; k += blockDim.x) sc[k] = 0;
   __syncthreads();
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
     int c = color[v] & 0xff;
-    if (color[v] != 0 && c >= 1 && c <= max_col) atomicAdd(sc + c, 1);
+    if (color[v] != 0 && c >= 1 && c <= max_col) atomicAdd(sc + color_key(m, v, c), 1);
   }
   __syncthreads();
-  if (threadIdx.x >= 1 && threadIdx.x <= max_col && sc[threadIdx.x])
-    atomicAdd(cnt + threadIdx.x, sc[threadIdx.x]);
+  for (int k = threadIdx.x; k < kColorKeys; k += blockDim.x)
+    if (sc[k]) atomicAdd(cnt + k, sc[k]);
 }
 
 /* before a round: its number, and the list it fills starts empty */
@@ -429,37 +443,39 @@ __global__ void k_color_offsets(const int* cnt, int* part_off, int* cursor, int 
   int acc = 0;
   for (int c = 1; c <= max_col; ++c) {
     part_off[c - 1] = acc;
-    cursor[c] = acc;
-    acc += cnt[c];
+    for (int b = 0; b < kDegBins; ++b) {
+      cursor[c * kDegBins + b] = acc;
+      acc += cnt[c * kDegBins + b];
+    }
   }
   part_off[max_col] = acc;
 }
 
-/* vertices into their color's part; per block, the slots are counted in
- * shared memory and reserved with one global atomic per color (a global
- * atomic per vertex on at most 31 cursors serialises) */
-__global__ void k_color_scatter(int nb_nodes, const int* nbp, int* color, int* cursor, int* parts,
+/* vertices into their color's part, by degree bin; per block, the slots are
+ * counted in shared memory and reserved with one global atomic per key (a
+ * global atomic per vertex on a few cursors serialises) */
+__global__ void k_color_scatter(DMesh m, int nb_nodes, const int* nbp, int* color, int* cursor, int* parts,
                                 int max_col) {
   if (nbp) nb_nodes = nbp[0];
-  __shared__ int cnt[32], base[32];
+  __shared__ int cnt[kColorKeys], base[kColorKeys];
   for (int v0 = blockIdx.x * blockDim.x; v0 < nb_nodes; v0 += gridDim.x * blockDim.x) {
-    if (threadIdx.x < 32) cnt[threadIdx.x] = 0;
+    for (int k = threadIdx.x; k < kColorKeys; k += blockDim.x) cnt[k] = 0;
     __syncthreads();
     const int v = v0 + threadIdx.x;
-    int c = 0, slot = 0;
+    int key = -1, slot = 0;
     if (v < nb_nodes) {
       const int cw = color[v];
       if (cw != 0 && (cw & 0xff) >= 1 && (cw & 0xff) <= max_col) {
-        c = cw & 0xff;
-        slot = atomicAdd(cnt + c, 1);
+        key = color_key(m, v, cw & 0xff);
+        slot = atomicAdd(cnt + key, 1);
       }
       color[v] = 0;
     }
     __syncthreads();
-    if (threadIdx.x >= 1 && threadIdx.x <= max_col && cnt[threadIdx.x] > 0)
-      base[threadIdx.x] = atomicAdd(cursor + threadIdx.x, cnt[threadIdx.x]);
+    for (int k = threadIdx.x; k < kColorKeys; k += blockDim.x)
+      if (cnt[k] > 0) base[k] = atomicAdd(cursor + k, cnt[k]);
     __syncthreads();
-    if (c) parts[base[c] + slot] = v;
+    if (key >= 0) parts[base[key] + slot] = v;
     __syncthreads();
   }
 }
@@ -503,14 +519,14 @@ void color_finish(const DMesh& m, int hint, int max_col, HeurWs& ws, int* parts,
                   unsigned* tick, cudaStream_t s) {
   ProfScope ps("color_jp", s, 0.0);
   const int g = grid_for(hint);
-  int* cnt = ws.cnt + 4;      /* 32 slots */
-  int* cursor = ws.cnt + 40;  /* 32 slots */
-  cudaMemsetAsync(cnt, 0, sizeof(int) * 32, s);
+  int* cnt = ws.color_keys;                 /* kColorKeys slots */
+  int* cursor = ws.color_keys + kColorKeys;  /* kColorKeys slots */
+  cudaMemsetAsync(cnt, 0, sizeof(int) * kColorKeys, s);
   k_color_count<<<g, TRN_THREADS, 0, s>>>(m, hint, ws.color, cnt, max_col);
   note_launch();
   k_color_offsets<<<1, 32, 0, s>>>(cnt, part_off, cursor, max_col, tick);
   note_launch();
-  k_color_scatter<<<g, TRN_THREADS, 0, s>>>(hint, m.nb, ws.color, cursor, parts, max_col);
+  k_color_scatter<<<g, TRN_THREADS, 0, s>>>(m, hint, m.nb, ws.color, cursor, parts, max_col);
   note_launch();
   check_launch("color_jp");
 }
@@ -540,6 +556,7 @@ void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {
   cudaMalloc(&ws->mate, sizeof(int) * (size_t) capa_elem);
   cudaMalloc(&ws->rank, sizeof(uint32_t) * 4 * (size_t) capa_elem);
   cudaMalloc(&ws->cnt, sizeof(int) * 128);
+  cudaMalloc(&ws->color_keys, sizeof(int) * 2 * kColorKeys);
   cudaMalloc(&ws->list_a, sizeof(int) * big);
   cudaMalloc(&ws->list_b, sizeof(int) * big);
   cudaMalloc(&ws->fix_list, sizeof(int) * (size_t) capa_node);
@@ -554,6 +571,7 @@ void heur_ws_free(HeurWs* ws) {
   cudaFree(ws->mate);
   cudaFree(ws->rank);
   cudaFree(ws->cnt);
+  cudaFree(ws->color_keys);
   cudaFree(ws->list_a);
   cudaFree(ws->list_b);
   cudaFree(ws->fix_list);

@@ -196,6 +196,7 @@ struct HeurWs {
   int* mate = nullptr;
   uint32_t* rank = nullptr;      /* four flip ranks per swap dual row */
   int* cnt = nullptr;            /* small device counters */
+  int* color_keys = nullptr;     /* counts and cursors of the coloring's (color, degree) keys */
   int* list_a = nullptr;         /* two worklists (activity, coloring) */
   int* list_b = nullptr;
   int* fix_list = nullptr;       /* vertices tagged for repair */
