@@ -60,6 +60,9 @@ struct orc_mesh {
   /* Swap / Match state (swapping.h, matching.h) */
   int *map, *dual, *dual_n, *matched;
   signed char *visited, *degree;
+  int swap_rule;      /* ORC_SWAP_*: the reference's matching, or an emulation */
+  int *hs_mate, *hs_choice;
+  uint64_t* hs_prop;
   /* Refine hashtable (hashtable.h) as an open-addressing map (min,max)->id */
   int64_t* hkey;
   int* hval;
@@ -386,6 +389,9 @@ orc_mesh* orc_create(int capa_node, int capa_elem, int bucket) {
   m->matched = (int*) malloc(ce * sizeof(int));
   m->visited = (signed char*) calloc(ce, 1);
   m->degree = (signed char*) calloc(ce, 1);
+  m->hs_mate = (int*) malloc(ce * sizeof(int));
+  m->hs_choice = (int*) malloc(ce * sizeof(int));
+  m->hs_prop = (uint64_t*) calloc(ce, sizeof(uint64_t));
   if (!m->points || !m->tensor || !m->elems || !m->stenc || !m->vicin || !m->dual) {
     orc_destroy(m);
     return NULL;
@@ -404,7 +410,8 @@ void orc_destroy(orc_mesh* m) {
   free(m->alive); free(m->tags); free(m->activ); free(m->fixes);
   for (int i = 0; i < MAX_PART; ++i) free(m->subset[i]);
   free(m->map); free(m->dual); free(m->dual_n); free(m->matched);
-  free(m->visited); free(m->degree); free(m->hkey); free(m->hval); free(m->log.a);
+  free(m->visited); free(m->degree); free(m->hs_mate); free(m->hs_choice); free(m->hs_prop);
+  free(m->hkey); free(m->hval); free(m->log.a);
   free(m);
 }
 
@@ -1149,6 +1156,122 @@ static void match_and_update(orc_mesh* m, int vertex, ivec* stack) {
   } while (stack->n);
 }
 
+/* ---- emulated matching rules (analysis only; ORC_SWAP_REFERENCE is the
+ * reference) ---------------------------------------------------------- */
+
+/* the reference's loop without the degree-1 stack: each row in order takes
+ * free neighbours, stopping at the first one ever listed as a candidate in
+ * this call (matching.cpp:115-132 without lines 124-129) */
+static void match_sequential_rows(orc_mesh* m, int nt) {
+  for (int i = 0; i < nt; ++i) {
+    const int c = D(m, i)[0];
+    if (m->visited[c]) continue;
+    m->visited[c] = 1;
+    for (int a = 1; a < m->dual_n[i]; ++a) {
+      const int n = D(m, i)[a];
+      if (m->visited[n]) continue;
+      m->visited[n] = 1;
+      m->matched[c] = n;
+      m->matched[n] = MATCHED;
+      if (m->map[n] < 0) continue;
+      break;
+    }
+  }
+}
+
+static uint64_t hs_mix(uint64_t x) {
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ULL;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebULL;
+  return x ^ (x >> 31);
+}
+
+static int hs_row_of(orc_mesh* m, int e, int nt) {
+  const int x = m->map[e];
+  return (x >= 0 && x < nt && D(m, x)[0] == e) ? x : -1;
+}
+
+/* weight of dual edge (row i, slot q) in the round-synchronous handshake:
+ * a symmetric hash (random rule) or the edge's slot in the row of its
+ * lower-id candidate end, then the hash (row-slot rule) */
+static uint32_t hs_weight(orc_mesh* m, int nt, int i, int q, int round, int level) {
+  const int c = D(m, i)[0], n = D(m, i)[q];
+  const int lo = c < n ? c : n, hi = c < n ? n : c;
+  const uint64_t h = hs_mix(((uint64_t) (uint32_t) lo << 32 | (uint32_t) hi) ^
+                            ((uint64_t) (round + 16 * level) * 0xd1b54a32d192ed03ULL));
+  if (m->swap_rule == ORC_SWAP_HANDSHAKE_RANDOM) return (uint32_t) (h >> 32) | 1u;
+  int pos = q;
+  const int xn = hs_row_of(m, n, nt);
+  if (xn >= 0 && n < c)
+    for (int a = 1; a < m->dual_n[xn]; ++a)
+      if (D(m, xn)[a] == c) pos = a;
+  return ((uint32_t) (4 - pos) << 30) | ((uint32_t) (h >> 34)) | 1u;
+}
+
+/* the GPU free mode's rule: rounds of proposals along each unmatched
+ * candidate's heaviest free edge; mutual candidate pairs match, a
+ * non-candidate accepts its heaviest proposer */
+static void match_handshake_emul(orc_mesh* m, int nt, int level) {
+  int* mate = m->hs_mate;
+  int* choice = m->hs_choice;
+  uint64_t* prop = m->hs_prop;
+  for (int i = 0; i < nt; ++i)
+    for (int a = 0; a < m->dual_n[i]; ++a) {
+      mate[D(m, i)[a]] = -1;
+      prop[D(m, i)[a]] = 0;
+    }
+  for (int r = 0; r < 4; ++r) {
+    for (int i = 0; i < nt; ++i) {
+      const int c = D(m, i)[0];
+      int best = -1;
+      uint32_t bw = 0;
+      if (mate[c] == -1)
+        for (int q = 1; q < m->dual_n[i]; ++q) {
+          if (mate[D(m, i)[q]] != -1) continue;
+          const uint32_t w = hs_weight(m, nt, i, q, r, level);
+          if (w > bw) { bw = w; best = q; }
+        }
+      choice[i] = best < 0 ? -1 : D(m, i)[best];
+      if (best >= 0) {
+        const uint64_t key = ((uint64_t) bw << 32) | (uint32_t) c;
+        if (key > prop[D(m, i)[best]]) prop[D(m, i)[best]] = key;
+      }
+    }
+    /* decisions read this round's proposals only, then apply */
+    ivec acc = {0};
+    for (int i = 0; i < nt; ++i) {
+      const int n = choice[i];
+      if (n < 0) continue;
+      const int c = D(m, i)[0];
+      const int x = hs_row_of(m, n, nt);
+      int ok;
+      if (x >= 0) {
+        ok = choice[x] == c && c < n;
+      } else {
+        int q = 1;
+        while (D(m, i)[q] != n) ++q;
+        ok = prop[n] == (((uint64_t) hs_weight(m, nt, i, q, r, level) << 32) | (uint32_t) c);
+      }
+      if (ok) { iv_push(&acc, c); iv_push(&acc, n); }
+    }
+    for (int p = 0; p < acc.n; p += 2) {
+      mate[acc.a[p]] = acc.a[p + 1];
+      mate[acc.a[p + 1]] = acc.a[p];
+      m->matched[acc.a[p]] = acc.a[p + 1];
+    }
+    free(acc.a);
+    for (int i = 0; i < nt; ++i)
+      for (int a = 1; a < m->dual_n[i]; ++a) prop[D(m, i)[a]] = 0;
+  }
+}
+
+int orc_set_swap_rule(orc_mesh* m, int rule) {
+  if (rule < ORC_SWAP_REFERENCE || rule > ORC_SWAP_HANDSHAKE_ROWSLOT) return ORC_ERR_INVALID;
+  m->swap_rule = rule;
+  return ORC_OK;
+}
+
 /* Swap::swap, swapping.cpp:55-149; returns 2 on a committed flip */
 static int swap_pair(orc_mesh* m, int id1, int id2, int index) {
   int cur1[3] = {-1, -1, -1}, cur2[3] = {-1, -1, -1};
@@ -1270,7 +1393,12 @@ int orc_swap(orc_mesh* m) {
     for (int i = 0; i < m->capa_elem; ++i) m->matched[i] = -1;
     for (int i = 0; i < list.n; ++i)
       m->degree[D(m, i)[0]] = (signed char) (m->dual_n[i] - 1);
-    for (int i = 0; i < list.n; ++i) match_and_update(m, i, &stack);
+    if (m->swap_rule == ORC_SWAP_REFERENCE)
+      for (int i = 0; i < list.n; ++i) match_and_update(m, i, &stack);
+    else if (m->swap_rule == ORC_SWAP_SEQUENTIAL_ROWS)
+      match_sequential_rows(m, list.n);
+    else
+      match_handshake_emul(m, list.n, levels);
     /* processFlips, swapping.cpp:251-269 (pairs are disjoint: order-free) */
     int npairs = 0;
     for (int index = 0; index < list.n; ++index) {

@@ -64,6 +64,19 @@ double orc_complexity(const orc_mesh* m);
 /* per-kernel counters of the last run: [0]=evaluated [1]=tasks [2]=committed [3]=levels */
 void orc_counters(const orc_mesh* m, int out[4]);
 
+/* Swap matching rule, for the analysis of the GPU free mode only:
+ * ORC_SWAP_REFERENCE (default) is the reference's greedy with its degree-1
+ * stack (matching.cpp:81-135); the others are emulations: the same loop
+ * without the stack, and the GPU's round-synchronous handshake with random
+ * or row-slot edge weights. */
+enum {
+  ORC_SWAP_REFERENCE = 0,
+  ORC_SWAP_SEQUENTIAL_ROWS = 1,
+  ORC_SWAP_HANDSHAKE_RANDOM = 2,
+  ORC_SWAP_HANDSHAKE_ROWSLOT = 3,
+};
+int orc_set_swap_rule(orc_mesh* m, int rule);
+
 const int32_t* orc_log(const orc_mesh* m, size_t* n);
 void orc_log_clear(orc_mesh* m);
 

@@ -52,6 +52,7 @@ def lib():
         L.orc_log.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
         L.orc_log.restype = ctypes.POINTER(ctypes.c_int32)
         L.orc_log_clear.argtypes = [vp]
+        L.orc_set_swap_rule.argtypes = [vp, ip]
         L.orc_eigen.argtypes = [vp, vp, vp, vp]
         L.orc_interpolate.argtypes = [vp, vp, ip]
         L.orc_quality.argtypes = [vp] * 6
@@ -187,6 +188,13 @@ class Oracle:
         alive = np.zeros(nn, np.uint8); tags = np.zeros(nn, np.uint8)
         self.L.orc_export(self.h, _p(pts), _p(ten), _p(el), _p(alive), _p(tags))
         return State(pts, ten, el, alive, tags)
+
+    SWAP_RULES = {"reference": 0, "sequential_rows": 1, "handshake_random": 2, "handshake_rowslot": 3}
+
+    def set_swap_rule(self, rule: str) -> None:
+        """Swap matching rule (analysis of the GPU free mode; "reference" is
+        the reference's own)."""
+        self._chk(self.L.orc_set_swap_rule(self.h, self.SWAP_RULES[rule]), "set_swap_rule")
 
     def log(self) -> np.ndarray:
         n = ctypes.c_size_t(0)

@@ -1,0 +1,54 @@
+"""Why the GPU free mode ranks swap-matching edges by their row slot.
+
+The oracle runs the whole round with the reference's heuristics; only the
+swap stage's matching is replaced by an emulated rule (oracle
+ORC_SWAP_*): the reference's loop without its degree-1 stack, and the GPU's
+round-synchronous handshake with random or row-slot edge weights. On the
+same input (2M-triangle workload's generator at 120 x 120, 3 rounds) the
+final meshes show what each part of the reference's rule contributes to the
+metric edge-length histogram: the sequential row-order loop alone gives the
+reference's histogram, random weights lose in-range edges, and row-slot
+weights give the reference's in-range fraction back. Deterministic: the
+oracle is single-threaded."""
+import numpy as np
+import pytest
+
+from tests import oracle_lib
+from tests.helpers import check_invariants, in_range_fraction, metric_lengths
+from tests.oracle_lib import Oracle
+from trinity_b200 import meshgen
+
+EDGES = np.array([0, 0.5, 1 / np.sqrt(2), 0.85, 1.0, 1.2, np.sqrt(2), 2.0, np.inf])
+
+
+@pytest.fixture(scope="module")
+def finals(oracle_built):
+    m, u, c = meshgen.make_config("c2", 120)
+    out = {}
+    for rule in Oracle.SWAP_RULES:
+        o = Oracle(m, u, capa_scale=9, bucket=c["bucket"])
+        o.set_swap_rule(rule)
+        oracle_lib.run_pipeline(o, c)
+        st = o.state()
+        h, _ = np.histogram(metric_lengths(st), EDGES)
+        out[rule] = (st, h / h.sum(), in_range_fraction(st))
+    return out
+
+
+def test_every_rule_keeps_the_mesh_valid(finals):
+    for st, _, _ in finals.values():
+        check_invariants(st)
+
+
+def test_sequential_row_loop_gives_the_reference_histogram(finals):
+    _, h_ref, _ = finals["reference"]
+    _, h_seq, _ = finals["sequential_rows"]
+    assert np.abs(h_seq - h_ref).max() <= 0.0025, (h_seq.round(4), h_ref.round(4))
+
+
+def test_row_slot_weights_restore_the_in_range_fraction(finals):
+    f_ref = finals["reference"][2]
+    f_rand = finals["handshake_random"][2]
+    f_slot = finals["handshake_rowslot"][2]
+    assert f_rand < f_slot
+    assert abs(f_slot - f_ref) <= 0.001, (f_slot, f_ref)
