@@ -65,3 +65,17 @@ def test_shard_meshes_balanced_and_complete():
         loads = [sum(sizes[i] for i in lst) for lst in sh]
         assert max(loads) - min(loads) <= max(sizes)
         assert sh == shard_meshes(sizes, world)
+
+
+def test_reference_arm_only_rank0_prints():
+    """Under torchrun the reference arm runs on rank 0 only: another rank
+    exits 0 at once and prints nothing."""
+    import subprocess
+    import sys
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2", MASTER_ADDR="127.0.0.1",
+               MASTER_PORT=str(_free_port()))
+    r = subprocess.run([sys.executable, os.path.join(repo, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--steps", "1", "--warmup", "3"], env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-500:]
+    assert r.stdout.strip() == ""
