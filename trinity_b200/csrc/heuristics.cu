@@ -25,7 +25,8 @@
  *                   symmetric hash.
  *   color_jp        Jones-Plassmann first-fit coloring of the interior
  *                   vertices with colors 1..max_col; a vertex left without a
- *                   free color is not smoothed, as in the reference.
+ *                   free color is not smoothed, as in the reference. Each
+ *                   class lists its vertices grouped by stencil length.
  */
 #include "trn_internal.h"
 
