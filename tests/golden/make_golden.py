@@ -22,13 +22,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 
-from tests.oracle_lib import REF_EXACT, ORACLE_DIR, digest, read_snapshot  # noqa: E402
+from tests.oracle_lib import REF_EXACT, REF_SRC, ORACLE_DIR, digest, read_snapshot  # noqa: E402
 from trinity_b200 import meshgen  # noqa: E402
 
-REF_SRC = "/root/reference"
 
 # (name, generator config, grid side override, rounds)
-CASES = [("c1", "c1", None, 3), ("c2_n60", "c2", 60, 2), ("c4_n50", "c4", 50, 2)]
+CASES = [("c1", "c1", None, 3), ("c2_n60", "c2", 60, 2), ("c4_n50", "c4", 50, 2),
+         ("c2", "c2", None, 3)]
 FIXTURE_CASES = [("grid4_shock4", "examples/mesh/GRID4.mesh", "examples/solut/shock4.bb", 2, 3, 64, 1.0, 2)]
 
 
@@ -48,7 +48,7 @@ def run_ref(mesh, bb, rounds, depth, bucket, target, norm, tmp, tag):
 
 
 def main():
-    subprocess.run(["make", "-s", "-C", ORACLE_DIR, "ref"], check=True)
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR, "ref", f"REF={REF_SRC}"], check=True)
     out = {}
     with tempfile.TemporaryDirectory() as tmp:
         for tag, cfg, n, rounds in CASES:

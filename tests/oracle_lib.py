@@ -16,6 +16,10 @@ ORACLE_DIR = os.path.join(REPO, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
 REF_EXACT = os.path.join(ORACLE_DIR, "_ref", "trinity_ref_exact")
 REF_TIMED = os.path.join(ORACLE_DIR, "_ref", "trinity_ref")
+# trinity's own source tree (read only where it is mounted: golden fixtures,
+# the C++ shim compile test and trinity's GRID4 fixture); one variable, one
+# default
+REF_SRC = os.environ.get("TRN_REFERENCE_DIR", "/root/reference")
 
 LOG_MIS, LOG_MATCH, LOG_COLORING = 1, 2, 3
 TAG_BOUND, TAG_CORNER = 4, 8

@@ -6,8 +6,9 @@ import subprocess
 
 import pytest
 
+from tests.oracle_lib import REF_SRC as REF
+
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = "/root/reference"
 
 
 @pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "src")), reason="reference sources not mounted")

@@ -1,11 +1,18 @@
 """Replay parity: the GPU fed the oracle's independent sets, matchings and
 colorings reproduces the reference's 1-thread run bit for bit after every
 stage (metric tensors and points, element array, vertex liveness and tags)."""
+import json
+import os
+
 import pytest
 
 from tests.helpers import gpu_mesh, gpu_state, oracle_run, run_gpu_stages
+from tests.oracle_lib import Oracle, digest, run_pipeline
+from trinity_b200 import meshgen
 
 CASES = [("c1", 40, 2), ("c1", None, 3), ("c2", 60, 2), ("c4", 50, 2)]
+GOLD = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                   "ref_stage_digests.json")))
 
 
 @pytest.mark.gpu
@@ -49,3 +56,33 @@ def test_grouped_smoothing_same_results(oracle_built, lanes, prec):
         assert not st.diff(runs[1][stage]), stage
         if prec == "fp64":
             assert not st.diff(states[stage]), stage
+
+
+@pytest.mark.gpu
+def test_replay_full_size_workload_matches_reference_digests(oracle_built):
+    """The full 2M-triangle workload (1000 x 1000 jittered grid, depth 2,
+    bucket 128, target 0.7, L^2, 3 rounds): fed the oracle's decisions, the
+    GPU's state after the metric and after every stage of every round hashes
+    to the digests of the reference's own 1-thread run (written by
+    tests/golden/make_golden.py), so capacity, bucket and id-ordering effects
+    that only appear at this size are covered too."""
+    want = GOLD["c2"]["stages"]
+    m, u, c = meshgen.make_config("c2")
+    o = Oracle(m, u, capa_scale=9, bucket=c["bucket"])
+    run_pipeline(o, c)
+    log = o.log()
+    del o
+    g = gpu_mesh(m, u, c)
+    assert digest(gpu_state(g)) == want["load"], "load"
+    g.set_replay(log)
+    seen = []
+
+    def check(stage):
+        got = digest(gpu_state(g))
+        bad = [k for k in got if got[k] != want[stage][k]]
+        assert not bad, f"stage {stage}: {bad} differ from the reference"
+        seen.append(stage)
+
+    run_gpu_stages(g, c, check)
+    g.close()
+    assert len(seen) == 1 + 4 * c["rounds"]

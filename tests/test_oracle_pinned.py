@@ -8,12 +8,11 @@ import os
 import pytest
 
 from tests.oracle_lib import REF_EXACT as REF_EXACT_BIN
-from tests.oracle_lib import Oracle, digest, run_pipeline
+from tests.oracle_lib import REF_SRC, Oracle, digest, run_pipeline
 from trinity_b200 import meshgen
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = json.load(open(os.path.join(HERE, "golden", "ref_stage_digests.json")))
-REF_SRC = "/root/reference"
 
 
 def _check(name, m, u, params, bucket):
@@ -28,7 +27,7 @@ def _check(name, m, u, params, bucket):
     run_pipeline(o, params, log_stage=check)
 
 
-@pytest.mark.parametrize("name", ["c1", "c2_n60", "c4_n50"])
+@pytest.mark.parametrize("name", ["c1", "c2_n60", "c4_n50", "c2"])
 def test_oracle_matches_reference_digests(oracle_built, name):
     g = GOLD[name]
     m, u, c = meshgen.make_config(g["config"]["name"], g["config"]["n"])
