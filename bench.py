@@ -57,7 +57,6 @@ def workload_config(grid=None):
         "workload": "unit square 1000x1000 grid, 1,002,001 vertices / 2,000,000 triangles, "
                     "interior jitter 0.2h (seed 2), field tanh+gauss+waves, target 0.7, "
                     "L^2 norm, depth 2, bucket 128, 3 rounds",
-        "mode": "free (GPU heuristics)",
         "data": "synthetic, generated by trinity_b200/meshgen.py",
         "l2": "working set larger than L2 (mesh restored every step)",
     }
@@ -175,10 +174,12 @@ def b200_arm(args, rank, world, local_rank):
     # CUDA events (the events cost ~9 % of throughput, so they stay out of
     # the timed region except around the dominant kernel) ----
     _lib.profile_enable(True)
+    _lib.profile_count_bytes(True, g.capacity()[0])
     for _ in range(min(args.steps, 2)):
         g.reload()
         run_step(api, g, c, heur, kern)
     prof_all = _lib.profile_read()
+    _lib.profile_count_bytes(False)
     _lib.profile_enable(False)
     dom_name = max(prof_all, key=lambda r: r["ms"])["kernel"] if prof_all else None
 
@@ -295,7 +296,11 @@ def b200_arm(args, rank, world, local_rank):
         peaks = json.load(open(pk))
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     if dom:
-        per_launch_bytes = dom["bytes"] / max(dom["launches"], 1)
+        # algorithmic bytes per launch: counted on the device in the profiled
+        # steps (the same deterministic launches as the timed ones); the time
+        # per launch from the timed steps' events
+        dom_all = next(r for r in prof_all if r["kernel"] == dom["kernel"])
+        per_launch_bytes = dom_all["bytes"] / max(dom_all["launches"], 1)
         per_launch_s = dom["ms"] / max(dom["launches"], 1) / 1e3
         achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
         roofline = {"kernel": dom["kernel"], "bound": "hbm", "achieved": round(achieved, 2),
@@ -306,6 +311,9 @@ def b200_arm(args, rank, world, local_rank):
                                     "caches (mean of the 7 class launches of the first pass)",
                     "launches": dom["launches"],
                     "avg_launch_us": round(per_launch_s * 1e6, 2),
+                    "algorithmic_bytes_per_launch": round(per_launch_bytes),
+                    "bytes_source": "counted on the device (distinct entries per launch)"
+                    if dom_all.get("bytes_counted") else "launcher's model",
                     "share_of_kernel_time": round(
                         sum(r["ms"] for r in prof_all if r["kernel"] == dom["kernel"])
                         / sum(r["ms"] for r in prof_all), 3),
@@ -318,15 +326,17 @@ def b200_arm(args, rank, world, local_rank):
         "round_ms_per_step": round(tms_max / args.steps, 3),
         "metric_ms_per_step": round(float(np.mean(metric_ms)), 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": cfg,
+        "data": "synthetic", "mode": "free (GPU heuristics)", "config": cfg,
         "e2e": {"value": round(e2e_tin_all / e2e_max, 1) if e2e_max > 0 else None, "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "note": "pinned host arrays -> C ABI load, metric, 3 rounds, compact export of the "
                         "adapted mesh (points, triangles, metric) into pinned host arrays; wall clock"},
         "gpu_launches": int(launches),
         "roofline": roofline,
-        "kernels": sorted(({"kernel": r["kernel"], "launches": r["launches"], "ms": round(r["ms"], 3)}
-                           for r in prof_all), key=lambda r: -r["ms"])[:10],
+        "kernels": sorted(({"kernel": r["kernel"], "launches": r["launches"], "ms": round(r["ms"], 3),
+                            "gbs": round(r["bytes"] / (r["ms"] / 1e3) / 1e9, 1) if r["ms"] > 0 else None,
+                            "bytes": "counted" if r.get("bytes_counted") else "model"}
+                           for r in prof_all), key=lambda r: -r["ms"]),
         "kernels_note": f"{min(args.steps, 2)} profiled steps (every launch timed), before the timed region",
         "final_mesh": {"nodes": final[2], "triangles": final[3]},
         "launch_shapes": dict(tuned, chosen_by="defaults (--no-tune)" if args.no_tune
@@ -375,6 +385,15 @@ def _metric_lengths(pts, tri, ten):
     return np.where(np.abs(l0 - l1) < 1e-9, l0, geo)
 
 
+def tensor_error(t32, t64):
+    """per vertex, |T32 - T64| / max |T64| over the components (m11, m12,
+    m22): median, RMS, 99th percentile, max, and the fraction above 1e-5"""
+    e = np.abs(t32 - t64).max(axis=1) / np.maximum(np.abs(t64).max(axis=1), 1e-300)
+    return {"rel_err_median": float(np.median(e)), "rel_err_rms": float(np.sqrt(np.mean(e ** 2))),
+            "rel_err_p99": float(np.percentile(e, 99)), "rel_err_max": float(e.max()),
+            "fraction_above_1e-5": round(float(np.mean(e > 1e-5)), 6)}
+
+
 def precision_form(args):
     """The mixed-precision form on the ~4M-triangle mesh (1414x1414 grid,
     jitter 0.2h, multi-feature field, depth 2): (1) one smoothing pass from
@@ -388,6 +407,21 @@ def precision_form(args):
     tags = tags_of(m)
     out = {"workload": f"unit square {m.nb_nodes} vertices / {m.nb_elems} triangles, jitter 0.2h "
                        "(seed 3), field tanh+gauss+waves, target 0.7, L^2, depth 2, bucket 128"}
+    # (0) the metric recovery itself in both forms, from the same input
+    rec = {}
+    for prec in ("fp64", "mixed"):
+        g = api.Mesh((m.nb_nodes, m.nb_elems), c["bucket"], c["depth"], 0, c["rounds"])
+        g.load_arrays(m.points, m.tris, tags, u)
+        g.set_precision(prec)
+        api.Metrics(g, c["target"], c["norm"]).run()
+        rec[prec] = (g.export()[1], g.last_time_ms())
+        g.close()
+    out["metric_recovery"] = dict(tensor_error(rec["mixed"][0], rec["fp64"][0]),
+                                  ms_fp64=round(rec["fp64"][1], 3), ms_mixed=round(rec["mixed"][1], 3),
+                                  note="Metrics::run from the same input: FP32 patch means (FP64 coordinate "
+                                       "and value differences), FP32 eigen-clamp and scalings, FP64 "
+                                       "complexity sum, against the FP64 form (itself the oracle's "
+                                       "tensors to the last bits)")
     gs = {}
     for prec in ("fp64", "mixed"):
         g = api.Mesh((m.nb_nodes, m.nb_elems), c["bucket"], c["depth"], 0, c["rounds"])
@@ -412,6 +446,8 @@ def precision_form(args):
     derr = np.linalg.norm(p32[live] - p64[live], axis=1)[moved] / d64[moved]
     terr = (np.abs(t32[live] - t64[live]) / np.maximum(np.abs(t64[live]).max(axis=1, keepdims=True), 1e-300))
     flip = derr > 1e-3     # a different accept / back-off decision, not rounding
+    same = np.ones(live.sum(), bool)
+    same[np.flatnonzero(moved)[flip]] = False
     out["same_state_smoothing_pass"] = {
         "vertices_moved_fp64": int(moved.sum()),
         "decision_differs_fraction": round(float(flip.mean()), 6) if derr.size else 0.0,
@@ -421,8 +457,9 @@ def precision_form(args):
         "displacement_rel_err_rms": float(np.sqrt(np.mean(derr ** 2))) if derr.size else 0.0,
         "displacement_rel_err_median": float(np.median(derr)) if derr.size else 0.0,
         "tensor_rel_err_max": float(terr.max()), "tensor_rel_err_rms": float(np.sqrt(np.mean(terr ** 2))),
-        "note": "same FP64 state, same coloring; metric recovery itself is FP64 in both forms "
-                "(tensor error 0 after Metrics::run)"}
+        "tensor_same_decision": tensor_error(t32[live][same], t64[live][same]),
+        "note": "same FP64 state (recovered in FP64), same coloring, only the smoothing pass in FP32; "
+                "tensor errors relative to each tensor's largest component"}
     for prec, (g, _) in gs.items():
         g.close()
     bins = np.concatenate([np.linspace(0, 3, 31), [np.inf]])
@@ -507,13 +544,10 @@ def adjoint_form(args):
 
 
 # ------------------------------------------------------------------ batch
-def batch_arm(args, rank, world, local_rank):
-    """The batched workload: 256 unit-square meshes of sides log-uniform in
-    [32, 512] (2k-520k triangles), shock fields with random (a, b), target 0.8,
-    3 rounds, depth 1; adapted concurrently (one stream per mesh, a pool of
-    host threads), each round one captured CUDA graph per mesh, sharded by size
-    across ranks. Compared with the same concurrency without graphs and with
-    adapting the meshes one at a time with the per-stage calls."""
+def _batch_run(args, rank, world, local_rank, steps, candidates=None):
+    """Adapt the batched workload's meshes of this rank concurrently; returns
+    the rank-0 summary (aggregate triangles/s, per-mesh round times, the same
+    without graphs and one mesh at a time) or None on other ranks."""
     import torch
     from trinity_b200 import api
     from trinity_b200.dist import reduce_stats, shard_meshes
@@ -533,7 +567,7 @@ def batch_arm(args, rank, world, local_rank):
     # launch shapes: one table for the whole batch, chosen by timing the
     # concurrent batch itself (api.batch_autotune: coordinate descent)
     tuned, trials = api.batch_autotune(meshes, p["target"], p["norm"], p["rounds"], p["depth"],
-                                       threads=threads, graph=True)
+                                       threads=threads, graph=True, candidates=candidates)
 
     def run(nthreads, graph):
         for g in meshes:
@@ -550,7 +584,7 @@ def batch_arm(args, rank, world, local_rank):
     l0 = _lib_launches()
     wall, tins, mss = 0.0, 0, []
     with Clocks(torch.cuda.current_device()) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             w, ms, tin = run(threads, True)
             wall += w
             tins += int(tin.sum())
@@ -562,20 +596,20 @@ def batch_arm(args, rank, world, local_rank):
     dist_on = world > 1
     agg = reduce_stats([tins, wall, int(seq_tin.sum()), seq_w, int(ptin.sum()), pw], [0, 2, 4], [1, 3, 5],
                        device="cuda" if dist_on else "cpu")
+    for g in meshes:
+        g.close()
     if rank != 0:
         return None
     conc = np.concatenate(mss)
     return {
-        "metric": "adapted triangles/s per full round (batch of 256 meshes)", "value": round(agg[0] / agg[1], 1),
-        "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(agg[1] / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "256 unit-square meshes, side log-uniform in [32, 512] (seed 5), "
-                               "shock field tanh(a (y - 0.5 - b sin 2 pi x)), a ~ U[10, 100], b ~ U[0, 0.3], "
-                               "target 0.8, L^2, 3 rounds, depth 1, bucket 128, capacity 8x input",
-                   "mode": f"concurrent: one stream per mesh, {threads} host threads, each round one captured "
-                           "CUDA graph per mesh; wall time of metric + rounds",
-                   "meshes_on_rank0": len(meshes)},
+        "value": round(agg[0] / agg[1], 1), "unit": UNIT, "steps": steps,
+        "ms_per_step": round(agg[1] / steps * 1e3, 3),
+        "workload": "256 unit-square meshes, side log-uniform in [32, 512] (seed 5), "
+                    "shock field tanh(a (y - 0.5 - b sin 2 pi x)), a ~ U[10, 100], b ~ U[0, 0.3], "
+                    "target 0.8, L^2, 3 rounds, depth 1, bucket 128, capacity 8x input",
+        "how": f"concurrent: one stream per mesh, {threads} host threads, each round one captured "
+               "CUDA graph per mesh; wall time of metric + rounds",
+        "meshes_on_rank0": len(meshes),
         "gpu_launches": int(launches),
         "launch_shapes": dict(tuned, chosen_by="api.batch_autotune (whole-batch timing, "
                                                 "changes no result)", trials_s=trials),
@@ -588,6 +622,34 @@ def batch_arm(args, rank, world, local_rank):
                               "p99": round(float(np.percentile(conc, 99)), 3)},
         "clocks": clk.summary(),
     }
+
+
+def batch_arm(args, rank, world, local_rank):
+    """The batched workload: 256 unit-square meshes of sides log-uniform in
+    [32, 512] (2k-520k triangles), shock fields with random (a, b), target 0.8,
+    3 rounds, depth 1; adapted concurrently (one stream per mesh, a pool of
+    host threads), each round one captured CUDA graph per mesh, sharded by size
+    across ranks. Compared with the same concurrency without graphs and with
+    adapting the meshes one at a time with the per-stage calls."""
+    r = _batch_run(args, rank, world, local_rank, args.steps)
+    if r is None:
+        return None
+    return {
+        "metric": "adapted triangles/s per full round (batch of 256 meshes)", "value": r["value"],
+        "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "mode": r["how"],
+        "config": {"workload": r["workload"], "meshes_on_rank0": r["meshes_on_rank0"]},
+        "gpu_launches": r["gpu_launches"], "launch_shapes": r["launch_shapes"],
+        "concurrent_without_graphs": r["concurrent_without_graphs"], "one_at_a_time": r["one_at_a_time"],
+        "per_mesh_round_ms": r["per_mesh_round_ms"], "clocks": r["clocks"],
+    }
+
+
+# the batched form inside the default run: a shorter shape search (the
+# smoothing block and the grouped-search lanes, the two that moved the batch
+# most when the full search ran) and two timed batches
+BATCH_FORM_CANDIDATES = {"group_lanes": [8, 16], "smooth_threads": [128, 256]}
 
 
 def _lib_launches():
@@ -627,17 +689,29 @@ def physical_cores():
 
 
 def cpu_baseline():
-    """The reference on the host cores, one full adaptation of the workload."""
+    """The reference on the host cores: the median of three full adaptations
+    of the workload on all physical cores, plus one on a single thread of a
+    400 x 400 sample of the same generator (a full single-thread run takes
+    about a minute)."""
     _, _, c = meshgen.make_config(WORKLOAD)
     if not os.path.exists(REF_BIN):
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                 "sample": "unavailable: oracle/_ref/trinity_ref not built"}
     mp, bp = ensure_files()
     cores = physical_cores()
-    tin, ms, j = reference_once(mp, bp, c, cores)
+    runs = sorted((reference_once(mp, bp, c, cores) for _ in range(3)), key=lambda r: r[0] / r[1])
+    tin, ms, j = runs[1]
+    d = os.path.join(tempfile.gettempdir(), "trinity_b200_bench")
+    smp, sbp, sc = meshgen.write_config(WORKLOAD, d, 400)
+    tin1, ms1, _ = reference_once(smp, sbp, sc, 1)
     return {"value": round(tin / (ms / 1e3), 1), "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"one full adaptation of the workload (metric + 3 rounds; rounds timed: "
-                      f"{ms:.0f} ms, metric {j['metric_ms']:.0f} ms)",
+            "sample": f"median of 3 full adaptations of the workload (metric + 3 rounds; rounds timed: "
+                      f"{ms:.0f} ms, metric {j['metric_ms']:.0f} ms, Mesh::load {j.get('load_ms', 0):.0f} ms)",
+            "runs_triangles_per_s": [round(r[0] / (r[1] / 1e3), 1) for r in runs],
+            "one_thread": {"value": round(tin1 / (ms1 / 1e3), 1), "unit": UNIT, "cores": 1,
+                           "sample": "the same generator at 400 x 400 (320k triangles), 3 rounds"},
+            "build": "g++ -O3 -funroll-loops -march=x86-64-v3 (built where the sources are, run on "
+                     "this host), OpenMP, NDEBUG",
             "final_mesh": {"nodes": j["nodes_out"], "triangles": j["elems_out"]}}
 
 
@@ -646,7 +720,6 @@ def reference_arm(args, rank, world):
         return None
     _, _, c = meshgen.make_config(WORKLOAD)
     _, _, _, cfg = workload_config()
-    cfg["mode"] = "reference OpenMP build, its own heuristics"
     if not os.path.exists(REF_BIN):
         return {"impl": "reference", "unavailable": "oracle/_ref/trinity_ref was not built "
                 "(needs the reference sources at build time)"}
@@ -666,7 +739,8 @@ def reference_arm(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_sum / args.steps, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "mode": "reference OpenMP build, its own heuristics", "config": cfg,
         "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": "full adaptation per step (metric + 3 rounds), rounds timed by "
                                    "the harness around each kernel run"},
@@ -714,6 +788,10 @@ def main():
                 print(json.dumps(line), flush=True)
             return
         line = b200_arm(args, rank, world, local_rank)
+        if not args.no_forms and world == 1:
+            bf = _batch_run(args, rank, world, local_rank, 2, BATCH_FORM_CANDIDATES)
+            if line is not None and bf is not None:
+                line.setdefault("forms", {})["batch"] = bf
         if line is not None:
             if world == 1 and not args.no_cpu_baseline:
                 line["cpu_baseline"] = cpu_baseline()

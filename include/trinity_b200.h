@@ -62,6 +62,19 @@ int trn_mesh_load_arrays(trn_mesh* mesh, int nb_nodes, int nb_elems, const doubl
 int trn_mesh_reload(trn_mesh* mesh);
 /* replaces Mesh::store(path) (mesh.h:66, io.cpp:164-255) */
 int trn_mesh_store(trn_mesh* mesh, const char* path);
+/* the binary form of the mesh (points, tags, triangles; renumbered like
+ * trn_mesh_store), which trn_mesh_load reads in place of the .mesh text: a
+ * sidecar that skips the text parse. No counterpart in the reference (its
+ * loader reads the text, io.cpp:53-161). */
+int trn_mesh_store_binary(trn_mesh* mesh, const char* path);
+/* the files as trn_mesh_load reads them (text with one thread per chunk of
+ * each section, or the binary form), into host arrays: 0-based triangles,
+ * tags 0 / 4 (boundary) / 12 (corner), the .bb values (solut_path may be
+ * NULL). Needs no mesh and no GPU. Always sets the counts; fills the arrays
+ * (any may be NULL) when they hold cap_nodes / cap_elems entries. */
+int trn_read_mesh_files(const char* mesh_path, const char* solut_path, int* nb_nodes, int* nb_elems,
+                        double* points, int* tris, uint8_t* tags, double* solut, int cap_nodes,
+                        int cap_elems);
 /* metric field in medit .sol format (the reference writes none; an addition) */
 int trn_mesh_store_sol(trn_mesh* mesh, const char* path);
 /* copy out the raw state: nb_nodes / nb_elems entries (any pointer may be NULL) */
@@ -80,6 +93,9 @@ int trn_mesh_qualities(trn_mesh* mesh, double* q);
  * quality[0] = min(quality[0], q_min), quality[1] = max(quality[1], q_max),
  * quality[2] = mean over live elements */
 int trn_mesh_quality_stats(trn_mesh* mesh, double quality[3]);
+/* the vertex and element slots the mesh was created with (Mesh::capa,
+ * mesh.h:98-103) */
+int trn_mesh_capacity(trn_mesh* mesh, int* capa_nodes, int* capa_elems);
 /* slot counts (deleted entities included) and live counts */
 int trn_mesh_counts(trn_mesh* mesh, int* nb_nodes, int* nb_elems, int* live_nodes,
                     int* live_elems);
@@ -200,14 +216,40 @@ int trn_set_precision(trn_mesh* mesh, int mode);
 /* free-mode options: seed of the hash priorities; exact_sum = 1 takes the
  * metric complexity sum in element order (bit-compatible with the reference) */
 int trn_set_options(trn_mesh* mesh, uint64_t seed, int exact_sum);
-/* free-mode swap matching: which flip a candidate element prefers.
- * TRN_SWAP_ROW_ORDER (default) ranks its edges by their slot in its dual row,
- * the order in which the reference's greedy matching (matching.cpp:103-135)
- * takes them; TRN_SWAP_GAIN ranks them by the quality their flip gains and
- * makes better meshes than the reference. No counterpart in the reference. */
+/* free-mode swap matching (swapping.cpp:404, Match::computeGreedyMatching,
+ * matching.cpp:81-135).
+ * TRN_SWAP_GREEDY (default): the reference's greedy loop itself (each
+ * candidate takes its free neighbours in row order up to the first one that
+ * is a candidate), over the candidates in the order (id mod 4, id) instead
+ * of increasing id, computed exactly in parallel; the final metric
+ * edge-length histogram stays within half a point per bin of the
+ * reference's.
+ * TRN_SWAP_ROW_ORDER: a round-synchronous handshake whose edges weigh their
+ * slot in the dual row; maximal, so it flips more pairs than the reference.
+ * TRN_SWAP_GAIN: the handshake with edges ranked by the quality their flip
+ * gains, which makes better meshes than the reference. */
 #define TRN_SWAP_ROW_ORDER 0
 #define TRN_SWAP_GAIN 1
+#define TRN_SWAP_GREEDY 2
 int trn_set_swap_match(trn_mesh* mesh, int policy);
+/* most coarsening or swapping levels one call runs while they still change
+ * the mesh (default 100000); past it the call stops with
+ * TRN_ERR_NO_PROGRESS. The reference loops without a bound
+ * (coarsening.cpp:480-503, swapping.cpp:395-425). */
+int trn_set_level_cap(trn_mesh* mesh, int cap);
+
+/* The solver-coupled loop: after some rounds, renumber the adapted mesh as
+ * Mesh::store + Mesh::load would (io.cpp:164-255, io.cpp:53-161; live
+ * vertices and elements in slot order), on the device and without the
+ * 8-decimal rounding of the stored file, keeping boundary and corner tags;
+ * then give the field evaluated on it (one value per vertex of
+ * trn_mesh_export, in that order) and run trn_metric_run again. The
+ * reference recomputes nothing between rounds (main.cpp:50); its adaptive
+ * loop goes through files (README.md:8, scripts/bench_run.py:77-110).
+ * trn_mesh_compact clears the field (set it before the next metric run) and
+ * makes the compacted state the one trn_mesh_reload returns to. */
+int trn_mesh_compact(trn_mesh* mesh);
+int trn_mesh_set_solution(trn_mesh* mesh, const double* solut, int n);
 
 /* last metric complexity (Metrics::field.complexity) */
 double trn_last_complexity(trn_mesh* mesh);
@@ -225,6 +267,13 @@ int trn_profile_enable(int on);
 /* time only the launches of the named kernel (NULL or "" = all): each timed
  * launch adds two events to its stream, which costs throughput */
 int trn_profile_only(const char* name);
+/* kernels that can count their algorithmic bytes on the device (distinct
+ * entries touched, each once per launch) report those instead of the
+ * launcher's figure: for profiled runs, the counting adds atomics; max_nodes
+ * sizes the bitmap of distinct vertices. trn_profile_counted(i): how many of
+ * entry i's launches were counted. */
+int trn_profile_count_bytes(int on, int max_nodes);
+int trn_profile_counted(int i);
 int trn_profile_count(void);
 /* kernels launched by this library since the process started */
 unsigned long long trn_launch_count(void);
@@ -240,11 +289,14 @@ int trn_profile_entry(int i, char* name, int name_len, long long* launches, doub
  * array of about 6 MB that every GPU loading this library holds until exit.
  * Limits: V <= TRN_NOALLOC_MAX_NODES, T <= TRN_NOALLOC_MAX_ELEMS, at most
  * TRN_NOALLOC_BUCKET triangles around a vertex; larger inputs return
- * TRN_ERR_CAPACITY. Same tensors as trn_metric_run on the same mesh. The
- * first call on a device looks up the array's device address, so make it
- * before any stream capture. Calls share the array: calls that overlap on the
- * GPU (other streams or host threads) race; serialise them. Runs on `stream`
- * (a cudaStream_t, NULL = default stream) and returns when done. */
+ * TRN_ERR_CAPACITY. The tensors are those of trn_metric_run on the same mesh
+ * with the complexity summed by its fixed-shape tree (the default; a mesh
+ * set to exact_sum or replay sums in element order instead, which can differ
+ * in the last bits). The first call on a device looks up the array's device
+ * address, so make it before any stream capture. Calls share the array:
+ * calls that overlap on the GPU (other streams or host threads) race;
+ * serialise them. Runs on `stream` (a cudaStream_t of the current device,
+ * NULL = default stream) and returns when done. */
 #define TRN_NOALLOC_MAX_NODES 16384
 #define TRN_NOALLOC_MAX_ELEMS 32768
 #define TRN_NOALLOC_BUCKET 32

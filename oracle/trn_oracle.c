@@ -1179,6 +1179,42 @@ static void match_sequential_rows(orc_mesh* m, int nt) {
   }
 }
 
+/* the GPU free mode's default rule: the same loop (without the degree-1
+ * stack), over the rows in the order (candidate id mod 4, candidate id) */
+static int interleaved_before(const orc_mesh* m, int i, int j) {
+  const int a = m->dual[(size_t) i * 4], b = m->dual[(size_t) j * 4];
+  if ((a & 3) != (b & 3)) return (a & 3) < (b & 3);
+  return a < b;
+}
+
+static void match_interleaved_rows(orc_mesh* m, int nt) {
+  int* order = (int*) malloc(sizeof(int) * (size_t) (nt > 0 ? nt : 1));
+  int k = 0;
+  for (int cls = 0; cls < 4; ++cls)
+    for (int i = 0; i < nt; ++i)
+      if ((D(m, i)[0] & 3) == cls) order[k++] = i;
+  /* within a class the rows are in list order, i.e. increasing candidate id;
+   * check it rather than assume it */
+  for (int a = 1; a < k; ++a)
+    if (!interleaved_before(m, order[a - 1], order[a])) m->err = ORC_ERR_INVALID;
+  for (int a = 0; a < k; ++a) {
+    const int i = order[a];
+    const int c = D(m, i)[0];
+    if (m->visited[c]) continue;
+    m->visited[c] = 1;
+    for (int q = 1; q < m->dual_n[i]; ++q) {
+      const int n = D(m, i)[q];
+      if (m->visited[n]) continue;
+      m->visited[n] = 1;
+      m->matched[c] = n;
+      m->matched[n] = MATCHED;
+      if (m->map[n] < 0) continue;
+      break;
+    }
+  }
+  free(order);
+}
+
 static uint64_t hs_mix(uint64_t x) {
   x ^= x >> 30;
   x *= 0xbf58476d1ce4e5b9ULL;
@@ -1267,7 +1303,7 @@ static void match_handshake_emul(orc_mesh* m, int nt, int level) {
 }
 
 int orc_set_swap_rule(orc_mesh* m, int rule) {
-  if (rule < ORC_SWAP_REFERENCE || rule > ORC_SWAP_HANDSHAKE_ROWSLOT) return ORC_ERR_INVALID;
+  if (rule < ORC_SWAP_REFERENCE || rule > ORC_SWAP_GREEDY_INTERLEAVED) return ORC_ERR_INVALID;
   m->swap_rule = rule;
   return ORC_OK;
 }
@@ -1397,6 +1433,8 @@ int orc_swap(orc_mesh* m) {
       for (int i = 0; i < list.n; ++i) match_and_update(m, i, &stack);
     else if (m->swap_rule == ORC_SWAP_SEQUENTIAL_ROWS)
       match_sequential_rows(m, list.n);
+    else if (m->swap_rule == ORC_SWAP_GREEDY_INTERLEAVED)
+      match_interleaved_rows(m, list.n);
     else
       match_handshake_emul(m, list.n, levels);
     /* processFlips, swapping.cpp:251-269 (pairs are disjoint: order-free) */

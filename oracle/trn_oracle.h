@@ -67,13 +67,15 @@ void orc_counters(const orc_mesh* m, int out[4]);
 /* Swap matching rule, for the analysis of the GPU free mode only:
  * ORC_SWAP_REFERENCE (default) is the reference's greedy with its degree-1
  * stack (matching.cpp:81-135); the others are emulations: the same loop
- * without the stack, and the GPU's round-synchronous handshake with random
- * or row-slot edge weights. */
+ * without the stack, the GPU's round-synchronous handshake with random
+ * or row-slot edge weights, and the GPU free mode's default, the loop
+ * without the stack over the rows in the order (id mod 4, id). */
 enum {
   ORC_SWAP_REFERENCE = 0,
   ORC_SWAP_SEQUENTIAL_ROWS = 1,
   ORC_SWAP_HANDSHAKE_RANDOM = 2,
   ORC_SWAP_HANDSHAKE_ROWSLOT = 3,
+  ORC_SWAP_GREEDY_INTERLEAVED = 4,
 };
 int orc_set_swap_rule(orc_mesh* m, int rule);
 

@@ -139,7 +139,7 @@ def read_snapshot(path: str) -> State:
 class Oracle:
     """One mesh in the C oracle; mirrors the reference's kernel calls."""
 
-    def __init__(self, mesh, solut, capa_scale: int = 9, bucket: int = 64):
+    def __init__(self, mesh, solut, capa_scale: int = 9, bucket: int = 64, tags=None):
         L = lib()
         self.L = L
         self.h = L.orc_create(mesh.nb_nodes * capa_scale, mesh.nb_elems * capa_scale, bucket)
@@ -147,7 +147,7 @@ class Oracle:
             raise MemoryError("oracle allocation failed")
         pts = np.ascontiguousarray(mesh.points, dtype=np.float64)
         tris = np.ascontiguousarray(mesh.tris, dtype=np.int32)
-        tags = tags_of(mesh)
+        tags = tags_of(mesh) if tags is None else np.ascontiguousarray(tags, dtype=np.uint8)
         u = np.ascontiguousarray(solut, dtype=np.float64)
         rc = L.orc_load(self.h, mesh.nb_nodes, mesh.nb_elems, _p(pts), _p(tris), _p(tags), _p(u))
         if rc:
@@ -193,7 +193,8 @@ class Oracle:
         self.L.orc_export(self.h, _p(pts), _p(ten), _p(el), _p(alive), _p(tags))
         return State(pts, ten, el, alive, tags)
 
-    SWAP_RULES = {"reference": 0, "sequential_rows": 1, "handshake_random": 2, "handshake_rowslot": 3}
+    SWAP_RULES = {"reference": 0, "sequential_rows": 1, "handshake_random": 2, "handshake_rowslot": 3,
+                  "greedy_interleaved": 4}
 
     def set_swap_rule(self, rule: str) -> None:
         """Swap matching rule (analysis of the GPU free mode; "reference" is
@@ -245,3 +246,14 @@ def digest(st: State) -> dict:
         a = np.ascontiguousarray(getattr(st, name))
         out[name] = hashlib.sha256(a.tobytes()).hexdigest()
     return out
+
+
+def compact_state(st: State):
+    """Mesh::store's renumbering (io.cpp:164-255) at full precision: the live
+    vertices in slot order (points, tags) and the live elements in slot
+    order, renumbered; returns (points, tris, tags)."""
+    keep = np.flatnonzero(st.alive)
+    newid = -np.ones(st.nb_nodes, np.int64)
+    newid[keep] = np.arange(keep.shape[0])
+    tri = st.active_elems()
+    return st.points[keep].copy(), newid[tri].astype(np.int32), st.tags[keep].copy()

@@ -64,6 +64,13 @@ def lib():
         L.trn_set_replay.argtypes = [pmesh, vp, sz]
         L.trn_set_options.argtypes = [pmesh, ctypes.c_uint64, ip]
         L.trn_set_swap_match.argtypes = [pmesh, ip]
+        L.trn_set_level_cap.argtypes = [pmesh, ip]
+        L.trn_mesh_compact.argtypes = [pmesh]
+        L.trn_mesh_capacity.argtypes = [pmesh, ctypes.POINTER(ip), ctypes.POINTER(ip)]
+        L.trn_mesh_store_binary.argtypes = [pmesh, ctypes.c_char_p]
+        L.trn_read_mesh_files.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ip),
+                                          ctypes.POINTER(ip), vp, vp, vp, vp, ip, ip]
+        L.trn_mesh_set_solution.argtypes = [pmesh, vp, ip]
         L.trn_last_complexity.argtypes = [pmesh]
         L.trn_last_complexity.restype = dp
         L.trn_last_time_ms.argtypes = [pmesh]
@@ -90,6 +97,8 @@ def lib():
                                         ctypes.POINTER(dp), ctypes.POINTER(dp)]
         L.trn_launch_count.restype = ctypes.c_ulonglong
         L.trn_profile_only.argtypes = [ctypes.c_char_p]
+        L.trn_profile_count_bytes.argtypes = [ip, ip]
+        L.trn_profile_counted.argtypes = [ip]
         L.trn_quality_adjoint.argtypes = [pmesh, vp, vp, dp, ip, dp, dp, ip, ctypes.POINTER(dp), vp, vp]
         L.trn_smooth_gradient_run.argtypes = [pmesh, ip, ip, dp, ip, sp]
         _lib = L
@@ -122,8 +131,16 @@ def profile_read() -> list[dict]:
         by = ctypes.c_double()
         L.trn_profile_entry(i, name, 64, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(by))
         out.append({"kernel": name.value.decode(), "launches": n.value, "ms": ms.value,
-                    "bytes": by.value})
+                    "bytes": by.value, "bytes_counted": L.trn_profile_counted(i) == n.value > 0})
     return out
+
+
+def profile_count_bytes(on: bool, max_nodes: int = 0) -> None:
+    """Kernels that can count their algorithmic bytes on the device do so
+    (profiled runs: the counting adds atomics)."""
+    rc = lib().trn_profile_count_bytes(1 if on else 0, int(max_nodes))
+    if rc:
+        raise TrinityError(rc, "byte counters: device allocation failed")
 
 
 def launch_count() -> int:

@@ -24,7 +24,7 @@ import numpy as np
 from ._lib import Stats, TrinityError, lib
 
 __all__ = ["Mesh", "Metrics", "Partit", "Refine", "Coarse", "Swap", "Smooth", "Stats",
-           "TrinityError", "EPSILON", "H_MAX", "find", "batch_adapt"]
+           "TrinityError", "EPSILON", "H_MAX", "find", "batch_adapt", "adaptive_loop", "read_mesh_files"]
 
 EPSILON = 1.0e-9   # header.h:50, the h_min the CLI passes (parser.cpp:95)
 H_MAX = 0.4        # parser.cpp:96
@@ -96,8 +96,24 @@ class Mesh:
         """Back to the state right after the last load (device-side copy)."""
         self._check(self._L.trn_mesh_reload(self.h))
 
+    def compact(self) -> None:
+        """Renumber the adapted mesh on the device as a store + load would
+        (live vertices and elements in slot order, full precision, boundary
+        and corner tags kept); clears the nodal field."""
+        self._check(self._L.trn_mesh_compact(self.h))
+
+    def set_solution(self, solut) -> None:
+        """The nodal field for the next metric run: one value per vertex slot
+        in use (the rows of ``export()``)."""
+        u = np.ascontiguousarray(solut, dtype=np.float64)
+        self._check(self._L.trn_mesh_set_solution(self.h, _p(u), int(u.shape[0])))
+
     def store(self, path: str) -> None:
         self._check(self._L.trn_mesh_store(self.h, path.encode()))
+
+    def store_binary(self, path: str) -> None:
+        """The mesh in the binary form ``load`` also reads (no text parse)."""
+        self._check(self._L.trn_mesh_store_binary(self.h, path.encode()))
 
     def store_sol(self, path: str) -> None:
         self._check(self._L.trn_mesh_store_sol(self.h, path.encode()))
@@ -106,6 +122,12 @@ class Mesh:
         v = [ctypes.c_int() for _ in range(4)]
         self._check(self._L.trn_mesh_counts(self.h, *[ctypes.byref(x) for x in v]))
         return tuple(x.value for x in v)
+
+    def capacity(self):
+        """(vertex slots, element slots) the mesh was created with."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._check(self._L.trn_mesh_capacity(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def export(self):
         """(points[V,2], tensor[V,3], tris[T,3], alive[V], tags[V]) of all slots in use."""
@@ -159,14 +181,21 @@ class Mesh:
     def set_options(self, seed: int = 0x7472696E697479, exact_sum: bool = False) -> None:
         self._check(self._L.trn_set_options(self.h, seed, 1 if exact_sum else 0))
 
-    SWAP_MATCH = {"row_order": 0, "gain": 1}
+    SWAP_MATCH = {"row_order": 0, "gain": 1, "greedy": 2}
 
-    def set_swap_match(self, policy: str = "row_order") -> None:
-        """Free-mode swap matching: "row_order" (the reference's preference,
-        the default) or "gain" (each candidate prefers its best flip)."""
+    def set_swap_match(self, policy: str = "greedy") -> None:
+        """Free-mode swap matching: "greedy" (the reference's greedy loop over
+        the candidates in the order (id mod 4, id), computed exactly in
+        parallel; the default), "row_order" (a handshake preferring the
+        reference's row slots) or "gain" (each candidate prefers its best
+        flip)."""
         if policy not in self.SWAP_MATCH:
             raise ValueError(f"swap matching policy {policy!r}: one of {sorted(self.SWAP_MATCH)}")
         self._check(self._L.trn_set_swap_match(self.h, self.SWAP_MATCH[policy]))
+
+    def set_level_cap(self, cap: int) -> None:
+        """Most coarsening / swapping levels a call runs (TRN_ERR_NO_PROGRESS past it)."""
+        self._check(self._L.trn_set_level_cap(self.h, cap))
 
     def last_time_ms(self) -> float:
         return self._L.trn_last_time_ms(self.h)
@@ -375,3 +404,47 @@ class Smooth:
         m = self.mesh
         m._check(m._L.trn_smooth_run(m.h, self.algo.max_part, self.level,
                                      ctypes.byref(total) if total is not None else None))
+
+
+def read_mesh_files(mesh_path: str, solut_path: str | None = None):
+    """The .mesh (text or binary) and .bb files as ``Mesh.load`` reads them,
+    on the host: (points[V,2], tris[T,3] 0-based, tags[V], solut[V] or None)."""
+    L = lib()
+    nv, nt = ctypes.c_int(), ctypes.c_int()
+    sp = solut_path.encode() if solut_path else None
+    rc = L.trn_read_mesh_files(mesh_path.encode(), sp, ctypes.byref(nv), ctypes.byref(nt),
+                               None, None, None, None, 0, 0)
+    if rc:
+        raise TrinityError(rc, f"cannot read {mesh_path}")
+    pts = np.zeros((nv.value, 2)); tri = np.zeros((nt.value, 3), np.int32)
+    tags = np.zeros(nv.value, np.uint8)
+    u = np.zeros(nv.value) if solut_path else None
+    rc = L.trn_read_mesh_files(mesh_path.encode(), sp, ctypes.byref(nv), ctypes.byref(nt), _p(pts), _p(tri),
+                               _p(tags), _p(u) if u is not None else None, nv.value, nt.value)
+    if rc:
+        raise TrinityError(rc, f"cannot read {mesh_path} / {solut_path}")
+    return pts, tri, tags, u
+
+
+def adaptive_loop(mesh: Mesh, field, cycles: int, target: float, norm: int = 2, depth: int = 1,
+                  rounds: int = 3, max_part: int = 8, on_cycle=None):
+    """The solver-coupled loop trinity is written for (README.md:8; the
+    reference's scripts/bench_run.py:77-110 runs it through files): for each
+    cycle, evaluate ``field(points) -> values`` on the current mesh, recover
+    the metric, run ``rounds`` rounds of refine / coarsen / swap / smooth,
+    then renumber the adapted mesh on the device for the next cycle. The
+    first cycle uses the mesh as loaded. ``on_cycle(k, mesh)`` is called
+    after each cycle's rounds, before the renumbering."""
+    heur = Partit(mesh, max_part)
+    kern = (Refine(mesh, depth), Coarse(mesh, heur), Swap(mesh), Smooth(mesh, heur, depth))
+    for k in range(cycles):
+        if k > 0:
+            mesh.compact()
+        pts = mesh.export()[0]
+        mesh.set_solution(field(pts))
+        Metrics(mesh, target, norm).run()
+        for _ in range(rounds):
+            for kk in kern:
+                kk.run()
+        if on_cycle is not None:
+            on_cycle(k, mesh)

@@ -30,6 +30,7 @@
  */
 #include "trn_internal.h"
 
+#include <algorithm>
 #include <cstdio>
 
 namespace trn {
@@ -340,6 +341,239 @@ void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* d
   check_launch("match_handshake");
 }
 
+/* ---------------- greedy matching in interleaved element order ----------------
+ *
+ * The reference's matching (Match::computeGreedyMatching / matchAndUpdate,
+ * matching.cpp:81-135) is a loop over the dual rows in list order, i.e. in
+ * increasing candidate id: a row whose candidate is still free marks it
+ * taken, then takes its free neighbours in slot order, going past each
+ * neighbour that is not itself a candidate (the "continue" of
+ * matching.cpp:124) and stopping at the first one that is; the candidate's
+ * partner is the last neighbour taken. This is that loop without the
+ * degree-1 stack, over the rows in the order (id mod 4, id): four
+ * interleaved sweeps of the candidate ids.
+ *
+ * Its result is computed exactly, in parallel, as the greedy matching of an
+ * order is: in each round a row decides once it comes first, under that
+ * order, among the undecided rows that list any of its elements; such rows
+ * share no element with one another, so they decide independently, and what
+ * each finds is what the sequential loop would have found. Rows propose
+ * their key with a 64-bit atomicMin on every element of their row into the
+ * round's buffer (keys of later rounds compare lower, so no buffer needs
+ * clearing between rounds); a row is ready when every element holds its own
+ * key. A round decides the ready rows and lets the others propose for the
+ * next round into the other buffer, so one launch per round. The rounds
+ * run over a compacted list of the undecided rows; once that list is short
+ * one block finishes the remaining rounds with block barriers. After
+ * kGreedyRounds rounds any row still undecided stays unmatched (a valid, if
+ * not maximal, matching). On the 2M-triangle workload the deepest level
+ * needs 48 rounds, the mean is 12.
+ *
+ * The four-way interleave keeps the chains of dependent rows short (a plain
+ * increasing-id sweep has chains as long as a row of the grid), and the
+ * final meshes' metric edge-length histograms stay within half a point per
+ * bin of the reference's, where a maximal handshake matching, which flips
+ * more pairs, is a point and a half off. */
+constexpr int kGreedyRounds = 64;
+constexpr int kGreedyTail = 2048;   /* undecided rows left to the one-block rounds */
+
+struct GreedyArgs {
+  const int* dual;
+  const int* dual_n;
+  const int* map;
+  int* vis;                 /* per element: -1 free, else taken */
+  unsigned long long* mk0;  /* per element: lowest key proposed, even rounds */
+  unsigned long long* mk1;  /* odd rounds */
+  int* list0;               /* undecided rows, even rounds */
+  int* list1;
+  int* cnt;                 /* [3] list lengths, by round mod 3 */
+  int* ran;                 /* [kGreedyRounds] round r ran on the grid */
+};
+
+__device__ __forceinline__ unsigned long long greedy_key(int r, int c) {
+  return ((unsigned long long) (kGreedyRounds - r) << 40) | ((unsigned long long) (c & 3) << 32) |
+         (uint32_t) c;
+}
+
+/* "is a candidate" as matching.cpp:124 asks it: the element has a row in the
+ * map, which keeps the rows of earlier levels of the same call (it is reset
+ * once per call, swapping.cpp:161-162) */
+__device__ __forceinline__ bool greedy_is_row(const GreedyArgs& a, int ntasks, int e) {
+  (void) ntasks;
+  return a.map[e] >= 0;
+}
+
+__device__ __forceinline__ void greedy_reset_item(const GreedyArgs& a, int i) {
+  for (int q = 0; q < a.dual_n[i]; ++q) {
+    const int e = a.dual[i * 4 + q];
+    a.vis[e] = -1;
+    a.mk0[e] = ~0ULL;
+    a.mk1[e] = ~0ULL;
+  }
+}
+
+__device__ __forceinline__ void greedy_propose(const GreedyArgs& a, int r, int i) {
+  unsigned long long* mk = (r & 1) ? a.mk1 : a.mk0;
+  const unsigned long long key = greedy_key(r, a.dual[i * 4]);
+  for (int q = 0; q < a.dual_n[i]; ++q) atomicMin(mk + a.dual[i * 4 + q], key);
+}
+
+/* row i in round r: decide it when it is first on all its elements (and
+ * return false), else propose it for round r + 1 (and return true) */
+__device__ __forceinline__ bool greedy_item(const GreedyArgs& a, int ntasks, int r, int i, int* pairs,
+                                            int* npairs) {
+  const unsigned long long* mk = (r & 1) ? a.mk1 : a.mk0;
+  const int c = a.dual[i * 4];
+  const int dn = a.dual_n[i];
+  const unsigned long long key = greedy_key(r, c);
+  bool ready = true;
+  for (int q = 0; q < dn; ++q) ready &= (mk[a.dual[i * 4 + q]] == key);
+  if (!ready) {
+    greedy_propose(a, r + 1, i);
+    return true;
+  }
+  if (a.vis[c] != -1) return false;
+  a.vis[c] = 1;
+  int partner = -1;
+  for (int q = 1; q < dn; ++q) {
+    const int n = a.dual[i * 4 + q];
+    if (a.vis[n] != -1) continue;
+    a.vis[n] = 1;
+    partner = n;
+    if (greedy_is_row(a, ntasks, n)) break;
+  }
+  if (partner >= 0) {
+    const int p = atomicAdd(npairs, 1);
+    pairs[2 * p] = c;
+    pairs[2 * p + 1] = partner;
+  }
+  return false;
+}
+
+__global__ void k_greedy_reset(GreedyArgs a, const int* ntasks_dev, int min_n) {
+  const int ntasks = *ntasks_dev;
+  if (ntasks < min_n) return;
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) greedy_reset_item(a, i);
+}
+
+/* round 0's proposals; every row starts undecided */
+__global__ void k_greedy_start(GreedyArgs a, const int* ntasks_dev, int min_n) {
+  const int ntasks = *ntasks_dev;
+  if (ntasks < min_n) return;
+  if (trn_tid() == 0) a.cnt[0] = ntasks;
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
+    greedy_propose(a, 0, i);
+    a.list0[i] = i;
+  }
+}
+
+/* round r on the grid, while more than kGreedyTail rows are undecided and
+ * every earlier round ran here */
+__global__ void k_greedy_round(GreedyArgs a, const int* ntasks_dev, int r, int* pairs, int* npairs) {
+  if (r > 0 && !a.ran[r - 1]) return;
+  const int n = a.cnt[r % 3];
+  if (n <= kGreedyTail) return;
+  const int ntasks = *ntasks_dev;
+  const int* in = (r & 1) ? a.list1 : a.list0;
+  int* out = (r & 1) ? a.list0 : a.list1;
+  if (trn_tid() == 0) {
+    a.ran[r] = 1;
+    a.cnt[(r + 2) % 3] = 0;   /* round r + 1's output */
+  }
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int i = in[q];
+    if (greedy_item(a, ntasks, r, i, pairs, npairs)) trn_append(out, a.cnt + (r + 1) % 3, i);
+  }
+}
+
+/* the remaining rounds in one block; with `whole`, the level's reset and
+ * first proposals too (a list the host knows to be short) */
+__global__ void __launch_bounds__(kFusedThreads) k_greedy_tail(GreedyArgs a, const int* ntasks_dev,
+                                                               int* pairs, int* npairs, int whole,
+                                                               int lim) {
+  const int ntasks = *ntasks_dev;
+  if (whole ? ntasks > lim : ntasks < lim) return;
+  __shared__ int s_r;
+  if (whole) {
+    if (threadIdx.x == 0) *npairs = 0;
+    for (int i = threadIdx.x; i < ntasks; i += blockDim.x) greedy_reset_item(a, i);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ntasks; i += blockDim.x) {
+      greedy_propose(a, 0, i);
+      a.list0[i] = i;
+    }
+    if (threadIdx.x == 0) {
+      a.cnt[0] = ntasks;
+      a.cnt[1] = 0;
+      s_r = 0;
+    }
+  } else if (threadIdx.x == 0) {
+    int r = 0;
+    while (r < kGreedyRounds && a.ran[r]) ++r;
+    s_r = r;
+  }
+  __syncthreads();
+  for (int r = s_r; r < kGreedyRounds; ++r) {
+    const int n = a.cnt[r % 3];
+    if (n == 0) break;
+    const int* in = (r & 1) ? a.list1 : a.list0;
+    int* out = (r & 1) ? a.list0 : a.list1;
+    if (threadIdx.x == 0) a.cnt[(r + 2) % 3] = 0;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+      const int i = in[q];
+      if (greedy_item(a, ntasks, r, i, pairs, npairs)) {
+        const int k = atomicAdd(a.cnt + (r + 1) % 3, 1);
+        out[k] = i;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual_n, const int* ntasks,
+                  const int* map, HeurWs& ws, int* pairs, int* npairs, cudaStream_t s, long long bound) {
+  (void) m;
+  ProfScope ps("match_greedy", s, 0.0);
+  const GreedyArgs a{dual, dual_n, map, ws.mate, ws.prop, ws.prop2, ws.choice, ws.choice2, ws.cnt,
+                     ws.cnt + 8};
+  if (bound >= 0 && bound <= kFusedThreads) {   /* known short: one block */
+    k_greedy_tail<<<1, kFusedThreads, 0, s>>>(a, ntasks, pairs, npairs, 1, kFusedThreads);
+    note_launch();
+    check_launch("match_greedy");
+    return;
+  }
+  /* grid rounds for a list the host knows, or may, be long: about two
+   * rounds per halving of the list down to kGreedyTail rows (measured on
+   * the 2M-triangle workload), at most kGreedyRounds - 8 */
+  int rounds = kGreedyRounds - 8;
+  if (bound >= 0) {
+    rounds = 4;
+    for (long long n = bound; n > kGreedyTail; n /= 2) rounds += 2;
+    rounds = std::min(rounds, kGreedyRounds - 8);
+  }
+  const int g = grid_bounded(bound, nb_elems);
+  const int min_n = bound < 0 ? kFusedThreads + 1 : 0;
+  cudaMemsetAsync(npairs, 0, sizeof(int), s);
+  cudaMemsetAsync(ws.cnt, 0, sizeof(int) * (8 + kGreedyRounds), s);
+  k_greedy_reset<<<g, TRN_THREADS, 0, s>>>(a, ntasks, min_n);
+  note_launch();
+  k_greedy_start<<<g, TRN_THREADS, 0, s>>>(a, ntasks, min_n);
+  note_launch();
+  for (int r = 0; r < rounds; ++r) {
+    k_greedy_round<<<g, TRN_THREADS, 0, s>>>(a, ntasks, r, pairs, npairs);
+    note_launch();
+  }
+  /* the rounds left; when the list is unknown, the whole short-list form
+   * too, each returning at once when the count is not its case */
+  k_greedy_tail<<<1, kFusedThreads, 0, s>>>(a, ntasks, pairs, npairs, 0, min_n);
+  note_launch();
+  if (bound < 0) {
+    k_greedy_tail<<<1, kFusedThreads, 0, s>>>(a, ntasks, pairs, npairs, 1, kFusedThreads);
+    note_launch();
+  }
+  check_launch("match_greedy");
+}
+
 /* ---------------- coloring ---------------- */
 /* color word: 0 = uncolored, else (round + 1) << 8 | color, color 0xff =
  * none. Vertices that take no part get kNotColored: to their neighbours a
@@ -552,6 +786,8 @@ void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {
   cudaMemset(ws->state2, 0, big);
   cudaMalloc(&ws->prop, sizeof(unsigned long long) * (size_t) capa_elem);
   cudaMalloc(&ws->choice, sizeof(int) * (size_t) capa_elem);
+  cudaMalloc(&ws->choice2, sizeof(int) * (size_t) capa_elem);
+  cudaMalloc(&ws->prop2, sizeof(unsigned long long) * (size_t) capa_elem);
   cudaMalloc(&ws->color, sizeof(int) * (size_t) capa_node);
   cudaMemset(ws->color, 0, sizeof(int) * (size_t) capa_node);
   cudaMalloc(&ws->mate, sizeof(int) * (size_t) capa_elem);
@@ -568,6 +804,8 @@ void heur_ws_free(HeurWs* ws) {
   cudaFree(ws->state2);
   cudaFree(ws->prop);
   cudaFree(ws->choice);
+  cudaFree(ws->choice2);
+  cudaFree(ws->prop2);
   cudaFree(ws->color);
   cudaFree(ws->mate);
   cudaFree(ws->rank);

@@ -12,13 +12,14 @@
  *                     deterministic two-level tree
  *   k_normalize       global scale target/complexity and eigenvalue clamp to
  *                     [1/h_max^2, 1/h_min^2] (metric.cpp:188-238)
+ *   k_*_f32           the same recovery in FP32 for the mixed-precision form
  *
  * Patch order matters: the reference sums over the patch in ascending element
  * id (std::set order, mesh.cpp:396-432), so each thread gathers the stencils
  * of the vertex and of its neighbours, sorts and deduplicates them first.
  */
 #include "trn_internal.h"
-#include "trn_numeric.cuh"
+#include "trn_mixed.cuh"
 
 namespace trn {
 
@@ -126,6 +127,89 @@ __global__ void k_hessian_local(DMesh m, int nb_nodes, const double2* __restrict
   }
 }
 
+/* ---- the mixed-precision form of the recovery ----
+ * The same patch means in FP32. Every coordinate difference is taken in
+ * FP64 and then rounded; each nodal value enters as its difference to the
+ * patch centre's value (the element's three P1 basis gradients sum to zero,
+ * so this changes nothing in exact arithmetic and removes the cancellation
+ * of summing values of nearly equal size, which single precision could not
+ * afford); area x basis gradient is formed directly from the rotated edges
+ * (area x 2/area x edge), so no division per element. The eigen-clamp, the
+ * local L^p scale and the global scaling are FP32 too; the complexity sum
+ * stays FP64. */
+__device__ __forceinline__ void elem_edges_f32(const DMesh& m, int4 t, float* area, float* ey, float* ex) {
+  const double2 p0 = m.pts[t.x], p1 = m.pts[t.y], p2 = m.pts[t.z];
+  /* rotated edges: area x d[2j] = 2 ey[j], area x d[2j+1] = 2 ex[j] */
+  ey[0] = (float) (p1.y - p2.y);
+  ex[0] = (float) (p2.x - p1.x);
+  ey[1] = (float) (p2.y - p0.y);
+  ex[1] = (float) (p0.x - p2.x);
+  ey[2] = (float) (p0.y - p1.y);
+  ex[2] = (float) (p1.x - p0.x);
+  const float c0 = (float) (p1.x - p0.x), c1 = (float) (p2.x - p0.x);
+  const float c2 = (float) (p1.y - p0.y), c3 = (float) (p2.y - p0.y);
+  *area = 0.5f * (c0 * c3 - c1 * c2);
+}
+
+__global__ void k_gradient_f32(DMesh m, int nb_nodes, const double* __restrict__ solut,
+                               double2* __restrict__ grad) {
+  if (trn_failed(m)) return;
+  int patch[TRN_MAX_PATCH];
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    const int n = gather_patch(m, v, patch);
+    const double uv = solut[v];
+    float tot = 0.f, gx = 0.f, gy = 0.f;
+    for (int i = 0; i < n; ++i) {
+      const int4 t = m.tri[patch[i]];
+      float area, ey[3], ex[3];
+      elem_edges_f32(m, t, &area, ey, ex);
+      const float s[3] = {(float) (solut[t.x] - uv), (float) (solut[t.y] - uv), (float) (solut[t.z] - uv)};
+      tot += area;
+      gx += 2.f * (s[0] * ey[0] + s[1] * ey[1] + s[2] * ey[2]);
+      gy += 2.f * (s[0] * ex[0] + s[1] * ex[1] + s[2] * ex[2]);
+    }
+    const float it = __frcp_rn(tot);
+    grad[v] = make_double2((double) (gx * it), (double) (gy * it));
+  }
+}
+
+__global__ void k_hessian_local_f32(DMesh m, int nb_nodes, const double2* __restrict__ grad, float scale_exp) {
+  if (trn_failed(m)) return;
+  int patch[TRN_MAX_PATCH];
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    const int n = gather_patch(m, v, patch);
+    const double2 gv = grad[v];
+    float tot = 0.f, h[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int i = 0; i < n; ++i) {
+      const int4 t = m.tri[patch[i]];
+      float area, ey[3], ex[3];
+      elem_edges_f32(m, t, &area, ey, ex);
+      const int id[3] = {t.x, t.y, t.z};
+      tot += area;
+      for (int j = 0; j < 3; ++j) {
+        const double2 g = grad[id[j]];
+        const float dx = (float) (g.x - gv.x), dy = (float) (g.y - gv.y);
+        h[0] += 2.f * (dx * ey[j]);
+        h[1] += 2.f * (dx * ex[j]);
+        h[2] += 2.f * (dy * ey[j]);
+        h[3] += 2.f * (dy * ex[j]);
+      }
+    }
+    const float it = __frcp_rn(tot);
+    const float t0 = h[0] * it, t1 = 0.5f * (h[1] + h[2]) * it, t2 = h[3] * it;
+    float mm[4] = {t0, t1, t1, t2}, val[2], vec[4];
+    trnf_eigen(mm, val, vec);
+    val[0] = trnf_max(fabsf(val[0]), 1.e-9f);
+    val[1] = trnf_max(fabsf(val[1]), 1.e-9f);
+    const float scale_loc = powf(val[0] * val[1], scale_exp);
+    val[0] *= scale_loc;
+    val[1] *= scale_loc;
+    const float c0 = val[0] * vec[0], c1 = val[0] * vec[2], c2 = val[1] * vec[1], c3 = val[1] * vec[3];
+    m.ten[v] = make_double4((double) (vec[0] * c0 + vec[1] * c2), (double) (vec[0] * c1 + vec[1] * c3),
+                            (double) (vec[2] * c1 + vec[3] * c3), 0.0);
+  }
+}
+
 __global__ void k_complexity_term(DMesh m, int nb_elems, double* __restrict__ terms) {
   if (trn_failed(m)) return;
   for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
@@ -215,6 +299,24 @@ __global__ void k_normalize(DMesh m, int nb_nodes, const double* complexity, dou
   }
 }
 
+__global__ void k_normalize_f32(DMesh m, int nb_nodes, const double* complexity, double target,
+                                double eig_min, double eig_max) {
+  if (trn_failed(m)) return;
+  const float fact = (float) (target / *complexity);
+  const float lo = (float) eig_max, hi = (float) eig_min;
+  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
+    const double4 t = m.ten[v];
+    float mm[4] = {(float) t.x, (float) t.y, (float) t.y, (float) t.z}, val[2], vec[4];
+    trnf_eigen(mm, val, vec);
+    for (int j = 0; j < 2; ++j) val[j] = trnf_max(trnf_min(val[j] * fact, hi), lo);
+    const float c0 = val[0] * vec[0], c1 = val[0] * vec[2], c2 = val[1] * vec[1], c3 = val[1] * vec[3];
+    const float r0 = vec[0] * c0 + vec[1] * c2, r1 = vec[0] * c1 + vec[1] * c3, r2 = vec[2] * c1 + vec[3] * c3;
+    m.ten[v] = make_double4((double) r0, (double) r1, (double) r2, 0.0);
+    if (m.tenf) m.tenf[v] = make_float4(r0, r1, r2, 0.f);
+    if (m.lten) reinterpret_cast<float4*>(m.lten)[v] = trnf_log_tensor(r0, r1, r2);
+  }
+}
+
 void sum_tree(const double* in, int n, double* partial, double* out, cudaStream_t s) {
   const int nb = grid_for(n);
   k_sum_partial<<<nb, TRN_THREADS, 0, s>>>(in, n, partial);
@@ -225,7 +327,35 @@ void sum_tree(const double* in, int n, double* partial, double* out, cudaStream_
 
 void metric_run(const DMesh& m, int nb_nodes, int nb_elems, const double* solut, double2* grad,
                 double* terms, double* complexity, bool exact_sum, const MetricParams& p,
-                cudaStream_t s, const MetricSaves* keep) {
+                cudaStream_t s, const MetricSaves* keep, bool fp32) {
+  if (fp32) {
+    const double V = nb_nodes, E = nb_elems;
+    {
+    ProfScope ps("metric_gradient", s, V * (2 * kIdx + kAvgDeg * kIdx * 2 + 8 + kPt + 16) + E * kTri);
+    k_gradient_f32<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, solut, grad);
+    note_launch();
+    }
+    {
+    ProfScope ps("metric_hessian", s, V * (2 * kIdx + kAvgDeg * kIdx * 2 + 16 + kPt + kTen) + E * kTri);
+    k_hessian_local_f32<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, grad, (float) p.scale_exp);
+    note_launch();
+    }
+    ProfScope ps("metric_complexity", s, E * (kTri + 8) + V * (kPt + kTen));
+    k_complexity_term<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, terms);
+    note_launch();
+    if (exact_sum) {
+      k_sum_sequential<<<1, 32, 0, s>>>(terms, nb_elems, complexity);
+      note_launch();
+    } else {
+      sum_tree(terms, nb_elems, terms + m.capa_elem, complexity, s);
+    }
+    ProfScope ps2("metric_normalize", s, V * 2 * kTen);
+    k_normalize_f32<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, complexity, p.target,
+                                                                p.eig_min, p.eig_max);
+    note_launch();
+    check_launch("metric_run");
+    return;
+  }
   double* atot = keep ? keep->atot : nullptr;
   double4* hsym = keep ? keep->hsym : nullptr;
   double4* mloc = keep ? keep->mloc : nullptr;

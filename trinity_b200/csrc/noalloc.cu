@@ -25,7 +25,10 @@
  *
  * The computation is the same kernels, in the same order, as trn_metric_run
  * (gradient, Hessian with local L^p scaling, complexity with the fixed-shape
- * tree sum, global scaling), so the tensors are identical to it.
+ * tree sum, global scaling), so the tensors are identical to it when that
+ * mesh also sums with the tree (its default; exact_sum and replay sum in
+ * element order). The kernels run on the caller's stream with the address
+ * looked up for the current device, so the stream must belong to it.
  */
 #include "trn_internal.h"
 #include "trn_libm.h"

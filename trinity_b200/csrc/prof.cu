@@ -26,6 +26,7 @@ struct Pending {
   int id;
   cudaEvent_t a, b;
   double bytes;
+  int slot;   /* device byte counter of the scope, -1: the launcher's figure */
 };
 
 struct Total {
@@ -33,6 +34,7 @@ struct Total {
   long long launches = 0;
   double ms = 0.0;
   double bytes = 0.0;
+  long long counted = 0;   /* launches whose bytes the kernel counted */
 };
 
 struct Profiler {
@@ -42,6 +44,14 @@ struct Profiler {
   std::vector<cudaEvent_t> pool;
   std::vector<Pending> pending;
   std::vector<Total> totals;
+  /* counted bytes: one device counter per scope, and a vertex bitmap the
+   * counting kernels mark distinct entries in */
+  bool counting = false;
+  unsigned long long* d_bytes = nullptr;
+  std::vector<unsigned long long> h_bytes;
+  int next_slot = 0;
+  unsigned* d_seen = nullptr;
+  size_t seen_words = 0;
 
   cudaEvent_t get() {
     if (pool.empty()) {
@@ -70,8 +80,11 @@ Profiler& prof() {
 
 }  // namespace
 
-ProfScope::ProfScope(const char* name, cudaStream_t s, double bytes) : stream_(s) {
+constexpr int kByteSlots = 16384;
+
+ProfScope::ProfScope(const char* name, cudaStream_t s, double bytes, ByteCount* count) : stream_(s) {
   Profiler& p = prof();
+  if (count) *count = ByteCount();
   if (!p.on) return;
   cudaStreamCaptureStatus cs;
   if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) return;
@@ -79,6 +92,13 @@ ProfScope::ProfScope(const char* name, cudaStream_t s, double bytes) : stream_(s
   if (!p.only.empty() && p.only != name) return;
   id_ = p.id_of(name);
   bytes_ = bytes;
+  if (count && p.counting && p.d_bytes && p.next_slot < kByteSlots) {
+    slot_ = p.next_slot++;
+    count->bytes = p.d_bytes + slot_;
+    count->seen = p.d_seen;
+    cudaMemsetAsync(count->bytes, 0, sizeof(unsigned long long), s);
+    cudaMemsetAsync(p.d_seen, 0, sizeof(unsigned) * p.seen_words, s);
+  }
   a_ = p.get();
   cudaEventRecord(a_, s);
 }
@@ -89,7 +109,7 @@ ProfScope::~ProfScope() {
   std::lock_guard<std::mutex> lock(p.mu);
   cudaEvent_t b = p.get();
   cudaEventRecord(b, stream_);
-  p.pending.push_back({id_, a_, b, bytes_});
+  p.pending.push_back({id_, a_, b, bytes_, slot_});
 }
 
 static std::atomic<unsigned long long> g_launches{0};
@@ -111,6 +131,12 @@ unsigned long long thread_launches() { return t_launches; }
 void prof_flush() {
   Profiler& p = prof();
   std::lock_guard<std::mutex> lock(p.mu);
+  if (p.next_slot > 0) {
+    if (!p.pending.empty()) cudaEventSynchronize(p.pending.back().b);
+    p.h_bytes.resize((size_t) p.next_slot);
+    cudaMemcpy(p.h_bytes.data(), p.d_bytes, sizeof(unsigned long long) * (size_t) p.next_slot,
+               cudaMemcpyDeviceToHost);
+  }
   for (auto& q : p.pending) {
     cudaEventSynchronize(q.b);
     float ms = 0.f;
@@ -118,11 +144,13 @@ void prof_flush() {
     Total& t = p.totals[q.id];
     t.launches += 1;
     t.ms += ms;
-    t.bytes += q.bytes;
+    t.bytes += q.slot >= 0 ? (double) p.h_bytes[(size_t) q.slot] : q.bytes;
+    if (q.slot >= 0) t.counted += 1;
     p.pool.push_back(q.a);
     p.pool.push_back(q.b);
   }
   p.pending.clear();
+  p.next_slot = 0;
 }
 
 }  // namespace trn
@@ -155,11 +183,47 @@ int trn_profile_only(const char* name) {
   return 0;
 }
 
+/* algorithmic bytes counted by the kernels that can count them (distinct
+ * entries each launch touches, marked on the device) instead of the
+ * launchers' figures; for profiled, untimed runs: the counting costs atomics.
+ * max_nodes sizes the bitmap of distinct vertices. */
+int trn_profile_count_bytes(int on, int max_nodes) {
+  trn::Profiler& p = trn::prof();
+  trn::prof_flush();
+  std::lock_guard<std::mutex> lock(p.mu);
+  p.counting = on != 0;
+  if (on) {
+    if (!p.d_bytes && cudaMalloc(&p.d_bytes, sizeof(unsigned long long) * trn::kByteSlots) != cudaSuccess) {
+      p.d_bytes = nullptr;
+      p.counting = false;
+      return 5;
+    }
+    const size_t words = ((size_t) (max_nodes > 0 ? max_nodes : 1) + 31) / 32;
+    if (words > p.seen_words) {
+      cudaFree(p.d_seen);
+      if (cudaMalloc(&p.d_seen, sizeof(unsigned) * words) != cudaSuccess) {
+        p.d_seen = nullptr;
+        p.seen_words = 0;
+        p.counting = false;
+        return 5;
+      }
+      p.seen_words = words;
+    }
+  }
+  return 0;
+}
+
 unsigned long long trn_launch_count(void) { return trn::g_launches.load(); }
 
 int trn_profile_count(void) {
   trn::prof_flush();
   return (int) trn::prof().totals.size();
+}
+
+int trn_profile_counted(int i) {
+  trn::Profiler& p = trn::prof();
+  if (i < 0 || i >= (int) p.totals.size()) return -1;
+  return (int) p.totals[i].counted;
 }
 
 int trn_profile_entry(int i, char* name, int name_len, long long* launches, double* ms,

@@ -29,8 +29,19 @@ __global__ void k_smooth_pre(DMesh m, int nb_nodes) {
     if (m.alive[v]) m.activ[v] = (m.tags[v] & TRN_TAG_BOUND) ? 0 : 1;
 }
 
+/* Element metrics of the back-off: the log-Euclidean mean of an element's
+ * three tensors (and the square root of its determinant) does not depend on
+ * where the moved vertex sits, only on its new tensor, so it is computed once
+ * per stencil element before the tries and kept in shared memory (kj slots a
+ * thread, stride blockDim.x so that a warp's slots are contiguous); the
+ * tries only redo the geometry. Elements past the kj-th (rare: long
+ * stencils) take the metric inline. Same operations, same bits as
+ * evaluating the whole quality in every try. */
 template <bool F32>
-__device__ int move_laplacian(const DMesh& m, int i) {
+using JmT = LogT<F32>;
+
+template <bool F32>
+__device__ int move_laplacian(const DMesh& m, int i, JmT<F32>* jc, int kj) {
   const int* vc = m.vic + (size_t) i * m.bucket;
   const int* st = m.stenc + (size_t) i * m.bucket;
   const int deg = trn_deg(m, i);
@@ -76,6 +87,14 @@ __device__ int move_laplacian(const DMesh& m, int i) {
   const LogT<F32> lnew = log_of<F32>(tn[0], tn[1], tn[2]);
   ten_store<F32>(m, i, tnew);
   log_store<F32>(m, i, lnew);
+  const int nj = deg < kj ? deg : kj;
+  for (int a = 0; a < nj; ++a) {
+    const int4 n = m.tri[st[a]];
+    const LogT<F32> l0 = (n.x == i) ? lnew : log_load<F32>(m, n.x);
+    const LogT<F32> l1 = (n.y == i) ? lnew : log_load<F32>(m, n.y);
+    const LogT<F32> l2 = (n.z == i) ? lnew : log_load<F32>(m, n.z);
+    jc[(size_t) a * blockDim.x] = qmetric_x(l0, l1, l2);
+  }
   double qual[TRN_MAX_DEG];
   bool valid;
   int retry = 0;
@@ -93,10 +112,16 @@ __device__ int move_laplacian(const DMesh& m, int i) {
       const double2 p2 = (n.z == i) ? pa : m.pts[n.z];
       valid = false;
       if (trn_ccw(p0, p1, p2)) {
-        const LogT<F32> l0 = (n.x == i) ? lnew : log_load<F32>(m, n.x);
-        const LogT<F32> l1 = (n.y == i) ? lnew : log_load<F32>(m, n.y);
-        const LogT<F32> l2 = (n.z == i) ? lnew : log_load<F32>(m, n.z);
-        qual[a] = quality_x(p0, p1, p2, l0, l1, l2);
+        JmT<F32> jm;
+        if (a < nj) {
+          jm = jc[(size_t) a * blockDim.x];
+        } else {
+          const LogT<F32> l0 = (n.x == i) ? lnew : log_load<F32>(m, n.x);
+          const LogT<F32> l1 = (n.y == i) ? lnew : log_load<F32>(m, n.y);
+          const LogT<F32> l2 = (n.z == i) ? lnew : log_load<F32>(m, n.z);
+          jm = qmetric_x(l0, l1, l2);
+        }
+        qual[a] = qgeom_x(p0, p1, p2, jm);
         valid = (qual[a] > q_min);
       }
     }
@@ -112,28 +137,58 @@ __device__ int move_laplacian(const DMesh& m, int i) {
   return valid ? 1 : 0;
 }
 
+/* the algorithmic bytes of one listed vertex (profiled runs only): its list
+ * entry and flags; when it moves, its own point, tensor and logarithm read
+ * and written, its stencil and adjacency rows, its elements' records and
+ * qualities (read and written), and the point, tensor and logarithm of each
+ * neighbour that no other vertex of the launch has counted yet (a bitmap
+ * over the vertices keeps them distinct) */
+template <bool F32>
+__device__ unsigned long long smooth_bytes(const DMesh& m, int v, bool moved, unsigned* seen) {
+  constexpr unsigned long long kTenB = F32 ? 16 + 32 : 32;   /* FP32 reads its copy, writes both */
+  constexpr unsigned long long kLogB = F32 ? 16 : 32;
+  unsigned long long b = 4 + 1 + 4;
+  if (!moved) return b;
+  const int deg = trn_deg(m, v), nv = m.vdeg[v];
+  b += 4 + 2 * (16 + kTenB + kLogB);
+  b += (unsigned long long) deg * (4 + 16 + 8 + 8) + (unsigned long long) nv * 4;
+  const int* vc = m.vic + (size_t) v * m.bucket;
+  for (int k = 0; k < nv; ++k) {
+    const int w = vc[k];
+    const unsigned bit = 1u << (w & 31);
+    if (!(atomicOr(seen + (w >> 5), bit) & bit)) b += 16 + (F32 ? 16 : 32) + kLogB;
+  }
+  return b;
+}
+
 template <bool F32>
 __global__ void __launch_bounds__(256, 3) k_smooth_move(DMesh m, const int* __restrict__ list, int n,
-                                                       const int* off, int c, int* counters) {
+                                                       const int* off, int c, int* counters, int kj,
+                                                       ByteCount bc) {
+  extern __shared__ __align__(16) unsigned char smooth_smem[];
+  JmT<F32>* jc = reinterpret_cast<JmT<F32>*>(smooth_smem) + threadIdx.x;
   if (trn_failed(m)) return;
   if (off) {   /* color class c of a device-side partition */
     list += off[c];
     n = off[c + 1] - off[c];
   }
   int tasks = 0, commit = 0;
+  unsigned long long bytes = 0;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
     const int v = list[q];
     if (v < 0 || v >= m.capa_node) {
       trn_set_error(m.err, TRN_DERR_REPLAY);
       continue;
     }
-    if (!m.activ[v]) continue;
-    if (m.vdeg[v] == 0) continue;
+    const bool moved = m.activ[v] && m.vdeg[v] != 0;
+    if (bc.bytes) bytes += smooth_bytes<F32>(m, v, moved, bc.seen);
+    if (!moved) continue;
     tasks++;
-    commit += move_laplacian<F32>(m, v);
+    commit += move_laplacian<F32>(m, v, jc, kj);
   }
   if (tasks) atomicAdd(counters, tasks);
   if (commit) atomicAdd(counters + 1, commit);
+  if (bytes) atomicAdd(bc.bytes, bytes);
 }
 
 /* The same move with G lanes per vertex: lane j gathers the neighbours
@@ -315,7 +370,8 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
    * at most every vertex) */
   const double own = 4 + 1 + 8 + 2 * (kPt + kTen) + kAvgDeg * (2 * kIdx + kTri + 2 * kQ);
   const double nbr = (double) std::min<long long>((long long) m.capa_node, 6LL * n) * (kPt + kTen);
-  ProfScope ps("smooth_move", s, n * own + nbr);
+  ByteCount bc;
+  ProfScope ps("smooth_move", s, n * own + nbr, &bc);
   const int t = tune().smooth_threads;
   const int lanes = tune().smooth_lanes;
   const int g = grid_for((long long) hint * lanes, t);
@@ -326,8 +382,13 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
     if (fp32) k_smooth_move_grp<true, 4><<<g, t, 0, s>>>(m, list, n, off, c, counters);
     else k_smooth_move_grp<false, 4><<<g, t, 0, s>>>(m, list, n, off, c, counters);
   } else {
-    if (fp32) k_smooth_move<true><<<g, t, 0, s>>>(m, list, n, off, c, counters);
-    else k_smooth_move<false><<<g, t, 0, s>>>(m, list, n, off, c, counters);
+    /* element-metric slots a thread: what 40 KB of shared memory a block
+     * holds, at most 8 (FP64) or 12 (FP32) */
+    const int slot = fp32 ? (int) sizeof(float4) : (int) sizeof(double4);
+    const int kj = std::min(fp32 ? 12 : 8, (40 << 10) / (t * slot));
+    const size_t smem = (size_t) kj * t * slot;
+    if (fp32) k_smooth_move<true><<<g, t, smem, s>>>(m, list, n, off, c, counters, kj, bc);
+    else k_smooth_move<false><<<g, t, smem, s>>>(m, list, n, off, c, counters, kj, bc);
   }
   note_launch();
   check_launch("smooth_move");

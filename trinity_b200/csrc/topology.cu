@@ -211,6 +211,41 @@ __global__ void k_pack_tris(DMesh m, const int* __restrict__ list, const int* co
   }
 }
 
+/* the live vertices and elements as a freshly loaded mesh: points and tags
+ * of the listed vertices, elements renumbered into int4 records */
+__global__ void k_pack_nodes_load(DMesh m, const int* __restrict__ list, const int* count,
+                                  int* __restrict__ newid, double2* __restrict__ pts,
+                                  uint8_t* __restrict__ tags) {
+  const int n = *count;
+  for (int k = trn_tid(); k < n; k += trn_grid_stride()) {
+    const int v = list[k];
+    newid[v] = k;
+    pts[k] = m.pts[v];
+    tags[k] = m.tags[v];
+  }
+}
+
+__global__ void k_pack_tris_load(DMesh m, const int* __restrict__ list, const int* count,
+                                 const int* __restrict__ newid, int4* __restrict__ out) {
+  const int n = *count;
+  for (int k = trn_tid(); k < n; k += trn_grid_stride()) {
+    const int4 t = m.tri[list[k]];
+    out[k] = make_int4(newid[t.x], newid[t.y], newid[t.z], 0);
+  }
+}
+
+void pack_nodes_load(const DMesh& m, const int* list, const int* count, int* newid, double2* pts,
+                     uint8_t* tags, cudaStream_t s) {
+  k_pack_nodes_load<<<grid_for(m.capa_node), TRN_THREADS, 0, s>>>(m, list, count, newid, pts, tags);
+  note_launch();
+}
+
+void pack_tris_load(const DMesh& m, const int* list, const int* count, const int* newid, int4* out,
+                    cudaStream_t s) {
+  k_pack_tris_load<<<grid_for(m.capa_elem), TRN_THREADS, 0, s>>>(m, list, count, newid, out);
+  note_launch();
+}
+
 void pack_nodes(const DMesh& m, const int* list, const int* count, int* newid, double* pts, double* ten,
                 cudaStream_t s) {
   k_pack_nodes<<<grid_for(m.capa_node), TRN_THREADS, 0, s>>>(m, list, count, newid, pts, ten);

@@ -77,6 +77,7 @@ struct trn_mesh {
   bool round_fp32 = false;
   uint64_t round_seed = 0;
   int round_swap_match = 0;
+  int round_level_cap = 0;
   unsigned long long round_launches = 0;
   /* replay */
   bool replay = false;
@@ -86,7 +87,8 @@ struct trn_mesh {
   /* options */
   uint64_t seed = 0x7472696e697479ULL;
   bool exact_sum = false;
-  int swap_match = TRN_SWAP_ROW_ORDER;
+  int swap_match = TRN_SWAP_GREEDY;
+  int level_cap = kLoopCap;   /* coarsening / swapping levels per call */
   bool fp32 = false;   /* mixed-precision form of the metric arithmetic */
   double last_complexity = 0.0;
   double last_ms = 0.0;
@@ -205,19 +207,6 @@ void release(trn_mesh* m) {
 struct Reader {
   std::vector<char> buf;
   size_t pos = 0;
-  bool open(const char* path) {
-    FILE* f = std::fopen(path, "rb");
-    if (!f) return false;
-    std::fseek(f, 0, SEEK_END);
-    long n = std::ftell(f);
-    std::fseek(f, 0, SEEK_SET);
-    buf.resize((size_t) n + 1);
-    size_t got = std::fread(buf.data(), 1, (size_t) n, f);
-    std::fclose(f);
-    buf[got] = 0;
-    buf.resize(got + 1);
-    return true;
-  }
   void skip_ws() {
     while (pos < buf.size() && (buf[pos] == ' ' || buf[pos] == '\t' || buf[pos] == '\n' || buf[pos] == '\r'))
       ++pos;
@@ -422,14 +411,15 @@ int trn_mesh_reload(trn_mesh* m) {
   return init_from_device(m);
 }
 
-int trn_mesh_load(trn_mesh* m, const char* mesh_path, const char* solut_path) {
-  if (!m || !mesh_path) return fail(m, TRN_ERR_INVALID, "load: null path");
-  Reader r;
-  if (!r.open(mesh_path)) return fail(m, TRN_ERR_IO, std::string("cannot open ") + mesh_path);
+/* the token-by-token reader (any whitespace between numbers), for text that
+ * is not laid out one record per line */
+static int load_tokens(trn_mesh* m, Reader& r, MeshInput* in) {
   long nv = r.find("Vertices");
   if (nv <= 0) return fail(m, TRN_ERR_IO, "mesh: no Vertices section");
-  std::vector<double> pts((size_t) nv * 2);
-  std::vector<uint8_t> tags((size_t) nv, 0);
+  std::vector<double>& pts = in->pts;
+  std::vector<uint8_t>& tags = in->tags;
+  pts.assign((size_t) nv * 2, 0.0);
+  tags.assign((size_t) nv, 0);
   for (long i = 0; i < nv; ++i) {
     long tag;
     if (!r.next_double(&pts[2 * i]) || !r.next_double(&pts[2 * i + 1]) || !r.next_long(&tag))
@@ -451,7 +441,8 @@ int trn_mesh_load(trn_mesh* m, const char* mesh_path, const char* solut_path) {
   }
   long nt = r.find("Triangles");
   if (nt <= 0) return fail(m, TRN_ERR_IO, "mesh: no Triangles section");
-  std::vector<int> tris((size_t) nt * 3);
+  std::vector<int>& tris = in->tris;
+  tris.assign((size_t) nt * 3, 0);
   for (long i = 0; i < nt; ++i) {
     long a, b, c, tag;
     if (!r.next_long(&a) || !r.next_long(&b) || !r.next_long(&c) || !r.next_long(&tag))
@@ -472,22 +463,119 @@ int trn_mesh_load(trn_mesh* m, const char* mesh_path, const char* solut_path) {
   } else {
     r.pos = after_t;
   }
+  in->nv = nv;
+  in->nt = nt;
+  return TRN_OK;
+}
+
+/* Mesh::load, io.cpp:53-161: a medit .mesh (or the binary form written by
+ * trn_mesh_store_binary) and an optional .bb nodal solution */
+int trn_mesh_load(trn_mesh* m, const char* mesh_path, const char* solut_path) {
+  if (!m || !mesh_path) return fail(m, TRN_ERR_INVALID, "load: null path");
+  MeshInput in;
+  {
+    Reader r;
+    if (!read_file(mesh_path, &r.buf)) return fail(m, TRN_ERR_IO, std::string("cannot open ") + mesh_path);
+    std::string err;
+    const int prc = is_binary_mesh(r.buf) ? parse_mesh_binary(r.buf, &in, &err) : parse_mesh_text(r.buf, &in, &err);
+    if (prc > 0) return fail(m, TRN_ERR_IO, err);
+    if (prc < 0) {
+      in = MeshInput();
+      const int rc = load_tokens(m, r, &in);
+      if (rc) return rc;
+    }
+  }
+  const long nv = in.nv, nt = in.nt;
   if (nv != m->size0[0] || nt != m->size0[1])
     return fail(m, TRN_ERR_IO, "mesh: sizes differ from the ones the mesh was created with");
-  std::vector<double> u((size_t) nv, 0.0);
+  std::vector<double> u;
   if (solut_path) {
     Reader rb;
-    if (!rb.open(solut_path)) return fail(m, TRN_ERR_IO, std::string("cannot open ") + solut_path);
-    long hdr[4] = {0, 0, 0, 0};
-    for (int k = 0; k < 4; ++k)
-      if (!rb.next_long(&hdr[k])) return fail(m, TRN_ERR_IO, "bb: bad header");
-    if (hdr[2] != nv) return fail(m, TRN_ERR_IO, "bb: wrong number of vertices in solution file");
-    rb.pos = 0;
-    rb.skip_line();
-    for (long i = 0; i < nv; ++i)
-      if (!rb.next_double(&u[i])) return fail(m, TRN_ERR_IO, "bb: truncated values");
+    if (!read_file(solut_path, &rb.buf)) return fail(m, TRN_ERR_IO, std::string("cannot open ") + solut_path);
+    std::string err;
+    const int prc = parse_bb_text(rb.buf, nv, &u, &err);
+    if (prc > 0) return fail(m, TRN_ERR_IO, err);
+    if (prc < 0) {
+      u.assign((size_t) nv, 0.0);
+      rb.pos = 0;
+      rb.skip_line();
+      for (long i = 0; i < nv; ++i)
+        if (!rb.next_double(&u[i])) return fail(m, TRN_ERR_IO, "bb: truncated values");
+    }
+  } else {
+    u.assign((size_t) nv, 0.0);
   }
-  return trn_mesh_load_arrays(m, (int) nv, (int) nt, pts.data(), tris.data(), tags.data(), u.data());
+  return trn_mesh_load_arrays(m, (int) nv, (int) nt, in.pts.data(), in.tris.data(), in.tags.data(), u.data());
+}
+
+/* the .mesh (text or binary) and .bb files as trn_mesh_load reads them, into
+ * host arrays, without a mesh or a GPU: the counts always, the arrays when
+ * their capacities (vertices, triangles) suffice */
+int trn_read_mesh_files(const char* mesh_path, const char* solut_path, int* nb_nodes, int* nb_elems,
+                        double* points, int* tris, uint8_t* tags, double* solut, int cap_nodes,
+                        int cap_elems) {
+  if (!mesh_path || !nb_nodes || !nb_elems) return TRN_ERR_INVALID;
+  MeshInput in;
+  Reader r;
+  if (!read_file(mesh_path, &r.buf)) return TRN_ERR_IO;
+  std::string err;
+  int prc = is_binary_mesh(r.buf) ? parse_mesh_binary(r.buf, &in, &err) : parse_mesh_text(r.buf, &in, &err);
+  if (prc > 0) return TRN_ERR_IO;
+  if (prc < 0) {
+    in = MeshInput();
+    if (load_tokens(nullptr, r, &in)) return TRN_ERR_IO;
+  }
+  *nb_nodes = (int) in.nv;
+  *nb_elems = (int) in.nt;
+  if (in.nv > cap_nodes || in.nt > cap_elems) return TRN_OK;
+  if (points) std::memcpy(points, in.pts.data(), sizeof(double) * 2 * (size_t) in.nv);
+  if (tris) std::memcpy(tris, in.tris.data(), sizeof(int) * 3 * (size_t) in.nt);
+  if (tags) std::memcpy(tags, in.tags.data(), (size_t) in.nv);
+  if (solut_path && solut) {
+    Reader rb;
+    if (!read_file(solut_path, &rb.buf)) return TRN_ERR_IO;
+    std::vector<double> u;
+    prc = parse_bb_text(rb.buf, in.nv, &u, &err);
+    if (prc > 0) return TRN_ERR_IO;
+    if (prc < 0) {
+      u.assign((size_t) in.nv, 0.0);
+      rb.pos = 0;
+      rb.skip_line();
+      for (long i = 0; i < in.nv; ++i)
+        if (!rb.next_double(&u[i])) return TRN_ERR_IO;
+    }
+    std::memcpy(solut, u.data(), sizeof(double) * (size_t) in.nv);
+  }
+  return TRN_OK;
+}
+
+/* the mesh as trn_mesh_compact would renumber it (points, tags, 0-based
+ * triangles), in the binary form trn_mesh_load reads */
+int trn_mesh_store_binary(trn_mesh* m, const char* path) {
+  if (!m || !path || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "store_binary: no mesh or path");
+  const size_t nn = (size_t) m->nb_nodes, ne = (size_t) m->nb_elems;
+  std::vector<double> pts(2 * nn);
+  std::vector<int> tri(3 * ne);
+  std::vector<uint8_t> alive(nn), tags(nn);
+  int rc = trn_mesh_export(m, pts.data(), nullptr, tri.data(), alive.data(), tags.data());
+  if (rc) return rc;
+  std::vector<int> newid(nn, -1);
+  std::vector<double> cp;
+  std::vector<uint8_t> ct;
+  for (size_t i = 0; i < nn; ++i)
+    if (alive[i]) {
+      newid[i] = (int) ct.size();
+      cp.push_back(pts[2 * i]);
+      cp.push_back(pts[2 * i + 1]);
+      ct.push_back(tags[i]);
+    }
+  std::vector<int> cti;
+  for (size_t e = 0; e < ne; ++e)
+    if (tri[3 * e] >= 0)
+      for (int k = 0; k < 3; ++k) cti.push_back(newid[(size_t) tri[3 * e + k]]);
+  if (write_mesh_binary(path, (long) ct.size(), (long) cti.size() / 3, cp.data(), ct.data(), cti.data()))
+    return fail(m, TRN_ERR_IO, std::string("cannot write ") + path);
+  return TRN_OK;
 }
 
 int trn_mesh_export(trn_mesh* m, double* points, double* tensor, int* tris, uint8_t* alive,
@@ -519,6 +607,13 @@ int trn_mesh_export(trn_mesh* m, double* points, double* tensor, int* tris, uint
     tris[3 * i + 1] = e4[i].y;
     tris[3 * i + 2] = e4[i].z;
   }
+  return TRN_OK;
+}
+
+int trn_mesh_capacity(trn_mesh* m, int* capa_nodes, int* capa_elems) {
+  if (!m) return TRN_ERR_INVALID;
+  if (capa_nodes) *capa_nodes = m->capa_node;
+  if (capa_elems) *capa_elems = m->capa_elem;
   return TRN_OK;
 }
 
@@ -562,6 +657,73 @@ int trn_mesh_export_compact(trn_mesh* m, double* points, int* tris, double* tens
   CK(cudaStreamSynchronize(s));
   *nb_nodes = nv;
   *nb_elems = ne;
+  return TRN_OK;
+}
+
+/* The solver-coupled loop (the adaptive loop the reference is written for,
+ * README.md:8, scripts/bench_run.py:77-110: evaluate the field on the
+ * adapted mesh, recover the metric, adapt again). The reference closes the
+ * loop through files: Mesh::store (io.cpp:164-255, coordinates printed with
+ * 8 decimals, boundary only as RequiredVertices) and a fresh Mesh::load.
+ * trn_mesh_compact does the same renumbering on the device, without the
+ * rounding and keeping the boundary and corner tags: live vertices in slot
+ * order, live elements in slot order, every structure rebuilt as a load
+ * builds it. The state becomes the one trn_mesh_reload returns to. */
+int trn_mesh_compact(trn_mesh* m) {
+  if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "compact: no mesh loaded");
+  m->err.clear();
+  cudaStream_t s = m->stream;
+  DMesh& d = m->d;
+  compact_u8(d.alive, m->nb_nodes, m->list, m->scan, s);
+  int rc = sync_status(m, m->scan.count);
+  if (rc) return rc;
+  const int nv = m->h_status[S_COUNT];
+  flag_live_tris(d, m->nb_elems, m->flag, s);
+  /* the element list goes to the stage buffer: m->list still holds the vertices */
+  int* elist = reinterpret_cast<int*>(m->stage);
+  compact_u8(m->flag, m->nb_elems, elist, m->scan, s);
+  if ((rc = sync_status(m, m->scan.count))) return rc;
+  const int ne = m->h_status[S_COUNT];
+  if (nv <= 0 || ne <= 0) return fail(m, TRN_ERR_INVALID, "compact: empty mesh");
+  if (nv > m->n0_nodes || ne > m->n0_elems) {
+    double2* p0 = nullptr;
+    int4* t0 = nullptr;
+    uint8_t* g0 = nullptr;
+    if ((rc = dmalloc(m, &p0, (size_t) nv)) || (rc = dmalloc(m, &t0, (size_t) ne)) ||
+        (rc = dmalloc(m, &g0, (size_t) nv))) {
+      cudaFree(p0);
+      cudaFree(t0);
+      cudaFree(g0);
+      return rc;
+    }
+    CK(cudaStreamSynchronize(s));
+    cudaFree(m->pts0);
+    cudaFree(m->tri0);
+    cudaFree(m->tags0);
+    m->pts0 = p0;
+    m->tri0 = t0;
+    m->tags0 = g0;
+  }
+  /* the vertex list's length on the device again (the element compaction
+   * reused the scan's counter, which now holds ne) */
+  int nv_host = nv;
+  CK(cudaMemcpyAsync(m->status + S_COUNT, &nv_host, sizeof(int), cudaMemcpyHostToDevice, s));
+  pack_nodes_load(d, m->list, m->status + S_COUNT, m->target, m->pts0, m->tags0, s);
+  pack_tris_load(d, elist, m->scan.count, m->target, m->tri0, s);
+  CK(cudaStreamSynchronize(s));
+  CK(cudaMemsetAsync(m->solut, 0, sizeof(double) * (size_t) m->capa_node, s));
+  m->n0_nodes = nv;
+  m->n0_elems = ne;
+  return init_from_device(m);
+}
+
+/* a new nodal field for the vertex slots in use (after trn_mesh_compact:
+ * the live vertices in their new order), for the next trn_metric_run */
+int trn_mesh_set_solution(trn_mesh* m, const double* solut, int n) {
+  if (!m || !solut) return fail(m, TRN_ERR_INVALID, "set_solution: null argument");
+  if (n != m->nb_nodes) return fail(m, TRN_ERR_INVALID, "set_solution: one value per vertex slot in use");
+  CK(cudaMemcpyAsync(m->solut, solut, sizeof(double) * (size_t) n, cudaMemcpyHostToDevice, m->stream));
+  CK(cudaStreamSynchronize(m->stream));
   return TRN_OK;
 }
 
@@ -691,9 +853,16 @@ int trn_set_options(trn_mesh* m, uint64_t seed, int exact_sum) {
   return TRN_OK;
 }
 
+int trn_set_level_cap(trn_mesh* m, int cap) {
+  if (!m) return TRN_ERR_INVALID;
+  if (cap < 1) return fail(m, TRN_ERR_INVALID, "level cap: must be at least 1");
+  m->level_cap = cap;
+  return TRN_OK;
+}
+
 int trn_set_swap_match(trn_mesh* m, int policy) {
   if (!m) return TRN_ERR_INVALID;
-  if (policy != TRN_SWAP_ROW_ORDER && policy != TRN_SWAP_GAIN)
+  if (policy != TRN_SWAP_ROW_ORDER && policy != TRN_SWAP_GAIN && policy != TRN_SWAP_GREEDY)
     return fail(m, TRN_ERR_INVALID, "swap matching: unknown policy");
   m->swap_match = policy;
   return TRN_OK;
@@ -717,8 +886,7 @@ int trn_metric_run(trn_mesh* m, double target_factor, int norm, double h_min, do
   p.eig_max = 1 / trn_pow(h_max, 2);
   begin_timing(m);
   metric_run(m->d, m->nb_nodes, m->nb_elems, m->solut, m->grad, m->terms, m->complexity,
-             m->exact_sum || m->replay, p, m->stream);
-  if (m->fp32) log_cache(m->d, m->nb_nodes, true, m->stream);
+             m->exact_sum || m->replay, p, m->stream, nullptr, m->fp32);
   CK(cudaMemcpyAsync(m->h_status + H_WIDE, m->complexity, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
   int rc = sync_status(m);
   if (rc) return rc;
@@ -786,7 +954,7 @@ void enq_coarsen_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphCo
                 m->status + S_NINDEP, s, bound);
   collapse(dl, m->indep, m->status + S_NINDEP, m->target, nullptr, s, bound);
   fix_list(dl, dl.fix_list, dl.fix_n, s, bound < 0 ? -1 : 16 * bound);
-  level_end(m->status, kLevelCoarsen, kLoopCap, act_list(m, 1), act_list(m, 0),
+  level_end(m->status, kLevelCoarsen, m->level_cap, act_list(m, 1), act_list(m, 0),
             bound < 0 ? m->capa_node : (int) std::max(bound, 1LL), s, h, use_h);
 }
 
@@ -804,13 +972,17 @@ void enq_swap_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphCondi
   uint32_t* rank = m->swap_match == TRN_SWAP_GAIN ? m->hws.rank : nullptr;
   swap_filter_dual(dl, act_list(m, 0), m->status + S_ACT, m->dual, m->dual_n, m->map, rank,
                    m->status + S_NTASK, m->fp32, s, bound);
-  match_handshake(dl, m->capa_elem, m->dual, m->dual_n, m->status + S_NTASK, m->map, rank,
-                  seed_of(m, 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s, bound);
+  if (m->swap_match == TRN_SWAP_GREEDY)
+    match_greedy(dl, m->capa_elem, m->dual, m->dual_n, m->status + S_NTASK, m->map, m->hws, m->pairs,
+                 m->status + S_NPAIRS, s, bound);
+  else
+    match_handshake(dl, m->capa_elem, m->dual, m->dual_n, m->status + S_NTASK, m->map, rank,
+                    seed_of(m, 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s, bound);
   cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s);
   swap_flip(dl, m->pairs, m->status + S_NPAIRS, m->map, m->dual, m->dual_n, m->status + S_NTASK,
             m->status + S_COMMIT, true, m->fp32, s, bound);
   fix_list(dl, dl.fix_list, dl.fix_n, s, bound < 0 ? -1 : 4 * bound);
-  level_end(m->status, kLevelSwap, kLoopCap, act_list(m, 1), act_list(m, 0),
+  level_end(m->status, kLevelSwap, m->level_cap, act_list(m, 1), act_list(m, 0),
             bound < 0 ? m->capa_elem : (int) std::max(bound, 1LL), s, h, use_h);
 }
 
@@ -873,7 +1045,7 @@ int trn_coarsen_run(trn_mesh* m, int max_colors, trn_stats* st) {
     collapse(m->d, m->d_log + off, m->d_log + off - 1, m->target, m->flag, s);
     fix_tagged(m->d, m->nb_nodes, s);
     task += nb_indep;
-    if (++level > kLoopCap) return fail(m, TRN_ERR_NO_PROGRESS, "coarsen: level cap reached");
+    if (++level > m->level_cap) return fail(m, TRN_ERR_NO_PROGRESS, "coarsen: level cap reached");
   } while (nb_indep);
   int rc = sync_status(m);
   if (rc) return rc;
@@ -918,7 +1090,7 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
     commit = m->h_status[S_COMMIT];
     eval += ntasks;
     task += commit / 2;
-    if (++level > kLoopCap) return fail(m, TRN_ERR_NO_PROGRESS, "swap: level cap reached");
+    if (++level > m->level_cap) return fail(m, TRN_ERR_NO_PROGRESS, "swap: level cap reached");
   } while (commit);
   return end_timing(m, st, eval, task);
 }
@@ -1137,6 +1309,7 @@ int capture_round(trn_mesh* m, int depth) {
   m->round_fp32 = m->fp32;
   m->round_seed = m->seed;
   m->round_swap_match = m->swap_match;
+  m->round_level_cap = m->level_cap;
   m->round_launches = thread_launches() - l0;
   return TRN_OK;
 }
@@ -1151,7 +1324,8 @@ int trn_round_graph_run(trn_mesh* m, int depth, trn_stats stats[4]) {
   if (m->replay) return fail(m, TRN_ERR_INVALID, "round: a captured round runs the free mode only");
   m->err.clear();
   if (!m->round_exec || m->round_depth != depth || m->round_fp32 != m->fp32 || m->round_seed != m->seed ||
-      m->round_swap_match != m->swap_match || !(m->round_tune == m->tune)) {
+      m->round_swap_match != m->swap_match || m->round_level_cap != m->level_cap ||
+      !(m->round_tune == m->tune)) {
     int rc = capture_round(m, depth);
     if (rc) return rc;
   }

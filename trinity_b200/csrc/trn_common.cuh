@@ -174,8 +174,53 @@ __device__ __forceinline__ int trn_iunique(int* a, int n) {
   return k;
 }
 
-/* adjacency of v from its (canonical) stencil */
+/* adjacency of v from its (canonical) stencil: the other two vertices of
+ * each element, sorted, without duplicates. A stencil of up to 12 elements
+ * stays in registers (its element loads all in flight, an odd-even
+ * transposition network over the 24 ids, no local memory); longer ones sort
+ * in a local array. Both give the same rows. */
+constexpr int kVicRegs = 24;
+
 __device__ __forceinline__ void build_one_vicin(const DMesh& m, int v) {
+  if (m.alive[v] && trn_deg(m, v) <= kVicRegs / 2) {
+    const int* s = m.stenc + (size_t) v * m.bucket;
+    const int d = trn_deg(m, v);
+    int r[kVicRegs];
+#pragma unroll
+    for (int a = 0; a < kVicRegs / 2; ++a) {
+      int x = 0x7fffffff, y = 0x7fffffff;
+      if (a < d) {
+        const int4 n = m.tri[s[a]];
+        if (v == n.x) { x = n.y; y = n.z; }
+        else if (v == n.y) { x = n.z; y = n.x; }
+        else if (v == n.z) { x = n.x; y = n.y; }
+      }
+      r[2 * a] = x;
+      r[2 * a + 1] = y;
+    }
+#pragma unroll
+    for (int p = 0; p < kVicRegs; ++p)
+#pragma unroll
+      for (int a = p & 1; a + 1 < kVicRegs; a += 2) {
+        const int lo = min(r[a], r[a + 1]), hi = max(r[a], r[a + 1]);
+        r[a] = lo;
+        r[a + 1] = hi;
+      }
+    int* out = m.vic + (size_t) v * m.bucket;
+    int k = 0;
+#pragma unroll
+    for (int a = 0; a < kVicRegs; ++a)
+      if (r[a] != 0x7fffffff && (a == 0 || r[a] != r[a - 1])) {
+        if (k < m.bucket) out[k] = r[a];
+        ++k;
+      }
+    if (k > m.bucket) {
+      trn_set_error(m.err, TRN_DERR_BUCKET);
+      k = m.bucket;
+    }
+    m.vdeg[v] = k;
+    return;
+  }
   int buf[2 * TRN_MAX_DEG];
   int k = 0;
   if (m.alive[v]) {

@@ -9,6 +9,8 @@
 #include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <string>
+#include <vector>
 
 #include "trn_common.cuh"
 
@@ -91,6 +93,24 @@ void scan_i64(const long long* in, long long* out, int n, ScanWs& ws, cudaStream
  * *ws.count receives the number kept */
 void compact_u8(const uint8_t* flags, int n, int* list, ScanWs& ws, cudaStream_t s);
 
+/* mesh files (mesh_io.cu): an input mesh as loaded (0-based triangles,
+ * boundary / corner tags) */
+struct MeshInput {
+  long nv = 0, nt = 0;
+  std::vector<double> pts;
+  std::vector<int> tris;
+  std::vector<uint8_t> tags;
+};
+bool read_file(const char* path, std::vector<char>* buf);
+/* 0: parsed; 1: malformed (*err says why); -1: not one record per line,
+ * read it token by token instead */
+int parse_mesh_text(const std::vector<char>& buf, MeshInput* out, std::string* err);
+int parse_bb_text(const std::vector<char>& buf, long nv, std::vector<double>* u, std::string* err);
+bool is_binary_mesh(const std::vector<char>& buf);
+int parse_mesh_binary(const std::vector<char>& buf, MeshInput* out, std::string* err);
+int write_mesh_binary(const char* path, long nv, long nt, const double* pts, const uint8_t* tags,
+                      const int* tris);
+
 /* topology (topology.cu) */
 void build_stencils(const DMesh& m, int nb_nodes, int nb_elems, cudaStream_t s);
 void build_vicin(const DMesh& m, int nb_nodes, bool only_flagged, cudaStream_t s);
@@ -107,6 +127,12 @@ void expand_tris(const int* raw, int nb_elems, int nb_nodes, int4* out, int* err
 void pack_nodes(const DMesh& m, const int* list, const int* count, int* newid, double* pts, double* ten,
                 cudaStream_t s);
 void flag_live_tris(const DMesh& m, int nb_elems, uint8_t* flag, cudaStream_t s);
+/* the listed live vertices (points, tags) and elements (renumbered through
+ * newid) packed as a load would place them */
+void pack_nodes_load(const DMesh& m, const int* list, const int* count, int* newid, double2* pts,
+                     uint8_t* tags, cudaStream_t s);
+void pack_tris_load(const DMesh& m, const int* list, const int* count, const int* newid, int4* out,
+                    cudaStream_t s);
 void pack_tris(const DMesh& m, const int* list, const int* count, const int* newid, int* out,
                cudaStream_t s);
 
@@ -124,9 +150,13 @@ struct MetricSaves {
   double4* hsym = nullptr;
   double4* mloc = nullptr;
 };
+/* fp32: the mixed-precision form's recovery (FP32 patch means with FP64
+ * coordinate and value differences, FP32 normalisations, FP64 complexity
+ * sum; writes the FP32 tensor copy and logarithm cache too) */
 void metric_run(const DMesh& m, int nb_nodes, int nb_elems, const double* solut,
                 double2* grad, double* terms, double* complexity, bool exact_sum,
-                const MetricParams& p, cudaStream_t s, const MetricSaves* keep = nullptr);
+                const MetricParams& p, cudaStream_t s, const MetricSaves* keep = nullptr,
+                bool fp32 = false);
 /* deterministic two-level sum of n doubles; partial holds grid_for(n) slots */
 void sum_tree(const double* in, int n, double* partial, double* out, cudaStream_t s);
 
@@ -191,7 +221,9 @@ struct HeurWs {
   uint8_t* state = nullptr;      /* per vertex / element */
   uint8_t* state2 = nullptr;     /* second buffer of the independent-set rounds */
   unsigned long long* prop = nullptr;
+  unsigned long long* prop2 = nullptr;   /* second key buffer of the greedy matching */
   int* choice = nullptr;
+  int* choice2 = nullptr;                /* second row list of the greedy matching */
   int* color = nullptr;
   int* mate = nullptr;
   uint32_t* rank = nullptr;      /* four flip ranks per swap dual row */
@@ -209,6 +241,12 @@ void heur_ws_free(HeurWs* ws);
 void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* dual_n,
                      const int* ntasks, const int* map, const uint32_t* rank, Seed seed, HeurWs& ws,
                      int* pairs, int* npairs, cudaStream_t s, long long bound = -1);
+/* the reference's greedy matching loop over the dual rows, in the order
+ * (candidate id mod 4, candidate id), computed exactly by rounds of rows that
+ * come first on all their elements; pairs as match_handshake */
+void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual_n, const int* ntasks,
+                  const int* map, HeurWs& ws, int* pairs, int* npairs, cudaStream_t s,
+                  long long bound = -1);
 /* a fixed number of independent-set rounds over a device-counted candidate
  * list; undecided candidates are re-activated (next level) */
 void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, Seed seed,
@@ -268,9 +306,18 @@ void check_launch(const char* what);
 /* per-launch device timing (prof.cu): brackets the launches issued during its
  * lifetime with events on stream s when profiling is enabled; bytes is the
  * launcher's algorithmic byte count for them */
+/* where a counting kernel adds its algorithmic bytes (bytes == nullptr: not
+ * counting) and the zeroed bitmap it marks distinct vertices in */
+struct ByteCount {
+  unsigned long long* bytes = nullptr;
+  unsigned* seen = nullptr;
+};
+
 class ProfScope {
  public:
-  ProfScope(const char* name, cudaStream_t s, double bytes = 0.0);
+  /* count: filled when the profiler counts bytes (trn_profile_count_bytes);
+   * the launcher hands it to its kernel */
+  ProfScope(const char* name, cudaStream_t s, double bytes = 0.0, ByteCount* count = nullptr);
   ~ProfScope();
   ProfScope(const ProfScope&) = delete;
   ProfScope& operator=(const ProfScope&) = delete;
@@ -279,6 +326,7 @@ class ProfScope {
   cudaStream_t stream_;
   cudaEvent_t a_ = nullptr;
   int id_ = -1;
+  int slot_ = -1;
   double bytes_ = 0.0;
 };
 void prof_flush();

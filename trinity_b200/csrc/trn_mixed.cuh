@@ -101,12 +101,18 @@ __device__ __forceinline__ void trnf_interp_finish(float* lm, int nb, float* res
   res[2] = vec[2] * c1 + vec[3] * c3;
 }
 
-/* quality from cached FP32 logarithms; coordinate differences and the area in FP64 */
-__device__ __forceinline__ double trnf_quality_l(double2 pa, double2 pb, double2 pc, float4 la,
-                                                 float4 lb, float4 lc) {
+/* quality from cached FP32 logarithms; coordinate differences and the area
+ * in FP64. In two halves like trn_quality_l: the tensor mean and the square
+ * root of its determinant (j0, j1, j2, sqrt det), then the geometry. */
+__device__ __forceinline__ float4 trnf_quality_metric(float4 la, float4 lb, float4 lc) {
   float lm[4] = {la.x + lb.x + lc.x, la.y + lb.y + lc.y, la.z + lb.z + lc.z, la.w + lb.w + lc.w};
   float j[3], det;
   trnf_interp_finish(lm, 3, j, &det);
+  return make_float4(j[0], j[1], j[2], sqrtf(det));
+}
+
+__device__ __forceinline__ double trnf_quality_geom(double2 pa, double2 pb, double2 pc, float4 jm) {
+  const float j[3] = {jm.x, jm.y, jm.z};
   const float e[6] = {(float) (pb.x - pa.x), (float) (pb.y - pa.y), (float) (pc.x - pb.x),
                       (float) (pc.y - pb.y), (float) (pa.x - pc.x), (float) (pa.y - pc.y)};
   float perim = 0.f;
@@ -119,7 +125,12 @@ __device__ __forceinline__ double trnf_quality_l(double2 pa, double2 pb, double2
   const float mean = trnf_min(perim * 0.333333343f, 3.f * ip);
   const float mm = mean * (2.f - mean);
   const float norm = 20.78460969082653f * (mm * mm * mm);  /* 12 sqrt(3) */
-  return (double) ((float) area * norm * sqrtf(det) * (ip * ip));
+  return (double) ((float) area * norm * jm.w * (ip * ip));
+}
+
+__device__ __forceinline__ double trnf_quality_l(double2 pa, double2 pb, double2 pc, float4 la,
+                                                 float4 lb, float4 lc) {
+  return trnf_quality_geom(pa, pb, pc, trnf_quality_metric(la, lb, lc));
 }
 
 __device__ __forceinline__ float4 tenf_of(double4 t) {
@@ -184,6 +195,21 @@ __device__ __forceinline__ double quality_x(double2 a, double2 b, double2 c, dou
 __device__ __forceinline__ double quality_x(double2 a, double2 b, double2 c, float4 la, float4 lb,
                                            float4 lc) {
   return trnf_quality_l(a, b, c, la, lb, lc);
+}
+
+/* the two halves of quality_x (a position-independent element metric, then
+ * the geometry), same bits as quality_x */
+__device__ __forceinline__ double4 qmetric_x(double4 la, double4 lb, double4 lc) {
+  return trn_quality_metric(la, lb, lc);
+}
+__device__ __forceinline__ float4 qmetric_x(float4 la, float4 lb, float4 lc) {
+  return trnf_quality_metric(la, lb, lc);
+}
+__device__ __forceinline__ double qgeom_x(double2 a, double2 b, double2 c, double4 jm) {
+  return trn_quality_geom(a, b, c, jm);
+}
+__device__ __forceinline__ double qgeom_x(double2 a, double2 b, double2 c, float4 jm) {
+  return trnf_quality_geom(a, b, c, jm);
 }
 
 /* quality of element (v0, v1, v2) from the cached logarithms */

@@ -117,10 +117,15 @@ __device__ __forceinline__ void trn_interp_finish(double* log_mat, int nb, doubl
   res[2] = cache[3];
 }
 
-/* numeric::computeQuality, numeric.cpp:251-306, from the vertices' cached
- * tensor logarithms */
-__device__ __forceinline__ double trn_quality_l(double2 pa, double2 pb, double2 pc,
-                                                double4 la, double4 lb, double4 lc) {
+/* numeric::computeQuality, numeric.cpp:251-306, in two halves. The first
+ * depends only on the three vertex tensors: their log-Euclidean mean
+ * (jacob) and the square root of its determinant, returned as
+ * (j0, j1, j2, sqrt det). The second takes the three points. A caller that
+ * evaluates one element at several positions of a vertex whose tensor does
+ * not change (the smoothing back-off) computes the first half once; the
+ * operations and their order are those of the whole function, so the bits
+ * are the same. */
+__device__ __forceinline__ double4 trn_quality_metric(double4 la, double4 lb, double4 lc) {
   double lm[4] = {0, 0, 0, 0};
   double jacob[3];
   trn_interp_addl(lm, la);
@@ -128,6 +133,11 @@ __device__ __forceinline__ double trn_quality_l(double2 pa, double2 pb, double2 
   trn_interp_addl(lm, lc);
   trn_interp_finish(lm, 3, jacob);
   double det = jacob[0] * jacob[2] - jacob[1] * jacob[1];
+  return make_double4(jacob[0], jacob[1], jacob[2], sqrt(det));
+}
+
+__device__ __forceinline__ double trn_quality_geom(double2 pa, double2 pb, double2 pc, double4 jm) {
+  const double jacob[3] = {jm.x, jm.y, jm.z};
   double coef[6];
   coef[0] = pb.x - pa.x;
   coef[1] = pb.y - pa.y;
@@ -149,7 +159,13 @@ __device__ __forceinline__ double trn_quality_l(double2 pa, double2 pb, double2 
   double area = 0.5 * fabs(c0 * c3 - c1 * c2);
   double mean = trn_dmin(perim / 3, 3 / perim);
   double norm = 12 * sqrt(3.0) * trn_pow(mean * (2. - mean), 3);
-  return area * norm * sqrt(det) / trn_pow(perim, 2);
+  return area * norm * jm.w / trn_pow(perim, 2);
+}
+
+/* numeric::computeQuality from the vertices' cached tensor logarithms */
+__device__ __forceinline__ double trn_quality_l(double2 pa, double2 pb, double2 pc,
+                                                double4 la, double4 lb, double4 lc) {
+  return trn_quality_geom(pa, pb, pc, trn_quality_metric(la, lb, lc));
 }
 
 /* numeric::computeQuality from the tensors themselves */
