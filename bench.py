@@ -489,6 +489,38 @@ def precision_form(args):
     return out
 
 
+# ------------------------------------------------------------------ files
+def io_form():
+    """Reading the workload's files (87 MB .mesh, 20 MB .bb): the host-side
+    text parse (one thread per chunk of each section), the whole load onto
+    the device (parse, copies, stencils and adjacency), and the same from the
+    binary sidecar; best of three. The reference's Mesh::load on the same
+    files is timed by the CPU-baseline runs of the same process."""
+    import torch
+    from trinity_b200 import api
+    mp, bp = ensure_files()
+    m_n, m_e = api.find("Vertices", mp), api.find("Triangles", mp)
+
+    def best(fn):
+        t = 1e300
+        for _ in range(3):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            t = min(t, time.perf_counter() - t0)
+        return round(t * 1e3, 1)
+    out = {"files_mb": round((os.path.getsize(mp) + os.path.getsize(bp)) / 1e6, 1),
+           "host_threads": os.cpu_count()}
+    out["text_parse_ms"] = best(lambda: api.read_mesh_files(mp, bp))
+    g = api.Mesh((m_n, m_e), 128, 2, 0, 3)
+    out["text_load_to_device_ms"] = best(lambda: g.load(mp, bp))
+    binp = os.path.join(os.path.dirname(mp), "c2.trnb")
+    g.store_binary(binp)
+    out["binary_load_to_device_ms"] = best(lambda: g.load(binp, bp))
+    g.close()
+    return out
+
+
 # ------------------------------------------------------------------ adjoint
 def adjoint_form(args):
     """The differentiation form on the 2M-triangle mesh jittered by +-0.3h with
@@ -708,6 +740,7 @@ def cpu_baseline():
             "sample": f"median of 3 full adaptations of the workload (metric + 3 rounds; rounds timed: "
                       f"{ms:.0f} ms, metric {j['metric_ms']:.0f} ms, Mesh::load {j.get('load_ms', 0):.0f} ms)",
             "runs_triangles_per_s": [round(r[0] / (r[1] / 1e3), 1) for r in runs],
+            "mesh_load_ms": j.get("load_ms"),
             "one_thread": {"value": round(tin1 / (ms1 / 1e3), 1), "unit": UNIT, "cores": 1,
                            "sample": "the same generator at 400 x 400 (320k triangles), 3 rounds"},
             "build": "g++ -O3 -funroll-loops -march=x86-64-v3 (built where the sources are, run on "
@@ -793,8 +826,12 @@ def main():
             if line is not None and bf is not None:
                 line.setdefault("forms", {})["batch"] = bf
         if line is not None:
+            if world == 1 and not args.no_forms:
+                line.setdefault("forms", {})["io"] = io_form()
             if world == 1 and not args.no_cpu_baseline:
                 line["cpu_baseline"] = cpu_baseline()
+                if "io" in line.get("forms", {}):
+                    line["forms"]["io"]["reference_mesh_load_ms"] = line["cpu_baseline"].get("mesh_load_ms")
             print(json.dumps(line), flush=True)
     finally:
         if world > 1:

@@ -35,3 +35,46 @@ def test_batch_equals_one_at_a_time():
         st = gpu_state(g)
         assert not st.diff(want)
         check_invariants(st)
+
+
+@pytest.mark.gpu
+def test_batch_meshes_are_valid_and_match_the_reference_build(tmp_path):
+    """The first 12 meshes of the 256-mesh workload (sides 37 to 301),
+    adapted concurrently with captured rounds: every one conforming, CCW and
+    a disk, most metric edge lengths in [1/sqrt 2, sqrt 2]; the largest
+    (side 301, 181k triangles) within 2 % of the reference build's final
+    triangle count and 1 point of its in-range fraction on the same input."""
+    import os
+    import subprocess
+    from tests.helpers import in_range_fraction
+    from tests.oracle_lib import REF_TIMED, read_snapshot
+    from trinity_b200.api import batch_adapt
+    p = meshgen.BATCH_PARAMS
+    items = []
+    for k, it in enumerate(meshgen.batch_meshes()):
+        if k == 12:
+            break
+        items.append(it)
+    meshes = [_load(m, u, p) for m, u, _ in items]
+    batch_adapt(meshes, p["target"], p["norm"], p["rounds"], p["depth"], threads=4, graph=True)
+    states = [gpu_state(g) for g in meshes]
+    for (m, _, spec), st in zip(items, states):
+        check_invariants(st)
+        assert in_range_fraction(st) >= 0.9, (spec, in_range_fraction(st))
+    big = int(np.argmax([m.nb_elems for m, _, _ in items]))
+    m, u, spec = items[big]
+    if not os.path.exists(REF_TIMED):
+        pytest.skip("reference build (oracle/_ref) absent")
+    mp, bp, out = str(tmp_path / "b.mesh"), str(tmp_path / "b.bb"), str(tmp_path / "f.bin")
+    meshgen.write_mesh(mp, m)
+    meshgen.write_bb(bp, u)
+    subprocess.run([REF_TIMED, mp, bp, str(p["rounds"]), str(p["depth"]), str(p["bucket"]), str(p["target"]),
+                    str(p["norm"]), "--capa-depth", "4", "--final", out], check=True, capture_output=True,
+                   timeout=600, env=dict(os.environ, OMP_NUM_THREADS="8"))
+    ref = read_snapshot(out)
+    st = states[big]
+    n_gpu, n_ref = st.active_elems().shape[0], ref.active_elems().shape[0]
+    assert abs(n_gpu - n_ref) <= 0.02 * n_ref, (spec, n_gpu, n_ref)
+    assert abs(in_range_fraction(st) - in_range_fraction(ref)) <= 0.01, spec
+    for g in meshes:
+        g.close()

@@ -85,3 +85,29 @@ def test_cli_runs_the_reference_command_line(tmp_path):
     txt = open(out).read()
     assert txt.startswith("MeshVersionFormatted 1") and "RequiredVertices" in txt
     assert os.path.exists(str(tmp_path / "adapted.sol"))
+
+
+@pytest.mark.gpu
+def test_store_and_sol_give_the_in_memory_histogram(tmp_path):
+    """Mesh::store's .mesh and the .sol beside it, read back by the histogram
+    tool: the same tensors (17 digits) in the .mesh vertex order, and the
+    in-memory mesh's metric edge-length histogram (coordinates are stored
+    with 8 decimals, so bin counts may move by a few edges)."""
+    import numpy as np
+    from tests.helpers import gpu_mesh, in_range_fraction, run_gpu_stages
+    from trinity_b200 import histogram
+    m, u, c = meshgen.make_config("c2", 80)
+    g = gpu_mesh(m, u, c)
+    run_gpu_stages(g, c, lambda s: None)
+    mp, sp = str(tmp_path / "a.mesh"), str(tmp_path / "a.sol")
+    g.store(mp)
+    g.store_sol(sp)
+    pts, tri, ten = g.export_compact()
+    sol = histogram.read_sol(sp)
+    assert np.array_equal(sol.view(np.uint64), np.ascontiguousarray(ten).view(np.uint64))
+    h = histogram.of_files(mp, sp)
+    mem = histogram.histogram(pts, tri, ten)
+    assert h["triangles"] == tri.shape[0] and h["vertices"] == pts.shape[0]
+    assert np.abs(np.array(h["fractions"]) - np.array(mem["fractions"])).max() < 1e-3
+    assert abs(h["in_range_fraction"] - in_range_fraction(gpu_state(g))) < 1e-3
+    g.close()

@@ -141,6 +141,54 @@ __device__ __forceinline__ bool flip_eval(const DMesh& m, int id1, int id2, int 
   return true;
 }
 
+/* flip_eval by two lanes of a warp: both find the new elements and test
+ * them, lane `half` 0 evaluates the first new element's quality and lane 1
+ * the second's, and they trade results; the same values as flip_eval.
+ * Both lanes of the pair must call it (mask: the pair's two lanes). */
+template <bool F32>
+__device__ __forceinline__ bool flip_eval2(const DMesh& m, int id1, int id2, int c1[3], int c2[3],
+                                           double* q0, double* q1, int half, unsigned mask) {
+  const int4 a = m.tri[id1], b = m.tri[id2];
+  const int o1[3] = {a.x, a.y, a.z};
+  const int o2[3] = {b.x, b.y, b.z};
+  c1[0] = c1[1] = c1[2] = c2[0] = c2[1] = c2[2] = -1;
+  for (int i = 0; i < 3; ++i) {
+    int j = (i + 1) % 3, k = (i + 2) % 3;
+    if (o1[i] == o2[1] && o1[j] == o2[0]) {
+      c1[0] = o1[i]; c1[1] = o2[2]; c1[2] = o1[k];
+      c2[0] = o1[k]; c2[1] = o2[2]; c2[2] = o1[j];
+      break;
+    }
+    if (o1[i] == o2[2] && o1[j] == o2[1]) {
+      c1[0] = o1[i]; c1[1] = o2[0]; c1[2] = o1[k];
+      c2[0] = o1[k]; c2[1] = o2[0]; c2[2] = o1[j];
+      break;
+    }
+    if (o1[i] == o2[0] && o1[j] == o2[2]) {
+      c1[0] = o1[i]; c1[1] = o2[1]; c1[2] = o1[k];
+      c2[0] = o1[k]; c2[1] = o2[1]; c2[2] = o1[j];
+      break;
+    }
+  }
+  bool ok = c1[0] >= 0;
+  double q = 0;
+  if (ok) {
+    const double2 p10 = m.pts[c1[0]], p11 = m.pts[c1[1]], p12 = m.pts[c1[2]];
+    const double2 p22 = m.pts[c2[2]];
+    ok = trn_ccw(p10, p11, p12) && trn_ccw(p12, p11, p22);
+    if (ok) {
+      /* lane 0: (c1[0], c1[1], c1[2]); lane 1: (c1[2], c1[1], c2[2]) */
+      const int va = half ? c1[2] : c1[0], vc = half ? c2[2] : c1[2];
+      const double2 pa = half ? p12 : p10, pc = half ? p22 : p12;
+      q = quality_x(pa, p11, pc, log_load<F32>(m, va), log_load<F32>(m, c1[1]), log_load<F32>(m, vc));
+    }
+  }
+  const double other = __shfl_xor_sync(mask, q, 1);
+  *q0 = half ? other : q;
+  *q1 = half ? q : other;
+  return ok;
+}
+
 /* the matching rank of the flip of the edge shared by elements a and b: the
  * change of the smaller quality, min(q_new) - min(q_old), in [-1, 1], or
  * -1.5 when the flip is impossible, quantized to the upper 22 bits of a
@@ -229,6 +277,80 @@ __device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int*
   return 2;
 }
 
+/* flip_pair with the two new qualities on two lanes: the pair's lanes run
+ * the tests together, then lane 0 alone commits, with the same writes */
+template <bool F32>
+__device__ int flip_pair2(const DMesh& m, int id1, int id2, int index, const int* map,
+                          const int* dual, const int* dual_n, int ntasks, bool strict_map, int half,
+                          unsigned mask) {
+  int c1[3], c2[3];
+  double q0, q1;
+  if (!flip_eval2<F32>(m, id1, id2, c1, c2, &q0, &q1, half, mask)) return 0;
+  const double q_old = trn_dmin(m.qual[id1], m.qual[id2]);
+  const double q_new = trn_dmin(q0, q1);
+  if (q_new < q_old || half) return (q_new < q_old) ? 0 : 2;
+  m.tri[id1] = make_int4(c1[0], c1[1], c1[2], 0);
+  m.tri[id2] = make_int4(c2[0], c2[1], c2[2], 0);
+  trn_stenc_append(m, c2[0], id2);
+  trn_stenc_append(m, c2[1], id1);
+  m.qual[id1] = q0;
+  m.qual[id2] = q1;
+  const int fv[4] = {c1[0], c1[1], c1[2], c2[2]};
+  int fx[4], nf = 0;
+  for (int j = 0; j < 4; ++j)
+    if (trn_byte_cas01(m.fixes + fv[j])) fx[nf++] = fv[j];
+  if (m.fix_list) trn_list_push_n(m.fix_list, m.fix_n, fx, nf);
+  int act[8], na = 0;
+  for (int q = 0; q < dual_n[index]; ++q) {
+    const int t = dual[index * 4 + q];
+    if (trn_byte_cas01(m.activ + t)) act[na++] = t;
+  }
+  const int x = map[id2];
+  if (x > -1 && (!strict_map || (x < ntasks && dual[x * 4] == id2)))
+    for (int q = 0; q < dual_n[x]; ++q) {
+      const int t = dual[x * 4 + q];
+      if (trn_byte_cas01(m.activ + t)) act[na++] = t;
+    }
+  if (m.act_next) trn_list_push_n(m.act_next, m.act_next_n, act, na);
+  return 2;
+}
+
+/* two lanes per pair; the grid-stride loop keeps the lanes of a pair
+ * together (both see the same p), so every shuffle has its partner */
+template <bool F32>
+__global__ void k_swap_flip2(DMesh m, const int* __restrict__ pairs, const int* npairs,
+                             const int* __restrict__ map, const int* __restrict__ dual,
+                             const int* __restrict__ dual_n, const int* ntasks_dev, int* commit,
+                             int strict_map) {
+  if (trn_failed(m)) return;
+  const int np = *npairs;
+  const int ntasks = *ntasks_dev;
+  const int half = threadIdx.x & 1;
+  const unsigned mask = 3u << (threadIdx.x & 30);
+  int local = 0;
+  const int stride = (gridDim.x * blockDim.x) >> 1;
+  for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 1; p < np; p += stride) {
+    const int k1 = pairs[2 * p], k2 = pairs[2 * p + 1];
+    bool ok = k1 >= 0 && k1 < m.capa_elem && k2 >= 0 && k2 < m.capa_elem;
+    int index = -1;
+    if (ok) {
+      index = map[k1];
+      ok = index >= 0 && index < ntasks && dual[index * 4] == k1;
+      if (ok) {
+        ok = false;
+        for (int q = 1; q < dual_n[index]; ++q) ok |= (dual[index * 4 + q] == k2);
+      }
+    }
+    if (!ok) {
+      if (!half) trn_set_error(m.err, TRN_DERR_REPLAY);
+      continue;
+    }
+    const int r = flip_pair2<F32>(m, k1, k2, index, map, dual, dual_n, ntasks, strict_map != 0, half, mask);
+    if (!half) local += r;
+  }
+  if (local) atomicAdd(commit, local);
+}
+
 template <bool F32>
 __global__ void k_swap_flip(DMesh m, const int* __restrict__ pairs, const int* npairs,
                             const int* __restrict__ map, const int* __restrict__ dual,
@@ -315,12 +437,14 @@ void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* m
                bool fp32, cudaStream_t s, long long bound) {
   ProfScope ps("swap_flip", s, 0.0);
   const int ft = tune().flip_threads;
+  /* two lanes a pair: the grid sized for twice the pairs */
+  const int g = grid_bounded(bound < 0 ? bound : 2 * bound, 2LL * m.capa_elem, ft);
   if (fp32)
-    k_swap_flip<true><<<grid_bounded(bound, m.capa_elem, ft), ft, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
-                                                                   ntasks, commit, strict_map ? 1 : 0);
+    k_swap_flip2<true><<<g, ft, 0, s>>>(m, pairs, npairs, map, dual, dual_n, ntasks, commit,
+                                        strict_map ? 1 : 0);
   else
-    k_swap_flip<false><<<grid_bounded(bound, m.capa_elem, ft), ft, 0, s>>>(m, pairs, npairs, map, dual, dual_n,
-                                                                    ntasks, commit, strict_map ? 1 : 0);
+    k_swap_flip2<false><<<g, ft, 0, s>>>(m, pairs, npairs, map, dual, dual_n, ntasks, commit,
+                                         strict_map ? 1 : 0);
   note_launch();
   check_launch("swap_flip");
 }
