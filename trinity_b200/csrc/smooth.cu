@@ -290,8 +290,20 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
   lsum.finish(nb_neigh, tn);
   const double4 tnew = make_double4(tn[0], tn[1], tn[2], 0.0);
   const LogT<F32> lnew = log_of<F32>(tn[0], tn[1], tn[2]);
-  constexpr int KQ = 2;   /* qualities kept per lane; later ones are recomputed */
+  constexpr int KQ = 2;   /* qualities and element metrics kept per lane; later ones are recomputed */
   double qv[KQ];
+  /* the element metrics of this lane's first KQ elements: they do not depend
+   * on where the vertex sits, so the tries below only redo the geometry */
+  JmT<F32> jv[KQ];
+#pragma unroll
+  for (int j = 0; j < KQ; ++j) {
+    const int a = lane + j * G;
+    if (a < deg) {
+      const int4 n = m.tri[st[a]];
+      jv[j] = qmetric_x((n.x == i) ? lnew : log_load<F32>(m, n.x), (n.y == i) ? lnew : log_load<F32>(m, n.y),
+                        (n.z == i) ? lnew : log_load<F32>(m, n.z));
+    }
+  }
   bool valid;
   int retry = 0;
   double weight = 1;
@@ -303,8 +315,21 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
     int j = 0;
     for (int a = lane; ok && a < deg; a += G, ++j) {
       double q = 0;
-      ok = elem_quality_at<F32>(m, i, m.tri[st[a]], pa, lnew, &q) && (q > q_min);
-      if (j < KQ) qv[j] = q;
+      if (j < KQ) {
+        const int4 n = m.tri[st[a]];
+        const double2 p0 = (n.x == i) ? pa : m.pts[n.x];
+        const double2 p1 = (n.y == i) ? pa : m.pts[n.y];
+        const double2 p2 = (n.z == i) ? pa : m.pts[n.z];
+        ok = trn_ccw(p0, p1, p2);
+        if (ok) {
+          q = qgeom_x(p0, p1, p2, j == 0 ? jv[0] : jv[1]);
+          ok = q > q_min;
+        }
+        if (j == 0) qv[0] = q;
+        else qv[1] = q;
+      } else {
+        ok = elem_quality_at<F32>(m, i, m.tri[st[a]], pa, lnew, &q) && (q > q_min);
+      }
     }
     valid = __all_sync(gmask, ok);
     weight *= 0.5;
@@ -313,7 +338,7 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
     int j = 0;
     for (int a = lane; a < deg; a += G, ++j) {
       double q = 0;
-      if (j < KQ) q = qv[j];
+      if (j < KQ) q = (j == 0) ? qv[0] : qv[1];
       else elem_quality_at<F32>(m, i, m.tri[st[a]], pa, lnew, &q);
       m.qual[st[a]] = q;
     }
@@ -328,7 +353,8 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
 
 template <bool F32, int G>
 __global__ void __launch_bounds__(256) k_smooth_move_grp(DMesh m, const int* __restrict__ list, int n,
-                                                         const int* off, int c, int* counters) {
+                                                         const int* off, int c, int* counters,
+                                                         ByteCount bc) {
   if (trn_failed(m)) return;
   if (off) {
     list += off[c];
@@ -339,20 +365,23 @@ __global__ void __launch_bounds__(256) k_smooth_move_grp(DMesh m, const int* __r
   const long long g0 = ((long long) blockIdx.x * blockDim.x + threadIdx.x) / G;
   const long long gs = ((long long) gridDim.x * blockDim.x) / G;
   int tasks = 0, commit = 0;
+  unsigned long long bytes = 0;
   for (long long q = g0; q < n; q += gs) {
     const int v = list[q];
     if (v < 0 || v >= m.capa_node) {
       if (lane == 0) trn_set_error(m.err, TRN_DERR_REPLAY);
       continue;
     }
-    if (!m.activ[v]) continue;
-    if (m.vdeg[v] == 0) continue;
+    const bool moved = m.activ[v] && m.vdeg[v] != 0;
+    if (bc.bytes && lane == 0) bytes += smooth_bytes<F32>(m, v, moved, bc.seen);
+    if (!moved) continue;
     tasks++;
     commit += move_laplacian_grp<F32, G>(m, v, lane, gmask);
   }
   if (lane == 0) {
     if (tasks) atomicAdd(counters, tasks);
     if (commit) atomicAdd(counters + 1, commit);
+    if (bytes) atomicAdd(bc.bytes, bytes);
   }
 }
 
@@ -376,11 +405,11 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
   const int lanes = tune().smooth_lanes;
   const int g = grid_for((long long) hint * lanes, t);
   if (lanes == 8) {
-    if (fp32) k_smooth_move_grp<true, 8><<<g, t, 0, s>>>(m, list, n, off, c, counters);
-    else k_smooth_move_grp<false, 8><<<g, t, 0, s>>>(m, list, n, off, c, counters);
+    if (fp32) k_smooth_move_grp<true, 8><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc);
+    else k_smooth_move_grp<false, 8><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc);
   } else if (lanes == 4) {
-    if (fp32) k_smooth_move_grp<true, 4><<<g, t, 0, s>>>(m, list, n, off, c, counters);
-    else k_smooth_move_grp<false, 4><<<g, t, 0, s>>>(m, list, n, off, c, counters);
+    if (fp32) k_smooth_move_grp<true, 4><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc);
+    else k_smooth_move_grp<false, 4><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc);
   } else {
     /* element-metric slots a thread: what 40 KB of shared memory a block
      * holds, at most 8 (FP64) or 12 (FP32) */
