@@ -4,6 +4,7 @@ stage (metric tensors and points, element array, vertex liveness and tags)."""
 import json
 import os
 
+import numpy as np
 import pytest
 
 from tests.helpers import gpu_mesh, gpu_state, oracle_run, run_gpu_stages
@@ -86,3 +87,37 @@ def test_replay_full_size_workload_matches_reference_digests(oracle_built):
     run_gpu_stages(g, c, check)
     g.close()
     assert len(seen) == 1 + 4 * c["rounds"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,n", [("c1", None), ("c2", 120)])
+def test_free_swap_matching_is_the_oracle_interleaved_greedy(oracle_built, name, n):
+    """The free mode's swap matching computes the reference's greedy loop over
+    the candidates in the order (id mod 4, id) exactly: from the same state
+    (the oracle's decisions replayed through the metric, refinement and
+    coarsening of the first round), a free-mode swap stage ends bit-identical
+    to the oracle's swap stage run with that rule (ORC_SWAP_GREEDY_INTERLEAVED),
+    every level's candidates, rows, matching and flips included."""
+    from trinity_b200.api import Coarse, Metrics, Partit, Refine, Swap
+    m, u, c = meshgen.make_config(name, n)
+    c = dict(c, rounds=1)
+    o = Oracle(m, u, capa_scale=9, bucket=c["bucket"])
+    o.metric(c["target"], c["norm"])
+    o.refine(c["depth"])
+    o.coarsen()
+    log = o.log()
+    o.set_swap_rule("greedy_interleaved")
+    o.swap()
+    want = o.state()
+    g = gpu_mesh(m, u, c)
+    g.set_replay(log)
+    heur = Partit(g, 8)
+    Metrics(g, c["target"], c["norm"]).run()
+    Refine(g, c["depth"]).run()
+    Coarse(g, heur).run()
+    g.set_replay(np.zeros(0, np.int32))   # free mode from here on
+    g.set_swap_match("greedy")
+    Swap(g).run()
+    d = gpu_state(g).diff(want)
+    assert not d, d
+    g.close()

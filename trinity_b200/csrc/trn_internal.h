@@ -221,9 +221,12 @@ struct HeurWs {
   uint8_t* state = nullptr;      /* per vertex / element */
   uint8_t* state2 = nullptr;     /* second buffer of the independent-set rounds */
   unsigned long long* prop = nullptr;
-  unsigned long long* prop2 = nullptr;   /* second key buffer of the greedy matching */
   int* choice = nullptr;
-  int* choice2 = nullptr;                /* second row list of the greedy matching */
+  int* choice2 = nullptr;    /* greedy matching: second front list */
+  int* ecnt = nullptr;       /* greedy matching: rows listing each element */
+  int4* erows = nullptr;     /*   and those rows */
+  int* pred = nullptr;       /*   per row: earlier rows not yet decided */
+  int* greedy_ran = nullptr; /*   which rounds ran on the grid */
   int* color = nullptr;
   int* mate = nullptr;
   uint32_t* rank = nullptr;      /* four flip ranks per swap dual row */
@@ -242,8 +245,8 @@ void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* d
                      const int* ntasks, const int* map, const uint32_t* rank, Seed seed, HeurWs& ws,
                      int* pairs, int* npairs, cudaStream_t s, long long bound = -1);
 /* the reference's greedy matching loop over the dual rows, in the order
- * (candidate id mod 4, candidate id), computed exactly by rounds of rows that
- * come first on all their elements; pairs as match_handshake */
+ * (candidate id mod 4, candidate id), computed exactly by rounds over the
+ * rows whose earlier neighbours have all decided; pairs as match_handshake */
 void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual_n, const int* ntasks,
                   const int* map, HeurWs& ws, int* pairs, int* npairs, cudaStream_t s,
                   long long bound = -1);
