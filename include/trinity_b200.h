@@ -185,13 +185,15 @@ int trn_smooth_gradient_run(trn_mesh* mesh, int max_colors, int steps, double ma
 /* Launch shapes (none changes a result): cfg[0] smoothing block (32..256),
  * cfg[1] collapse-target search block, cfg[2] lanes per vertex of the
  * grouped search (4, 8, 16), cfg[3] longest level list the grouped search
- * takes, cfg[4] flip block, cfg[5] lanes per smoothed vertex (1, 4, 8). Per mesh; a captured round is recaptured when
+ * takes, cfg[4] flip block, cfg[5] lanes per smoothed vertex (1, 4, 8),
+ * cfg[6] registers of the smoothing kernel (0: as many as it uses, up to
+ * 128; 1: capped for three 256-thread blocks per SM). Per mesh; a captured round is recaptured when
  * they change. trn_autotune chooses them on the loaded mesh by coordinate
  * descent over candidates, timing metric + `rounds` rounds from the input
  * (twice each, the faster counts), then reloads the mesh; meshes of similar
  * size can share the result through trn_set_tune. No counterpart in the
  * reference. */
-#define TRN_TUNE_N 6
+#define TRN_TUNE_N 7
 int trn_get_tune(trn_mesh* mesh, int cfg[TRN_TUNE_N]);
 int trn_set_tune(trn_mesh* mesh, const int cfg[TRN_TUNE_N]);
 int trn_autotune(trn_mesh* mesh, double target_factor, int lp_norm, double h_min, double h_max,

@@ -61,6 +61,8 @@ struct orc_mesh {
   int *map, *dual, *dual_n, *matched;
   signed char *visited, *degree;
   int swap_rule;      /* ORC_SWAP_*: the reference's matching, or an emulation */
+  int swap_strict_map; /* flips re-activate only rows of the current level */
+  int swap_nt;        /* rows of the current level */
   int *hs_mate, *hs_choice;
   uint64_t* hs_prop;
   /* Refine hashtable (hashtable.h) as an open-addressing map (min,max)->id */
@@ -1302,6 +1304,11 @@ static void match_handshake_emul(orc_mesh* m, int nt, int level) {
   }
 }
 
+int orc_set_swap_strict_map(orc_mesh* m, int on) {
+  m->swap_strict_map = on != 0;
+  return ORC_OK;
+}
+
 int orc_set_swap_rule(orc_mesh* m, int rule) {
   if (rule < ORC_SWAP_REFERENCE || rule > ORC_SWAP_GREEDY_INTERLEAVED) return ORC_ERR_INVALID;
   m->swap_rule = rule;
@@ -1351,7 +1358,11 @@ static int swap_pair(orc_mesh* m, int id1, int id2, int index) {
     int t = D(m, index)[a];
     if (m->activ[t] == 0) m->activ[t] = 1;
   }
-  if (m->map[id2] > -1) {
+  /* the reference follows the map even to a row of an earlier level of the
+   * call; with swap_strict_map (the GPU free mode's rule) only to a row of
+   * the current level */
+  if (m->map[id2] > -1 &&
+      (!m->swap_strict_map || (m->map[id2] < m->swap_nt && D(m, m->map[id2])[0] == id2))) {
     int x = m->map[id2];
     for (int a = 0; a < m->dual_n[x]; ++a) {
       int t = D(m, x)[a];
@@ -1456,7 +1467,10 @@ int orc_swap(orc_mesh* m) {
     for (int index = 0; index < list.n; ++index) {
       int k1 = D(m, index)[0];
       int k2 = m->matched[k1];
-      if (k2 > -1) commit += swap_pair(m, k1, k2, index);
+      if (k2 > -1) {
+        m->swap_nt = list.n;
+        commit += swap_pair(m, k1, k2, index);
+      }
     }
     commit_total += commit;
     fix_tagged(m);

@@ -78,6 +78,11 @@ enum {
   ORC_SWAP_GREEDY_INTERLEAVED = 4,
 };
 int orc_set_swap_rule(orc_mesh* m, int rule);
+/* flips re-activate the elements of their partner's row only when that row
+ * belongs to the current level (the GPU free mode's rule: its rows are
+ * numbered in append order, so a row index of an earlier level names an
+ * unrelated row); the reference follows any row the map names */
+int orc_set_swap_strict_map(orc_mesh* m, int on);
 
 const int32_t* orc_log(const orc_mesh* m, size_t* n);
 void orc_log_clear(orc_mesh* m);

@@ -57,6 +57,7 @@ def lib():
         L.orc_log.restype = ctypes.POINTER(ctypes.c_int32)
         L.orc_log_clear.argtypes = [vp]
         L.orc_set_swap_rule.argtypes = [vp, ip]
+        L.orc_set_swap_strict_map.argtypes = [vp, ip]
         L.orc_eigen.argtypes = [vp, vp, vp, vp]
         L.orc_interpolate.argtypes = [vp, vp, ip]
         L.orc_quality.argtypes = [vp] * 6
@@ -200,6 +201,10 @@ class Oracle:
         """Swap matching rule (analysis of the GPU free mode; "reference" is
         the reference's own)."""
         self._chk(self.L.orc_set_swap_rule(self.h, self.SWAP_RULES[rule]), "set_swap_rule")
+
+    def set_swap_strict_map(self, on: bool) -> None:
+        """Flips re-activate only rows of the current level (the GPU free mode's rule)."""
+        self._chk(self.L.orc_set_swap_strict_map(self.h, 1 if on else 0), "set_swap_strict_map")
 
     def log(self) -> np.ndarray:
         n = ctypes.c_size_t(0)

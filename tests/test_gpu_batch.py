@@ -14,6 +14,7 @@ def _load(m, u, p):
     g = Mesh((m.nb_nodes, m.nb_elems), p["bucket"], p["depth"], 0, p["rounds"],
              capa_scale=p["capa_scale"])
     g.load_arrays(m.points, m.tris, tags_of(m), u)
+    g.set_swap_match(p["swap_match"])
     return g
 
 
@@ -45,7 +46,8 @@ def test_batch_meshes_are_valid_and_match_the_reference_build(tmp_path):
     of the reference build's final triangle count and 1 point of its fraction
     of metric edge lengths in [1/sqrt 2, sqrt 2], each on the same input. (The
     smaller ones, coarse grids under steep shocks, end far from unit lengths
-    after 3 rounds of depth 1 in both codes.)"""
+    after 3 rounds of depth 1 in both codes.) The workload's swap matching is
+    the row-slot handshake (meshgen.BATCH_PARAMS)."""
     import os
     import subprocess
     from tests.helpers import in_range_fraction

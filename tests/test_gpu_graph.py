@@ -98,14 +98,15 @@ def test_graph_batch_equals_plain_batch():
 
 
 ODD_TUNE = dict(smooth_threads=64, filter_threads=512, group_lanes=4, group_max=65536, flip_threads=128,
-                smooth_lanes=4)
+                smooth_lanes=4, smooth_regs=0)
 
 
 @pytest.mark.parametrize("graph", [False, True])
 def test_launch_shapes_change_no_result(graph):
     m, u, c = meshgen.make_config("c2", 100)
     states = []
-    for cfg in (None, ODD_TUNE, dict(ODD_TUNE, group_lanes=16, group_max=0, smooth_threads=256, smooth_lanes=8)):
+    for cfg in (None, ODD_TUNE, dict(ODD_TUNE, group_lanes=16, group_max=0, smooth_threads=256, smooth_lanes=8),
+                dict(ODD_TUNE, smooth_lanes=1, smooth_regs=1)):
         g = gpu_mesh(m, u, c)
         if cfg:
             g.set_tune(cfg)

@@ -97,7 +97,9 @@ def test_free_swap_matching_is_the_oracle_interleaved_greedy(oracle_built, name,
     (the oracle's decisions replayed through the metric, refinement and
     coarsening of the first round), a free-mode swap stage ends bit-identical
     to the oracle's swap stage run with that rule (ORC_SWAP_GREEDY_INTERLEAVED),
-    every level's candidates, rows, matching and flips included."""
+    every level's candidates, rows, matching and flips included. The oracle
+    also takes the free mode's re-activation rule (a flip re-activates its
+    partner's row only when that row is of the current level)."""
     from trinity_b200.api import Coarse, Metrics, Partit, Refine, Swap
     m, u, c = meshgen.make_config(name, n)
     c = dict(c, rounds=1)
@@ -107,6 +109,7 @@ def test_free_swap_matching_is_the_oracle_interleaved_greedy(oracle_built, name,
     o.coarsen()
     log = o.log()
     o.set_swap_rule("greedy_interleaved")
+    o.set_swap_strict_map(True)
     o.swap()
     want = o.state()
     g = gpu_mesh(m, u, c)

@@ -203,7 +203,8 @@ class Mesh:
     def stream(self) -> int:
         return self._L.trn_mesh_stream(self.h)
 
-    TUNE_KEYS = ("smooth_threads", "filter_threads", "group_lanes", "group_max", "flip_threads", "smooth_lanes")
+    TUNE_KEYS = ("smooth_threads", "filter_threads", "group_lanes", "group_max", "flip_threads", "smooth_lanes",
+                 "smooth_regs")
 
     def get_tune(self) -> dict:
         a = np.zeros(len(self.TUNE_KEYS), dtype=np.int32)

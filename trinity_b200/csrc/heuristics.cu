@@ -374,7 +374,7 @@ void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* d
  * bin of the reference's, where a maximal handshake matching, which flips
  * more pairs, is a point and a half off. */
 constexpr int kGreedyRounds = 256;
-constexpr int kGreedyTail = 2048;   /* a front this short goes to the one-block rounds */
+constexpr int kGreedyTail = 4096;   /* a front this short goes to the one-block rounds */
 
 struct GreedyArgs {
   const int* dual;
@@ -382,9 +382,9 @@ struct GreedyArgs {
   const int* map;
   int* vis;         /* per element: -1 free, else taken */
   int* ecnt;        /* per element: rows listing it */
-  int4* erows;      /* per element: those rows (at most four) */
-  int* pred;        /* per row: earlier rows sharing an element, not yet decided */
-  int* list0;       /* fronts, even rounds */
+  int4* erows;      /* per element: those rows' candidates (at most four) */
+  int* pred;        /* per candidate element: earlier rows sharing an element, not yet decided */
+  int* list0;       /* fronts (candidate ids), even rounds */
   int* list1;
   int* cnt;         /* [3] front lengths, by round mod 3 */
   int* ran;         /* [kGreedyRounds] round r ran on the grid */
@@ -411,39 +411,43 @@ __device__ __forceinline__ void greedy_reset_item(const GreedyArgs& a, int i) {
   }
 }
 
-/* row i onto the lists of its elements */
+/* row i onto the lists of its elements; a row is named by its candidate
+ * element, whose id is also its key, so no list entry needs a second load */
 __device__ __forceinline__ void greedy_list_item(const GreedyArgs& a, int i, int* err) {
+  const int c = a.dual[i * 4];
   for (int q = 0; q < a.dual_n[i]; ++q) {
     const int e = a.dual[i * 4 + q];
     const int k = atomicAdd(a.ecnt + e, 1);
-    if (k < 4) reinterpret_cast<int*>(a.erows + e)[k] = i;
+    if (k < 4) reinterpret_cast<int*>(a.erows + e)[k] = c;
     else trn_set_error(err, TRN_DERR_INVALID);
   }
 }
 
-/* how many earlier rows row i waits for; true when none */
+/* how many earlier rows row i waits for (kept by its candidate); true when none */
 __device__ __forceinline__ bool greedy_pred_item(const GreedyArgs& a, int i) {
-  const unsigned long long ki = greedy_key(a.dual[i * 4]);
+  const int c = a.dual[i * 4];
+  const unsigned long long ki = greedy_key(c);
   int p = 0;
   for (int q = 0; q < a.dual_n[i]; ++q) {
     const int e = a.dual[i * 4 + q];
     const int n = min(a.ecnt[e], 4);
     const int4 r = a.erows[e];
     for (int k = 0; k < n; ++k) {
-      const int j = erow_at(r, k);
-      if (j != i && greedy_key(a.dual[j * 4]) < ki) ++p;
+      const int cj = erow_at(r, k);
+      if (cj != c && greedy_key(cj) < ki) ++p;
     }
   }
-  a.pred[i] = p;
+  a.pred[c] = p;
   return p == 0;
 }
 
-/* decide row i (all its earlier neighbours have), then count down its later
- * neighbours; push(j) puts a row whose count reaches zero on the next front */
+/* decide the row of candidate c (all its earlier neighbours have), then
+ * count down its later neighbours; push(cj) puts a row whose count reaches
+ * zero on the next front */
 template <class Push>
-__device__ __forceinline__ void greedy_decide(const GreedyArgs& a, int i, int* pairs, int* npairs,
+__device__ __forceinline__ void greedy_decide(const GreedyArgs& a, int c, int* pairs, int* npairs,
                                               Push push) {
-  const int c = a.dual[i * 4];
+  const int i = a.map[c];
   const int dn = a.dual_n[i];
   if (a.vis[c] == -1) {
     a.vis[c] = 1;
@@ -467,8 +471,8 @@ __device__ __forceinline__ void greedy_decide(const GreedyArgs& a, int i, int* p
     const int n = min(a.ecnt[e], 4);
     const int4 r = a.erows[e];
     for (int k = 0; k < n; ++k) {
-      const int j = erow_at(r, k);
-      if (j != i && greedy_key(a.dual[j * 4]) > ki && atomicSub(a.pred + j, 1) == 1) push(j);
+      const int cj = erow_at(r, k);
+      if (cj != c && greedy_key(cj) > ki && atomicSub(a.pred + cj, 1) == 1) push(cj);
     }
   }
 }
@@ -490,7 +494,7 @@ __global__ void k_greedy_start(GreedyArgs a, const int* ntasks_dev, int min_n) {
   const int ntasks = *ntasks_dev;
   if (ntasks < min_n) return;
   for (int i = trn_tid(); i < ntasks; i += trn_grid_stride())
-    if (greedy_pred_item(a, i)) trn_append(a.list0, a.cnt, i);
+    if (greedy_pred_item(a, i)) trn_append(a.list0, a.cnt, a.dual[i * 4]);
 }
 
 /* round r on the grid, while the front holds more than kGreedyTail rows and
@@ -528,7 +532,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_greedy_tail(GreedyArgs a, con
     for (int i = threadIdx.x; i < ntasks; i += blockDim.x) greedy_list_item(a, i, err);
     __syncthreads();
     for (int i = threadIdx.x; i < ntasks; i += blockDim.x)
-      if (greedy_pred_item(a, i)) a.list0[atomicAdd(a.cnt, 1)] = i;
+      if (greedy_pred_item(a, i)) a.list0[atomicAdd(a.cnt, 1)] = a.dual[i * 4];
     if (threadIdx.x == 0) s_r = 0;
   } else if (threadIdx.x == 0) {
     int r = 0;
@@ -560,14 +564,15 @@ void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual
     check_launch("match_greedy");
     return;
   }
-  /* grid rounds for a list the host knows, or may, be long: about two
-   * rounds per halving of the list down to kGreedyTail rows (measured on
-   * the 2M-triangle workload), at most 24 */
+  /* grid rounds, each a launch that returns at once when the front is
+   * short: three per two halvings of the list bound down to kGreedyTail
+   * rows (on the 2M-triangle workload the fronts of the first level stay
+   * above 4,096 rows for about 16 rounds), at most 24 */
   int rounds = 24;
   if (bound >= 0) {
-    rounds = 4;
-    for (long long n = bound; n > kGreedyTail; n /= 2) rounds += 2;
-    rounds = std::min(rounds, 24);
+    int halvings = 0;
+    for (long long n = bound; n > kGreedyTail; n /= 2) ++halvings;
+    rounds = std::min((3 * halvings + 1) / 2, 24);
   }
   const int g = grid_bounded(bound, nb_elems);
   const int min_n = bound < 0 ? kFusedThreads + 1 : 0;

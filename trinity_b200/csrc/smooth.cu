@@ -161,10 +161,12 @@ __device__ unsigned long long smooth_bytes(const DMesh& m, int v, bool moved, un
   return b;
 }
 
-template <bool F32>
-__global__ void __launch_bounds__(256, 3) k_smooth_move(DMesh m, const int* __restrict__ list, int n,
-                                                       const int* off, int c, int* counters, int kj,
-                                                       ByteCount bc) {
+/* Tight: registers capped for three 256-thread blocks per SM (more warps to
+ * hide the gathers' latency, some spills); else up to 128 (two blocks) */
+template <bool F32, bool Tight>
+__global__ void __launch_bounds__(256, Tight ? 3 : 2) k_smooth_move(DMesh m, const int* __restrict__ list,
+                                                                   int n, const int* off, int c, int* counters,
+                                                                   int kj, ByteCount bc) {
   extern __shared__ __align__(16) unsigned char smooth_smem[];
   JmT<F32>* jc = reinterpret_cast<JmT<F32>*>(smooth_smem) + threadIdx.x;
   if (trn_failed(m)) return;
@@ -351,10 +353,10 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
   return valid ? 1 : 0;
 }
 
-template <bool F32, int G>
-__global__ void __launch_bounds__(256) k_smooth_move_grp(DMesh m, const int* __restrict__ list, int n,
-                                                         const int* off, int c, int* counters,
-                                                         ByteCount bc) {
+template <bool F32, int G, bool Tight>
+__global__ void __launch_bounds__(256, Tight ? 3 : 1) k_smooth_move_grp(DMesh m, const int* __restrict__ list,
+                                                                       int n, const int* off, int c,
+                                                                       int* counters, ByteCount bc) {
   if (trn_failed(m)) return;
   if (off) {
     list += off[c];
@@ -404,20 +406,27 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
   const int t = tune().smooth_threads;
   const int lanes = tune().smooth_lanes;
   const int g = grid_for((long long) hint * lanes, t);
-  if (lanes == 8) {
-    if (fp32) k_smooth_move_grp<true, 8><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc);
-    else k_smooth_move_grp<false, 8><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc);
-  } else if (lanes == 4) {
-    if (fp32) k_smooth_move_grp<true, 4><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc);
-    else k_smooth_move_grp<false, 4><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc);
+  const bool tight = tune().smooth_regs != 0;
+  if (lanes == 8 || lanes == 4) {
+#define TRN_GRP(F, G, T) k_smooth_move_grp<F, G, T><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc)
+    if (lanes == 8) {
+      if (fp32) { if (tight) TRN_GRP(true, 8, true); else TRN_GRP(true, 8, false); }
+      else { if (tight) TRN_GRP(false, 8, true); else TRN_GRP(false, 8, false); }
+    } else {
+      if (fp32) { if (tight) TRN_GRP(true, 4, true); else TRN_GRP(true, 4, false); }
+      else { if (tight) TRN_GRP(false, 4, true); else TRN_GRP(false, 4, false); }
+    }
+#undef TRN_GRP
   } else {
     /* element-metric slots a thread: what 40 KB of shared memory a block
      * holds, at most 8 (FP64) or 12 (FP32) */
     const int slot = fp32 ? (int) sizeof(float4) : (int) sizeof(double4);
     const int kj = std::min(fp32 ? 12 : 8, (40 << 10) / (t * slot));
     const size_t smem = (size_t) kj * t * slot;
-    if (fp32) k_smooth_move<true><<<g, t, smem, s>>>(m, list, n, off, c, counters, kj, bc);
-    else k_smooth_move<false><<<g, t, smem, s>>>(m, list, n, off, c, counters, kj, bc);
+#define TRN_ONE(F, T) k_smooth_move<F, T><<<g, t, smem, s>>>(m, list, n, off, c, counters, kj, bc)
+    if (fp32) { if (tight) TRN_ONE(true, true); else TRN_ONE(true, false); }
+    else { if (tight) TRN_ONE(false, true); else TRN_ONE(false, false); }
+#undef TRN_ONE
   }
   note_launch();
   check_launch("smooth_move");

@@ -972,9 +972,11 @@ void enq_swap_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphCondi
   uint32_t* rank = m->swap_match == TRN_SWAP_GAIN ? m->hws.rank : nullptr;
   swap_filter_dual(dl, act_list(m, 0), m->status + S_ACT, m->dual, m->dual_n, m->map, rank,
                    m->status + S_NTASK, m->fp32, s, bound);
+  /* a captured round knows no list length, but the capacity bounds it and
+   * sizes the matching's rounds for the mesh at hand */
   if (m->swap_match == TRN_SWAP_GREEDY)
     match_greedy(dl, m->capa_elem, m->dual, m->dual_n, m->status + S_NTASK, m->map, m->hws, m->pairs,
-                 m->status + S_NPAIRS, s, bound);
+                 m->status + S_NPAIRS, s, bound < 0 ? (long long) m->capa_elem : bound);
   else
     match_handshake(dl, m->capa_elem, m->dual, m->dual_n, m->status + S_NTASK, m->map, rank,
                     seed_of(m, 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s, bound);
@@ -1357,6 +1359,7 @@ int trn_get_tune(trn_mesh* m, int cfg[TRN_TUNE_N]) {
   cfg[3] = t.group_max;
   cfg[4] = t.flip_threads;
   cfg[5] = t.smooth_lanes;
+  cfg[6] = t.smooth_regs;
   return TRN_OK;
 }
 
@@ -1364,7 +1367,8 @@ int trn_set_tune(trn_mesh* m, const int cfg[TRN_TUNE_N]) {
   if (!m || !cfg) return TRN_ERR_INVALID;
   auto pow2_in = [](int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; };
   if (!pow2_in(cfg[0], 32, 256) || !pow2_in(cfg[1], 32, 1024) || (cfg[2] != 4 && cfg[2] != 8 && cfg[2] != 16) ||
-      cfg[3] < 0 || !pow2_in(cfg[4], 32, 1024) || (cfg[5] != 1 && cfg[5] != 4 && cfg[5] != 8))
+      cfg[3] < 0 || !pow2_in(cfg[4], 32, 1024) || (cfg[5] != 1 && cfg[5] != 4 && cfg[5] != 8) ||
+      (cfg[6] != 0 && cfg[6] != 1))
     return fail(m, TRN_ERR_INVALID, "set_tune: value out of range");
   m->tune.smooth_threads = cfg[0];
   m->tune.filter_threads = cfg[1];
@@ -1372,6 +1376,7 @@ int trn_set_tune(trn_mesh* m, const int cfg[TRN_TUNE_N]) {
   m->tune.group_max = cfg[3];
   m->tune.flip_threads = cfg[4];
   m->tune.smooth_lanes = cfg[5];
+  m->tune.smooth_regs = cfg[6];
   return TRN_OK;
 }
 
@@ -1408,10 +1413,11 @@ int trn_autotune(trn_mesh* m, double target_factor, int norm, double h_min, doub
     *out = best;
     return TRN_OK;
   };
-  int* fields[TRN_TUNE_N] = {&m->tune.smooth_lanes, &m->tune.smooth_threads, &m->tune.filter_threads,
-                             &m->tune.group_lanes, &m->tune.group_max, &m->tune.flip_threads};
+  int* fields[TRN_TUNE_N] = {&m->tune.smooth_lanes, &m->tune.smooth_threads, &m->tune.smooth_regs,
+                             &m->tune.filter_threads, &m->tune.group_lanes, &m->tune.group_max,
+                             &m->tune.flip_threads};
   const std::vector<std::vector<int>> cands = {
-      {1, 4, 8}, {64, 128, 256}, {128, 256, 512}, {4, 8, 16}, {4096, 16384, 65536}, {128, 256, 512}};
+      {1, 4, 8}, {64, 128, 256}, {0, 1}, {128, 256, 512}, {4, 8, 16}, {4096, 16384, 65536}, {128, 256, 512}};
   for (int f = 0; f < TRN_TUNE_N && rc == TRN_OK; ++f) {
     int best_v = *fields[f];
     double best_ms = 1e300;
