@@ -615,40 +615,89 @@ __global__ void k_color_init(DMesh m, int nb_nodes, int* list, int* n, int* colo
   }
 }
 
+/* one vertex of a round: true when it must wait (a neighbour still
+ * competing has a higher priority), else it takes the smallest color unused
+ * by neighbours colored in earlier rounds */
+__device__ __forceinline__ bool color_item(const DMesh& m, int v, int* color, int max_col, uint64_t seed,
+                                           int round) {
+  const uint64_t pv = trn_prio(seed, v);
+  const int* vc = m.vic + (size_t) v * m.bucket;
+  const int nv = m.vdeg[v];
+  unsigned used = 0;
+  for (int b = 0; b < nv; ++b) {
+    const int w = vc[b];
+    const int cw = *(volatile int*) (color + w);
+    const int rw = cw >> 8;
+    if (cw == 0 || rw == round + 1) {
+      if (trn_prio(seed, w) > pv) return true;
+    } else {
+      used |= 1u << (cw & 0xff & 31);
+    }
+  }
+  int c = 1;
+  while (c <= max_col && (used & (1u << c))) ++c;
+  color[v] = ((round + 1) << 8) | (c <= max_col ? c : 0xff);
+  return false;
+}
+
+/* a list this short goes to the one-block rounds (k_color_tail) */
+constexpr int kColorTail = 4096;
+
 /* one round over the still-uncolored vertices; those that must wait go to the
- * next list. A vertex takes the smallest color unused by neighbours colored in
- * earlier rounds once its priority beats every neighbour still competing
- * (uncolored, or colored in this very round) */
+ * next list. A vertex takes the smallest color unused by neighbours colored
+ * in earlier rounds once its priority beats every neighbour still competing
+ * (uncolored, or colored in this very round). A list of at most kColorTail
+ * vertices is left to the one-block tail: the round marks the coloring
+ * frozen (1 + the list's buffer) and it and the later rounds of the batch do
+ * nothing. */
 __global__ void k_color_round(DMesh m, const int* __restrict__ list, const int* n_in, int* color,
-                              int max_col, Seed sd, const int* round_ctr, int* next, int* n_next) {
-  if (trn_failed(m)) return;
+                              int max_col, Seed sd, const int* round_ctr, int* next, int* n_next,
+                              int* frozen, int cur) {
+  if (trn_failed(m) || *frozen) return;
   const int n = *n_in;
+  if (n <= kColorTail) {
+    if (trn_tid() == 0) *frozen = 1 + cur;
+    return;
+  }
   const uint64_t seed = trn_seed(sd);
   const int round = *round_ctr;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
     const int v = list[q];
-    const uint64_t pv = trn_prio(seed, v);
-    const int* vc = m.vic + (size_t) v * m.bucket;
-    const int nv = m.vdeg[v];
-    bool is_max = true;
-    unsigned used = 0;
-    for (int b = 0; b < nv; ++b) {
-      const int w = vc[b];
-      const int cw = *(volatile int*) (color + w);
-      const int rw = cw >> 8;
-      if (cw == 0 || rw == round + 1) {
-        if (trn_prio(seed, w) > pv) { is_max = false; break; }
-      } else {
-        used |= 1u << (cw & 0xff & 31);
-      }
+    if (color_item(m, v, color, max_col, seed, round)) trn_append(next, n_next, v);
+  }
+}
+
+/* the rounds left, in one block, from the frozen list: until no vertex
+ * waits (at most kColorTailRounds rounds; a vertex still waiting then is
+ * not smoothed, like one that finds no free color) */
+constexpr int kColorTailRounds = 512;
+
+__global__ void __launch_bounds__(1024) k_color_tail(DMesh m, int* list_a, int* list_b, int* counts, int* color,
+                                                     int max_col, Seed sd, int* round_ctr, int* frozen) {
+  const int f = *frozen;
+  if (trn_failed(m) || f == 0) return;
+  const uint64_t seed = trn_seed(sd);
+  int cur = f - 1;
+  int round = *round_ctr;
+  for (int it = 0; it < kColorTailRounds; ++it) {
+    const int n = counts[cur];
+    if (n == 0) break;
+    int* in = cur ? list_b : list_a;
+    int* out = cur ? list_a : list_b;
+    if (it > 0) ++round;
+    if (threadIdx.x == 0) counts[cur ^ 1] = 0;
+    __syncthreads();
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+      const int v = in[q];
+      if (color_item(m, v, color, max_col, seed, round)) out[atomicAdd(counts + (cur ^ 1), 1)] = v;
     }
-    if (!is_max) {
-      trn_append(next, n_next, v);
-      continue;
-    }
-    int c = 1;
-    while (c <= max_col && (used & (1u << c))) ++c;
-    color[v] = ((round + 1) << 8) | (c <= max_col ? c : 0xff);
+    __syncthreads();
+    cur ^= 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *round_ctr = round;
+    counts[0] = counts[1] = 0;   /* done: the batch's end sees nothing left */
   }
 }
 
@@ -680,9 +729,10 @@ __global__ void k_color_count(DMesh m, int nb_nodes, const int* color, int* cnt,
     if (sc[k]) atomicAdd(cnt + k, sc[k]);
 }
 
-/* before a round: its number, and the list it fills starts empty */
-__global__ void k_color_step(int* round_ctr, int* n_next) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+/* before a round: its number, and the list it fills starts empty (nothing
+ * once the coloring is frozen for the tail) */
+__global__ void k_color_step(int* round_ctr, int* n_next, const int* frozen) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || *frozen) return;
   *round_ctr += 1;
   *n_next = 0;
 }
@@ -746,6 +796,7 @@ static int* color_counts(HeurWs& ws) { return ws.cnt + 80; }   /* two list count
 static int* color_round(HeurWs& ws) { return ws.cnt + 82; }
 static int* color_batch_no(HeurWs& ws) { return ws.cnt + 83; }
 int* color_cont(HeurWs& ws) { return ws.cnt + 84; }
+static int* color_frozen(HeurWs& ws) { return ws.cnt + 85; }
 
 void color_begin(const DMesh& m, int hint, HeurWs& ws, cudaStream_t s) {
   ProfScope ps("color_jp", s, 0.0);
@@ -753,6 +804,7 @@ void color_begin(const DMesh& m, int hint, HeurWs& ws, cudaStream_t s) {
   cudaMemsetAsync(counts, 0, sizeof(int) * 2, s);
   cudaMemsetAsync(color_round(ws), 0xff, sizeof(int), s);   /* -1: the first step makes it 0 */
   cudaMemsetAsync(color_batch_no(ws), 0, sizeof(int), s);
+  cudaMemsetAsync(color_frozen(ws), 0, sizeof(int), s);
   k_color_init<<<grid_for(hint), TRN_THREADS, 0, s>>>(m, hint, ws.list_a, counts, ws.color);
   note_launch();
 }
@@ -765,12 +817,16 @@ void color_batch(const DMesh& m, int hint, int max_col, Seed sd, HeurWs& ws, cud
   int* counts = color_counts(ws);
   for (int r = 0; r < 8; ++r) {
     const int cur = r & 1;
-    k_color_step<<<1, 32, 0, s>>>(color_round(ws), counts + (cur ^ 1));
+    k_color_step<<<1, 32, 0, s>>>(color_round(ws), counts + (cur ^ 1), color_frozen(ws));
     note_launch();
     k_color_round<<<g, TRN_THREADS, 0, s>>>(m, lists[cur], counts + cur, ws.color, max_col, sd,
-                                            color_round(ws), lists[cur ^ 1], counts + (cur ^ 1));
+                                            color_round(ws), lists[cur ^ 1], counts + (cur ^ 1),
+                                            color_frozen(ws), cur);
     note_launch();
   }
+  k_color_tail<<<1, 1024, 0, s>>>(m, ws.list_a, ws.list_b, counts, ws.color, max_col, sd, color_round(ws),
+                                  color_frozen(ws));
+  note_launch();
   /* an even number of rounds: the vertices still waiting are in list_a */
   k_color_batch_end<<<1, 32, 0, s>>>(counts, color_batch_no(ws), color_cont(ws), h, use_h ? 1 : 0);
   note_launch();
