@@ -186,8 +186,8 @@ int trn_smooth_gradient_run(trn_mesh* mesh, int max_colors, int steps, double ma
  * cfg[1] collapse-target search block, cfg[2] lanes per vertex of the
  * grouped search (4, 8, 16), cfg[3] longest level list the grouped search
  * takes, cfg[4] flip block, cfg[5] lanes per smoothed vertex (1, 4, 8),
- * cfg[6] registers of the smoothing kernel (0: as many as it uses, up to
- * 128; 1: capped for three 256-thread blocks per SM). Per mesh; a captured round is recaptured when
+ * cfg[6] registers of the smoothing kernel (0: up to 128, two 256-thread
+ * blocks per SM; 1: capped for three). Per mesh; a captured round is recaptured when
  * they change. trn_autotune chooses them on the loaded mesh by coordinate
  * descent over candidates, timing metric + `rounds` rounds from the input
  * (twice each, the faster counts), then reloads the mesh; meshes of similar

@@ -353,128 +353,101 @@ void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* d
  * degree-1 stack, over the rows in the order (id mod 4, id): four
  * interleaved sweeps of the candidate ids.
  *
- * Its result is computed exactly, in parallel, as a dependency schedule: a
- * row's outcome depends only on the rows before it in that order that list
- * one of its elements (an element is listed by at most four rows: its own
- * and those of up to three adjacent candidates). Each element keeps the
- * rows that list it; each row counts the earlier rows it shares an element
- * with; the rows with no earlier neighbour form the first front. A round
- * decides every row of the front — they share no element, so they decide
- * independently, and what each finds is what the sequential loop would
- * have found — and counts down its later neighbours, which join the next
- * front when their count reaches zero. One launch per round over the front
- * only; once the front is short one block runs the remaining rounds with
- * block barriers. After kGreedyRounds rounds any row still waiting stays
- * unmatched (a valid, if not maximal, matching). On the 2M-triangle
- * workload the deepest level needs 48 rounds, the mean is 12.
+ * Its result is computed exactly, in parallel, as the greedy matching of an
+ * order is: in each round a row decides once it comes first, under that
+ * order, among the undecided rows that list any of its elements; such rows
+ * share no element with one another, so they decide independently, and what
+ * each finds is what the sequential loop would have found. Rows propose
+ * their key with a 64-bit atomicMin on every element of their row into the
+ * round's buffer (keys of later rounds compare lower, so no buffer needs
+ * clearing between rounds); a row is ready when every element holds its own
+ * key. A round decides the ready rows and lets the others propose for the
+ * next round into the other buffer, so one launch per round. The rounds
+ * run over a compacted list of the undecided rows; once that list is short
+ * one block finishes the remaining rounds with block barriers. After
+ * kGreedyRounds rounds any row still undecided stays unmatched (a valid, if
+ * not maximal, matching). On the 2M-triangle workload the deepest level
+ * needs 48 rounds, the mean is 12.
  *
  * The four-way interleave keeps the chains of dependent rows short (a plain
  * increasing-id sweep has chains as long as a row of the grid), and the
  * final meshes' metric edge-length histograms stay within half a point per
  * bin of the reference's, where a maximal handshake matching, which flips
  * more pairs, is a point and a half off. */
-constexpr int kGreedyRounds = 256;
-constexpr int kGreedyTail = 4096;   /* a front this short goes to the one-block rounds */
+constexpr int kGreedyRounds = 64;
+constexpr int kGreedyTail = 2048;   /* undecided rows left to the one-block rounds */
 
 struct GreedyArgs {
   const int* dual;
   const int* dual_n;
   const int* map;
-  int* vis;         /* per element: -1 free, else taken */
-  int* ecnt;        /* per element: rows listing it */
-  int4* erows;      /* per element: those rows' candidates (at most four) */
-  int* pred;        /* per candidate element: earlier rows sharing an element, not yet decided */
-  int* list0;       /* fronts (candidate ids), even rounds */
+  int* vis;                 /* per element: -1 free, else taken */
+  unsigned long long* mk0;  /* per element: lowest key proposed, even rounds */
+  unsigned long long* mk1;  /* odd rounds */
+  int* list0;               /* undecided rows, even rounds */
   int* list1;
-  int* cnt;         /* [3] front lengths, by round mod 3 */
-  int* ran;         /* [kGreedyRounds] round r ran on the grid */
+  int* cnt;                 /* [3] list lengths, by round mod 3 */
+  int* ran;                 /* [kGreedyRounds] round r ran on the grid */
 };
 
-__device__ __forceinline__ unsigned long long greedy_key(int c) {
-  return ((unsigned long long) (c & 3) << 32) | (uint32_t) c;
+__device__ __forceinline__ unsigned long long greedy_key(int r, int c) {
+  return ((unsigned long long) (kGreedyRounds - r) << 40) | ((unsigned long long) (c & 3) << 32) |
+         (uint32_t) c;
 }
 
 /* "is a candidate" as matching.cpp:124 asks it: the element has a row in the
  * map, which keeps the rows of earlier levels of the same call (it is reset
  * once per call, swapping.cpp:161-162) */
-__device__ __forceinline__ bool greedy_is_row(const GreedyArgs& a, int e) { return a.map[e] >= 0; }
-
-__device__ __forceinline__ int erow_at(int4 r, int k) {
-  return k == 0 ? r.x : k == 1 ? r.y : k == 2 ? r.z : r.w;
+__device__ __forceinline__ bool greedy_is_row(const GreedyArgs& a, int ntasks, int e) {
+  (void) ntasks;
+  return a.map[e] >= 0;
 }
 
 __device__ __forceinline__ void greedy_reset_item(const GreedyArgs& a, int i) {
   for (int q = 0; q < a.dual_n[i]; ++q) {
     const int e = a.dual[i * 4 + q];
     a.vis[e] = -1;
-    a.ecnt[e] = 0;
+    a.mk0[e] = ~0ULL;
+    a.mk1[e] = ~0ULL;
   }
 }
 
-/* row i onto the lists of its elements; a row is named by its candidate
- * element, whose id is also its key, so no list entry needs a second load */
-__device__ __forceinline__ void greedy_list_item(const GreedyArgs& a, int i, int* err) {
+__device__ __forceinline__ void greedy_propose(const GreedyArgs& a, int r, int i) {
+  unsigned long long* mk = (r & 1) ? a.mk1 : a.mk0;
+  const unsigned long long key = greedy_key(r, a.dual[i * 4]);
+  for (int q = 0; q < a.dual_n[i]; ++q) atomicMin(mk + a.dual[i * 4 + q], key);
+}
+
+/* row i in round r: decide it when it is first on all its elements (and
+ * return false), else propose it for round r + 1 (and return true) */
+__device__ __forceinline__ bool greedy_item(const GreedyArgs& a, int ntasks, int r, int i, int* pairs,
+                                            int* npairs) {
+  const unsigned long long* mk = (r & 1) ? a.mk1 : a.mk0;
   const int c = a.dual[i * 4];
-  for (int q = 0; q < a.dual_n[i]; ++q) {
-    const int e = a.dual[i * 4 + q];
-    const int k = atomicAdd(a.ecnt + e, 1);
-    if (k < 4) reinterpret_cast<int*>(a.erows + e)[k] = c;
-    else trn_set_error(err, TRN_DERR_INVALID);
-  }
-}
-
-/* how many earlier rows row i waits for (kept by its candidate); true when none */
-__device__ __forceinline__ bool greedy_pred_item(const GreedyArgs& a, int i) {
-  const int c = a.dual[i * 4];
-  const unsigned long long ki = greedy_key(c);
-  int p = 0;
-  for (int q = 0; q < a.dual_n[i]; ++q) {
-    const int e = a.dual[i * 4 + q];
-    const int n = min(a.ecnt[e], 4);
-    const int4 r = a.erows[e];
-    for (int k = 0; k < n; ++k) {
-      const int cj = erow_at(r, k);
-      if (cj != c && greedy_key(cj) < ki) ++p;
-    }
-  }
-  a.pred[c] = p;
-  return p == 0;
-}
-
-/* decide the row of candidate c (all its earlier neighbours have), then
- * count down its later neighbours; push(cj) puts a row whose count reaches
- * zero on the next front */
-template <class Push>
-__device__ __forceinline__ void greedy_decide(const GreedyArgs& a, int c, int* pairs, int* npairs,
-                                              Push push) {
-  const int i = a.map[c];
   const int dn = a.dual_n[i];
-  if (a.vis[c] == -1) {
-    a.vis[c] = 1;
-    int partner = -1;
-    for (int q = 1; q < dn; ++q) {
-      const int n = a.dual[i * 4 + q];
-      if (a.vis[n] != -1) continue;
-      a.vis[n] = 1;
-      partner = n;
-      if (greedy_is_row(a, n)) break;
-    }
-    if (partner >= 0) {
-      const int p = atomicAdd(npairs, 1);
-      pairs[2 * p] = c;
-      pairs[2 * p + 1] = partner;
-    }
+  const unsigned long long key = greedy_key(r, c);
+  bool ready = true;
+  for (int q = 0; q < dn; ++q) ready &= (mk[a.dual[i * 4 + q]] == key);
+  if (!ready) {
+    greedy_propose(a, r + 1, i);
+    return true;
   }
-  const unsigned long long ki = greedy_key(c);
-  for (int q = 0; q < dn; ++q) {
-    const int e = a.dual[i * 4 + q];
-    const int n = min(a.ecnt[e], 4);
-    const int4 r = a.erows[e];
-    for (int k = 0; k < n; ++k) {
-      const int cj = erow_at(r, k);
-      if (cj != c && greedy_key(cj) > ki && atomicSub(a.pred + cj, 1) == 1) push(cj);
-    }
+  if (a.vis[c] != -1) return false;
+  a.vis[c] = 1;
+  int partner = -1;
+  for (int q = 1; q < dn; ++q) {
+    const int n = a.dual[i * 4 + q];
+    if (a.vis[n] != -1) continue;
+    a.vis[n] = 1;
+    partner = n;
+    if (greedy_is_row(a, ntasks, n)) break;
   }
+  if (partner >= 0) {
+    const int p = atomicAdd(npairs, 1);
+    pairs[2 * p] = c;
+    pairs[2 * p + 1] = partner;
+  }
+  return false;
 }
 
 __global__ void k_greedy_reset(GreedyArgs a, const int* ntasks_dev, int min_n) {
@@ -483,57 +456,57 @@ __global__ void k_greedy_reset(GreedyArgs a, const int* ntasks_dev, int min_n) {
   for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) greedy_reset_item(a, i);
 }
 
-__global__ void k_greedy_list(GreedyArgs a, const int* ntasks_dev, int min_n, int* err) {
-  const int ntasks = *ntasks_dev;
-  if (ntasks < min_n) return;
-  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) greedy_list_item(a, i, err);
-}
-
-/* the counts, and the rows waiting for none: the first front */
+/* round 0's proposals; every row starts undecided */
 __global__ void k_greedy_start(GreedyArgs a, const int* ntasks_dev, int min_n) {
   const int ntasks = *ntasks_dev;
   if (ntasks < min_n) return;
-  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride())
-    if (greedy_pred_item(a, i)) trn_append(a.list0, a.cnt, a.dual[i * 4]);
+  if (trn_tid() == 0) a.cnt[0] = ntasks;
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
+    greedy_propose(a, 0, i);
+    a.list0[i] = i;
+  }
 }
 
-/* round r on the grid, while the front holds more than kGreedyTail rows and
+/* round r on the grid, while more than kGreedyTail rows are undecided and
  * every earlier round ran here */
-__global__ void k_greedy_round(GreedyArgs a, int r, int* pairs, int* npairs) {
+__global__ void k_greedy_round(GreedyArgs a, const int* ntasks_dev, int r, int* pairs, int* npairs) {
   if (r > 0 && !a.ran[r - 1]) return;
   const int n = a.cnt[r % 3];
   if (n <= kGreedyTail) return;
+  const int ntasks = *ntasks_dev;
   const int* in = (r & 1) ? a.list1 : a.list0;
   int* out = (r & 1) ? a.list0 : a.list1;
-  int* n_out = a.cnt + (r + 1) % 3;
   if (trn_tid() == 0) {
     a.ran[r] = 1;
     a.cnt[(r + 2) % 3] = 0;   /* round r + 1's output */
   }
-  for (int q = trn_tid(); q < n; q += trn_grid_stride())
-    greedy_decide(a, in[q], pairs, npairs, [&](int j) { out[atomicAdd(n_out, 1)] = j; });
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int i = in[q];
+    if (greedy_item(a, ntasks, r, i, pairs, npairs)) trn_append(out, a.cnt + (r + 1) % 3, i);
+  }
 }
 
-/* the remaining rounds in one block; with `whole`, the level's reset, lists
- * and first front too (a list the host knows to be short) */
+/* the remaining rounds in one block; with `whole`, the level's reset and
+ * first proposals too (a list the host knows to be short) */
 __global__ void __launch_bounds__(kFusedThreads) k_greedy_tail(GreedyArgs a, const int* ntasks_dev,
                                                                int* pairs, int* npairs, int whole,
-                                                               int lim, int* err) {
+                                                               int lim) {
   const int ntasks = *ntasks_dev;
   if (whole ? ntasks > lim : ntasks < lim) return;
   __shared__ int s_r;
   if (whole) {
-    if (threadIdx.x == 0) {
-      *npairs = 0;
-      a.cnt[0] = a.cnt[1] = a.cnt[2] = 0;
-    }
+    if (threadIdx.x == 0) *npairs = 0;
     for (int i = threadIdx.x; i < ntasks; i += blockDim.x) greedy_reset_item(a, i);
     __syncthreads();
-    for (int i = threadIdx.x; i < ntasks; i += blockDim.x) greedy_list_item(a, i, err);
-    __syncthreads();
-    for (int i = threadIdx.x; i < ntasks; i += blockDim.x)
-      if (greedy_pred_item(a, i)) a.list0[atomicAdd(a.cnt, 1)] = a.dual[i * 4];
-    if (threadIdx.x == 0) s_r = 0;
+    for (int i = threadIdx.x; i < ntasks; i += blockDim.x) {
+      greedy_propose(a, 0, i);
+      a.list0[i] = i;
+    }
+    if (threadIdx.x == 0) {
+      a.cnt[0] = ntasks;
+      a.cnt[1] = 0;
+      s_r = 0;
+    }
   } else if (threadIdx.x == 0) {
     int r = 0;
     while (r < kGreedyRounds && a.ran[r]) ++r;
@@ -545,56 +518,58 @@ __global__ void __launch_bounds__(kFusedThreads) k_greedy_tail(GreedyArgs a, con
     if (n == 0) break;
     const int* in = (r & 1) ? a.list1 : a.list0;
     int* out = (r & 1) ? a.list0 : a.list1;
-    int* n_out = a.cnt + (r + 1) % 3;
     if (threadIdx.x == 0) a.cnt[(r + 2) % 3] = 0;
-    for (int q = threadIdx.x; q < n; q += blockDim.x)
-      greedy_decide(a, in[q], pairs, npairs, [&](int j) { out[atomicAdd(n_out, 1)] = j; });
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+      const int i = in[q];
+      if (greedy_item(a, ntasks, r, i, pairs, npairs)) {
+        const int k = atomicAdd(a.cnt + (r + 1) % 3, 1);
+        out[k] = i;
+      }
+    }
     __syncthreads();
   }
 }
 
 void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual_n, const int* ntasks,
                   const int* map, HeurWs& ws, int* pairs, int* npairs, cudaStream_t s, long long bound) {
+  (void) m;
   ProfScope ps("match_greedy", s, 0.0);
-  const GreedyArgs a{dual, dual_n, map, ws.mate, ws.ecnt, ws.erows, ws.pred, ws.choice, ws.choice2,
-                     ws.cnt, ws.greedy_ran};
+  const GreedyArgs a{dual, dual_n, map, ws.mate, ws.prop, ws.prop2, ws.choice, ws.choice2, ws.cnt,
+                     ws.cnt + 8};
   if (bound >= 0 && bound <= kFusedThreads) {   /* known short: one block */
-    k_greedy_tail<<<1, kFusedThreads, 0, s>>>(a, ntasks, pairs, npairs, 1, kFusedThreads, m.err);
+    k_greedy_tail<<<1, kFusedThreads, 0, s>>>(a, ntasks, pairs, npairs, 1, kFusedThreads);
     note_launch();
     check_launch("match_greedy");
     return;
   }
-  /* grid rounds, each a launch that returns at once when the front is
-   * short: three per two halvings of the list bound down to kGreedyTail
-   * rows (on the 2M-triangle workload the fronts of the first level stay
-   * above 4,096 rows for about 16 rounds), at most 24 */
-  int rounds = 24;
+  /* grid rounds, each a launch that returns at once when few rows wait:
+   * about two per halving of the list bound down to kGreedyTail rows (on
+   * the 2M-triangle workload the first level has more than 2,048 rows
+   * waiting for 18 rounds), at most kGreedyRounds - 8 */
+  int rounds = kGreedyRounds - 8;
   if (bound >= 0) {
-    int halvings = 0;
-    for (long long n = bound; n > kGreedyTail; n /= 2) ++halvings;
-    rounds = std::min((3 * halvings + 1) / 2, 24);
+    rounds = 4;
+    for (long long n = bound; n > kGreedyTail; n /= 2) rounds += 2;
+    rounds = std::min(rounds, kGreedyRounds - 8);
   }
   const int g = grid_bounded(bound, nb_elems);
   const int min_n = bound < 0 ? kFusedThreads + 1 : 0;
   cudaMemsetAsync(npairs, 0, sizeof(int), s);
-  cudaMemsetAsync(ws.cnt, 0, sizeof(int) * 3, s);
-  cudaMemsetAsync(ws.greedy_ran, 0, sizeof(int) * kGreedyRounds, s);
+  cudaMemsetAsync(ws.cnt, 0, sizeof(int) * (8 + kGreedyRounds), s);
   k_greedy_reset<<<g, TRN_THREADS, 0, s>>>(a, ntasks, min_n);
-  note_launch();
-  k_greedy_list<<<g, TRN_THREADS, 0, s>>>(a, ntasks, min_n, m.err);
   note_launch();
   k_greedy_start<<<g, TRN_THREADS, 0, s>>>(a, ntasks, min_n);
   note_launch();
   for (int r = 0; r < rounds; ++r) {
-    k_greedy_round<<<g, TRN_THREADS, 0, s>>>(a, r, pairs, npairs);
+    k_greedy_round<<<g, TRN_THREADS, 0, s>>>(a, ntasks, r, pairs, npairs);
     note_launch();
   }
   /* the rounds left; when the list is unknown, the whole short-list form
    * too, each returning at once when the count is not its case */
-  k_greedy_tail<<<1, kFusedThreads, 0, s>>>(a, ntasks, pairs, npairs, 0, min_n, m.err);
+  k_greedy_tail<<<1, kFusedThreads, 0, s>>>(a, ntasks, pairs, npairs, 0, min_n);
   note_launch();
   if (bound < 0) {
-    k_greedy_tail<<<1, kFusedThreads, 0, s>>>(a, ntasks, pairs, npairs, 1, kFusedThreads, m.err);
+    k_greedy_tail<<<1, kFusedThreads, 0, s>>>(a, ntasks, pairs, npairs, 1, kFusedThreads);
     note_launch();
   }
   check_launch("match_greedy");
@@ -869,10 +844,7 @@ void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {
   cudaMalloc(&ws->prop, sizeof(unsigned long long) * (size_t) capa_elem);
   cudaMalloc(&ws->choice, sizeof(int) * (size_t) capa_elem);
   cudaMalloc(&ws->choice2, sizeof(int) * (size_t) capa_elem);
-  cudaMalloc(&ws->ecnt, sizeof(int) * (size_t) capa_elem);
-  cudaMalloc(&ws->erows, sizeof(int4) * (size_t) capa_elem);
-  cudaMalloc(&ws->pred, sizeof(int) * (size_t) capa_elem);
-  cudaMalloc(&ws->greedy_ran, sizeof(int) * 256);
+  cudaMalloc(&ws->prop2, sizeof(unsigned long long) * (size_t) capa_elem);
   cudaMalloc(&ws->color, sizeof(int) * (size_t) capa_node);
   cudaMemset(ws->color, 0, sizeof(int) * (size_t) capa_node);
   cudaMalloc(&ws->mate, sizeof(int) * (size_t) capa_elem);
@@ -890,10 +862,7 @@ void heur_ws_free(HeurWs* ws) {
   cudaFree(ws->prop);
   cudaFree(ws->choice);
   cudaFree(ws->choice2);
-  cudaFree(ws->ecnt);
-  cudaFree(ws->erows);
-  cudaFree(ws->pred);
-  cudaFree(ws->greedy_ran);
+  cudaFree(ws->prop2);
   cudaFree(ws->color);
   cudaFree(ws->mate);
   cudaFree(ws->rank);

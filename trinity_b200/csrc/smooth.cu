@@ -354,7 +354,7 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
 }
 
 template <bool F32, int G, bool Tight>
-__global__ void __launch_bounds__(256, Tight ? 3 : 1) k_smooth_move_grp(DMesh m, const int* __restrict__ list,
+__global__ void __launch_bounds__(256, Tight ? 3 : 2) k_smooth_move_grp(DMesh m, const int* __restrict__ list,
                                                                        int n, const int* off, int c,
                                                                        int* counters, ByteCount bc) {
   if (trn_failed(m)) return;

@@ -50,16 +50,18 @@ void level_end(int* status, int kind, int cap, const int* next, int* cur, int hi
                cudaGraphConditionalHandle h, bool use_h);
 
 /* launch shapes the autotuner (trn_autotune) chooses; none of them changes
- * a result. Each mesh keeps its own table; the C-ABI entry that drives a
- * mesh makes it the calling thread's table for the launchers. */
+ * a result. The defaults are the tuner's choice on the 2M-triangle workload
+ * (the smoothing by 4 lanes a vertex in 256-thread blocks). Each mesh keeps
+ * its own table; the C-ABI entry that drives a mesh makes it the calling
+ * thread's table for the launchers. */
 struct Tune {
-  int smooth_threads = 128;   /* k_smooth_move block: 64, 128, 256 */
+  int smooth_threads = 256;   /* k_smooth_move block: 64, 128, 256 */
   int filter_threads = 256;   /* one-lane collapse-target search block: 128, 256, 512 */
   int group_lanes = 8;        /* lanes per vertex of the grouped search: 4, 8, 16 */
   int group_max = 16384;      /* longest level list the grouped search takes */
   int flip_threads = 256;     /* k_swap_flip block: 128, 256, 512 */
-  int smooth_lanes = 1;       /* lanes per smoothed vertex: 1, 4, 8 */
-  int smooth_regs = 1;        /* smoothing registers: 0 as used (up to 128), 1 capped (80) */
+  int smooth_lanes = 4;       /* lanes per smoothed vertex: 1, 4, 8 */
+  int smooth_regs = 1;        /* smoothing registers: 0 up to 128, 1 capped at 80 (three 256-thread blocks) */
   bool operator==(const Tune& o) const {
     return smooth_threads == o.smooth_threads && filter_threads == o.filter_threads &&
            group_lanes == o.group_lanes && group_max == o.group_max && flip_threads == o.flip_threads &&
@@ -222,12 +224,9 @@ struct HeurWs {
   uint8_t* state = nullptr;      /* per vertex / element */
   uint8_t* state2 = nullptr;     /* second buffer of the independent-set rounds */
   unsigned long long* prop = nullptr;
+  unsigned long long* prop2 = nullptr;   /* second key buffer of the greedy matching */
   int* choice = nullptr;
-  int* choice2 = nullptr;    /* greedy matching: second front list */
-  int* ecnt = nullptr;       /* greedy matching: rows listing each element */
-  int4* erows = nullptr;     /*   and those rows */
-  int* pred = nullptr;       /*   per row: earlier rows not yet decided */
-  int* greedy_ran = nullptr; /*   which rounds ran on the grid */
+  int* choice2 = nullptr;                /* second row list of the greedy matching */
   int* color = nullptr;
   int* mate = nullptr;
   uint32_t* rank = nullptr;      /* four flip ranks per swap dual row */
@@ -246,8 +245,8 @@ void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* d
                      const int* ntasks, const int* map, const uint32_t* rank, Seed seed, HeurWs& ws,
                      int* pairs, int* npairs, cudaStream_t s, long long bound = -1);
 /* the reference's greedy matching loop over the dual rows, in the order
- * (candidate id mod 4, candidate id), computed exactly by rounds over the
- * rows whose earlier neighbours have all decided; pairs as match_handshake */
+ * (candidate id mod 4, candidate id), computed exactly by rounds of rows that
+ * come first on all their elements; pairs as match_handshake */
 void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual_n, const int* ntasks,
                   const int* map, HeurWs& ws, int* pairs, int* npairs, cudaStream_t s,
                   long long bound = -1);
