@@ -42,10 +42,11 @@ from trinity_b200 import meshgen  # noqa: E402
 
 WORKLOAD = "c2"
 # DRAM traffic per launch of the kernel that dominates the 2M-triangle step,
-# measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, caches kept
-# between launches, the 7 class launches of the timed step's first smoothing
-# pass); a live run has no hardware counters, so the figure is carried here
-MEASURED_TRAFFIC = {"smooth_move": 455.6e6}
+# measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, caches
+# flushed before each launch, 7 consecutive launches of the timed step's
+# first round, default launch shape); a live run has no hardware counters,
+# so the figure is carried here
+MEASURED_TRAFFIC = {"smooth_move": 442.8e6}
 METRIC = "adapted triangles/s per full round"
 UNIT = "triangles/s"
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "trinity_ref")
@@ -307,8 +308,8 @@ def b200_arm(args, rank, world, local_rank):
                     "peak": hbm_peak, "peak_source": "measured" if peaks else "fallback",
                     "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
                     "traffic": MEASURED_TRAFFIC.get(dom["kernel"]) if not args.grid else None,
-                    "traffic_note": "DRAM read + write bytes per launch, ncu on this workload with warm "
-                                    "caches (mean of the 7 class launches of the first pass)",
+                    "traffic_note": "DRAM read + write bytes per launch, ncu on this workload, caches flushed "
+                                    "before each launch (mean of 7 consecutive launches of the timed step)",
                     "launches": dom["launches"],
                     "avg_launch_us": round(per_launch_s * 1e6, 2),
                     "algorithmic_bytes_per_launch": round(per_launch_bytes),
