@@ -35,6 +35,85 @@
 
 namespace trn {
 
+/* ---------------- persistent rounds ----------------
+ * A round-synchronous heuristic runs as one cooperative launch (all blocks
+ * resident at once, which cudaLaunchCooperativeKernel guarantees) whose
+ * rounds are separated by a grid barrier, instead of one launch per round.
+ * The barrier is a counter and a generation word: each block's thread 0
+ * notes the generation, arrives, and the last to arrive resets the counter
+ * and advances the generation, which the others poll. The poll is bounded:
+ * past kBarrierPolls it records a failure in the barrier and in the mesh's
+ * error word and the block leaves the kernel (the host then reports
+ * TRN_ERR_NO_PROGRESS), so no wait can outlive a fault elsewhere. Used for
+ * calls that are not being captured into a graph; a captured round keeps the
+ * per-round launches. */
+struct GridBar {
+  unsigned count;
+  unsigned gen;
+  int err;
+};
+constexpr long long kBarrierPolls = 1LL << 24;
+
+__device__ __forceinline__ bool grid_sync(GridBar* b, int* mesh_err) {
+  __syncthreads();
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = &b->gen;
+    volatile int* verr = &b->err;
+    const unsigned g = *vgen;
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
+      b->count = 0;
+      __threadfence();
+      atomicAdd(&b->gen, 1u);
+    } else {
+      long long polls = 0;
+      while (*vgen == g) {
+        if (*verr || ++polls > kBarrierPolls) {
+          atomicExch(&b->err, 1);
+          trn_set_error(mesh_err, TRN_DERR_NO_PROGRESS);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok && !*verr;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+static GridBar* grid_bar(HeurWs& ws) { return reinterpret_cast<GridBar*>(ws.cnt + 100); }
+
+/* a cooperative launch of `kernel` with as many blocks as fit on the device
+ * at once (and no more than the items need); false when it could not launch
+ * (the caller then takes the per-round launches) */
+template <class K, class... Args>
+static bool coop_launch(K kernel, long long items, cudaStream_t s, Args... args) {
+  int dev = 0, sms = 0, coop = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, TRN_THREADS, 0) != cudaSuccess ||
+      per_sm <= 0)
+    return false;
+  cudaStreamCaptureStatus cs;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+  const long long need = (items + TRN_THREADS - 1) / TRN_THREADS;
+  const int grid = (int) std::max(1LL, std::min<long long>((long long) per_sm * sms, need));
+  void* argv[] = {static_cast<void*>(&args)...};
+  if (cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), grid, TRN_THREADS, argv, 0, s) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  note_launch();
+  return true;
+}
+
 /* ---------------- independent set ---------------- */
 
 
@@ -118,10 +197,35 @@ __global__ void __launch_bounds__(kFusedThreads) k_mis_fused(DMesh m, uint8_t* s
   for (int q = threadIdx.x; q < n; q += blockDim.x) mis_finish_item(m, state, other, cand[q], indep, nindep);
 }
 
+/* all the rounds and the collection in one cooperative launch */
+__global__ void k_mis_persist(DMesh m, uint8_t* s0, uint8_t* s1, const int* __restrict__ cand,
+                              const int* count, Seed sd, int rounds, int* indep, int* nindep, GridBar* bar) {
+  if (trn_failed(m)) return;
+  const int n = *count;
+  if (trn_tid() == 0) *nindep = 0;
+  const uint64_t base = trn_seed(sd);
+  for (int r = 0; r < rounds; ++r) {
+    const uint8_t* in = (r & 1) ? s1 : s0;
+    uint8_t* out = (r & 1) ? s0 : s1;
+    const uint64_t seed = base + 0x9e3779b97f4a7c15ULL * r;
+    for (int q = trn_tid(); q < n; q += trn_grid_stride()) mis_item(m, in, out, cand[q], seed);
+    if (!grid_sync(bar, m.err)) return;
+  }
+  uint8_t* state = (rounds & 1) ? s1 : s0;
+  uint8_t* other = (rounds & 1) ? s0 : s1;
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) mis_finish_item(m, state, other, cand[q], indep, nindep);
+}
+
 void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, Seed sd,
                    HeurWs& ws, int* indep, int* nindep, cudaStream_t s, long long bound) {
   ProfScope ps("mis_jp", s, 0.0);
   uint8_t* buf[2] = {ws.state, ws.state2};
+  if (bound > kFusedThreads &&
+      coop_launch(k_mis_persist, bound, s, m, buf[0], buf[1], cand, count, sd, rounds, indep, nindep,
+                  grid_bar(ws))) {
+    check_launch("mis_jp_rounds");
+    return;
+  }
   if (bound >= 0 && bound <= kFusedThreads) {   /* known short: the one-block form only */
     k_mis_fused<<<1, kFusedThreads, 0, s>>>(m, buf[0], buf[1], cand, count, sd, rounds, indep, nindep,
                                             kFusedThreads);
@@ -530,6 +634,38 @@ __global__ void __launch_bounds__(kFusedThreads) k_greedy_tail(GreedyArgs a, con
   }
 }
 
+/* the whole matching of a level in one cooperative launch: reset, first
+ * proposals, then rounds until no row waits (at most kGreedyRounds) */
+__global__ void k_greedy_persist(GreedyArgs a, const int* ntasks_dev, int* pairs, int* npairs, GridBar* bar,
+                                 int* err) {
+  const int ntasks = *ntasks_dev;
+  if (trn_tid() == 0) {
+    *npairs = 0;
+    a.cnt[0] = ntasks;
+    a.cnt[1] = 0;
+    a.cnt[2] = 0;
+  }
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) greedy_reset_item(a, i);
+  if (!grid_sync(bar, err)) return;
+  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
+    greedy_propose(a, 0, i);
+    a.list0[i] = i;
+  }
+  if (!grid_sync(bar, err)) return;
+  for (int r = 0; r < kGreedyRounds; ++r) {
+    const int n = *(volatile int*) (a.cnt + r % 3);
+    if (n == 0) break;
+    const int* in = (r & 1) ? a.list1 : a.list0;
+    int* out = (r & 1) ? a.list0 : a.list1;
+    if (trn_tid() == 0) a.cnt[(r + 2) % 3] = 0;
+    for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+      const int i = in[q];
+      if (greedy_item(a, ntasks, r, i, pairs, npairs)) trn_append(out, a.cnt + (r + 1) % 3, i);
+    }
+    if (!grid_sync(bar, err)) return;
+  }
+}
+
 void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual_n, const int* ntasks,
                   const int* map, HeurWs& ws, int* pairs, int* npairs, cudaStream_t s, long long bound) {
   (void) m;
@@ -539,6 +675,11 @@ void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual
   if (bound >= 0 && bound <= kFusedThreads) {   /* known short: one block */
     k_greedy_tail<<<1, kFusedThreads, 0, s>>>(a, ntasks, pairs, npairs, 1, kFusedThreads);
     note_launch();
+    check_launch("match_greedy");
+    return;
+  }
+  if (coop_launch(k_greedy_persist, bound < 0 ? nb_elems : bound, s, a, ntasks, pairs, npairs, grid_bar(ws),
+                  m.err)) {
     check_launch("match_greedy");
     return;
   }
@@ -823,9 +964,53 @@ void color_finish(const DMesh& m, int hint, int max_col, HeurWs& ws, int* parts,
   check_launch("color_jp");
 }
 
+/* every round of the coloring in one cooperative launch, until no vertex
+ * waits (at most kColorTailRounds rounds); the list counts rotate over
+ * three words so that the one a round fills starts at zero */
+__global__ void k_color_persist(DMesh m, int* list_a, int* list_b, int* counts, int* rot, int* color,
+                                int max_col, Seed sd, int* round_ctr, GridBar* bar) {
+  if (trn_failed(m)) return;
+  const uint64_t seed = trn_seed(sd);
+  int round = *round_ctr;
+  if (trn_tid() == 0) {
+    rot[0] = counts[0];
+    rot[1] = 0;
+    rot[2] = 0;
+  }
+  if (!grid_sync(bar, m.err)) return;
+  int it = 0;
+  for (; it < kColorTailRounds; ++it) {
+    const int n = *(volatile int*) (rot + it % 3);
+    if (n == 0) break;
+    ++round;
+    int* in = (it & 1) ? list_b : list_a;
+    int* out = (it & 1) ? list_a : list_b;
+    if (trn_tid() == 0) rot[(it + 2) % 3] = 0;
+    for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+      const int v = in[q];
+      if (color_item(m, v, color, max_col, seed, round)) trn_append(out, rot + (it + 1) % 3, v);
+    }
+    if (!grid_sync(bar, m.err)) return;
+  }
+  if (trn_tid() == 0) {
+    *round_ctr = round;
+    counts[0] = counts[1] = 0;
+  }
+}
+
 void color_jp(const DMesh& m, int hint, int max_col, Seed sd, HeurWs& ws, int* parts, int* part_off,
               unsigned* tick, cudaStream_t s) {
   color_begin(m, hint, ws, s);
+  bool done;
+  {
+    ProfScope ps("color_jp", s, 0.0);
+    done = coop_launch(k_color_persist, hint, s, m, ws.list_a, ws.list_b, color_counts(ws), ws.cnt + 104,
+                       ws.color, max_col, sd, color_round(ws), grid_bar(ws));
+  }
+  if (done) {
+    color_finish(m, hint, max_col, ws, parts, part_off, tick, s);
+    return;
+  }
   int cont = 1;
   while (cont) {
     color_batch(m, hint, max_col, sd, ws, s, 0, false);
@@ -850,6 +1035,7 @@ void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {
   cudaMalloc(&ws->mate, sizeof(int) * (size_t) capa_elem);
   cudaMalloc(&ws->rank, sizeof(uint32_t) * 4 * (size_t) capa_elem);
   cudaMalloc(&ws->cnt, sizeof(int) * 128);
+  cudaMemset(ws->cnt, 0, sizeof(int) * 128);   /* the grid barrier's words start at zero */
   cudaMalloc(&ws->color_keys, sizeof(int) * 2 * kColorKeys);
   cudaMalloc(&ws->list_a, sizeof(int) * big);
   cudaMalloc(&ws->list_b, sizeof(int) * big);
