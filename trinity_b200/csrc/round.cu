@@ -20,28 +20,7 @@ __global__ void k_level_end(int* status, int kind, int cap, const int* __restric
   const int n = status[S_ACT + 1];
   for (int i = trn_tid(); i < n; i += trn_grid_stride()) cur[i] = next[i];
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const int ntask = status[S_NTASK];
-  int go;
-  if (kind == kLevelCoarsen) {
-    const int nindep = status[S_NINDEP];
-    status[S_EVAL] += ntask;
-    status[S_TASK] += nindep;
-    go = ntask > 0 && nindep > 0;
-  } else {
-    const int commit = status[S_COMMIT];
-    status[S_EVAL] += ntask;
-    status[S_TASK] += commit / 2;
-    go = commit > 0;
-  }
-  const int level = ++status[S_LEVEL];
-  if (go && level > cap) {
-    atomicCAS(status + S_ERR, 0, TRN_DERR_NO_PROGRESS);
-    go = 0;
-  }
-  status[S_ACT] = n;
-  status[S_CONT] = go;
-  ++*reinterpret_cast<unsigned*>(status + S_TICK);
-  if (use_h) cudaGraphSetConditional(h, go);
+  level_end_decide(status, kind, cap, h, use_h);
 }
 
 void level_end(int* status, int kind, int cap, const int* next, int* cur, int hint, cudaStream_t s,

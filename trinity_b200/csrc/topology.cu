@@ -12,6 +12,8 @@
  *                    the vertex's bucket held in registers/local memory.
  */
 #include "trn_internal.h"
+
+#include <algorithm>
 #include "trn_mixed.cuh"
 
 namespace trn {
@@ -119,6 +121,36 @@ __global__ void k_fix_list(DMesh m, const int* __restrict__ list, const int* cou
     m.fixes[v] = 0;
     fix_stencil(m, v, buf);
   }
+}
+
+/* the repair of the listed vertices and the level's end in one launch; the
+ * level end runs even after an error (a captured loop must still read its
+ * condition, which then stops it) */
+__global__ void k_fix_level_end(DMesh m, const int* __restrict__ list, const int* count, int* status, int kind,
+                                int cap, const int* __restrict__ next, int* __restrict__ cur,
+                                cudaGraphConditionalHandle h, int use_h) {
+  const int na = status[S_ACT + 1];
+  for (int i = trn_tid(); i < na; i += trn_grid_stride()) cur[i] = next[i];
+  if (threadIdx.x == 0 && blockIdx.x == 0) level_end_decide(status, kind, cap, h, use_h);
+  if (trn_failed(m)) return;
+  int buf[TRN_MAX_DEG];
+  const int n = *count;
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int v = list[q];
+    if (!m.fixes[v]) continue;
+    m.fixes[v] = 0;
+    fix_stencil(m, v, buf);
+  }
+}
+
+void fix_list_level_end(const DMesh& m, const int* list, const int* count, long long bound, int* status,
+                        int kind, int cap, const int* next, int* cur, int hint, cudaStream_t s,
+                        cudaGraphConditionalHandle h, bool use_h) {
+  ProfScope ps("fix_tagged", s, 0.0);
+  const int g = std::max(grid_bounded(bound, m.capa_node), grid_for(hint));
+  k_fix_level_end<<<g, TRN_THREADS, 0, s>>>(m, list, count, status, kind, cap, next, cur, h, use_h ? 1 : 0);
+  note_launch();
+  check_launch("fix_list_level_end");
 }
 
 void fix_list(const DMesh& m, const int* list, const int* count, cudaStream_t s, long long bound) {

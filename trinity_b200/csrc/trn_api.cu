@@ -953,9 +953,9 @@ void enq_coarsen_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphCo
   mis_jp_rounds(dl, m->list, m->status + S_NTASK, kMisRounds, seed_of(m, 0x9e37ULL), m->hws, m->indep,
                 m->status + S_NINDEP, s, bound);
   collapse(dl, m->indep, m->status + S_NINDEP, m->target, nullptr, s, bound);
-  fix_list(dl, dl.fix_list, dl.fix_n, s, bound < 0 ? -1 : 16 * bound);
-  level_end(m->status, kLevelCoarsen, m->level_cap, act_list(m, 1), act_list(m, 0),
-            bound < 0 ? m->capa_node : (int) std::max(bound, 1LL), s, h, use_h);
+  fix_list_level_end(dl, dl.fix_list, dl.fix_n, bound < 0 ? -1 : 16 * bound, m->status, kLevelCoarsen,
+                     m->level_cap, act_list(m, 1), act_list(m, 0),
+                     bound < 0 ? m->capa_node : (int) std::max(bound, 1LL), s, h, use_h);
 }
 
 void enq_swap_begin(trn_mesh* m, cudaStream_t s, bool capture) {
@@ -983,9 +983,9 @@ void enq_swap_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphCondi
   cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s);
   swap_flip(dl, m->pairs, m->status + S_NPAIRS, m->map, m->dual, m->dual_n, m->status + S_NTASK,
             m->status + S_COMMIT, true, m->fp32, s, bound);
-  fix_list(dl, dl.fix_list, dl.fix_n, s, bound < 0 ? -1 : 4 * bound);
-  level_end(m->status, kLevelSwap, m->level_cap, act_list(m, 1), act_list(m, 0),
-            bound < 0 ? m->capa_elem : (int) std::max(bound, 1LL), s, h, use_h);
+  fix_list_level_end(dl, dl.fix_list, dl.fix_n, bound < 0 ? -1 : 4 * bound, m->status, kLevelSwap,
+                     m->level_cap, act_list(m, 1), act_list(m, 0),
+                     bound < 0 ? m->capa_elem : (int) std::max(bound, 1LL), s, h, use_h);
 }
 
 int max_colors_of(int max_colors) {

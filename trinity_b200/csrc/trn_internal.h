@@ -43,6 +43,41 @@ enum StatusSlot {
 constexpr int kLevelCoarsen = 0, kLevelSwap = 1;
 constexpr int kLevelCap = 100000;
 
+/* the decision at the end of a coarsening / swapping level, by one thread:
+ * the call's statistics, the level cap, the seed counter, and whether
+ * another level runs (S_CONT; also the captured loop's condition) */
+__device__ __forceinline__ void level_end_decide(int* status, int kind, int cap,
+                                                 cudaGraphConditionalHandle h, int use_h) {
+  const int ntask = status[S_NTASK];
+  int go;
+  if (kind == kLevelCoarsen) {
+    const int nindep = status[S_NINDEP];
+    status[S_EVAL] += ntask;
+    status[S_TASK] += nindep;
+    go = ntask > 0 && nindep > 0;
+  } else {
+    const int commit = status[S_COMMIT];
+    status[S_EVAL] += ntask;
+    status[S_TASK] += commit / 2;
+    go = commit > 0;
+  }
+  const int level = ++status[S_LEVEL];
+  if (go && level > cap) {
+    atomicCAS(status + S_ERR, 0, TRN_DERR_NO_PROGRESS);
+    go = 0;
+  }
+  status[S_ACT] = status[S_ACT + 1];
+  status[S_CONT] = go;
+  ++*reinterpret_cast<unsigned*>(status + S_TICK);
+  if (use_h) cudaGraphSetConditional(h, go);
+}
+
+/* the stencil repair of the listed vertices fused with the level's end (the
+ * two touch disjoint state): one launch instead of two per level */
+void fix_list_level_end(const DMesh& m, const int* list, const int* count, long long bound, int* status,
+                        int kind, int cap, const int* next, int* cur, int hint, cudaStream_t s,
+                        cudaGraphConditionalHandle h, bool use_h);
+
 /* end of a coarsening / swapping level (round.cu): next list into place,
  * statistics, level cap, seed counter, and the decision in S_CONT (also
  * handed to the loop node h when use_h) */
