@@ -187,7 +187,8 @@ int trn_smooth_gradient_run(trn_mesh* mesh, int max_colors, int steps, double ma
  * grouped search (4, 8, 16), cfg[3] longest level list the grouped search
  * takes, cfg[4] flip block, cfg[5] lanes per smoothed vertex (1, 4, 8),
  * cfg[6] registers of the smoothing kernel (0: up to 128, two 256-thread
- * blocks per SM; 1: capped for three). Per mesh; a captured round is recaptured when
+ * blocks per SM; 1: capped for three; 2: for four). Per mesh; a captured round
+ * is recaptured when
  * they change. trn_autotune chooses them on the loaded mesh by coordinate
  * descent over candidates, timing metric + `rounds` rounds from the input
  * (twice each, the faster counts), then reloads the mesh; meshes of similar
@@ -295,7 +296,7 @@ int trn_profile_entry(int i, char* name, int name_len, long long* launches, doub
  * with the complexity summed by its fixed-shape tree (the default; a mesh
  * set to exact_sum or replay sums in element order instead, which can differ
  * in the last bits). The first call on a device looks up the array's device
- * address, so make it before any stream capture. Calls share the array:
+ * address and keeps it. Calls share the array:
  * calls that overlap on the GPU (other streams or host threads) race;
  * serialise them. Runs on `stream` (a cudaStream_t of the current device,
  * NULL = default stream) and returns when done. */

@@ -88,24 +88,26 @@ __device__ __forceinline__ bool grid_sync(GridBar* b, int* mesh_err) {
 
 static GridBar* grid_bar(HeurWs& ws) { return reinterpret_cast<GridBar*>(ws.cnt + 100); }
 
-/* a cooperative launch of `kernel` with as many blocks as fit on the device
- * at once (and no more than the items need); false when it could not launch
- * (the caller then takes the per-round launches) */
+/* a cooperative launch of `kernel` with as many blocks of `threads` as fit
+ * on the device at once (and no more than the items need); false when it
+ * could not launch (the caller then takes the per-round launches). Large
+ * blocks keep the barrier's arrivals few (two 1024-thread blocks an SM: 296
+ * arrivals a round on 148 SMs). */
 template <class K, class... Args>
-static bool coop_launch(K kernel, long long items, cudaStream_t s, Args... args) {
+static bool coop_launch(K kernel, long long items, int threads, cudaStream_t s, Args... args) {
   int dev = 0, sms = 0, coop = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-  if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, TRN_THREADS, 0) != cudaSuccess ||
+  if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess ||
       per_sm <= 0)
     return false;
   cudaStreamCaptureStatus cs;
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
-  const long long need = (items + TRN_THREADS - 1) / TRN_THREADS;
+  const long long need = (items + threads - 1) / threads;
   const int grid = (int) std::max(1LL, std::min<long long>((long long) per_sm * sms, need));
   void* argv[] = {static_cast<void*>(&args)...};
-  if (cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), grid, TRN_THREADS, argv, 0, s) !=
+  if (cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), grid, threads, argv, 0, s) !=
       cudaSuccess) {
     cudaGetLastError();
     return false;
@@ -198,8 +200,10 @@ __global__ void __launch_bounds__(kFusedThreads) k_mis_fused(DMesh m, uint8_t* s
 }
 
 /* all the rounds and the collection in one cooperative launch */
-__global__ void k_mis_persist(DMesh m, uint8_t* s0, uint8_t* s1, const int* __restrict__ cand,
-                              const int* count, Seed sd, int rounds, int* indep, int* nindep, GridBar* bar) {
+__global__ void __launch_bounds__(kFusedThreads) k_mis_persist(DMesh m, uint8_t* s0, uint8_t* s1,
+                                                               const int* __restrict__ cand, const int* count,
+                                                               Seed sd, int rounds, int* indep, int* nindep,
+                                                               GridBar* bar) {
   if (trn_failed(m)) return;
   const int n = *count;
   if (trn_tid() == 0) *nindep = 0;
@@ -221,7 +225,7 @@ void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds
   ProfScope ps("mis_jp", s, 0.0);
   uint8_t* buf[2] = {ws.state, ws.state2};
   if (bound > kFusedThreads &&
-      coop_launch(k_mis_persist, bound, s, m, buf[0], buf[1], cand, count, sd, rounds, indep, nindep,
+      coop_launch(k_mis_persist, bound, kFusedThreads, s, m, buf[0], buf[1], cand, count, sd, rounds, indep, nindep,
                   grid_bar(ws))) {
     check_launch("mis_jp_rounds");
     return;
@@ -635,9 +639,13 @@ __global__ void __launch_bounds__(kFusedThreads) k_greedy_tail(GreedyArgs a, con
 }
 
 /* the whole matching of a level in one cooperative launch: reset, first
- * proposals, then rounds until no row waits (at most kGreedyRounds) */
-__global__ void k_greedy_persist(GreedyArgs a, const int* ntasks_dev, int* pairs, int* npairs, GridBar* bar,
-                                 int* err) {
+ * proposals, then rounds until no row waits (at most kGreedyRounds). Once
+ * kGreedyTail rows or fewer wait, the first block finishes the rounds alone,
+ * separated by block barriers, and the others return: a grid barrier costs
+ * more than such a round. */
+__global__ void __launch_bounds__(kFusedThreads) k_greedy_persist(GreedyArgs a, const int* ntasks_dev,
+                                                                  int* pairs, int* npairs, GridBar* bar,
+                                                                  int* err) {
   const int ntasks = *ntasks_dev;
   if (trn_tid() == 0) {
     *npairs = 0;
@@ -652,17 +660,25 @@ __global__ void k_greedy_persist(GreedyArgs a, const int* ntasks_dev, int* pairs
     a.list0[i] = i;
   }
   if (!grid_sync(bar, err)) return;
+  bool alone = false;
   for (int r = 0; r < kGreedyRounds; ++r) {
     const int n = *(volatile int*) (a.cnt + r % 3);
     if (n == 0) break;
+    if (!alone && n <= kGreedyTail) {
+      if (blockIdx.x != 0) return;
+      alone = true;
+    }
     const int* in = (r & 1) ? a.list1 : a.list0;
     int* out = (r & 1) ? a.list0 : a.list1;
-    if (trn_tid() == 0) a.cnt[(r + 2) % 3] = 0;
-    for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int t0 = alone ? (int) threadIdx.x : trn_tid();
+    const int ts = alone ? (int) blockDim.x : trn_grid_stride();
+    if (t0 == 0) a.cnt[(r + 2) % 3] = 0;
+    for (int q = t0; q < n; q += ts) {
       const int i = in[q];
       if (greedy_item(a, ntasks, r, i, pairs, npairs)) trn_append(out, a.cnt + (r + 1) % 3, i);
     }
-    if (!grid_sync(bar, err)) return;
+    if (alone) __syncthreads();
+    else if (!grid_sync(bar, err)) return;
   }
 }
 
@@ -678,7 +694,8 @@ void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual
     check_launch("match_greedy");
     return;
   }
-  if (coop_launch(k_greedy_persist, bound < 0 ? nb_elems : bound, s, a, ntasks, pairs, npairs, grid_bar(ws),
+  if (coop_launch(k_greedy_persist, bound < 0 ? nb_elems : bound, kFusedThreads, s, a, ntasks, pairs, npairs,
+                  grid_bar(ws),
                   m.err)) {
     check_launch("match_greedy");
     return;
@@ -966,9 +983,12 @@ void color_finish(const DMesh& m, int hint, int max_col, HeurWs& ws, int* parts,
 
 /* every round of the coloring in one cooperative launch, until no vertex
  * waits (at most kColorTailRounds rounds); the list counts rotate over
- * three words so that the one a round fills starts at zero */
-__global__ void k_color_persist(DMesh m, int* list_a, int* list_b, int* counts, int* rot, int* color,
-                                int max_col, Seed sd, int* round_ctr, GridBar* bar) {
+ * three words so that the one a round fills starts at zero. Once kColorTail
+ * vertices or fewer wait, the first block colors the rest alone. */
+__global__ void __launch_bounds__(kFusedThreads) k_color_persist(DMesh m, int* list_a, int* list_b,
+                                                                 int* counts, int* rot, int* color,
+                                                                 int max_col, Seed sd, int* round_ctr,
+                                                                 GridBar* bar) {
   if (trn_failed(m)) return;
   const uint64_t seed = trn_seed(sd);
   int round = *round_ctr;
@@ -979,20 +999,28 @@ __global__ void k_color_persist(DMesh m, int* list_a, int* list_b, int* counts, 
   }
   if (!grid_sync(bar, m.err)) return;
   int it = 0;
+  bool alone = false;
   for (; it < kColorTailRounds; ++it) {
     const int n = *(volatile int*) (rot + it % 3);
     if (n == 0) break;
+    if (!alone && n <= kColorTail) {
+      if (blockIdx.x != 0) return;
+      alone = true;
+    }
     ++round;
     int* in = (it & 1) ? list_b : list_a;
     int* out = (it & 1) ? list_a : list_b;
-    if (trn_tid() == 0) rot[(it + 2) % 3] = 0;
-    for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int t0 = alone ? (int) threadIdx.x : trn_tid();
+    const int ts = alone ? (int) blockDim.x : trn_grid_stride();
+    if (t0 == 0) rot[(it + 2) % 3] = 0;
+    for (int q = t0; q < n; q += ts) {
       const int v = in[q];
       if (color_item(m, v, color, max_col, seed, round)) trn_append(out, rot + (it + 1) % 3, v);
     }
-    if (!grid_sync(bar, m.err)) return;
+    if (alone) __syncthreads();
+    else if (!grid_sync(bar, m.err)) return;
   }
-  if (trn_tid() == 0) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
     *round_ctr = round;
     counts[0] = counts[1] = 0;
   }
@@ -1004,7 +1032,8 @@ void color_jp(const DMesh& m, int hint, int max_col, Seed sd, HeurWs& ws, int* p
   bool done;
   {
     ProfScope ps("color_jp", s, 0.0);
-    done = coop_launch(k_color_persist, hint, s, m, ws.list_a, ws.list_b, color_counts(ws), ws.cnt + 104,
+    done = coop_launch(k_color_persist, hint, kFusedThreads, s, m, ws.list_a, ws.list_b, color_counts(ws),
+                       ws.cnt + 104,
                        ws.color, max_col, sd, color_round(ws), grid_bar(ws));
   }
   if (done) {

@@ -21,7 +21,7 @@
  * Host code cannot use the array's name as a device address (in host code it
  * names a host-side stand-in), so the first call on each device looks the
  * address up with cudaGetSymbolAddress while that device is current and keeps
- * it; that first call should therefore come before any stream capture.
+ * it.
  *
  * The computation is the same kernels, in the same order, as trn_metric_run
  * (gradient, Hessian with local L^p scaling, complexity with the fixed-shape

@@ -161,10 +161,11 @@ __device__ unsigned long long smooth_bytes(const DMesh& m, int v, bool moved, un
   return b;
 }
 
-/* Tight: registers capped for three 256-thread blocks per SM (more warps to
- * hide the gathers' latency, some spills); else up to 128 (two blocks) */
-template <bool F32, bool Tight>
-__global__ void __launch_bounds__(256, Tight ? 3 : 2) k_smooth_move(DMesh m, const int* __restrict__ list,
+/* MinB: 256-thread blocks an SM the registers are capped for (2: up to 128,
+ * 3: 80, 4: 64); more warps hide more of the gathers' latency, at the cost of
+ * spills */
+template <bool F32, int MinB>
+__global__ void __launch_bounds__(256, MinB) k_smooth_move(DMesh m, const int* __restrict__ list,
                                                                    int n, const int* off, int c, int* counters,
                                                                    int kj, ByteCount bc) {
   extern __shared__ __align__(16) unsigned char smooth_smem[];
@@ -353,8 +354,8 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
   return valid ? 1 : 0;
 }
 
-template <bool F32, int G, bool Tight>
-__global__ void __launch_bounds__(256, Tight ? 3 : 2) k_smooth_move_grp(DMesh m, const int* __restrict__ list,
+template <bool F32, int G, int MinB>
+__global__ void __launch_bounds__(256, MinB) k_smooth_move_grp(DMesh m, const int* __restrict__ list,
                                                                        int n, const int* off, int c,
                                                                        int* counters, ByteCount bc) {
   if (trn_failed(m)) return;
@@ -406,16 +407,19 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
   const int t = tune().smooth_threads;
   const int lanes = tune().smooth_lanes;
   const int g = grid_for((long long) hint * lanes, t);
-  const bool tight = tune().smooth_regs != 0;
+  const int regs = tune().smooth_regs;
   if (lanes == 8 || lanes == 4) {
-#define TRN_GRP(F, G, T) k_smooth_move_grp<F, G, T><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc)
+#define TRN_GRP(F, G, B) k_smooth_move_grp<F, G, B><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc)
+#define TRN_GRP_B(F, G) \
+  do { if (regs == 0) TRN_GRP(F, G, 2); else if (regs == 1) TRN_GRP(F, G, 3); else TRN_GRP(F, G, 4); } while (0)
     if (lanes == 8) {
-      if (fp32) { if (tight) TRN_GRP(true, 8, true); else TRN_GRP(true, 8, false); }
-      else { if (tight) TRN_GRP(false, 8, true); else TRN_GRP(false, 8, false); }
+      if (fp32) TRN_GRP_B(true, 8);
+      else TRN_GRP_B(false, 8);
     } else {
-      if (fp32) { if (tight) TRN_GRP(true, 4, true); else TRN_GRP(true, 4, false); }
-      else { if (tight) TRN_GRP(false, 4, true); else TRN_GRP(false, 4, false); }
+      if (fp32) TRN_GRP_B(true, 4);
+      else TRN_GRP_B(false, 4);
     }
+#undef TRN_GRP_B
 #undef TRN_GRP
   } else {
     /* element-metric slots a thread: what 40 KB of shared memory a block
@@ -423,9 +427,12 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
     const int slot = fp32 ? (int) sizeof(float4) : (int) sizeof(double4);
     const int kj = std::min(fp32 ? 12 : 8, (40 << 10) / (t * slot));
     const size_t smem = (size_t) kj * t * slot;
-#define TRN_ONE(F, T) k_smooth_move<F, T><<<g, t, smem, s>>>(m, list, n, off, c, counters, kj, bc)
-    if (fp32) { if (tight) TRN_ONE(true, true); else TRN_ONE(true, false); }
-    else { if (tight) TRN_ONE(false, true); else TRN_ONE(false, false); }
+#define TRN_ONE(F, B) k_smooth_move<F, B><<<g, t, smem, s>>>(m, list, n, off, c, counters, kj, bc)
+#define TRN_ONE_B(F) \
+  do { if (regs == 0) TRN_ONE(F, 2); else if (regs == 1) TRN_ONE(F, 3); else TRN_ONE(F, 4); } while (0)
+    if (fp32) TRN_ONE_B(true);
+    else TRN_ONE_B(false);
+#undef TRN_ONE_B
 #undef TRN_ONE
   }
   note_launch();
