@@ -44,40 +44,21 @@ __device__ int identify_target(const DMesh& m, int source) {
   const int nv = m.vdeg[source];
   const double2 ps = m.pts[source];
   const TenT<F32> ts = ten_load<F32>(m, source);
-  /* neighbours in chunks of kPre, each chunk's tags, points and tensors
-   * loaded before any is used (a chunk's gathers in flight together, not
-   * one neighbour's at a time); slots past the row load the source's own */
-  constexpr int kPre = 4;
-  for (int b0 = 0; b0 < nv; b0 += kPre) {
-    int w[kPre];
-    unsigned char tg[kPre];
-    double2 pw[kPre];
-    TenT<F32> tw[kPre];
-#pragma unroll
-    for (int j = 0; j < kPre; ++j) w[j] = (b0 + j < nv) ? vc[b0 + j] : source;
-#pragma unroll
-    for (int j = 0; j < kPre; ++j) {
-      tg[j] = m.tags[w[j]];
-      pw[j] = m.pts[w[j]];
-      tw[j] = ten_load<F32>(m, w[j]);
-    }
-#pragma unroll
-    for (int j = 0; j < kPre; ++j) {
-      if (b0 + j >= nv) break;
-      const bool bound_destin = (tg[j] & TRN_TAG_BOUND) != 0;
-      if (bound_source && !bound_destin) continue;
-      double len;
-      if (length_lt<F32>(ps, pw[j], ts, tw[j], TRN_L_MIN, &len)) {
-        int p = nc;
-        while (p > 0 && lens[p - 1] > len) {
-          lens[p] = lens[p - 1];
-          cands[p] = cands[p - 1];
-          --p;
-        }
-        lens[p] = len;
-        cands[p] = w[j];
-        nc++;
+  for (int b = 0; b < nv; ++b) {
+    int neigh = vc[b];
+    bool bound_destin = (m.tags[neigh] & TRN_TAG_BOUND) != 0;
+    if (bound_source && !bound_destin) continue;
+    double len;
+    if (length_lt<F32>(ps, m.pts[neigh], ts, ten_load<F32>(m, neigh), TRN_L_MIN, &len)) {
+      int p = nc;
+      while (p > 0 && lens[p - 1] > len) {
+        lens[p] = lens[p - 1];
+        cands[p] = cands[p - 1];
+        --p;
       }
+      lens[p] = len;
+      cands[p] = neigh;
+      nc++;
     }
   }
   const int* st = m.stenc + (size_t) source * m.bucket;
@@ -134,13 +115,11 @@ __global__ void k_coarse_filter(DMesh m, int nb_nodes, int* __restrict__ target,
 /* free mode: one pass per level rebuilds the adjacency of each active vertex,
  * finds its target and appends the candidates (in no particular order: the
  * independent set is chosen by hashed priorities, not by list position),
- * marking them undecided for the independent-set rounds; registers capped
- * at 80 (three 256-thread blocks an SM) */
+ * marking them undecided for the independent-set rounds */
 template <bool F32>
-__global__ void __maxnreg__(80) k_coarse_filter_append(DMesh m, const int* __restrict__ act,
-                                                       const int* act_n, int* __restrict__ target,
-                                                       int* __restrict__ cand, int* count,
-                                                       uint8_t* __restrict__ state, int min_n) {
+__global__ void k_coarse_filter_append(DMesh m, const int* __restrict__ act, const int* act_n,
+                                       int* __restrict__ target, int* __restrict__ cand, int* count,
+                                       uint8_t* __restrict__ state, int min_n) {
   if (trn_failed(m)) return;
   const int n = *act_n;
   if (n < min_n) return;

@@ -484,6 +484,9 @@ void match_handshake(const DMesh& m, int nb_elems, const int* dual, const int* d
  * more pairs, is a point and a half off. */
 constexpr int kGreedyRounds = 64;
 constexpr int kGreedyTail = 2048;   /* undecided rows left to the one-block rounds */
+/* rows waiting above which a round runs as its own grid launch (measured:
+ * such rounds are faster launched than inside the cooperative kernel) */
+constexpr int kGreedyGrid = 1 << 15;
 
 struct GreedyArgs {
   const int* dual;
@@ -575,12 +578,13 @@ __global__ void k_greedy_start(GreedyArgs a, const int* ntasks_dev, int min_n) {
   }
 }
 
-/* round r on the grid, while more than kGreedyTail rows are undecided and
- * every earlier round ran here */
-__global__ void k_greedy_round(GreedyArgs a, const int* ntasks_dev, int r, int* pairs, int* npairs) {
+/* round r on the grid, while more than max(kGreedyTail, min_n - 1) rows
+ * are undecided and every earlier round ran here */
+__global__ void k_greedy_round(GreedyArgs a, const int* ntasks_dev, int r, int* pairs, int* npairs,
+                               int min_n) {
   if (r > 0 && !a.ran[r - 1]) return;
   const int n = a.cnt[r % 3];
-  if (n <= kGreedyTail) return;
+  if (n <= kGreedyTail || n < min_n) return;
   const int ntasks = *ntasks_dev;
   const int* in = (r & 1) ? a.list1 : a.list0;
   int* out = (r & 1) ? a.list0 : a.list1;
@@ -638,30 +642,36 @@ __global__ void __launch_bounds__(kFusedThreads) k_greedy_tail(GreedyArgs a, con
   }
 }
 
-/* the whole matching of a level in one cooperative launch: reset, first
- * proposals, then rounds until no row waits (at most kGreedyRounds). Once
- * kGreedyTail rows or fewer wait, the first block finishes the rounds alone,
- * separated by block barriers, and the others return: a grid barrier costs
- * more than such a round. */
+/* the matching of a level in one cooperative launch: with `whole`, the
+ * reset and first proposals, then rounds until no row waits (at most
+ * kGreedyRounds); else the rounds from the first one the grid launches did
+ * not run. Once kGreedyTail rows or fewer wait, the first block finishes the
+ * rounds alone, separated by block barriers, and the others return: a grid
+ * barrier costs more than such a round. */
 __global__ void __launch_bounds__(kFusedThreads) k_greedy_persist(GreedyArgs a, const int* ntasks_dev,
                                                                   int* pairs, int* npairs, GridBar* bar,
-                                                                  int* err) {
+                                                                  int* err, int whole) {
   const int ntasks = *ntasks_dev;
-  if (trn_tid() == 0) {
-    *npairs = 0;
-    a.cnt[0] = ntasks;
-    a.cnt[1] = 0;
-    a.cnt[2] = 0;
+  int r0 = 0;
+  if (whole) {
+    if (trn_tid() == 0) {
+      *npairs = 0;
+      a.cnt[0] = ntasks;
+      a.cnt[1] = 0;
+      a.cnt[2] = 0;
+    }
+    for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) greedy_reset_item(a, i);
+    if (!grid_sync(bar, err)) return;
+    for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
+      greedy_propose(a, 0, i);
+      a.list0[i] = i;
+    }
+    if (!grid_sync(bar, err)) return;
+  } else {
+    while (r0 < kGreedyRounds && a.ran[r0]) ++r0;
   }
-  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) greedy_reset_item(a, i);
-  if (!grid_sync(bar, err)) return;
-  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
-    greedy_propose(a, 0, i);
-    a.list0[i] = i;
-  }
-  if (!grid_sync(bar, err)) return;
   bool alone = false;
-  for (int r = 0; r < kGreedyRounds; ++r) {
+  for (int r = r0; r < kGreedyRounds; ++r) {
     const int n = *(volatile int*) (a.cnt + r % 3);
     if (n == 0) break;
     if (!alone && n <= kGreedyTail) {
@@ -694,9 +704,8 @@ void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual
     check_launch("match_greedy");
     return;
   }
-  if (coop_launch(k_greedy_persist, bound < 0 ? nb_elems : bound, kFusedThreads, s, a, ntasks, pairs, npairs,
-                  grid_bar(ws),
-                  m.err)) {
+  if (bound >= 0 && bound <= kGreedyGrid &&
+      coop_launch(k_greedy_persist, bound, kFusedThreads, s, a, ntasks, pairs, npairs, grid_bar(ws), m.err, 1)) {
     check_launch("match_greedy");
     return;
   }
@@ -718,9 +727,22 @@ void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual
   note_launch();
   k_greedy_start<<<g, TRN_THREADS, 0, s>>>(a, ntasks, min_n);
   note_launch();
+  /* a long list known: grid launches while more than kGreedyGrid rows wait,
+   * then the cooperative rounds */
+  const bool coop = bound > kGreedyGrid;
+  if (coop) {
+    rounds = 0;
+    for (long long n = bound; n > kGreedyGrid; n /= 2) rounds += 3;
+    rounds = std::min(rounds, kGreedyRounds - 8);
+  }
   for (int r = 0; r < rounds; ++r) {
-    k_greedy_round<<<g, TRN_THREADS, 0, s>>>(a, ntasks, r, pairs, npairs);
+    k_greedy_round<<<g, TRN_THREADS, 0, s>>>(a, ntasks, r, pairs, npairs, coop ? kGreedyGrid + 1 : 0);
     note_launch();
+  }
+  if (coop && coop_launch(k_greedy_persist, bound, kFusedThreads, s, a, ntasks, pairs, npairs, grid_bar(ws),
+                          m.err, 0)) {
+    check_launch("match_greedy");
+    return;
   }
   /* the rounds left; when the list is unknown, the whole short-list form
    * too, each returning at once when the count is not its case */
@@ -748,29 +770,61 @@ __global__ void k_color_init(DMesh m, int nb_nodes, int* list, int* n, int* colo
   }
 }
 
-/* one vertex of a round: true when it must wait (a neighbour still
- * competing has a higher priority), else it takes the smallest color unused
- * by neighbours colored in earlier rounds */
-__device__ __forceinline__ bool color_item(const DMesh& m, int v, int* color, int max_col, uint64_t seed,
-                                           int round) {
+/* One vertex of a round of the speculative first-fit coloring: true when it
+ * must wait. Each uncolored vertex holds a tentative color, chosen in the
+ * round before (tent[(round - 1) & 1], none in round 0). It keeps it when no
+ * neighbour colored in an earlier round has it and no neighbour still
+ * competing at the round's start (uncolored, or colored in this very round)
+ * with a higher priority holds the same tentative; two neighbours never keep
+ * the same color in one round, so the coloring is proper. Otherwise it
+ * chooses a new tentative for the next round (tent[round & 1]): the smallest
+ * color unused by the neighbours colored in earlier rounds and by the
+ * tentatives of its higher-priority competitors; with none left it waits
+ * without one, and when the colored neighbours alone use every color it
+ * takes none (0xff, not smoothed). A round reads only the state its start
+ * left (round-stamped colors, the other tentative buffer), so the result does
+ * not depend on timing. Unlike Jones-Plassmann, a vertex need not outrank
+ * every competing neighbour, only those that want its color: fewer rounds. */
+__device__ __forceinline__ bool color_item(const DMesh& m, int v, int* color, uint8_t* tent, int capa,
+                                           int max_col, uint64_t seed, int round) {
   const uint64_t pv = trn_prio(seed, v);
   const int* vc = m.vic + (size_t) v * m.bucket;
   const int nv = m.vdeg[v];
-  unsigned used = 0;
+  const uint8_t* prev = tent + (size_t) ((round - 1) & 1) * capa;
+  const int mine = round > 0 ? prev[v] : 0;
+  bool keep = mine != 0;
+  unsigned used = 0, wanted = 0;
   for (int b = 0; b < nv; ++b) {
     const int w = vc[b];
     const int cw = *(volatile int*) (color + w);
     const int rw = cw >> 8;
     if (cw == 0 || rw == round + 1) {
-      if (trn_prio(seed, w) > pv) return true;
+      if (round > 0 && trn_prio(seed, w) > pv) {
+        const int tw = prev[w];
+        wanted |= 1u << tw;
+        if (tw == mine) keep = false;
+      }
     } else {
       used |= 1u << (cw & 0xff & 31);
     }
   }
+  if (keep && !(used & (1u << mine))) {
+    color[v] = ((round + 1) << 8) | mine;
+    return false;
+  }
   int c = 1;
-  while (c <= max_col && (used & (1u << c))) ++c;
-  color[v] = ((round + 1) << 8) | (c <= max_col ? c : 0xff);
-  return false;
+  while (c <= max_col && ((used | wanted) & (1u << c))) ++c;
+  if (c > max_col) {
+    int f = 1;
+    while (f <= max_col && (used & (1u << f))) ++f;
+    if (f > max_col) {
+      color[v] = ((round + 1) << 8) | 0xff;
+      return false;
+    }
+    c = 0;
+  }
+  tent[(size_t) (round & 1) * capa + v] = (uint8_t) c;
+  return true;
 }
 
 /* a list this short goes to the one-block rounds (k_color_tail) */
@@ -784,8 +838,8 @@ constexpr int kColorTail = 4096;
  * frozen (1 + the list's buffer) and it and the later rounds of the batch do
  * nothing. */
 __global__ void k_color_round(DMesh m, const int* __restrict__ list, const int* n_in, int* color,
-                              int max_col, Seed sd, const int* round_ctr, int* next, int* n_next,
-                              int* frozen, int cur) {
+                              uint8_t* tent, int max_col, Seed sd, const int* round_ctr, int* next,
+                              int* n_next, int* frozen, int cur) {
   if (trn_failed(m) || *frozen) return;
   const int n = *n_in;
   if (n <= kColorTail) {
@@ -796,7 +850,7 @@ __global__ void k_color_round(DMesh m, const int* __restrict__ list, const int* 
   const int round = *round_ctr;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
     const int v = list[q];
-    if (color_item(m, v, color, max_col, seed, round)) trn_append(next, n_next, v);
+    if (color_item(m, v, color, tent, m.capa_node, max_col, seed, round)) trn_append(next, n_next, v);
   }
 }
 
@@ -806,7 +860,8 @@ __global__ void k_color_round(DMesh m, const int* __restrict__ list, const int* 
 constexpr int kColorTailRounds = 512;
 
 __global__ void __launch_bounds__(1024) k_color_tail(DMesh m, int* list_a, int* list_b, int* counts, int* color,
-                                                     int max_col, Seed sd, int* round_ctr, int* frozen) {
+                                                     uint8_t* tent, int max_col, Seed sd, int* round_ctr,
+                                                     int* frozen) {
   const int f = *frozen;
   if (trn_failed(m) || f == 0) return;
   const uint64_t seed = trn_seed(sd);
@@ -822,7 +877,8 @@ __global__ void __launch_bounds__(1024) k_color_tail(DMesh m, int* list_a, int* 
     __syncthreads();
     for (int q = threadIdx.x; q < n; q += blockDim.x) {
       const int v = in[q];
-      if (color_item(m, v, color, max_col, seed, round)) out[atomicAdd(counts + (cur ^ 1), 1)] = v;
+      if (color_item(m, v, color, tent, m.capa_node, max_col, seed, round))
+        out[atomicAdd(counts + (cur ^ 1), 1)] = v;
     }
     __syncthreads();
     cur ^= 1;
@@ -952,13 +1008,13 @@ void color_batch(const DMesh& m, int hint, int max_col, Seed sd, HeurWs& ws, cud
     const int cur = r & 1;
     k_color_step<<<1, 32, 0, s>>>(color_round(ws), counts + (cur ^ 1), color_frozen(ws));
     note_launch();
-    k_color_round<<<g, TRN_THREADS, 0, s>>>(m, lists[cur], counts + cur, ws.color, max_col, sd,
+    k_color_round<<<g, TRN_THREADS, 0, s>>>(m, lists[cur], counts + cur, ws.color, ws.tent, max_col, sd,
                                             color_round(ws), lists[cur ^ 1], counts + (cur ^ 1),
                                             color_frozen(ws), cur);
     note_launch();
   }
-  k_color_tail<<<1, 1024, 0, s>>>(m, ws.list_a, ws.list_b, counts, ws.color, max_col, sd, color_round(ws),
-                                  color_frozen(ws));
+  k_color_tail<<<1, 1024, 0, s>>>(m, ws.list_a, ws.list_b, counts, ws.color, ws.tent, max_col, sd,
+                                  color_round(ws), color_frozen(ws));
   note_launch();
   /* an even number of rounds: the vertices still waiting are in list_a */
   k_color_batch_end<<<1, 32, 0, s>>>(counts, color_batch_no(ws), color_cont(ws), h, use_h ? 1 : 0);
@@ -987,8 +1043,8 @@ void color_finish(const DMesh& m, int hint, int max_col, HeurWs& ws, int* parts,
  * vertices or fewer wait, the first block colors the rest alone. */
 __global__ void __launch_bounds__(kFusedThreads) k_color_persist(DMesh m, int* list_a, int* list_b,
                                                                  int* counts, int* rot, int* color,
-                                                                 int max_col, Seed sd, int* round_ctr,
-                                                                 GridBar* bar) {
+                                                                 uint8_t* tent, int max_col, Seed sd,
+                                                                 int* round_ctr, GridBar* bar) {
   if (trn_failed(m)) return;
   const uint64_t seed = trn_seed(sd);
   int round = *round_ctr;
@@ -1015,7 +1071,8 @@ __global__ void __launch_bounds__(kFusedThreads) k_color_persist(DMesh m, int* l
     if (t0 == 0) rot[(it + 2) % 3] = 0;
     for (int q = t0; q < n; q += ts) {
       const int v = in[q];
-      if (color_item(m, v, color, max_col, seed, round)) trn_append(out, rot + (it + 1) % 3, v);
+      if (color_item(m, v, color, tent, m.capa_node, max_col, seed, round))
+        trn_append(out, rot + (it + 1) % 3, v);
     }
     if (alone) __syncthreads();
     else if (!grid_sync(bar, m.err)) return;
@@ -1033,8 +1090,7 @@ void color_jp(const DMesh& m, int hint, int max_col, Seed sd, HeurWs& ws, int* p
   {
     ProfScope ps("color_jp", s, 0.0);
     done = coop_launch(k_color_persist, hint, kFusedThreads, s, m, ws.list_a, ws.list_b, color_counts(ws),
-                       ws.cnt + 104,
-                       ws.color, max_col, sd, color_round(ws), grid_bar(ws));
+                       ws.cnt + 104, ws.color, ws.tent, max_col, sd, color_round(ws), grid_bar(ws));
   }
   if (done) {
     color_finish(m, hint, max_col, ws, parts, part_off, tick, s);
@@ -1059,6 +1115,7 @@ void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {
   cudaMalloc(&ws->choice, sizeof(int) * (size_t) capa_elem);
   cudaMalloc(&ws->choice2, sizeof(int) * (size_t) capa_elem);
   cudaMalloc(&ws->prop2, sizeof(unsigned long long) * (size_t) capa_elem);
+  cudaMalloc(&ws->tent, 2 * (size_t) capa_node);
   cudaMalloc(&ws->color, sizeof(int) * (size_t) capa_node);
   cudaMemset(ws->color, 0, sizeof(int) * (size_t) capa_node);
   cudaMalloc(&ws->mate, sizeof(int) * (size_t) capa_elem);
@@ -1078,6 +1135,7 @@ void heur_ws_free(HeurWs* ws) {
   cudaFree(ws->choice);
   cudaFree(ws->choice2);
   cudaFree(ws->prop2);
+  cudaFree(ws->tent);
   cudaFree(ws->color);
   cudaFree(ws->mate);
   cudaFree(ws->rank);

@@ -264,6 +264,7 @@ struct HeurWs {
   int* choice = nullptr;
   int* choice2 = nullptr;                /* second row list of the greedy matching */
   int* color = nullptr;
+  uint8_t* tent = nullptr;       /* the coloring's tentative colors, two buffers of capa_node */
   int* mate = nullptr;
   uint32_t* rank = nullptr;      /* four flip ranks per swap dual row */
   int* cnt = nullptr;            /* small device counters */
