@@ -1,5 +1,5 @@
-"""Free mode (GPU heuristics: Jones-Plassmann MIS and coloring, handshake
-matching): every stage keeps the mesh conforming and positively oriented, and
+"""Free mode (GPU heuristics: seeded-priority MIS, speculative first-fit
+coloring, greedy or handshake matching): every stage keeps the mesh conforming and positively oriented, and
 the final mesh matches the reference's size and metric-length quality, against
 the oracle at small sizes and against the reference build at 500k triangles."""
 import os

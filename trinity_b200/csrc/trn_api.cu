@@ -949,7 +949,7 @@ void enq_coarsen_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphCo
   cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s);
   cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s);
   coarsen_filter_append(dl, act_list(m, 0), m->status + S_ACT, m->target, m->list, m->status + S_NTASK,
-                        m->hws.state, m->fp32, s, bound);
+                        m->hws.state, m->hws.choice, m->hws.cnt + 112, m->fp32, s, bound);
   mis_jp_rounds(dl, m->list, m->status + S_NTASK, kMisRounds, seed_of(m, 0x9e37ULL), m->hws, m->indep,
                 m->status + S_NINDEP, s, bound);
   collapse(dl, m->indep, m->status + S_NINDEP, m->target, nullptr, s, bound);

@@ -228,7 +228,7 @@ void collapse(const DMesh& m, const int* indep, const int* count, const int* tar
  * adjacency + target + unordered candidate append in one pass */
 void coarsen_list_active(const DMesh& m, int nb_nodes, int* act, int* act_n, cudaStream_t s);
 void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int* target, int* cand,
-                           int* count, uint8_t* state, bool fp32, cudaStream_t s,
+                           int* count, uint8_t* state, int* chk, int* chk_n, bool fp32, cudaStream_t s,
                            long long bound = -1);
 
 /* swapping (swap.cu) */
@@ -291,7 +291,8 @@ void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual
  * list; undecided candidates are re-activated (next level) */
 void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, Seed seed,
                    HeurWs& ws, int* indep, int* nindep, cudaStream_t s, long long bound = -1);
-/* Jones-Plassmann first-fit coloring of interior vertices, colors 1..max_col;
+/* speculative first-fit coloring of interior vertices (tentative colors,
+ * priority conflicts resolved round by round), colors 1..max_col;
  * parts: vertex ids grouped by color, part_off[c] offsets (c = 0..max_col).
  * hint: grid size (at least the vertex count). color_jp runs batches of 8
  * rounds while vertices wait (at most 8 batches), reading the decision back
