@@ -8,11 +8,8 @@
  *                    keeps every surviving element CCW with edges <= sqrt(2)
  *                    (Coarse::identifyTarget, coarsening.cpp:47-133); ties are
  *                    broken in adjacency order, like the reference's multimap
- *   k_coarse_filter_scan   free mode, long lists: adjacency and "any neighbour
- *                    closer than 1/sqrt(2)?" per active vertex; those with
- *                    one go onto a check list
  *   k_coarse_filter_group  the same search by 4, 8 or 16 lanes per vertex, for
- *                    levels that list few vertices and for the check list
+ *                    levels that list few vertices (free mode)
  *   k_collapse       per independent vertex: erase the 1-2 shell elements,
  *                    move the rest of the stencil to the target, relabel,
  *                    tag repairs, re-activate the 1-ring (Coarse::collapseEdge,
@@ -25,7 +22,6 @@
 #include "trn_mixed.cuh"
 
 #include <algorithm>
-#include <climits>
 
 namespace trn {
 
@@ -116,16 +112,14 @@ __global__ void k_coarse_filter(DMesh m, int nb_nodes, int* __restrict__ target,
   }
 }
 
-/* the first half of the search on long lists: per active vertex, its
- * adjacency and whether any neighbour could be a target (closer than
- * 1/sqrt(2), with identify_target's boundary rule); a vertex with one goes
- * onto the check list for the grouped search, the others get no target.
- * The simulated collapses of the few vertices with candidates then run in
- * full groups instead of as the long branches of a few lanes of every warp
- * (10.7 of 32 lanes active in the one-pass search at 600x600). */
+/* free mode: one pass per level rebuilds the adjacency of each active vertex,
+ * finds its target and appends the candidates (in no particular order: the
+ * independent set is chosen by hashed priorities, not by list position),
+ * marking them undecided for the independent-set rounds */
 template <bool F32>
-__global__ void k_coarse_filter_scan(DMesh m, const int* __restrict__ act, const int* act_n,
-                                     int* __restrict__ target, int* __restrict__ chk, int* chk_n, int min_n) {
+__global__ void k_coarse_filter_append(DMesh m, const int* __restrict__ act, const int* act_n,
+                                       int* __restrict__ target, int* __restrict__ cand, int* count,
+                                       uint8_t* __restrict__ state, int min_n) {
   if (trn_failed(m)) return;
   const int n = *act_n;
   if (n < min_n) return;
@@ -134,20 +128,12 @@ __global__ void k_coarse_filter_scan(DMesh m, const int* __restrict__ act, const
     if (m.activ[v] <= 0) continue;
     m.activ[v] = 0;
     build_one_vicin(m, v);
-    const bool bound_source = (m.tags[v] & TRN_TAG_BOUND) != 0;
-    const int* vc = m.vic + (size_t) v * m.bucket;
-    const int nv = m.vdeg[v];
-    const double2 ps = m.pts[v];
-    const TenT<F32> ts = ten_load<F32>(m, v);
-    bool any = false;
-    for (int b = 0; !any && b < nv; ++b) {
-      const int w = vc[b];
-      if (bound_source && !(m.tags[w] & TRN_TAG_BOUND)) continue;
-      double len;
-      any = length_lt<F32>(ps, m.pts[w], ts, ten_load<F32>(m, w), TRN_L_MIN, &len);
+    const int t = identify_target<F32>(m, v);
+    target[v] = t;
+    if (t > -1) {
+      state[v] = 1;
+      trn_append(cand, count, v);
     }
-    if (any) trn_append(chk, chk_n, v);
-    else target[v] = -1;
   }
 }
 
@@ -159,13 +145,12 @@ __global__ void k_coarse_filter_scan(DMesh m, const int* __restrict__ act, const
  * the smallest (length, adjacency index) among the valid candidates, which is
  * the first valid one in the serial search's stable length order, so the
  * targets are the same. Vertices with more than 32 neighbours fall back to
- * the serial search on the group's first lane. With `prebuilt`, the list is
- * the scan's check list (adjacency built, activity cleared). */
+ * the serial search on the group's first lane. */
 
 template <bool F32, int G>
 __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, const int* act_n,
                                       int* __restrict__ target, int* __restrict__ cand, int* count,
-                                      uint8_t* __restrict__ state, int max_n, int prebuilt) {
+                                      uint8_t* __restrict__ state, int max_n) {
   if (trn_failed(m)) return;
   const int n = *act_n;
   if (n > max_n) return;
@@ -180,9 +165,7 @@ __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, cons
     int vv = -1;
     if (gl == 0 && q < n) {
       const int x = act[q];
-      if (prebuilt) {
-        vv = x;
-      } else if (m.activ[x] > 0) {
+      if (m.activ[x] > 0) {
         m.activ[x] = 0;
         build_one_vicin(m, x);
         vv = x;
@@ -392,47 +375,49 @@ void coarsen_list_active(const DMesh& m, int nb_nodes, int* act, int* act_n, cud
 }
 
 void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int* target, int* cand,
-                           int* count, uint8_t* state, int* chk, int* chk_n, bool fp32, cudaStream_t s,
-                           long long bound) {
+                           int* count, uint8_t* state, bool fp32, cudaStream_t s, long long bound) {
   ProfScope ps("coarsen_filter", s, 0.0);
   cudaMemsetAsync(count, 0, sizeof(int), s);
   /* a level listing at most group_max vertices runs the grouped search
-   * alone (faster below ~16k listed vertices); a longer one the scan, then
-   * the grouped search over the scan's check list. A known bound picks the
-   * form; an unknown one (a captured round) launches both, and the one that
-   * is not the count's case returns at once. */
+   * (measured on B200 with 8 lanes: faster below ~16k listed vertices, 2x
+   * slower on full-mesh levels), a larger one the one-lane search. A known
+   * bound (the level's list length) picks the form; with an unknown one (a
+   * captured round) both are launched, and the one that is not the device
+   * count's case returns at once. group_lanes = 1: the one-lane search at
+   * every size (a launch shape for the tests: the same targets). */
   const Tune& t = tune();
-  const int gm = t.group_max;
-  const bool small = bound >= 0 && bound <= gm;
-  const bool large = bound > gm;
+  const bool one = t.group_lanes == 1;
+  const int gm = one ? -1 : t.group_max;
+  const bool small = !one && bound >= 0 && bound <= gm;
+  const bool large = one || bound > gm;
   const int g = grid_bounded(bound, m.capa_node, t.filter_threads);
-  const long long gb = bound < 0 ? -1 : bound * t.group_lanes;
-  const int gg = grid_bounded(small || bound < 0 ? gb : 0, (long long) gm * t.group_lanes);
-  const int gc = grid_bounded(gb, (long long) m.capa_node * t.group_lanes);
-  if (!small) cudaMemsetAsync(chk_n, 0, sizeof(int), s);
-#define TRN_GROUP(F, G, L, N, LIM, PRE, GRID) \
-  k_coarse_filter_group<F, G><<<GRID, TRN_THREADS, 0, s>>>(m, L, N, target, cand, count, state, LIM, PRE)
-#define TRN_GROUPS(F, L, N, LIM, PRE, GRID)                       \
-  do {                                                              \
-    if (t.group_lanes == 4) TRN_GROUP(F, 4, L, N, LIM, PRE, GRID);  \
-    else if (t.group_lanes == 16) TRN_GROUP(F, 16, L, N, LIM, PRE, GRID); \
-    else TRN_GROUP(F, 8, L, N, LIM, PRE, GRID);                     \
-    note_launch();                                                  \
-  } while (0)
+  const int gg = grid_bounded(bound < 0 ? -1 : bound * t.group_lanes, (long long) gm * t.group_lanes);
+#define TRN_GROUP(F, G)                                                                              \
+  k_coarse_filter_group<F, G><<<gg, TRN_THREADS, 0, s>>>(m, act, act_n, target, cand, count, state, gm)
   if (!large) {
-    if (fp32) TRN_GROUPS(true, act, act_n, gm, 0, gg);
-    else TRN_GROUPS(false, act, act_n, gm, 0, gg);
-  }
-  if (!small) {
-    const int min_n = large ? 0 : gm + 1;
-    if (fp32) k_coarse_filter_scan<true><<<g, t.filter_threads, 0, s>>>(m, act, act_n, target, chk, chk_n, min_n);
-    else k_coarse_filter_scan<false><<<g, t.filter_threads, 0, s>>>(m, act, act_n, target, chk, chk_n, min_n);
+    if (fp32) {
+      if (t.group_lanes == 4) TRN_GROUP(true, 4);
+      else if (t.group_lanes == 16) TRN_GROUP(true, 16);
+      else TRN_GROUP(true, 8);
+    } else {
+      if (t.group_lanes == 4) TRN_GROUP(false, 4);
+      else if (t.group_lanes == 16) TRN_GROUP(false, 16);
+      else TRN_GROUP(false, 8);
+    }
     note_launch();
-    if (fp32) TRN_GROUPS(true, chk, chk_n, INT_MAX, 1, gc);
-    else TRN_GROUPS(false, chk, chk_n, INT_MAX, 1, gc);
   }
-#undef TRN_GROUPS
 #undef TRN_GROUP
+  if (!small) {
+    /* alone (a known long list, or one lane throughout), it takes any count */
+    const int min_n = large ? 0 : gm + 1;
+    if (fp32)
+      k_coarse_filter_append<true><<<g, t.filter_threads, 0, s>>>(m, act, act_n, target, cand, count, state,
+                                                                   min_n);
+    else
+      k_coarse_filter_append<false><<<g, t.filter_threads, 0, s>>>(m, act, act_n, target, cand, count, state,
+                                                                    min_n);
+    note_launch();
+  }
   check_launch("coarsen_filter_append");
 }
 

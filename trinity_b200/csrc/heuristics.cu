@@ -202,57 +202,25 @@ __global__ void __launch_bounds__(kFusedThreads) k_mis_fused(DMesh m, uint8_t* s
   for (int q = threadIdx.x; q < n; q += blockDim.x) mis_finish_item(m, state, other, cand[q], indep, nindep);
 }
 
-/* All the rounds and the collection in one cooperative launch, each round
- * over a worklist: a candidate undecided at a round's start goes on to the
- * next round's list, whether it decides or not, and a candidate decided in
- * the round before only copies its state into the other buffer and leaves
- * (both buffers then hold it, so later rounds need not visit it). The
- * states, and so the set, are those of the rounds over the whole list; the
- * work is the undecided candidates, not rounds x candidates. Once kMisTail
- * entries or fewer are listed, the first block runs the rounds alone. */
-constexpr int kMisTail = 2048;
-
+/* all the rounds and the collection in one cooperative launch */
 __global__ void __launch_bounds__(kFusedThreads) k_mis_persist(DMesh m, uint8_t* s0, uint8_t* s1,
                                                                const int* __restrict__ cand, const int* count,
                                                                Seed sd, int rounds, int* indep, int* nindep,
-                                                               int* wl0, int* wl1, int* rot, GridBar* bar) {
+                                                               GridBar* bar) {
   if (trn_failed(m)) return;
-  const int n0 = *count;
-  if (trn_tid() == 0) {
-    *nindep = 0;
-    rot[0] = rot[1] = rot[2] = 0;
-  }
-  if (!grid_sync(bar, m.err)) return;
+  const int n = *count;
+  if (trn_tid() == 0) *nindep = 0;
   const uint64_t base = trn_seed(sd);
-  bool alone = false;
   for (int r = 0; r < rounds; ++r) {
-    const int n = r == 0 ? n0 : *(volatile int*) (rot + r % 3);
-    if (n == 0) break;
-    if (!alone && n <= kMisTail) {
-      alone = true;
-      if (blockIdx.x != 0) break;   /* the others wait at the barrier below */
-    }
     const uint8_t* in = (r & 1) ? s1 : s0;
     uint8_t* out = (r & 1) ? s0 : s1;
-    const int* list = r == 0 ? cand : ((r & 1) ? wl0 : wl1);
-    int* next = (r & 1) ? wl1 : wl0;
     const uint64_t seed = base + 0x9e3779b97f4a7c15ULL * r;
-    const int t0 = alone ? (int) threadIdx.x : trn_tid();
-    const int ts = alone ? (int) blockDim.x : trn_grid_stride();
-    if (t0 == 0) rot[(r + 2) % 3] = 0;
-    for (int q = t0; q < n; q += ts) {
-      const int v = list[q];
-      if (in[v] == 1) trn_append(next, rot + (r + 1) % 3, v);
-      mis_item(m, in, out, v, seed);
-    }
-    if (alone) __syncthreads();
-    else if (!grid_sync(bar, m.err)) return;
+    for (int q = trn_tid(); q < n; q += trn_grid_stride()) mis_item(m, in, out, cand[q], seed);
+    if (!grid_sync(bar, m.err)) return;
   }
-  if (alone && !grid_sync(bar, m.err)) return;
-  /* the collection over the whole list */
   uint8_t* state = (rounds & 1) ? s1 : s0;
   uint8_t* other = (rounds & 1) ? s0 : s1;
-  for (int q = trn_tid(); q < n0; q += trn_grid_stride()) mis_finish_item(m, state, other, cand[q], indep, nindep);
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) mis_finish_item(m, state, other, cand[q], indep, nindep);
 }
 
 void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds, Seed sd,
@@ -260,8 +228,8 @@ void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds
   ProfScope ps("mis_jp", s, 0.0);
   uint8_t* buf[2] = {ws.state, ws.state2};
   if (bound > kFusedThreads &&
-      coop_launch(k_mis_persist, bound, kFusedThreads, s, m, buf[0], buf[1], cand, count, sd, rounds, indep,
-                  nindep, ws.choice, ws.choice2, ws.cnt + 108, grid_bar(ws))) {
+      coop_launch(k_mis_persist, bound, kFusedThreads, s, m, buf[0], buf[1], cand, count, sd, rounds, indep, nindep,
+                  grid_bar(ws))) {
     check_launch("mis_jp_rounds");
     return;
   }
@@ -1147,8 +1115,8 @@ void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {
   cudaMalloc(&ws->state2, big);
   cudaMemset(ws->state2, 0, big);
   cudaMalloc(&ws->prop, sizeof(unsigned long long) * (size_t) capa_elem);
-  cudaMalloc(&ws->choice, sizeof(int) * big);    /* also the independent set's worklists */
-  cudaMalloc(&ws->choice2, sizeof(int) * big);
+  cudaMalloc(&ws->choice, sizeof(int) * (size_t) capa_elem);
+  cudaMalloc(&ws->choice2, sizeof(int) * (size_t) capa_elem);
   cudaMalloc(&ws->prop2, sizeof(unsigned long long) * (size_t) capa_elem);
   cudaMalloc(&ws->tent, 2 * (size_t) capa_node);
   cudaMalloc(&ws->color, sizeof(int) * (size_t) capa_node);

@@ -13,7 +13,7 @@
  *   k_swap_filter_dual  free mode: the filter and the rows in one pass, with
  *                  the quality change of each row's flips when the matching
  *                  ranks its edges by gain
- *   k_swap_flip    per matched pair: flip the shared edge when both new
+ *   k_swap_flip2   per matched pair (two lanes): flip the shared edge when both new
  *                  elements are CCW and the smaller quality does not drop;
  *                  stencil appends, repair tags, cached qualities and
  *                  re-activation of the dual rows (Swap::swap, swapping.cpp:55-149)
@@ -234,51 +234,16 @@ __global__ void k_swap_filter_dual(DMesh m, const int* __restrict__ act, const i
   }
 }
 
-/* Swap::swap, swapping.cpp:55-149 */
-template <bool F32>
-__device__ int flip_pair(const DMesh& m, int id1, int id2, int index, const int* map,
-                         const int* dual, const int* dual_n, int ntasks, bool strict_map) {
-  int c1[3], c2[3];
-  double q0, q1;
-  if (!flip_eval<F32>(m, id1, id2, c1, c2, &q0, &q1)) return 0;
-  const double q_old = trn_dmin(m.qual[id1], m.qual[id2]);
-  const double q_new = trn_dmin(q0, q1);
-  if (q_new < q_old) return 0;
-  m.tri[id1] = make_int4(c1[0], c1[1], c1[2], 0);
-  m.tri[id2] = make_int4(c2[0], c2[1], c2[2], 0);
-  trn_stenc_append(m, c2[0], id2);
-  trn_stenc_append(m, c2[1], id1);
-  m.qual[id1] = q0;
-  m.qual[id2] = q1;
-  /* repair tags and re-activations: the flag atomics are independent of one
-   * another, and the newly set ones go onto their lists with one atomic
-   * each, which keeps a flip's chain of dependent L2 round trips short */
-  const int fv[4] = {c1[0], c1[1], c1[2], c2[2]};
-  int fx[4], nf = 0;
-  for (int j = 0; j < 4; ++j)
-    if (trn_byte_cas01(m.fixes + fv[j])) fx[nf++] = fv[j];
-  if (m.fix_list) trn_list_push_n(m.fix_list, m.fix_n, fx, nf);
-  int act[8], na = 0;
-  for (int q = 0; q < dual_n[index]; ++q) {
-    const int t = dual[index * 4 + q];
-    if (trn_byte_cas01(m.activ + t)) act[na++] = t;
-  }
-  /* the reference follows the map even when it points at a row of an earlier
-   * level (the map is reset once per call, swapping.cpp:161-162); replay keeps
-   * that, the free mode (rows numbered in append order) only follows rows of
-   * the current level */
-  const int x = map[id2];
-  if (x > -1 && (!strict_map || (x < ntasks && dual[x * 4] == id2)))
-    for (int q = 0; q < dual_n[x]; ++q) {
-      const int t = dual[x * 4 + q];
-      if (trn_byte_cas01(m.activ + t)) act[na++] = t;
-    }
-  if (m.act_next) trn_list_push_n(m.act_next, m.act_next_n, act, na);
-  return 2;
-}
-
-/* flip_pair with the two new qualities on two lanes: the pair's lanes run
- * the tests together, then lane 0 alone commits, with the same writes */
+/* Swap::swap, swapping.cpp:55-149, with the two new qualities on two lanes:
+ * the pair's lanes run the tests together, then lane 0 alone commits the
+ * flip (new element records, stencil appends, cached qualities), tags the
+ * four vertices for repair and re-activates the dual rows. The reference
+ * follows the map even when it points at a row of an earlier level (the map
+ * is reset once per call, swapping.cpp:161-162); replay keeps that, the free
+ * mode (rows numbered in append order) only follows rows of the current
+ * level. Flag atomics are independent of one another and the newly set ones
+ * go onto their lists with one atomic each, which keeps a flip's chain of
+ * dependent L2 round trips short. */
 template <bool F32>
 __device__ int flip_pair2(const DMesh& m, int id1, int id2, int index, const int* map,
                           const int* dual, const int* dual_n, int ntasks, bool strict_map, int half,
@@ -347,36 +312,6 @@ __global__ void k_swap_flip2(DMesh m, const int* __restrict__ pairs, const int* 
     }
     const int r = flip_pair2<F32>(m, k1, k2, index, map, dual, dual_n, ntasks, strict_map != 0, half, mask);
     if (!half) local += r;
-  }
-  if (local) atomicAdd(commit, local);
-}
-
-template <bool F32>
-__global__ void k_swap_flip(DMesh m, const int* __restrict__ pairs, const int* npairs,
-                            const int* __restrict__ map, const int* __restrict__ dual,
-                            const int* __restrict__ dual_n, const int* ntasks_dev, int* commit,
-                            int strict_map) {
-  if (trn_failed(m)) return;
-  const int np = *npairs;
-  const int ntasks = *ntasks_dev;
-  int local = 0;
-  for (int p = trn_tid(); p < np; p += trn_grid_stride()) {
-    const int k1 = pairs[2 * p], k2 = pairs[2 * p + 1];
-    if (k1 < 0 || k1 >= m.capa_elem || k2 < 0 || k2 >= m.capa_elem) {
-      trn_set_error(m.err, TRN_DERR_REPLAY);
-      continue;
-    }
-    const int index = map[k1];
-    bool ok = index >= 0 && index < ntasks && dual[index * 4] == k1;
-    if (ok) {
-      ok = false;
-      for (int q = 1; q < dual_n[index]; ++q) ok |= (dual[index * 4 + q] == k2);
-    }
-    if (!ok) {
-      trn_set_error(m.err, TRN_DERR_REPLAY);
-      continue;
-    }
-    local += flip_pair<F32>(m, k1, k2, index, map, dual, dual_n, ntasks, strict_map != 0);
   }
   if (local) atomicAdd(commit, local);
 }

@@ -949,7 +949,7 @@ void enq_coarsen_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphCo
   cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s);
   cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s);
   coarsen_filter_append(dl, act_list(m, 0), m->status + S_ACT, m->target, m->list, m->status + S_NTASK,
-                        m->hws.state, m->hws.choice, m->hws.cnt + 112, m->fp32, s, bound);
+                        m->hws.state, m->fp32, s, bound);
   mis_jp_rounds(dl, m->list, m->status + S_NTASK, kMisRounds, seed_of(m, 0x9e37ULL), m->hws, m->indep,
                 m->status + S_NINDEP, s, bound);
   collapse(dl, m->indep, m->status + S_NINDEP, m->target, nullptr, s, bound);
@@ -1366,7 +1366,7 @@ int trn_get_tune(trn_mesh* m, int cfg[TRN_TUNE_N]) {
 int trn_set_tune(trn_mesh* m, const int cfg[TRN_TUNE_N]) {
   if (!m || !cfg) return TRN_ERR_INVALID;
   auto pow2_in = [](int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; };
-  if (!pow2_in(cfg[0], 32, 256) || !pow2_in(cfg[1], 32, 1024) || (cfg[2] != 4 && cfg[2] != 8 && cfg[2] != 16) ||
+  if (!pow2_in(cfg[0], 32, 256) || !pow2_in(cfg[1], 32, 1024) || (cfg[2] != 1 && cfg[2] != 4 && cfg[2] != 8 && cfg[2] != 16) ||
       cfg[3] < 0 || !pow2_in(cfg[4], 32, 1024) || (cfg[5] != 1 && cfg[5] != 4 && cfg[5] != 8) ||
       cfg[6] < 0 || cfg[6] > 2)
     return fail(m, TRN_ERR_INVALID, "set_tune: value out of range");

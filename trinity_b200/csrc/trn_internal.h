@@ -228,7 +228,7 @@ void collapse(const DMesh& m, const int* indep, const int* count, const int* tar
  * adjacency + target + unordered candidate append in one pass */
 void coarsen_list_active(const DMesh& m, int nb_nodes, int* act, int* act_n, cudaStream_t s);
 void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int* target, int* cand,
-                           int* count, uint8_t* state, int* chk, int* chk_n, bool fp32, cudaStream_t s,
+                           int* count, uint8_t* state, bool fp32, cudaStream_t s,
                            long long bound = -1);
 
 /* swapping (swap.cu) */
