@@ -25,12 +25,17 @@
 
 namespace trn {
 
-__global__ void k_coarse_pre(DMesh m, int nb_nodes) {
+/* with `act`, the active vertices also go onto the list act (free mode's
+ * first level; the list is unordered by design) */
+__global__ void k_coarse_pre(DMesh m, int nb_nodes, int* __restrict__ act, int* act_n) {
   nb_nodes = trn_nodes(m, nb_nodes);
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
-    if (m.tags[v] & TRN_TAG_CORNER) m.activ[v] = -1;
-    else m.activ[v] = m.alive[v] ? 1 : 0;
+    int8_t a;
+    if (m.tags[v] & TRN_TAG_CORNER) a = -1;
+    else a = m.alive[v] ? 1 : 0;
+    m.activ[v] = a;
     m.fixes[v] = 0;
+    if (act && a > 0) trn_append(act, act_n, v);
   }
 }
 
@@ -348,8 +353,9 @@ __global__ void k_collapse(DMesh m, const int* __restrict__ indep, const int* co
   }
 }
 
-void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s) {
-  k_coarse_pre<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s, int* act, int* act_n) {
+  if (act) cudaMemsetAsync(act_n, 0, sizeof(int), s);
+  k_coarse_pre<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, act, act_n);
   note_launch();
   check_launch("coarsen_pre");
 }
@@ -362,17 +368,7 @@ void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, bo
   check_launch("coarsen_filter");
 }
 
-__global__ void k_coarse_list_active(DMesh m, int nb_nodes, int* act, int* act_n) {
-  nb_nodes = trn_nodes(m, nb_nodes);
-  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride())
-    if (m.activ[v] > 0) trn_append(act, act_n, v);
-}
 
-void coarsen_list_active(const DMesh& m, int nb_nodes, int* act, int* act_n, cudaStream_t s) {
-  cudaMemsetAsync(act_n, 0, sizeof(int), s);
-  k_coarse_list_active<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, act, act_n);
-  note_launch();
-}
 
 void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int* target, int* cand,
                            int* count, uint8_t* state, bool fp32, cudaStream_t s, long long bound) {

@@ -532,16 +532,26 @@ __device__ __forceinline__ void greedy_propose(const GreedyArgs& a, int r, int i
   for (int q = 0; q < a.dual_n[i]; ++q) atomicMin(mk + a.dual[i * 4 + q], key);
 }
 
-/* row i in round r: decide it when it is first on all its elements (and
- * return false), else propose it for round r + 1 (and return true) */
-__device__ __forceinline__ bool greedy_item(const GreedyArgs& a, int ntasks, int r, int i, int* pairs,
-                                            int* npairs) {
+/* is row i first on all its elements in round r? The loads of the row's
+ * slots past its length read slot 0 again (always there), so that every
+ * load can be issued before any compare */
+__device__ __forceinline__ bool greedy_ready(const GreedyArgs& a, int r, int i) {
   const unsigned long long* mk = (r & 1) ? a.mk1 : a.mk0;
+  const int4 row = reinterpret_cast<const int4*>(a.dual)[i];
+  const int dn = a.dual_n[i];
+  const unsigned long long key = greedy_key(r, row.x);
+  const unsigned long long k0 = mk[row.x], k1 = mk[dn > 1 ? row.y : row.x];
+  const unsigned long long k2 = mk[dn > 2 ? row.z : row.x], k3 = mk[dn > 3 ? row.w : row.x];
+  return k0 == key && k1 == key && k2 == key && k3 == key;
+}
+
+/* row i in round r, its readiness known: decide it when it is first on all
+ * its elements (and return false), else propose it for round r + 1 (and
+ * return true) */
+__device__ __forceinline__ bool greedy_act(const GreedyArgs& a, int ntasks, int r, int i, bool ready,
+                                           int* pairs, int* npairs) {
   const int c = a.dual[i * 4];
   const int dn = a.dual_n[i];
-  const unsigned long long key = greedy_key(r, c);
-  bool ready = true;
-  for (int q = 0; q < dn; ++q) ready &= (mk[a.dual[i * 4 + q]] == key);
   if (!ready) {
     greedy_propose(a, r + 1, i);
     return true;
@@ -562,6 +572,11 @@ __device__ __forceinline__ bool greedy_item(const GreedyArgs& a, int ntasks, int
     pairs[2 * p + 1] = partner;
   }
   return false;
+}
+
+__device__ __forceinline__ bool greedy_item(const GreedyArgs& a, int ntasks, int r, int i, int* pairs,
+                                            int* npairs) {
+  return greedy_act(a, ntasks, r, i, greedy_ready(a, r, i), pairs, npairs);
 }
 
 __global__ void k_greedy_reset(GreedyArgs a, const int* ntasks_dev, int min_n) {
@@ -595,9 +610,19 @@ __global__ void k_greedy_round(GreedyArgs a, const int* ntasks_dev, int r, int* 
     a.ran[r] = 1;
     a.cnt[(r + 2) % 3] = 0;   /* round r + 1's output */
   }
-  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
-    const int i = in[q];
-    if (greedy_item(a, ntasks, r, i, pairs, npairs)) trn_append(out, a.cnt + (r + 1) % 3, i);
+  /* two rows a thread an iteration, both rows' loads issued before either
+   * is decided (a round is a chain of dependent gathers: list entry, row,
+   * keys); the rows of a round are independent of one another */
+  const int stride = trn_grid_stride();
+  for (int q = trn_tid(); q < n; q += 2 * stride) {
+    const int q2 = q + stride;
+    const bool two = q2 < n;
+    const int i1 = in[q];
+    const int i2 = two ? in[q2] : i1;
+    const bool ok1 = greedy_ready(a, r, i1);
+    const bool ok2 = greedy_ready(a, r, i2);
+    if (greedy_act(a, ntasks, r, i1, ok1, pairs, npairs)) trn_append(out, a.cnt + (r + 1) % 3, i1);
+    if (two && greedy_act(a, ntasks, r, i2, ok2, pairs, npairs)) trn_append(out, a.cnt + (r + 1) % 3, i2);
   }
 }
 

@@ -31,8 +31,11 @@ __global__ void k_swap_init_nodes(DMesh m, int nb_nodes) {
   for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) m.fixes[v] = 0;
 }
 
+/* with `act`, the live (active) elements also go onto the list act (free
+ * mode's first level; the list is unordered by design) */
 template <bool F32>
-__global__ void k_swap_init_elems(DMesh m, int nb_elems, int* __restrict__ map) {
+__global__ void k_swap_init_elems(DMesh m, int nb_elems, int* __restrict__ map, int* __restrict__ act,
+                                  int* act_n) {
   nb_elems = trn_elems(m, nb_elems);
   if (trn_failed(m)) return;
   for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
@@ -44,6 +47,7 @@ __global__ void k_swap_init_elems(DMesh m, int nb_elems, int* __restrict__ map) 
     }
     m.qual[i] = quality_of<F32>(m, t);
     m.activ[i] = 1;
+    if (act) trn_append(act, act_n, i);
   }
 }
 
@@ -316,13 +320,15 @@ __global__ void k_swap_flip2(DMesh m, const int* __restrict__ pairs, const int* 
   if (local) atomicAdd(commit, local);
 }
 
-void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, bool fp32, cudaStream_t s) {
+void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, bool fp32, cudaStream_t s, int* act,
+               int* act_n) {
   ProfScope ps("swap_init", s, (double) nb_nodes + (double) nb_elems * (kTri + kQ + 4 + 1) +
                                  (double) nb_elems / 2 * (kPt + kTen));
   k_swap_init_nodes<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
   note_launch();
-  if (fp32) k_swap_init_elems<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, map);
-  else k_swap_init_elems<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, map);
+  if (act) cudaMemsetAsync(act_n, 0, sizeof(int), s);
+  if (fp32) k_swap_init_elems<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, map, act, act_n);
+  else k_swap_init_elems<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, map, act, act_n);
   note_launch();
   check_launch("swap_init");
 }
@@ -340,18 +346,6 @@ void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual
   k_swap_dual<<<grid_for(ntasks), TRN_THREADS, 0, s>>>(m, list, ntasks, dual, dual_n, map);
   note_launch();
   check_launch("swap_dual");
-}
-
-__global__ void k_swap_list_active(DMesh m, int nb_elems, int* act, int* act_n) {
-  nb_elems = trn_elems(m, nb_elems);
-  for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride())
-    if (m.activ[i]) trn_append(act, act_n, i);
-}
-
-void swap_list_active(const DMesh& m, int nb_elems, int* act, int* act_n, cudaStream_t s) {
-  cudaMemsetAsync(act_n, 0, sizeof(int), s);
-  k_swap_list_active<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, act, act_n);
-  note_launch();
 }
 
 void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,

@@ -75,6 +75,11 @@ struct trn_mesh {
   Tune tune;                /* launch shapes (trn_autotune) */
   Tune round_tune;
   bool round_fp32 = false;
+  /* the cached element qualities equal a recomputation of every live
+   * element: set by a swap or smoothing call that ended without error,
+   * cleared by every other call that can change points, tensors, elements
+   * or the arithmetic form (all stage calls clear it as they begin) */
+  bool qual_fresh = false;
   uint64_t round_seed = 0;
   int round_swap_match = 0;
   int round_level_cap = 0;
@@ -134,6 +139,7 @@ int sync_status(trn_mesh* m, const int* count = nullptr) {
 }
 
 void begin_timing(trn_mesh* m) {
+  m->qual_fresh = false;
   set_thread_tune(&m->tune);
   cudaEventRecord(m->ev0, m->stream);
 }
@@ -369,6 +375,7 @@ static int init_from_device(trn_mesh* m) {
 
 int trn_mesh_load_arrays(trn_mesh* m, int nb_nodes, int nb_elems, const double* points,
                          const int* tris, const uint8_t* tags, const double* solut) {
+  if (m) m->qual_fresh = false;
   if (!m || !points || !tris || nb_nodes <= 0 || nb_elems <= 0) return fail(m, TRN_ERR_INVALID, "load: bad arguments");
   if (nb_nodes > m->capa_node || nb_elems > m->capa_elem)
     return fail(m, TRN_ERR_CAPACITY, "load: mesh larger than the capacity");
@@ -406,6 +413,7 @@ int trn_mesh_load_arrays(trn_mesh* m, int nb_nodes, int nb_elems, const double* 
 }
 
 int trn_mesh_reload(trn_mesh* m) {
+  if (m) m->qual_fresh = false;
   if (!m || !m->pts0) return fail(m, TRN_ERR_INVALID, "reload: nothing loaded");
   m->err.clear();
   return init_from_device(m);
@@ -471,6 +479,7 @@ static int load_tokens(trn_mesh* m, Reader& r, MeshInput* in) {
 /* Mesh::load, io.cpp:53-161: a medit .mesh (or the binary form written by
  * trn_mesh_store_binary) and an optional .bb nodal solution */
 int trn_mesh_load(trn_mesh* m, const char* mesh_path, const char* solut_path) {
+  if (m) m->qual_fresh = false;
   if (!m || !mesh_path) return fail(m, TRN_ERR_INVALID, "load: null path");
   MeshInput in;
   {
@@ -670,6 +679,7 @@ int trn_mesh_export_compact(trn_mesh* m, double* points, int* tris, double* tens
  * order, live elements in slot order, every structure rebuilt as a load
  * builds it. The state becomes the one trn_mesh_reload returns to. */
 int trn_mesh_compact(trn_mesh* m) {
+  if (m) m->qual_fresh = false;
   if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "compact: no mesh loaded");
   m->err.clear();
   cudaStream_t s = m->stream;
@@ -815,6 +825,7 @@ int trn_mesh_store_sol(trn_mesh* m, const char* path) {
 }
 
 int trn_set_replay(trn_mesh* m, const int32_t* log, size_t n) {
+  if (m) m->qual_fresh = false;
   if (!m) return TRN_ERR_INVALID;
   if (m->d_log) {
     cudaFree(m->d_log);
@@ -833,6 +844,7 @@ int trn_set_replay(trn_mesh* m, const int32_t* log, size_t n) {
 }
 
 int trn_set_precision(trn_mesh* m, int mode) {
+  if (m) m->qual_fresh = false;
   if (!m || (mode != TRN_PRECISION_FP64 && mode != TRN_PRECISION_MIXED))
     return fail(m, TRN_ERR_INVALID, "set_precision: unknown mode");
   const bool f = mode == TRN_PRECISION_MIXED;
@@ -938,8 +950,7 @@ void enq_refine(trn_mesh* m, int depth, cudaStream_t s) {
 
 void enq_coarsen_begin(trn_mesh* m, cudaStream_t s, bool capture) {
   stats_reset(m, s);
-  coarsen_pre(m->d, hint_nodes(m, capture), s);
-  coarsen_list_active(m->d, hint_nodes(m, capture), act_list(m, 0), m->status + S_ACT, s);
+  coarsen_pre(m->d, hint_nodes(m, capture), s, act_list(m, 0), m->status + S_ACT);
 }
 
 /* one free-mode coarsening level over list 0 (bound: its length, < 0 unknown) */
@@ -960,8 +971,8 @@ void enq_coarsen_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphCo
 
 void enq_swap_begin(trn_mesh* m, cudaStream_t s, bool capture) {
   stats_reset(m, s);
-  swap_init(m->d, hint_nodes(m, capture), hint_elems(m, capture), m->map, m->fp32, s);
-  swap_list_active(m->d, hint_elems(m, capture), act_list(m, 0), m->status + S_ACT, s);
+  swap_init(m->d, hint_nodes(m, capture), hint_elems(m, capture), m->map, m->fp32, s, act_list(m, 0),
+            m->status + S_ACT);
 }
 
 void enq_swap_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphConditionalHandle h,
@@ -1069,7 +1080,9 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
       if (rc) return rc;
       bound = m->h_status[S_ACT];
     } while (m->h_status[S_CONT]);
-    return end_timing(m, st, m->h_status[S_EVAL], m->h_status[S_TASK]);
+    const int rc = end_timing(m, st, m->h_status[S_EVAL], m->h_status[S_TASK]);
+    m->qual_fresh = rc == TRN_OK;
+    return rc;
   }
   swap_init(m->d, m->nb_nodes, m->nb_elems, m->map, m->fp32, s);
   int eval = 0, task = 0, commit = 0, level = 0;
@@ -1094,7 +1107,9 @@ int trn_swap_run(trn_mesh* m, trn_stats* st) {
     task += commit / 2;
     if (++level > m->level_cap) return fail(m, TRN_ERR_NO_PROGRESS, "swap: level cap reached");
   } while (commit);
-  return end_timing(m, st, eval, task);
+  const int rc = end_timing(m, st, eval, task);
+  m->qual_fresh = rc == TRN_OK;
+  return rc;
 }
 
 /* Smooth::run, smoothing.cpp:274-302 */
@@ -1102,6 +1117,7 @@ int trn_smooth_run(trn_mesh* m, int max_colors, int depth, trn_stats* st) {
   if (!m || m->nb_nodes <= 0) return fail(m, TRN_ERR_INVALID, "smooth: no mesh loaded");
   const int max_col = max_colors_of(max_colors);
   m->err.clear();
+  const bool fresh = m->qual_fresh;
   begin_timing(m);
   cudaStream_t s = m->stream;
   smooth_pre(m->d, m->nb_nodes, s);
@@ -1128,13 +1144,19 @@ int trn_smooth_run(trn_mesh* m, int max_colors, int depth, trn_stats* st) {
       classes.emplace_back(m->parts + a, b - a);
     }
   }
-  quality_all(m->d, m->nb_elems, m->fp32, s);
+  /* the cached qualities (smoothing.cpp:145-151); a swap or smoothing call
+   * just before left them equal to this recomputation, bit for bit (the
+   * flips and moves store the qualities of the elements they change, from
+   * the same arithmetic) */
+  if (!fresh) quality_all(m->d, m->nb_elems, m->fp32, s);
   CK(cudaMemsetAsync(m->status + S_SMOOTH_TASKS, 0, sizeof(int) * 2, s));
   for (int level = 0; level < depth; ++level)
     for (auto& c : classes) smooth_color(m->d, c.first, c.second, m->status + S_SMOOTH_TASKS, m->fp32, s);
   int rc = sync_status(m);
   if (rc) return rc;
-  return end_timing(m, st, m->h_status[S_SMOOTH_TASKS], m->h_status[S_SMOOTH_COMMIT]);
+  rc = end_timing(m, st, m->h_status[S_SMOOTH_TASKS], m->h_status[S_SMOOTH_COMMIT]);
+  m->qual_fresh = rc == TRN_OK;
+  return rc;
 }
 
 /* the element-quality functional J = sum_T q_T and its adjoint */

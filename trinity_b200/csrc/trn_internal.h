@@ -220,29 +220,31 @@ void refine_level(const DMesh& m, int hint_nodes, int hint_elems, RefineWs& ws, 
                   int* stats, bool fp32, cudaStream_t s);
 
 /* coarsening (coarsen.cu) */
-void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
+/* with act: the active vertices onto the list act too (*act_n their count) */
+void coarsen_pre(const DMesh& m, int nb_nodes, cudaStream_t s, int* act = nullptr, int* act_n = nullptr);
 void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, bool fp32, cudaStream_t s);
 void collapse(const DMesh& m, const int* indep, const int* count, const int* target,
               const uint8_t* cand_flag, cudaStream_t s, long long bound = -1);
-/* free mode: list the active vertices; then per level, over that list,
- * adjacency + target + unordered candidate append in one pass */
-void coarsen_list_active(const DMesh& m, int nb_nodes, int* act, int* act_n, cudaStream_t s);
+/* free mode, per level, over the list of active vertices (coarsen_pre lists
+ * them first): adjacency + target + unordered candidate append in one pass */
 void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int* target, int* cand,
                            int* count, uint8_t* state, bool fp32, cudaStream_t s,
                            long long bound = -1);
 
 /* swapping (swap.cu) */
-void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, bool fp32, cudaStream_t s);
+/* with act: the live elements onto the list act too (*act_n their count) */
+void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, bool fp32, cudaStream_t s,
+               int* act = nullptr, int* act_n = nullptr);
 void swap_filter(const DMesh& m, int nb_elems, uint8_t* flag, cudaStream_t s);
 void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual_n, int* map,
                cudaStream_t s);
 void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* map,
                const int* dual, const int* dual_n, const int* ntasks, int* commit, bool strict_map,
                bool fp32, cudaStream_t s, long long bound = -1);
-/* free mode: list the active elements; per level, filter and dual rows in
- * one pass over the list, *count rows; when rank is given, rank[4 r + e]:
- * the gain rank of the flip between row r's candidate and its neighbour e */
-void swap_list_active(const DMesh& m, int nb_elems, int* act, int* act_n, cudaStream_t s);
+/* free mode, per level: filter and dual rows in one pass over the list of
+ * active elements (swap_init lists them first), *count rows; when rank is
+ * given, rank[4 r + e]: the gain rank of the flip between row r's candidate
+ * and its neighbour e */
 void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,
                       int* map, uint32_t* rank, int* count, bool fp32, cudaStream_t s,
                       long long bound = -1);
