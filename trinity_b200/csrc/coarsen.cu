@@ -29,13 +29,16 @@ namespace trn {
  * first level; the list is unordered by design) */
 __global__ void k_coarse_pre(DMesh m, int nb_nodes, int* __restrict__ act, int* act_n) {
   nb_nodes = trn_nodes(m, nb_nodes);
-  for (int v = trn_tid(); v < nb_nodes; v += trn_grid_stride()) {
-    int8_t a;
-    if (m.tags[v] & TRN_TAG_CORNER) a = -1;
-    else a = m.alive[v] ? 1 : 0;
-    m.activ[v] = a;
-    m.fixes[v] = 0;
-    if (act && a > 0) trn_append(act, act_n, v);
+  for (int base = blockIdx.x * blockDim.x; base < nb_nodes; base += trn_grid_stride()) {
+    const int v = base + threadIdx.x;
+    int8_t a = 0;
+    if (v < nb_nodes) {
+      if (m.tags[v] & TRN_TAG_CORNER) a = -1;
+      else a = m.alive[v] ? 1 : 0;
+      m.activ[v] = a;
+      m.fixes[v] = 0;
+    }
+    if (act) trn_block_append(act, act_n, v, a > 0);
   }
 }
 
@@ -125,20 +128,23 @@ template <bool F32>
 __global__ void k_coarse_filter_append(DMesh m, const int* __restrict__ act, const int* act_n,
                                        int* __restrict__ target, int* __restrict__ cand, int* count,
                                        uint8_t* __restrict__ state, int min_n) {
-  if (trn_failed(m)) return;
+  if (trn_failed_block(m)) return;
   const int n = *act_n;
   if (n < min_n) return;
-  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
-    const int v = act[q];
-    if (m.activ[v] <= 0) continue;
-    m.activ[v] = 0;
-    build_one_vicin(m, v);
-    const int t = identify_target<F32>(m, v);
-    target[v] = t;
-    if (t > -1) {
-      state[v] = 1;
-      trn_append(cand, count, v);
+  for (int base = blockIdx.x * blockDim.x; base < n; base += trn_grid_stride()) {
+    const int q = base + threadIdx.x;
+    int v = -1, t = -1;
+    if (q < n) {
+      v = act[q];
+      if (m.activ[v] > 0) {
+        m.activ[v] = 0;
+        build_one_vicin(m, v);
+        t = identify_target<F32>(m, v);
+        target[v] = t;
+        if (t > -1) state[v] = 1;
+      }
     }
+    trn_block_append(cand, count, v, t > -1);
   }
 }
 
@@ -406,12 +412,9 @@ void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int
   if (!small) {
     /* alone (a known long list, or one lane throughout), it takes any count */
     const int min_n = large ? 0 : gm + 1;
-    if (fp32)
-      k_coarse_filter_append<true><<<g, t.filter_threads, 0, s>>>(m, act, act_n, target, cand, count, state,
-                                                                   min_n);
-    else
-      k_coarse_filter_append<false><<<g, t.filter_threads, 0, s>>>(m, act, act_n, target, cand, count, state,
-                                                                    min_n);
+    auto* kern = fp32 ? k_coarse_filter_append<true> : k_coarse_filter_append<false>;
+    kern<<<grid_resident(reinterpret_cast<const void*>(kern), t.filter_threads, g), t.filter_threads, 0, s>>>(
+        m, act, act_n, target, cand, count, state, min_n);
     note_launch();
   }
   check_launch("coarsen_filter_append");

@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_mis_persist(DMesh m, uint8_t*
                                                                const int* __restrict__ cand, const int* count,
                                                                Seed sd, int rounds, int* indep, int* nindep,
                                                                GridBar* bar) {
-  if (trn_failed(m)) return;
+  if (trn_failed_block(m)) return;
   const int n = *count;
   if (trn_tid() == 0) *nindep = 0;
   const uint64_t base = trn_seed(sd);
@@ -610,19 +610,11 @@ __global__ void k_greedy_round(GreedyArgs a, const int* ntasks_dev, int r, int* 
     a.ran[r] = 1;
     a.cnt[(r + 2) % 3] = 0;   /* round r + 1's output */
   }
-  /* two rows a thread an iteration, both rows' loads issued before either
-   * is decided (a round is a chain of dependent gathers: list entry, row,
-   * keys); the rows of a round are independent of one another */
-  const int stride = trn_grid_stride();
-  for (int q = trn_tid(); q < n; q += 2 * stride) {
-    const int q2 = q + stride;
-    const bool two = q2 < n;
-    const int i1 = in[q];
-    const int i2 = two ? in[q2] : i1;
-    const bool ok1 = greedy_ready(a, r, i1);
-    const bool ok2 = greedy_ready(a, r, i2);
-    if (greedy_act(a, ntasks, r, i1, ok1, pairs, npairs)) trn_append(out, a.cnt + (r + 1) % 3, i1);
-    if (two && greedy_act(a, ntasks, r, i2, ok2, pairs, npairs)) trn_append(out, a.cnt + (r + 1) % 3, i2);
+  for (int base = blockIdx.x * blockDim.x; base < n; base += trn_grid_stride()) {
+    const int q = base + threadIdx.x;
+    const int i = q < n ? in[q] : -1;
+    const bool wait = q < n && greedy_item(a, ntasks, r, i, pairs, npairs);
+    trn_block_append(out, a.cnt + (r + 1) % 3, i, wait);
   }
 }
 
@@ -708,12 +700,14 @@ __global__ void __launch_bounds__(kFusedThreads) k_greedy_persist(GreedyArgs a, 
     }
     const int* in = (r & 1) ? a.list1 : a.list0;
     int* out = (r & 1) ? a.list0 : a.list1;
-    const int t0 = alone ? (int) threadIdx.x : trn_tid();
-    const int ts = alone ? (int) blockDim.x : trn_grid_stride();
-    if (t0 == 0) a.cnt[(r + 2) % 3] = 0;
-    for (int q = t0; q < n; q += ts) {
-      const int i = in[q];
-      if (greedy_item(a, ntasks, r, i, pairs, npairs)) trn_append(out, a.cnt + (r + 1) % 3, i);
+    const int b0 = alone ? 0 : (int) (blockIdx.x * blockDim.x);
+    const int bs = alone ? (int) blockDim.x : trn_grid_stride();
+    if (b0 == 0 && threadIdx.x == 0) a.cnt[(r + 2) % 3] = 0;
+    for (int base = b0; base < n; base += bs) {
+      const int q = base + threadIdx.x;
+      const int i = q < n ? in[q] : -1;
+      const bool wait = q < n && greedy_item(a, ntasks, r, i, pairs, npairs);
+      trn_block_append(out, a.cnt + (r + 1) % 3, i, wait);
     }
     if (alone) __syncthreads();
     else if (!grid_sync(bar, err)) return;
@@ -1073,7 +1067,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_color_persist(DMesh m, int* l
                                                                  int* counts, int* rot, int* color,
                                                                  uint8_t* tent, int max_col, Seed sd,
                                                                  int* round_ctr, GridBar* bar) {
-  if (trn_failed(m)) return;
+  if (trn_failed_block(m)) return;
   const uint64_t seed = trn_seed(sd);
   int round = *round_ctr;
   if (trn_tid() == 0) {
@@ -1094,13 +1088,14 @@ __global__ void __launch_bounds__(kFusedThreads) k_color_persist(DMesh m, int* l
     ++round;
     int* in = (it & 1) ? list_b : list_a;
     int* out = (it & 1) ? list_a : list_b;
-    const int t0 = alone ? (int) threadIdx.x : trn_tid();
-    const int ts = alone ? (int) blockDim.x : trn_grid_stride();
-    if (t0 == 0) rot[(it + 2) % 3] = 0;
-    for (int q = t0; q < n; q += ts) {
-      const int v = in[q];
-      if (color_item(m, v, color, tent, m.capa_node, max_col, seed, round))
-        trn_append(out, rot + (it + 1) % 3, v);
+    const int b0 = alone ? 0 : (int) (blockIdx.x * blockDim.x);
+    const int bs = alone ? (int) blockDim.x : trn_grid_stride();
+    if (b0 == 0 && threadIdx.x == 0) rot[(it + 2) % 3] = 0;
+    for (int base = b0; base < n; base += bs) {
+      const int q = base + threadIdx.x;
+      const int v = q < n ? in[q] : -1;
+      const bool wait = q < n && color_item(m, v, color, tent, m.capa_node, max_col, seed, round);
+      trn_block_append(out, rot + (it + 1) % 3, v, wait);
     }
     if (alone) __syncthreads();
     else if (!grid_sync(bar, m.err)) return;

@@ -11,6 +11,9 @@
  * sums, and a tile-local scan that adds the tile offset and writes.
  */
 #include "trn_internal.h"
+#include <tuple>
+#include <mutex>
+#include <map>
 
 #include <cstdio>
 
@@ -198,6 +201,38 @@ void set_thread_tune(const Tune* t) { t_tune = t; }
 
 int grid_bounded(long long bound, long long cap, int threads) {
   return grid_for(bound < 0 ? cap : (bound < cap ? bound : cap), threads);
+}
+
+/* at most as many blocks as are resident at once on the device (one wave:
+ * a grid-stride kernel whose blocks hold more registers than grid_for's
+ * 8 a SM assumes would otherwise end on a partial wave) */
+int grid_resident(const void* kernel, int threads, int grid, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, size_t>, int> cache;
+  static const int sms = [] {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+  }();
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_tuple(kernel, threads, smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      per_sm = it->second;
+    } else {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 0;
+      }
+      cache[key] = per_sm;
+    }
+  }
+  if (per_sm <= 0) return grid;
+  const int cap = per_sm * sms;
+  return grid < cap ? grid : cap;
 }
 
 int grid_for(long long n, int threads) {

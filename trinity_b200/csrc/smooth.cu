@@ -409,7 +409,12 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
   const int g = grid_for((long long) hint * lanes, t);
   const int regs = tune().smooth_regs;
   if (lanes == 8 || lanes == 4) {
-#define TRN_GRP(F, G, B) k_smooth_move_grp<F, G, B><<<g, t, 0, s>>>(m, list, n, off, c, counters, bc)
+#define TRN_GRP(F, G, B)                                                                     \
+  do {                                                                                       \
+    auto* kern = k_smooth_move_grp<F, G, B>;                                                 \
+    kern<<<grid_resident(reinterpret_cast<const void*>(kern), t, g), t, 0, s>>>(m, list, n, off, c, \
+                                                                                counters, bc); \
+  } while (0)
 #define TRN_GRP_B(F, G) \
   do { if (regs == 0) TRN_GRP(F, G, 2); else if (regs == 1) TRN_GRP(F, G, 3); else TRN_GRP(F, G, 4); } while (0)
     if (lanes == 8) {
@@ -427,7 +432,12 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
     const int slot = fp32 ? (int) sizeof(float4) : (int) sizeof(double4);
     const int kj = std::min(fp32 ? 12 : 8, (40 << 10) / (t * slot));
     const size_t smem = (size_t) kj * t * slot;
-#define TRN_ONE(F, B) k_smooth_move<F, B><<<g, t, smem, s>>>(m, list, n, off, c, counters, kj, bc)
+#define TRN_ONE(F, B)                                                                           \
+  do {                                                                                          \
+    auto* kern = k_smooth_move<F, B>;                                                           \
+    kern<<<grid_resident(reinterpret_cast<const void*>(kern), t, g, smem), t, smem, s>>>(m, list, n, off, \
+                                                                                        c, counters, kj, bc); \
+  } while (0)
 #define TRN_ONE_B(F) \
   do { if (regs == 0) TRN_ONE(F, 2); else if (regs == 1) TRN_ONE(F, 3); else TRN_ONE(F, 4); } while (0)
     if (fp32) TRN_ONE_B(true);

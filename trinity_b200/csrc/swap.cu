@@ -37,17 +37,18 @@ template <bool F32>
 __global__ void k_swap_init_elems(DMesh m, int nb_elems, int* __restrict__ map, int* __restrict__ act,
                                   int* act_n) {
   nb_elems = trn_elems(m, nb_elems);
-  if (trn_failed(m)) return;
-  for (int i = trn_tid(); i < nb_elems; i += trn_grid_stride()) {
-    map[i] = -1;
-    int4 t = m.tri[i];
-    if (t.x < 0) {
-      m.activ[i] = 0;
-      continue;
+  if (trn_failed_block(m)) return;
+  for (int base = blockIdx.x * blockDim.x; base < nb_elems; base += trn_grid_stride()) {
+    const int i = base + threadIdx.x;
+    bool live = false;
+    if (i < nb_elems) {
+      map[i] = -1;
+      const int4 t = m.tri[i];
+      live = t.x >= 0;
+      if (live) m.qual[i] = quality_of<F32>(m, t);
+      m.activ[i] = live ? 1 : 0;
     }
-    m.qual[i] = quality_of<F32>(m, t);
-    m.activ[i] = 1;
-    if (act) trn_append(act, act_n, i);
+    if (act) trn_block_append(act, act_n, i, live);
   }
 }
 
@@ -353,10 +354,9 @@ void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dua
   ProfScope ps("swap_filter", s, 0.0);
   cudaMemsetAsync(count, 0, sizeof(int), s);
   const int g = grid_bounded(bound, m.capa_elem);
-  if (fp32)
-    k_swap_filter_dual<true><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, dual, dual_n, map, rank, count);
-  else
-    k_swap_filter_dual<false><<<g, TRN_THREADS, 0, s>>>(m, act, act_n, dual, dual_n, map, rank, count);
+  auto* kern = fp32 ? k_swap_filter_dual<true> : k_swap_filter_dual<false>;
+  kern<<<grid_resident(reinterpret_cast<const void*>(kern), TRN_THREADS, g), TRN_THREADS, 0, s>>>(
+      m, act, act_n, dual, dual_n, map, rank, count);
   note_launch();
   check_launch("swap_filter_dual");
 }
@@ -368,12 +368,9 @@ void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* m
   const int ft = tune().flip_threads;
   /* two lanes a pair: the grid sized for twice the pairs */
   const int g = grid_bounded(bound < 0 ? bound : 2 * bound, 2LL * m.capa_elem, ft);
-  if (fp32)
-    k_swap_flip2<true><<<g, ft, 0, s>>>(m, pairs, npairs, map, dual, dual_n, ntasks, commit,
-                                        strict_map ? 1 : 0);
-  else
-    k_swap_flip2<false><<<g, ft, 0, s>>>(m, pairs, npairs, map, dual, dual_n, ntasks, commit,
-                                         strict_map ? 1 : 0);
+  auto* kern = fp32 ? k_swap_flip2<true> : k_swap_flip2<false>;
+  kern<<<grid_resident(reinterpret_cast<const void*>(kern), ft, g), ft, 0, s>>>(
+      m, pairs, npairs, map, dual, dual_n, ntasks, commit, strict_map ? 1 : 0);
   note_launch();
   check_launch("swap_flip");
 }

@@ -283,6 +283,36 @@ __device__ __forceinline__ void trn_append(int* list, int* count, int id) {
   list[base + __popc(mask & ((1u << lane) - 1))] = id;
 }
 
+/* trn_failed read once for the whole block, so that every thread of a block
+ * that goes on to trn_block_append takes the same branch */
+__device__ __forceinline__ bool trn_failed_block(const DMesh& m) {
+  __shared__ int s_failed;
+  if (threadIdx.x == 0) s_failed = *(volatile int*) m.err;
+  __syncthreads();
+  return s_failed != 0;
+}
+
+/* append id to list[*count] when `want`. Every thread of the block calls it
+ * together (from a block-uniform loop): the warps count their appends in
+ * shared memory and the block reserves its slots with one global atomic.
+ * Appends of many warps onto one counter otherwise serialize in L2 (a few
+ * ns each: 62k warp atomics took 170 us when every live element of the 2M
+ * workload was listed). */
+__device__ __forceinline__ void trn_block_append(int* list, int* count, int id, bool want) {
+  __shared__ int s_n, s_base;
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  const unsigned mask = __ballot_sync(0xffffffffu, want);
+  int wbase = 0;
+  if (lane == 0 && mask) wbase = atomicAdd(&s_n, __popc(mask));
+  wbase = __shfl_sync(0xffffffffu, wbase, 0);
+  __syncthreads();
+  if (threadIdx.x == 0) s_base = s_n ? atomicAdd(count, s_n) : 0;
+  __syncthreads();
+  if (want) list[s_base + wbase + __popc(mask & ((1u << lane) - 1))] = id;
+}
+
 /* seed of a level's hashed priorities: base ^ (tick * mix), tick a device
  * counter that each coarsening / swapping level and each coloring advances,
  * so the seed sequence lives on the device (a captured round replays it) */

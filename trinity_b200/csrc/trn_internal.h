@@ -113,6 +113,8 @@ int grid_for(long long n, int threads = TRN_THREADS);
  * upper bound the host knows, < 0 = unknown) and at most `cap`; the kernels
  * stride over the true count, so the bound only sizes the launch */
 int grid_bounded(long long bound, long long cap, int threads = TRN_THREADS);
+/* grid capped at the blocks of `kernel` resident at once (one wave) */
+int grid_resident(const void* kernel, int threads, int grid, size_t smem = 0);
 
 /* scratch used by the scans: tile sums of up to max_n items */
 struct ScanWs {
