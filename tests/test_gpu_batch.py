@@ -44,7 +44,8 @@ def test_batch_meshes_are_valid_and_match_the_reference_build(tmp_path):
     adapted concurrently with captured rounds: every one conforming, CCW and
     a disk; the ones of 50k triangles or more (sides 195 to 511) within 2 %
     of the reference build's final triangle count and 1 point of its fraction
-    of metric edge lengths in [1/sqrt 2, sqrt 2], each on the same input. (The
+    of metric edge lengths in [1/sqrt 2, sqrt 2] (medians of 3 reference
+    runs: its OpenMP heuristics vary from run to run), each on the same input. (The
     smaller ones, coarse grids under steep shocks, end far from unit lengths
     after 3 rounds of depth 1 in both codes.) The workload's swap matching is
     the row-slot handshake (meshgen.BATCH_PARAMS)."""
@@ -72,15 +73,22 @@ def test_batch_meshes_are_valid_and_match_the_reference_build(tmp_path):
     assert len(big) >= 3
     for k in big:
         m, u, spec = items[k]
-        mp, bp, out = (str(tmp_path / f"b{k}.mesh"), str(tmp_path / f"b{k}.bb"), str(tmp_path / f"f{k}.bin"))
+        mp, bp = str(tmp_path / f"b{k}.mesh"), str(tmp_path / f"b{k}.bb")
         meshgen.write_mesh(mp, m)
         meshgen.write_bb(bp, u)
-        subprocess.run([REF_TIMED, mp, bp, str(p["rounds"]), str(p["depth"]), str(p["bucket"]),
-                        str(p["target"]), str(p["norm"]), "--capa-depth", "4", "--final", out], check=True,
-                       capture_output=True, timeout=600, env=dict(os.environ, OMP_NUM_THREADS="8"))
-        ref = read_snapshot(out)
+        # the reference's OpenMP heuristics differ from run to run (up to
+        # ~1.5 % in the final count on these meshes): the median of 3 runs
+        counts, fracs = [], []
+        for rep in range(3):
+            out = str(tmp_path / f"f{k}_{rep}.bin")
+            subprocess.run([REF_TIMED, mp, bp, str(p["rounds"]), str(p["depth"]), str(p["bucket"]),
+                            str(p["target"]), str(p["norm"]), "--capa-depth", "4", "--final", out], check=True,
+                           capture_output=True, timeout=600, env=dict(os.environ, OMP_NUM_THREADS="8"))
+            ref = read_snapshot(out)
+            counts.append(ref.active_elems().shape[0])
+            fracs.append(in_range_fraction(ref))
         st = states[k]
-        n_gpu, n_ref = st.active_elems().shape[0], ref.active_elems().shape[0]
-        assert abs(n_gpu - n_ref) <= 0.02 * n_ref, (spec, n_gpu, n_ref)
-        assert abs(in_range_fraction(st) - in_range_fraction(ref)) <= 0.01, (spec, in_range_fraction(st),
-                                                                             in_range_fraction(ref))
+        n_gpu, n_ref = st.active_elems().shape[0], float(np.median(counts))
+        assert abs(n_gpu - n_ref) <= 0.02 * n_ref, (spec, n_gpu, counts)
+        f_gpu, f_ref = in_range_fraction(st), float(np.median(fracs))
+        assert abs(f_gpu - f_ref) <= 0.01, (spec, f_gpu, fracs)

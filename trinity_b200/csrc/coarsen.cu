@@ -423,7 +423,7 @@ void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int
 void collapse(const DMesh& m, const int* indep, const int* count, const int* target,
               const uint8_t* cand_flag, cudaStream_t s, long long bound) {
   ProfScope ps("collapse", s, 0.0);
-  k_collapse<<<grid_bounded(bound, m.capa_node), TRN_THREADS, 0, s>>>(m, indep, count, target,
+  k_collapse<<<TRN_RESIDENT(k_collapse, grid_bounded(bound, m.capa_node), TRN_THREADS), TRN_THREADS, 0, s>>>(m, indep, count, target,
                                                                       cand_flag);
   note_launch();
   check_launch("collapse");

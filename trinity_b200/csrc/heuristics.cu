@@ -246,7 +246,7 @@ void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds
   const int g = grid_bounded(bound, m.capa_node);
   const int min_n = bound < 0 ? kFusedThreads + 1 : 0;
   for (int r = 0; r < rounds; ++r) {
-    k_mis_round_dev<<<g, TRN_THREADS, 0, s>>>(m, buf[r & 1], buf[(r + 1) & 1], cand, count, sd,
+    k_mis_round_dev<<<TRN_RESIDENT(k_mis_round_dev, g, TRN_THREADS), TRN_THREADS, 0, s>>>(m, buf[r & 1], buf[(r + 1) & 1], cand, count, sd,
                                                0x9e3779b97f4a7c15ULL * r, min_n);
     note_launch();
   }
@@ -758,7 +758,7 @@ void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual
     rounds = std::min(rounds, kGreedyRounds - 8);
   }
   for (int r = 0; r < rounds; ++r) {
-    k_greedy_round<<<g, TRN_THREADS, 0, s>>>(a, ntasks, r, pairs, npairs, coop ? kGreedyGrid + 1 : 0);
+    k_greedy_round<<<TRN_RESIDENT(k_greedy_round, g, TRN_THREADS), TRN_THREADS, 0, s>>>(a, ntasks, r, pairs, npairs, coop ? kGreedyGrid + 1 : 0);
     note_launch();
   }
   if (coop && coop_launch(k_greedy_persist, bound, kFusedThreads, s, a, ntasks, pairs, npairs, grid_bar(ws),
@@ -1030,7 +1030,7 @@ void color_batch(const DMesh& m, int hint, int max_col, Seed sd, HeurWs& ws, cud
     const int cur = r & 1;
     k_color_step<<<1, 32, 0, s>>>(color_round(ws), counts + (cur ^ 1), color_frozen(ws));
     note_launch();
-    k_color_round<<<g, TRN_THREADS, 0, s>>>(m, lists[cur], counts + cur, ws.color, ws.tent, max_col, sd,
+    k_color_round<<<TRN_RESIDENT(k_color_round, g, TRN_THREADS), TRN_THREADS, 0, s>>>(m, lists[cur], counts + cur, ws.color, ws.tent, max_col, sd,
                                             color_round(ws), lists[cur ^ 1], counts + (cur ^ 1),
                                             color_frozen(ws), cur);
     note_launch();

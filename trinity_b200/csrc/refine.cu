@@ -286,8 +286,8 @@ void refine_reset_hash(RefineWs& ws, cudaStream_t s) {
 
 void refine_filter(const DMesh& m, int nb_elems, RefineWs& ws, bool fp32, cudaStream_t s) {
   ProfScope ps("refine_filter", s, (double) nb_elems * (kTri + 16 + 8) + (double) nb_elems / 2 * (kPt + kTen));
-  if (fp32) k_ref_filter<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.cnt);
-  else k_ref_filter<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.cnt);
+  if (fp32) k_ref_filter<true><<<TRN_RESIDENT(k_ref_filter<true>, grid_for(nb_elems), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.cnt);
+  else k_ref_filter<false><<<TRN_RESIDENT(k_ref_filter<false>, grid_for(nb_elems), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.cnt);
   note_launch();
   check_launch("refine_filter");
 }
@@ -296,19 +296,19 @@ void refine_apply(const DMesh& m, int nb_nodes, int nb_elems, RefineWs& ws, bool
   {
   ProfScope ps("refine_steiner", s, (double) nb_elems * (16 + 8));
   if (fp32)
-    k_ref_steiner<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
+    k_ref_steiner<true><<<TRN_RESIDENT(k_ref_steiner<true>, grid_for(nb_elems), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
                                                                   ws.hkey, ws.hval, ws.hcap);
   else
-    k_ref_steiner<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
+    k_ref_steiner<false><<<TRN_RESIDENT(k_ref_steiner<false>, grid_for(nb_elems), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
                                                                    ws.hkey, ws.hval, ws.hcap);
   note_launch();
   }
   ProfScope ps("refine_cut", s, (double) nb_elems * (16 + 8 + kTri));
   if (fp32)
-    k_ref_cut<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.off, ws.hkey,
+    k_ref_cut<true><<<TRN_RESIDENT(k_ref_cut<true>, grid_for(nb_elems), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.off, ws.hkey,
                                                               ws.hval, ws.hcap);
   else
-    k_ref_cut<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.off, ws.hkey,
+    k_ref_cut<false><<<TRN_RESIDENT(k_ref_cut<false>, grid_for(nb_elems), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_elems, ws.info, ws.off, ws.hkey,
                                                                ws.hval, ws.hcap);
   note_launch();
   check_launch("refine_apply");

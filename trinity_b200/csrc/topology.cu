@@ -148,14 +148,14 @@ void fix_list_level_end(const DMesh& m, const int* list, const int* count, long 
                         cudaGraphConditionalHandle h, bool use_h) {
   ProfScope ps("fix_tagged", s, 0.0);
   const int g = std::max(grid_bounded(bound, m.capa_node), grid_for(hint));
-  k_fix_level_end<<<g, TRN_THREADS, 0, s>>>(m, list, count, status, kind, cap, next, cur, h, use_h ? 1 : 0);
+  k_fix_level_end<<<TRN_RESIDENT(k_fix_level_end, g, TRN_THREADS), TRN_THREADS, 0, s>>>(m, list, count, status, kind, cap, next, cur, h, use_h ? 1 : 0);
   note_launch();
   check_launch("fix_list_level_end");
 }
 
 void fix_list(const DMesh& m, const int* list, const int* count, cudaStream_t s, long long bound) {
   ProfScope ps("fix_tagged", s, 0.0);
-  k_fix_list<<<grid_bounded(bound, m.capa_node), TRN_THREADS, 0, s>>>(m, list, count);
+  k_fix_list<<<TRN_RESIDENT(k_fix_list, grid_bounded(bound, m.capa_node), TRN_THREADS), TRN_THREADS, 0, s>>>(m, list, count);
   note_launch();
 }
 
@@ -304,23 +304,23 @@ void count_live(const DMesh& m, int nb_nodes, int nb_elems, int* out, cudaStream
 void build_stencils(const DMesh& m, int nb_nodes, int nb_elems, cudaStream_t s) {
   ProfScope ps("build_stencils", s, 3.0 * nb_elems * (kTri + 2 * kIdx) + 2.0 * nb_nodes * kIdx);
   cudaMemsetAsync(m.deg, 0, sizeof(int) * (size_t) m.capa_node, s);
-  k_fill_stencils<<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems);
+  k_fill_stencils<<<TRN_RESIDENT(k_fill_stencils, grid_for(nb_elems), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_elems);
   note_launch();
-  k_sort_stencils<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  k_sort_stencils<<<TRN_RESIDENT(k_sort_stencils, grid_for(nb_nodes), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_nodes);
   note_launch();
   check_launch("build_stencils");
 }
 
 void build_vicin(const DMesh& m, int nb_nodes, bool only_flagged, cudaStream_t s) {
   ProfScope ps("build_vicin", s, (double) nb_nodes * (1 + 2 * kIdx + kAvgDeg * (kIdx + kTri + kIdx)));
-  k_build_vicin<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, only_flagged ? 1 : 0);
+  k_build_vicin<<<TRN_RESIDENT(k_build_vicin, grid_for(nb_nodes), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_nodes, only_flagged ? 1 : 0);
   note_launch();
   check_launch("build_vicin");
 }
 
 void fix_tagged(const DMesh& m, int nb_nodes, cudaStream_t s) {
   ProfScope ps("fix_tagged", s, (double) nb_nodes);
-  k_fix_tagged<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  k_fix_tagged<<<TRN_RESIDENT(k_fix_tagged, grid_for(nb_nodes), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_nodes);
   note_launch();
   check_launch("fix_tagged");
 }
@@ -349,15 +349,15 @@ __global__ void k_log_cache_f64(DMesh m, int nb_nodes) {
 }
 
 void log_cache(const DMesh& m, int nb_nodes, bool fp32, cudaStream_t s) {
-  if (fp32) k_log_cache_f32<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
-  else k_log_cache_f64<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  if (fp32) k_log_cache_f32<<<TRN_RESIDENT(k_log_cache_f32, grid_for(nb_nodes), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_nodes);
+  else k_log_cache_f64<<<TRN_RESIDENT(k_log_cache_f64, grid_for(nb_nodes), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_nodes);
   note_launch();
 }
 
 void quality_all(const DMesh& m, int nb_elems, bool fp32, cudaStream_t s) {
   ProfScope ps("quality_all", s, (double) nb_elems * (kTri + kQ) + (double) nb_elems / 2 * (kPt + kTen));
-  if (fp32) k_quality_all<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems);
-  else k_quality_all<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems);
+  if (fp32) k_quality_all<true><<<TRN_RESIDENT(k_quality_all<true>, grid_for(nb_elems), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_elems);
+  else k_quality_all<false><<<TRN_RESIDENT(k_quality_all<false>, grid_for(nb_elems), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_elems);
   note_launch();
   check_launch("quality_all");
 }

@@ -115,6 +115,7 @@ int grid_for(long long n, int threads = TRN_THREADS);
 int grid_bounded(long long bound, long long cap, int threads = TRN_THREADS);
 /* grid capped at the blocks of `kernel` resident at once (one wave) */
 int grid_resident(const void* kernel, int threads, int grid, size_t smem = 0);
+#define TRN_RESIDENT(kern, grid, threads) grid_resident(reinterpret_cast<const void*>(kern), (threads), (grid))
 
 /* scratch used by the scans: tile sums of up to max_n items */
 struct ScanWs {
