@@ -128,23 +128,22 @@ template <bool F32>
 __global__ void k_coarse_filter_append(DMesh m, const int* __restrict__ act, const int* act_n,
                                        int* __restrict__ target, int* __restrict__ cand, int* count,
                                        uint8_t* __restrict__ state, int min_n) {
-  if (trn_failed_block(m)) return;
+  if (trn_failed(m)) return;
   const int n = *act_n;
   if (n < min_n) return;
-  for (int base = blockIdx.x * blockDim.x; base < n; base += trn_grid_stride()) {
-    const int q = base + threadIdx.x;
-    int v = -1, t = -1;
-    if (q < n) {
-      v = act[q];
-      if (m.activ[v] > 0) {
-        m.activ[v] = 0;
-        build_one_vicin(m, v);
-        t = identify_target<F32>(m, v);
-        target[v] = t;
-        if (t > -1) state[v] = 1;
-      }
+  /* warp-aggregated appends: a block-wide one would make every thread wait
+   * for its block's longest search at each step */
+  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
+    const int v = act[q];
+    if (m.activ[v] <= 0) continue;
+    m.activ[v] = 0;
+    build_one_vicin(m, v);
+    const int t = identify_target<F32>(m, v);
+    target[v] = t;
+    if (t > -1) {
+      state[v] = 1;
+      trn_append(cand, count, v);
     }
-    trn_block_append(cand, count, v, t > -1);
   }
 }
 

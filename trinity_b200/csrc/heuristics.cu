@@ -127,12 +127,12 @@ static bool coop_launch(K kernel, long long items, int threads, cudaStream_t s, 
 /* free-mode round over a device-counted candidate list; states are read
  * from the previous round's buffer only (0 out / not a candidate,
  * 1 undecided, 2 in the set), so the outcome does not depend on timing */
-__device__ __forceinline__ void mis_item(const DMesh& m, const uint8_t* __restrict__ in,
-                                         uint8_t* __restrict__ out, int v, uint64_t seed) {
+__device__ __forceinline__ uint8_t mis_item(const DMesh& m, const uint8_t* __restrict__ in,
+                                            uint8_t* __restrict__ out, int v, uint64_t seed) {
   const uint8_t sv = in[v];
   if (sv != 1) {
     out[v] = sv;
-    return;
+    return sv;
   }
   const uint64_t pv = trn_prio(seed, v);
   const int* vc = m.vic + (size_t) v * m.bucket;
@@ -144,7 +144,9 @@ __device__ __forceinline__ void mis_item(const DMesh& m, const uint8_t* __restri
     if (sw == 2) { leave = true; break; }
     if (sw == 1 && trn_prio(seed, w) > pv) is_max = false;
   }
-  out[v] = leave ? 0 : (is_max ? 2 : 1);
+  const uint8_t st = leave ? 0 : (is_max ? 2 : 1);
+  out[v] = st;
+  return st;
 }
 
 /* collect the set; candidates still undecided are re-activated so that the
@@ -202,24 +204,40 @@ __global__ void __launch_bounds__(kFusedThreads) k_mis_fused(DMesh m, uint8_t* s
   for (int q = threadIdx.x; q < n; q += blockDim.x) mis_finish_item(m, state, other, cand[q], indep, nindep);
 }
 
-/* all the rounds and the collection in one cooperative launch */
+/* all the rounds and the collection in one cooperative launch; the rounds
+ * stop once no candidate is undecided (the later ones would change
+ * nothing: the same set as running them all). und[3]: per round mod 3,
+ * "a candidate is still undecided"; round r clears round r + 1's word, whose
+ * last readers (round r - 2's) finished before round r began */
 __global__ void __launch_bounds__(kFusedThreads) k_mis_persist(DMesh m, uint8_t* s0, uint8_t* s1,
                                                                const int* __restrict__ cand, const int* count,
                                                                Seed sd, int rounds, int* indep, int* nindep,
-                                                               GridBar* bar) {
+                                                               int* und, GridBar* bar) {
   if (trn_failed_block(m)) return;
   const int n = *count;
-  if (trn_tid() == 0) *nindep = 0;
+  if (trn_tid() == 0) {
+    *nindep = 0;
+    und[0] = 0;
+  }
+  if (!grid_sync(bar, m.err)) return;
   const uint64_t base = trn_seed(sd);
+  int done = rounds;
   for (int r = 0; r < rounds; ++r) {
     const uint8_t* in = (r & 1) ? s1 : s0;
     uint8_t* out = (r & 1) ? s0 : s1;
     const uint64_t seed = base + 0x9e3779b97f4a7c15ULL * r;
-    for (int q = trn_tid(); q < n; q += trn_grid_stride()) mis_item(m, in, out, cand[q], seed);
+    if (trn_tid() == 0) und[(r + 1) % 3] = 0;
+    bool open = false;
+    for (int q = trn_tid(); q < n; q += trn_grid_stride()) open |= mis_item(m, in, out, cand[q], seed) == 1;
+    if (__syncthreads_or(open) && threadIdx.x == 0) und[r % 3] = 1;
     if (!grid_sync(bar, m.err)) return;
+    if (*(volatile int*) (und + r % 3) == 0) {
+      done = r + 1;
+      break;
+    }
   }
-  uint8_t* state = (rounds & 1) ? s1 : s0;
-  uint8_t* other = (rounds & 1) ? s0 : s1;
+  uint8_t* state = (done & 1) ? s1 : s0;
+  uint8_t* other = (done & 1) ? s0 : s1;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) mis_finish_item(m, state, other, cand[q], indep, nindep);
 }
 
@@ -228,8 +246,8 @@ void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds
   ProfScope ps("mis_jp", s, 0.0);
   uint8_t* buf[2] = {ws.state, ws.state2};
   if (bound > kFusedThreads &&
-      coop_launch(k_mis_persist, bound, kFusedThreads, s, m, buf[0], buf[1], cand, count, sd, rounds, indep, nindep,
-                  grid_bar(ws))) {
+      coop_launch(k_mis_persist, bound, kFusedThreads, s, m, buf[0], buf[1], cand, count, sd, rounds, indep,
+                  nindep, ws.cnt + 108, grid_bar(ws))) {
     check_launch("mis_jp_rounds");
     return;
   }

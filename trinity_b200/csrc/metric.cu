@@ -332,12 +332,12 @@ void metric_run(const DMesh& m, int nb_nodes, int nb_elems, const double* solut,
     const double V = nb_nodes, E = nb_elems;
     {
     ProfScope ps("metric_gradient", s, V * (2 * kIdx + kAvgDeg * kIdx * 2 + 8 + kPt + 16) + E * kTri);
-    k_gradient_f32<<<TRN_RESIDENT(k_gradient_f32, grid_for(nb_nodes), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_nodes, solut, grad);
+    k_gradient_f32<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, solut, grad);
     note_launch();
     }
     {
     ProfScope ps("metric_hessian", s, V * (2 * kIdx + kAvgDeg * kIdx * 2 + 16 + kPt + kTen) + E * kTri);
-    k_hessian_local_f32<<<TRN_RESIDENT(k_hessian_local_f32, grid_for(nb_nodes), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_nodes, grad, (float) p.scale_exp);
+    k_hessian_local_f32<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, grad, (float) p.scale_exp);
     note_launch();
     }
     ProfScope ps("metric_complexity", s, E * (kTri + 8) + V * (kPt + kTen));
@@ -350,7 +350,7 @@ void metric_run(const DMesh& m, int nb_nodes, int nb_elems, const double* solut,
       sum_tree(terms, nb_elems, terms + m.capa_elem, complexity, s);
     }
     ProfScope ps2("metric_normalize", s, V * 2 * kTen);
-    k_normalize_f32<<<TRN_RESIDENT(k_normalize_f32, grid_for(nb_nodes), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_nodes, complexity, p.target,
+    k_normalize_f32<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, complexity, p.target,
                                                                 p.eig_min, p.eig_max);
     note_launch();
     check_launch("metric_run");
@@ -362,12 +362,12 @@ void metric_run(const DMesh& m, int nb_nodes, int nb_elems, const double* solut,
   const double V = nb_nodes, E = nb_elems;
   {
   ProfScope ps("metric_gradient", s, V * (2 * kIdx + kAvgDeg * kIdx * 2 + 8 + kPt + 16) + E * kTri);
-  k_gradient<<<TRN_RESIDENT(k_gradient, grid_for(nb_nodes), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_nodes, solut, grad, atot);
+  k_gradient<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, solut, grad, atot);
   note_launch();
   }
   {
   ProfScope ps("metric_hessian", s, V * (2 * kIdx + kAvgDeg * kIdx * 2 + 16 + kPt + kTen) + E * kTri);
-  k_hessian_local<<<TRN_RESIDENT(k_hessian_local, grid_for(nb_nodes), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_nodes, grad, p.scale_exp,
+  k_hessian_local<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, grad, p.scale_exp,
                                                                 hsym, mloc);
   note_launch();
   }
@@ -382,7 +382,7 @@ void metric_run(const DMesh& m, int nb_nodes, int nb_elems, const double* solut,
     sum_tree(terms, nb_elems, terms + m.capa_elem, complexity, s);
   }
   ProfScope ps2("metric_normalize", s, V * 2 * kTen);
-  k_normalize<<<TRN_RESIDENT(k_normalize, grid_for(nb_nodes), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_nodes, complexity, p.target,
+  k_normalize<<<grid_for(nb_nodes), TRN_THREADS, 0, s>>>(m, nb_nodes, complexity, p.target,
                                                           p.eig_min, p.eig_max);
   note_launch();
   check_launch("metric_run");

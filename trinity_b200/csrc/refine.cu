@@ -296,10 +296,10 @@ void refine_apply(const DMesh& m, int nb_nodes, int nb_elems, RefineWs& ws, bool
   {
   ProfScope ps("refine_steiner", s, (double) nb_elems * (16 + 8));
   if (fp32)
-    k_ref_steiner<true><<<TRN_RESIDENT(k_ref_steiner<true>, grid_for(nb_elems), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
+    k_ref_steiner<true><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
                                                                   ws.hkey, ws.hval, ws.hcap);
   else
-    k_ref_steiner<false><<<TRN_RESIDENT(k_ref_steiner<false>, grid_for(nb_elems), TRN_THREADS), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
+    k_ref_steiner<false><<<grid_for(nb_elems), TRN_THREADS, 0, s>>>(m, nb_elems, nb_nodes, ws.info, ws.off,
                                                                    ws.hkey, ws.hval, ws.hcap);
   note_launch();
   }

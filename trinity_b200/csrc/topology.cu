@@ -148,7 +148,7 @@ void fix_list_level_end(const DMesh& m, const int* list, const int* count, long 
                         cudaGraphConditionalHandle h, bool use_h) {
   ProfScope ps("fix_tagged", s, 0.0);
   const int g = std::max(grid_bounded(bound, m.capa_node), grid_for(hint));
-  k_fix_level_end<<<TRN_RESIDENT(k_fix_level_end, g, TRN_THREADS), TRN_THREADS, 0, s>>>(m, list, count, status, kind, cap, next, cur, h, use_h ? 1 : 0);
+  k_fix_level_end<<<g, TRN_THREADS, 0, s>>>(m, list, count, status, kind, cap, next, cur, h, use_h ? 1 : 0);
   note_launch();
   check_launch("fix_list_level_end");
 }
