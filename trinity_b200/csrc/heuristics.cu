@@ -204,40 +204,27 @@ __global__ void __launch_bounds__(kFusedThreads) k_mis_fused(DMesh m, uint8_t* s
   for (int q = threadIdx.x; q < n; q += blockDim.x) mis_finish_item(m, state, other, cand[q], indep, nindep);
 }
 
-/* all the rounds and the collection in one cooperative launch; the rounds
- * stop once no candidate is undecided (the later ones would change
- * nothing: the same set as running them all). und[3]: per round mod 3,
- * "a candidate is still undecided"; round r clears round r + 1's word, whose
- * last readers (round r - 2's) finished before round r began */
+/* all the rounds and the collection in one cooperative launch (stopping
+ * the rounds once no candidate is undecided was measured slower: the
+ * undecided flag's reduction costs more on the long levels than the rounds
+ * it saves on the short ones) */
 __global__ void __launch_bounds__(kFusedThreads) k_mis_persist(DMesh m, uint8_t* s0, uint8_t* s1,
                                                                const int* __restrict__ cand, const int* count,
                                                                Seed sd, int rounds, int* indep, int* nindep,
-                                                               int* und, GridBar* bar) {
+                                                               GridBar* bar) {
   if (trn_failed_block(m)) return;
   const int n = *count;
-  if (trn_tid() == 0) {
-    *nindep = 0;
-    und[0] = 0;
-  }
-  if (!grid_sync(bar, m.err)) return;
+  if (trn_tid() == 0) *nindep = 0;
   const uint64_t base = trn_seed(sd);
-  int done = rounds;
   for (int r = 0; r < rounds; ++r) {
     const uint8_t* in = (r & 1) ? s1 : s0;
     uint8_t* out = (r & 1) ? s0 : s1;
     const uint64_t seed = base + 0x9e3779b97f4a7c15ULL * r;
-    if (trn_tid() == 0) und[(r + 1) % 3] = 0;
-    bool open = false;
-    for (int q = trn_tid(); q < n; q += trn_grid_stride()) open |= mis_item(m, in, out, cand[q], seed) == 1;
-    if (__syncthreads_or(open) && threadIdx.x == 0) und[r % 3] = 1;
+    for (int q = trn_tid(); q < n; q += trn_grid_stride()) mis_item(m, in, out, cand[q], seed);
     if (!grid_sync(bar, m.err)) return;
-    if (*(volatile int*) (und + r % 3) == 0) {
-      done = r + 1;
-      break;
-    }
   }
-  uint8_t* state = (done & 1) ? s1 : s0;
-  uint8_t* other = (done & 1) ? s0 : s1;
+  uint8_t* state = (rounds & 1) ? s1 : s0;
+  uint8_t* other = (rounds & 1) ? s0 : s1;
   for (int q = trn_tid(); q < n; q += trn_grid_stride()) mis_finish_item(m, state, other, cand[q], indep, nindep);
 }
 
@@ -247,7 +234,7 @@ void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds
   uint8_t* buf[2] = {ws.state, ws.state2};
   if (bound > kFusedThreads &&
       coop_launch(k_mis_persist, bound, kFusedThreads, s, m, buf[0], buf[1], cand, count, sd, rounds, indep,
-                  nindep, ws.cnt + 108, grid_bar(ws))) {
+                  nindep, grid_bar(ws))) {
     check_launch("mis_jp_rounds");
     return;
   }
