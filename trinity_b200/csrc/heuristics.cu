@@ -522,14 +522,6 @@ __device__ __forceinline__ bool greedy_is_row(const GreedyArgs& a, int ntasks, i
   return a.map[e] >= 0;
 }
 
-__device__ __forceinline__ void greedy_reset_item(const GreedyArgs& a, int i) {
-  for (int q = 0; q < a.dual_n[i]; ++q) {
-    const int e = a.dual[i * 4 + q];
-    a.vis[e] = -1;
-    a.mk0[e] = ~0ULL;
-    a.mk1[e] = ~0ULL;
-  }
-}
 
 __device__ __forceinline__ void greedy_propose(const GreedyArgs& a, int r, int i) {
   unsigned long long* mk = (r & 1) ? a.mk1 : a.mk0;
@@ -584,11 +576,6 @@ __device__ __forceinline__ bool greedy_item(const GreedyArgs& a, int ntasks, int
   return greedy_act(a, ntasks, r, i, greedy_ready(a, r, i), pairs, npairs);
 }
 
-__global__ void k_greedy_reset(GreedyArgs a, const int* ntasks_dev, int min_n) {
-  const int ntasks = *ntasks_dev;
-  if (ntasks < min_n) return;
-  for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) greedy_reset_item(a, i);
-}
 
 /* round 0's proposals; every row starts undecided */
 __global__ void k_greedy_start(GreedyArgs a, const int* ntasks_dev, int min_n) {
@@ -623,8 +610,9 @@ __global__ void k_greedy_round(GreedyArgs a, const int* ntasks_dev, int r, int* 
   }
 }
 
-/* the remaining rounds in one block; with `whole`, the level's reset and
- * first proposals too (a list the host knows to be short) */
+/* the remaining rounds in one block; with `whole`, the level's first
+ * proposals too (a list the host knows to be short). The per-element state
+ * starts reset: the dual filter reset it for the rows it built. */
 __global__ void __launch_bounds__(kFusedThreads) k_greedy_tail(GreedyArgs a, const int* ntasks_dev,
                                                                int* pairs, int* npairs, int whole,
                                                                int lim) {
@@ -633,8 +621,6 @@ __global__ void __launch_bounds__(kFusedThreads) k_greedy_tail(GreedyArgs a, con
   __shared__ int s_r;
   if (whole) {
     if (threadIdx.x == 0) *npairs = 0;
-    for (int i = threadIdx.x; i < ntasks; i += blockDim.x) greedy_reset_item(a, i);
-    __syncthreads();
     for (int i = threadIdx.x; i < ntasks; i += blockDim.x) {
       greedy_propose(a, 0, i);
       a.list0[i] = i;
@@ -668,7 +654,8 @@ __global__ void __launch_bounds__(kFusedThreads) k_greedy_tail(GreedyArgs a, con
 }
 
 /* the matching of a level in one cooperative launch: with `whole`, the
- * reset and first proposals, then rounds until no row waits (at most
+ * first proposals (the dual filter reset the elements' state), then rounds
+ * until no row waits (at most
  * kGreedyRounds); else the rounds from the first one the grid launches did
  * not run. Once kGreedyTail rows or fewer wait, the first block finishes the
  * rounds alone, separated by block barriers, and the others return: a grid
@@ -685,8 +672,6 @@ __global__ void __launch_bounds__(kFusedThreads) k_greedy_persist(GreedyArgs a, 
       a.cnt[1] = 0;
       a.cnt[2] = 0;
     }
-    for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) greedy_reset_item(a, i);
-    if (!grid_sync(bar, err)) return;
     for (int i = trn_tid(); i < ntasks; i += trn_grid_stride()) {
       greedy_propose(a, 0, i);
       a.list0[i] = i;
@@ -750,8 +735,6 @@ void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual
   const int min_n = bound < 0 ? kFusedThreads + 1 : 0;
   cudaMemsetAsync(npairs, 0, sizeof(int), s);
   cudaMemsetAsync(ws.cnt, 0, sizeof(int) * (8 + kGreedyRounds), s);
-  k_greedy_reset<<<g, TRN_THREADS, 0, s>>>(a, ntasks, min_n);
-  note_launch();
   k_greedy_start<<<g, TRN_THREADS, 0, s>>>(a, ntasks, min_n);
   note_launch();
   /* a long list known: grid launches while more than kGreedyGrid rows wait,

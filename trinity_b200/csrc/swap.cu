@@ -217,7 +217,8 @@ __device__ __forceinline__ uint32_t flip_rank(const DMesh& m, int a, int b) {
 template <bool F32>
 __global__ void k_swap_filter_dual(DMesh m, const int* __restrict__ act, const int* act_n,
                                    int* __restrict__ dual, int* __restrict__ dual_n,
-                                   int* __restrict__ map, uint32_t* __restrict__ rank, int* count) {
+                                   int* __restrict__ map, uint32_t* __restrict__ rank, int* count,
+                                   GreedyReset gr) {
   if (trn_failed(m)) return;
   const int na = *act_n;
   for (int q = trn_tid(); q < na; q += trn_grid_stride()) {
@@ -231,6 +232,13 @@ __global__ void k_swap_filter_dual(DMesh m, const int* __restrict__ act, const i
     base = __shfl_sync(mask, base, leader);
     const int r = base + __popc(mask & ((1u << lane) - 1));
     const int dn = dual_row(m, k, r, dual, dual_n, map);
+    if (gr.vis)   /* the greedy matching's state of the row's elements (rows sharing one write the same) */
+      for (int e = 0; e < dn; ++e) {
+        const int x = dual[r * 4 + e];
+        gr.vis[x] = -1;
+        gr.mk0[x] = ~0ULL;
+        gr.mk1[x] = ~0ULL;
+      }
     if (rank) {
       uint32_t w[4] = {0u, 0u, 0u, 0u};
       for (int e = 1; e < dn; ++e) w[e] = flip_rank<F32>(m, k, dual[r * 4 + e]);
@@ -350,13 +358,14 @@ void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual
 }
 
 void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,
-                      int* map, uint32_t* rank, int* count, bool fp32, cudaStream_t s, long long bound) {
+                      int* map, uint32_t* rank, int* count, bool fp32, cudaStream_t s, long long bound,
+                      GreedyReset gr) {
   ProfScope ps("swap_filter", s, 0.0);
   cudaMemsetAsync(count, 0, sizeof(int), s);
   const int g = grid_bounded(bound, m.capa_elem);
   auto* kern = fp32 ? k_swap_filter_dual<true> : k_swap_filter_dual<false>;
   kern<<<grid_resident(reinterpret_cast<const void*>(kern), TRN_THREADS, g), TRN_THREADS, 0, s>>>(
-      m, act, act_n, dual, dual_n, map, rank, count);
+      m, act, act_n, dual, dual_n, map, rank, count, gr);
   note_launch();
   check_launch("swap_filter_dual");
 }

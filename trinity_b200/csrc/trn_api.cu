@@ -981,8 +981,10 @@ void enq_swap_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphCondi
   cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s);
   cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s);
   uint32_t* rank = m->swap_match == TRN_SWAP_GAIN ? m->hws.rank : nullptr;
+  GreedyReset gr;
+  if (m->swap_match == TRN_SWAP_GREEDY) gr = GreedyReset{m->hws.mate, m->hws.prop, m->hws.prop2};
   swap_filter_dual(dl, act_list(m, 0), m->status + S_ACT, m->dual, m->dual_n, m->map, rank,
-                   m->status + S_NTASK, m->fp32, s, bound);
+                   m->status + S_NTASK, m->fp32, s, bound, gr);
   /* a captured round knows no list length, but the capacity bounds it and
    * sizes the matching's rounds for the mesh at hand */
   if (m->swap_match == TRN_SWAP_GREEDY)

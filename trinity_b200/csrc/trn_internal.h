@@ -248,9 +248,17 @@ void swap_flip(const DMesh& m, const int* pairs, const int* npairs, const int* m
  * active elements (swap_init lists them first), *count rows; when rank is
  * given, rank[4 r + e]: the gain rank of the flip between row r's candidate
  * and its neighbour e */
+/* the greedy swap matching's per-element state, reset by the dual filter for
+ * the elements of the rows it builds (vis -1, both key buffers ~0), so the
+ * matching needs no reset pass; all null when another matching runs */
+struct GreedyReset {
+  int* vis = nullptr;
+  unsigned long long* mk0 = nullptr;
+  unsigned long long* mk1 = nullptr;
+};
 void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,
                       int* map, uint32_t* rank, int* count, bool fp32, cudaStream_t s,
-                      long long bound = -1);
+                      long long bound = -1, GreedyReset gr = GreedyReset());
 
 /* smoothing (smooth.cu) */
 void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
