@@ -43,10 +43,10 @@ from trinity_b200 import meshgen  # noqa: E402
 WORKLOAD = "c2"
 # DRAM traffic per launch of the kernel that dominates the 2M-triangle step,
 # measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum, caches
-# flushed before each launch, 7 consecutive launches of the timed step's
-# first round, default launch shape); a live run has no hardware counters,
-# so the figure is carried here
-MEASURED_TRAFFIC = {"smooth_move": 442.8e6}
+# flushed before each launch, the 7 class launches of the timed step's first
+# pass, default launch shape, one-wave grid); a live run has no hardware
+# counters, so the figure is carried here
+MEASURED_TRAFFIC = {"smooth_move": 474.6e6}
 METRIC = "adapted triangles/s per full round"
 UNIT = "triangles/s"
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "trinity_ref")
@@ -309,7 +309,8 @@ def b200_arm(args, rank, world, local_rank):
                     "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
                     "traffic": MEASURED_TRAFFIC.get(dom["kernel"]) if not args.grid else None,
                     "traffic_note": "DRAM read + write bytes per launch, ncu on this workload, caches flushed "
-                                    "before each launch (mean of 7 consecutive launches of the timed step)",
+                                    "before each launch (mean of the 7 class launches of the timed step's "
+                                    "first pass)",
                     "launches": dom["launches"],
                     "avg_launch_us": round(per_launch_s * 1e6, 2),
                     "algorithmic_bytes_per_launch": round(per_launch_bytes),
