@@ -185,7 +185,7 @@ int trn_smooth_gradient_run(trn_mesh* mesh, int max_colors, int steps, double ma
 /* Launch shapes (none changes a result): cfg[0] smoothing block (32..256),
  * cfg[1] collapse-target search block, cfg[2] lanes per vertex of the
  * grouped search (4, 8, 16; 1: the one-lane search throughout), cfg[3]
- * longest level list the grouped search takes without the scan first, cfg[4] flip block, cfg[5] lanes per smoothed vertex (1, 4, 8),
+ * longest level list the grouped search takes without the scan first, cfg[4] flip block, cfg[5] lanes per smoothed vertex (1, 2, 4, 8),
  * cfg[6] registers of the smoothing kernel (0: up to 128, two 256-thread
  * blocks per SM; 1: capped for three; 2: for four). Per mesh; a captured round
  * is recaptured when

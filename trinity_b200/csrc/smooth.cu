@@ -11,7 +11,7 @@
  *                  incident element stays CCW with quality above the old
  *                  stencil minimum, backing off the step 1, 1/2, .., 1/16
  *                  (Smooth::moveSmartLaplacian, smoothing.cpp:40-126).
- *   k_smooth_move_grp  the same with 4 or 8 lanes per vertex (launch shape
+ *   k_smooth_move_grp  the same with 2, 4 or 8 lanes per vertex (launch shape
  *                  smooth_lanes; the same results)
  * Vertices of one color share no element, so a class moves in parallel; the
  * classes run in order, as in the reference.
@@ -239,6 +239,24 @@ __device__ __forceinline__ bool elem_quality_at(const DMesh& m, int i, int4 n, d
   return true;
 }
 
+/* a[j] of a small register array, j known only at run time: predicated
+ * selects, so the array stays in registers */
+template <int K, class T>
+__device__ __forceinline__ T reg_pick(const T (&a)[K], int j) {
+  T r = a[0];
+#pragma unroll
+  for (int k = 1; k < K; ++k)
+    if (j == k) r = a[k];
+  return r;
+}
+
+template <int K, class T>
+__device__ __forceinline__ void reg_put(T (&a)[K], int j, T v) {
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    if (j == k) a[k] = v;
+}
+
 template <bool F32, int G>
 __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmask) {
   const int* vc = m.vic + (size_t) i * m.bucket;
@@ -293,7 +311,9 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
   lsum.finish(nb_neigh, tn);
   const double4 tnew = make_double4(tn[0], tn[1], tn[2], 0.0);
   const LogT<F32> lnew = log_of<F32>(tn[0], tn[1], tn[2]);
-  constexpr int KQ = 2;   /* qualities and element metrics kept per lane; later ones are recomputed */
+  /* qualities and element metrics kept per lane (a stencil of 6 elements
+   * fits: 2 a lane with 4 lanes, 3 with 2); later ones are recomputed */
+  constexpr int KQ = G >= 4 ? 2 : 3;
   double qv[KQ];
   /* the element metrics of this lane's first KQ elements: they do not depend
    * on where the vertex sits, so the tries below only redo the geometry */
@@ -325,11 +345,10 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
         const double2 p2 = (n.z == i) ? pa : m.pts[n.z];
         ok = trn_ccw(p0, p1, p2);
         if (ok) {
-          q = qgeom_x(p0, p1, p2, j == 0 ? jv[0] : jv[1]);
+          q = qgeom_x(p0, p1, p2, reg_pick(jv, j));
           ok = q > q_min;
         }
-        if (j == 0) qv[0] = q;
-        else qv[1] = q;
+        reg_put(qv, j, q);
       } else {
         ok = elem_quality_at<F32>(m, i, m.tri[st[a]], pa, lnew, &q) && (q > q_min);
       }
@@ -341,7 +360,7 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
     int j = 0;
     for (int a = lane; a < deg; a += G, ++j) {
       double q = 0;
-      if (j < KQ) q = (j == 0) ? qv[0] : qv[1];
+      if (j < KQ) q = reg_pick(qv, j);
       else elem_quality_at<F32>(m, i, m.tri[st[a]], pa, lnew, &q);
       m.qual[st[a]] = q;
     }
@@ -408,7 +427,7 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
   const int lanes = tune().smooth_lanes;
   const int g = grid_for((long long) hint * lanes, t);
   const int regs = tune().smooth_regs;
-  if (lanes == 8 || lanes == 4) {
+  if (lanes == 8 || lanes == 4 || lanes == 2) {
 #define TRN_GRP(F, G, B)                                                                     \
   do {                                                                                       \
     auto* kern = k_smooth_move_grp<F, G, B>;                                                 \
@@ -420,9 +439,12 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
     if (lanes == 8) {
       if (fp32) TRN_GRP_B(true, 8);
       else TRN_GRP_B(false, 8);
-    } else {
+    } else if (lanes == 4) {
       if (fp32) TRN_GRP_B(true, 4);
       else TRN_GRP_B(false, 4);
+    } else {
+      if (fp32) TRN_GRP_B(true, 2);
+      else TRN_GRP_B(false, 2);
     }
 #undef TRN_GRP_B
 #undef TRN_GRP

@@ -95,7 +95,7 @@ struct Tune {
   int group_lanes = 8;        /* lanes per vertex of the grouped search: 4, 8, 16 */
   int group_max = 16384;      /* longest level list the grouped search takes */
   int flip_threads = 256;     /* k_swap_flip block: 128, 256, 512 */
-  int smooth_lanes = 4;       /* lanes per smoothed vertex: 1, 4, 8 */
+  int smooth_lanes = 4;       /* lanes per smoothed vertex: 1, 2, 4, 8 */
   int smooth_regs = 1;        /* smoothing registers: 0 up to 128, 1 capped at 80 (three 256-thread
                                  blocks an SM), 2 at 64 (four) */
   bool operator==(const Tune& o) const {
