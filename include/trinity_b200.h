@@ -184,16 +184,17 @@ int trn_smooth_gradient_run(trn_mesh* mesh, int max_colors, int steps, double ma
 
 /* Launch shapes (none changes a result): cfg[0] smoothing block (32..256),
  * cfg[1] collapse-target search block, cfg[2] lanes per vertex of the
- * grouped search (4, 8, 16; 1: the one-lane search throughout), cfg[3]
- * longest level list the grouped search takes without the scan first, cfg[4] flip block, cfg[5] lanes per smoothed vertex (1, 2, 4, 8),
- * cfg[6] registers of the smoothing kernel (0: up to 128, two 256-thread
- * blocks per SM; 1: capped for three; 2: for four). Per mesh; a captured round
- * is recaptured when
- * they change. trn_autotune chooses them on the loaded mesh by coordinate
- * descent over candidates, timing metric + `rounds` rounds from the input
- * (twice each, the faster counts), then reloads the mesh; meshes of similar
- * size can share the result through trn_set_tune. No counterpart in the
- * reference. */
+ * grouped search (4, 8, 16; 1: the one-lane search at every level), cfg[3]
+ * longest level list the grouped search takes (longer ones run the one-lane
+ * search), cfg[4] flip block, cfg[5] lanes per smoothed vertex (1, 2, 4,
+ * 8), cfg[6] registers of the smoothing kernel (0: up to 128, two 256-thread
+ * blocks per SM; 1: capped for three; 2: for four). Per mesh; a captured
+ * round is recaptured when they change. trn_autotune chooses them on the
+ * loaded mesh by coordinate descent over candidates, timing metric +
+ * `rounds` rounds from the input (the best of three runs; a candidate
+ * replaces the value kept only when at least 1 % faster), then reloads the
+ * mesh; meshes of similar size can share the result through trn_set_tune.
+ * No counterpart in the reference. */
 #define TRN_TUNE_N 7
 int trn_get_tune(trn_mesh* mesh, int cfg[TRN_TUNE_N]);
 int trn_set_tune(trn_mesh* mesh, const int cfg[TRN_TUNE_N]);
@@ -240,6 +241,15 @@ int trn_set_swap_match(trn_mesh* mesh, int policy);
  * TRN_ERR_NO_PROGRESS. The reference loops without a bound
  * (coarsening.cpp:480-503, swapping.cpp:395-425). */
 int trn_set_level_cap(trn_mesh* mesh, int cap);
+/* Self-test of the bounded grid barrier that separates the rounds of the
+ * cooperative heuristics (independent set, coloring, greedy matching): a
+ * cooperative launch in which one block never arrives; the others give up
+ * after max_polls polls and mark the failure, which a real call reports as
+ * TRN_ERR_NO_PROGRESS. Returns TRN_ERR_NO_PROGRESS when the wait ran out
+ * and was reported (the expected outcome), TRN_OK if it did not, and
+ * TRN_ERR_CUDA when the device has no cooperative launch. No counterpart in
+ * the reference. */
+int trn_selftest_barrier(long long max_polls);
 
 /* The solver-coupled loop: after some rounds, renumber the adapted mesh as
  * Mesh::store + Mesh::load would (io.cpp:164-255, io.cpp:53-161; live

@@ -106,3 +106,23 @@ def test_level_cap_must_be_positive():
     g = _mesh(m)
     with pytest.raises(TrinityError):
         g.set_level_cap(0)
+
+
+@pytest.mark.gpu
+def test_grid_barrier_wait_runs_out_and_is_reported():
+    """The cooperative heuristics separate their rounds by a grid barrier
+    whose wait is bounded. A cooperative launch in which one block never
+    arrives: the others give up after 4,096 polls and mark the failure
+    (TRN_ERR_NO_PROGRESS), and the context stays usable: a mesh then adapts
+    with the cooperative rounds as before (a 300x300 mesh lists more than
+    1,024 collapse candidates, so its independent sets take the cooperative
+    launch)."""
+    from trinity_b200 import _lib
+    L = _lib.lib()
+    assert L.trn_selftest_barrier(4096) == ERR_NO_PROGRESS
+    m, u, c = meshgen.make_config("c1", 300)
+    g = _mesh(m)
+    g.load_arrays(m.points, m.tris, tags_of(m), u)
+    counts = _adapts(g, c)
+    assert counts[3] > 0
+    g.close()

@@ -65,6 +65,7 @@ def lib():
         L.trn_set_options.argtypes = [pmesh, ctypes.c_uint64, ip]
         L.trn_set_swap_match.argtypes = [pmesh, ip]
         L.trn_set_level_cap.argtypes = [pmesh, ip]
+        L.trn_selftest_barrier.argtypes = [ctypes.c_longlong]
         L.trn_mesh_compact.argtypes = [pmesh]
         L.trn_mesh_capacity.argtypes = [pmesh, ctypes.POINTER(ip), ctypes.POINTER(ip)]
         L.trn_mesh_store_binary.argtypes = [pmesh, ctypes.c_char_p]

@@ -57,7 +57,7 @@ struct GridBar {
 };
 constexpr long long kBarrierPolls = 1LL << 24;
 
-__device__ __forceinline__ bool grid_sync(GridBar* b, int* mesh_err) {
+__device__ __forceinline__ bool grid_sync(GridBar* b, int* mesh_err, long long max_polls = kBarrierPolls) {
   __syncthreads();
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
@@ -73,7 +73,7 @@ __device__ __forceinline__ bool grid_sync(GridBar* b, int* mesh_err) {
     } else {
       long long polls = 0;
       while (*vgen == g) {
-        if (*verr || ++polls > kBarrierPolls) {
+        if (*verr || ++polls > max_polls) {
           atomicExch(&b->err, 1);
           trn_set_error(mesh_err, TRN_DERR_NO_PROGRESS);
           ok = 0;
@@ -89,7 +89,21 @@ __device__ __forceinline__ bool grid_sync(GridBar* b, int* mesh_err) {
   return s_ok != 0;
 }
 
-static GridBar* grid_bar(HeurWs& ws) { return reinterpret_cast<GridBar*>(ws.cnt + 100); }
+/* the workspace's barrier, cleared before each cooperative launch (a
+ * barrier that gave up keeps its arrivals and failure mark) */
+static GridBar* grid_bar(HeurWs& ws, cudaStream_t s) {
+  GridBar* b = reinterpret_cast<GridBar*>(ws.cnt + 100);
+  cudaMemsetAsync(b, 0, sizeof(GridBar), s);
+  return b;
+}
+
+/* A cooperative launch whose first block never reaches the barrier: the
+ * others wait max_polls polls, give up and mark the error word (the bounded
+ * wait's failure path, for the tests). */
+__global__ void k_barrier_selftest(GridBar* bar, int* err, long long max_polls) {
+  if (blockIdx.x == 0) return;
+  grid_sync(bar, err, max_polls);
+}
 
 /* a cooperative launch of `kernel` with as many blocks of `threads` as fit
  * on the device at once (and no more than the items need); false when it
@@ -234,7 +248,7 @@ void mis_jp_rounds(const DMesh& m, const int* cand, const int* count, int rounds
   uint8_t* buf[2] = {ws.state, ws.state2};
   if (bound > kFusedThreads &&
       coop_launch(k_mis_persist, bound, kFusedThreads, s, m, buf[0], buf[1], cand, count, sd, rounds, indep,
-                  nindep, grid_bar(ws))) {
+                  nindep, grid_bar(ws, s))) {
     check_launch("mis_jp_rounds");
     return;
   }
@@ -717,7 +731,7 @@ void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual
     return;
   }
   if (bound >= 0 && bound <= kGreedyGrid &&
-      coop_launch(k_greedy_persist, bound, kFusedThreads, s, a, ntasks, pairs, npairs, grid_bar(ws), m.err, 1)) {
+      coop_launch(k_greedy_persist, bound, kFusedThreads, s, a, ntasks, pairs, npairs, grid_bar(ws, s), m.err, 1)) {
     check_launch("match_greedy");
     return;
   }
@@ -749,7 +763,7 @@ void match_greedy(const DMesh& m, int nb_elems, const int* dual, const int* dual
     k_greedy_round<<<TRN_RESIDENT(k_greedy_round, g, TRN_THREADS), TRN_THREADS, 0, s>>>(a, ntasks, r, pairs, npairs, coop ? kGreedyGrid + 1 : 0);
     note_launch();
   }
-  if (coop && coop_launch(k_greedy_persist, bound, kFusedThreads, s, a, ntasks, pairs, npairs, grid_bar(ws),
+  if (coop && coop_launch(k_greedy_persist, bound, kFusedThreads, s, a, ntasks, pairs, npairs, grid_bar(ws, s),
                           m.err, 0)) {
     check_launch("match_greedy");
     return;
@@ -1101,7 +1115,7 @@ void color_jp(const DMesh& m, int hint, int max_col, Seed sd, HeurWs& ws, int* p
   {
     ProfScope ps("color_jp", s, 0.0);
     done = coop_launch(k_color_persist, hint, kFusedThreads, s, m, ws.list_a, ws.list_b, color_counts(ws),
-                       ws.cnt + 104, ws.color, ws.tent, max_col, sd, color_round(ws), grid_bar(ws));
+                       ws.cnt + 104, ws.color, ws.tent, max_col, sd, color_round(ws), grid_bar(ws, s));
   }
   if (done) {
     color_finish(m, hint, max_col, ws, parts, part_off, tick, s);
@@ -1114,6 +1128,31 @@ void color_jp(const DMesh& m, int hint, int max_col, Seed sd, HeurWs& ws, int* p
     cudaStreamSynchronize(s);
   }
   color_finish(m, hint, max_col, ws, parts, part_off, tick, s);
+}
+
+/* the bounded barrier's failure path on the device: a cooperative launch of
+ * k_barrier_selftest on its own barrier and error word; *gave_up: the
+ * waiting blocks gave up and marked the error word. Returns the CUDA status. */
+cudaError_t barrier_selftest(long long max_polls, int* gave_up) {
+  *gave_up = 0;
+  int dev = 0, coop = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if (!coop) return cudaErrorNotSupported;
+  void* mem = nullptr;
+  cudaError_t e = cudaMalloc(&mem, sizeof(GridBar) + sizeof(int));
+  if (e != cudaSuccess) return e;
+  GridBar* bar = static_cast<GridBar*>(mem);
+  int* err = reinterpret_cast<int*>(static_cast<char*>(mem) + sizeof(GridBar));
+  cudaMemset(mem, 0, sizeof(GridBar) + sizeof(int));
+  void* argv[] = {&bar, &err, &max_polls};
+  e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_barrier_selftest), 4, 32, argv, 0, nullptr);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  int h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(mem);
+  *gave_up = h != 0;
+  return e;
 }
 
 void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem) {

@@ -865,6 +865,16 @@ int trn_set_options(trn_mesh* m, uint64_t seed, int exact_sum) {
   return TRN_OK;
 }
 
+int trn_selftest_barrier(long long max_polls) {
+  if (max_polls < 1) return TRN_ERR_INVALID;
+  int gave_up = 0;
+  if (barrier_selftest(max_polls, &gave_up) != cudaSuccess) {
+    cudaGetLastError();
+    return TRN_ERR_CUDA;
+  }
+  return gave_up ? TRN_ERR_NO_PROGRESS : TRN_OK;
+}
+
 int trn_set_level_cap(trn_mesh* m, int cap) {
   if (!m) return TRN_ERR_INVALID;
   if (cap < 1) return fail(m, TRN_ERR_INVALID, "level cap: must be at least 1");
@@ -1405,9 +1415,11 @@ int trn_set_tune(trn_mesh* m, const int cfg[TRN_TUNE_N]) {
 }
 
 /* Coordinate descent over the launch shapes on this mesh: for each parameter
- * in turn, every candidate is timed (the best of two runs of metric + rounds
- * from the loaded input, device time of the rounds) with the others at their
- * best so far. The shapes change no result, only the time. The mesh is
+ * in turn, the current value and then every other candidate is timed (the
+ * best of three runs of metric + rounds from the loaded input, device time
+ * of the rounds) with the others at their best so far; a candidate replaces
+ * the value kept only when it is at least 1 % faster (run-to-run noise is
+ * about that). The shapes change no result, only the time. The mesh is
  * reloaded at the end. */
 int trn_autotune(trn_mesh* m, double target_factor, int norm, double h_min, double h_max, int depth,
                  int rounds, int cfg[TRN_TUNE_N]) {
@@ -1417,7 +1429,7 @@ int trn_autotune(trn_mesh* m, double target_factor, int norm, double h_min, doub
   int rc = TRN_OK;
   auto measure = [&](double* out) -> int {
     double best = 1e300;
-    for (int rep = 0; rep < 2; ++rep) {
+    for (int rep = 0; rep < 3; ++rep) {
       int r;
       if ((r = trn_mesh_reload(m)) || (r = trn_metric_run(m, target_factor, norm, h_min, h_max, nullptr)))
         return r;
@@ -1444,12 +1456,14 @@ int trn_autotune(trn_mesh* m, double target_factor, int norm, double h_min, doub
       {1, 2, 4, 8}, {64, 128, 256}, {0, 1, 2}, {128, 256, 512}, {4, 8, 16}, {4096, 16384, 65536}, {128, 256, 512}};
   for (int f = 0; f < TRN_TUNE_N && rc == TRN_OK; ++f) {
     int best_v = *fields[f];
-    double best_ms = 1e300;
+    double best_ms;
+    if ((rc = measure(&best_ms))) break;
     for (int v : cands[f]) {
+      if (v == best_v) continue;
       *fields[f] = v;
       double ms;
       if ((rc = measure(&ms))) break;
-      if (ms < best_ms) {
+      if (ms < 0.99 * best_ms) {
         best_ms = ms;
         best_v = v;
       }

@@ -287,6 +287,9 @@ struct HeurWs {
   int* fix_list = nullptr;       /* vertices tagged for repair */
 };
 void heur_ws_alloc(HeurWs* ws, int capa_node, int capa_elem);
+/* the cooperative kernels' bounded grid barrier made to give up (one block
+ * never arrives): *gave_up when the waiting blocks marked the failure */
+cudaError_t barrier_selftest(long long max_polls, int* gave_up);
 void heur_ws_free(HeurWs* ws);
 /* handshake matching on the dual rows (*ntasks of them), edges ranked by
  * their slot in the row (rank == nullptr) or by rank[4 i + slot] (the flip
