@@ -91,12 +91,12 @@ void level_end(int* status, int kind, int cap, const int* next, int* cur, int hi
  * thread's table for the launchers. */
 struct Tune {
   int smooth_threads = 256;   /* k_smooth_move block: 64, 128, 256 */
-  int filter_threads = 256;   /* one-lane collapse-target search block: 128, 256, 512 */
-  int group_lanes = 8;        /* lanes per vertex of the grouped search: 4, 8, 16 */
+  int filter_threads = 128;   /* one-lane collapse-target search block: 128, 256, 512 */
+  int group_lanes = 16;       /* lanes per vertex of the grouped search: 1 (one-lane search), 4, 8, 16 */
   int group_max = 16384;      /* longest level list the grouped search takes */
   int flip_threads = 256;     /* k_swap_flip block: 128, 256, 512 */
   int smooth_lanes = 4;       /* lanes per smoothed vertex: 1, 2, 4, 8 */
-  int smooth_regs = 1;        /* smoothing registers: 0 up to 128, 1 capped at 80 (three 256-thread
+  int smooth_regs = 2;        /* smoothing registers: 0 up to 128, 1 capped at 80 (three 256-thread
                                  blocks an SM), 2 at 64 (four) */
   bool operator==(const Tune& o) const {
     return smooth_threads == o.smooth_threads && filter_threads == o.filter_threads &&
