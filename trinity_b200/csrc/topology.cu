@@ -110,22 +110,20 @@ __global__ void k_fix_tagged(DMesh m, int nb_nodes) {
   }
 }
 
-/* the same repair over the listed vertices only */
-__global__ void k_fix_list(DMesh m, const int* __restrict__ list, const int* count) {
-  if (trn_failed(m)) return;
-  int buf[TRN_MAX_DEG];
-  const int n = *count;
-  for (int q = trn_tid(); q < n; q += trn_grid_stride()) {
-    const int v = list[q];
-    if (!m.fixes[v]) continue;
-    m.fixes[v] = 0;
-    fix_stencil(m, v, buf);
-  }
-}
-
-/* the repair of the listed vertices and the level's end in one launch; the
- * level end runs even after an error (a captured loop must still read its
- * condition, which then stops it) */
+/* The repair of the listed vertices and the end of a free-mode coarsening
+ * or swapping level, in one launch (they touch disjoint state). A level
+ * reads the list of active entities in one buffer and appends the ones it
+ * re-activates to another; the level's end moves the new list into the
+ * first buffer (so every level runs the same kernels on the same buffers),
+ * and its first thread accumulates the call's statistics, bounds the number
+ * of levels, advances the seed counter and decides whether another level
+ * runs (level_end_decide): for a coarsening level, while it found
+ * candidates and collapsed some (the loop of Coarse::run,
+ * coarsening.cpp:480-503); for a swapping level, while it flipped some
+ * (Swap::run, swapping.cpp:395-425). The host-driven loop reads that
+ * decision back; a captured round hands it to the loop node. The level end
+ * runs even after an error (a captured loop must still read its condition,
+ * which then stops it). */
 __global__ void k_fix_level_end(DMesh m, const int* __restrict__ list, const int* count, int* status, int kind,
                                 int cap, const int* __restrict__ next, int* __restrict__ cur,
                                 cudaGraphConditionalHandle h, int use_h) {
@@ -153,11 +151,6 @@ void fix_list_level_end(const DMesh& m, const int* list, const int* count, long 
   check_launch("fix_list_level_end");
 }
 
-void fix_list(const DMesh& m, const int* list, const int* count, cudaStream_t s, long long bound) {
-  ProfScope ps("fix_tagged", s, 0.0);
-  k_fix_list<<<TRN_RESIDENT(k_fix_list, grid_bounded(bound, m.capa_node), TRN_THREADS), TRN_THREADS, 0, s>>>(m, list, count);
-  note_launch();
-}
 
 __global__ void k_flag_alive(DMesh m, int nb_nodes) {
   nb_nodes = trn_nodes(m, nb_nodes);

@@ -1247,7 +1247,7 @@ int trn_smooth_gradient_run(trn_mesh* m, int max_colors, int steps, double max_l
 /* ---------------- a captured round ----------------
  * The whole free-mode round as one CUDA graph: the refinement levels, then
  * coarsening, swapping and the coloring's batches as loop nodes whose body
- * is one level (the device decides, in k_level_end / k_color_batch_end,
+ * is one level (the device decides, in k_fix_level_end / k_color_batch_end,
  * whether it runs again), then the smoothing passes over the device-side
  * color classes. Grids are sized by the capacities; every count is read on
  * the device. The kernels and seeds are those of the per-stage calls, so a

@@ -78,11 +78,7 @@ void fix_list_level_end(const DMesh& m, const int* list, const int* count, long 
                         int kind, int cap, const int* next, int* cur, int hint, cudaStream_t s,
                         cudaGraphConditionalHandle h, bool use_h);
 
-/* end of a coarsening / swapping level (round.cu): next list into place,
- * statistics, level cap, seed counter, and the decision in S_CONT (also
- * handed to the loop node h when use_h) */
-void level_end(int* status, int kind, int cap, const int* next, int* cur, int hint, cudaStream_t s,
-               cudaGraphConditionalHandle h, bool use_h);
+
 
 /* launch shapes the autotuner (trn_autotune) chooses; none of them changes
  * a result. The defaults are the tuner's choice on the 2M-triangle workload
@@ -157,9 +153,6 @@ int write_mesh_binary(const char* path, long nv, long nt, const double* pts, con
 void build_stencils(const DMesh& m, int nb_nodes, int nb_elems, cudaStream_t s);
 void build_vicin(const DMesh& m, int nb_nodes, bool only_flagged, cudaStream_t s);
 void fix_tagged(const DMesh& m, int nb_nodes, cudaStream_t s);
-/* repair of the vertices listed in list[0..*count) */
-void fix_list(const DMesh& m, const int* list, const int* count, cudaStream_t s,
-              long long bound = -1);
 void flag_all_alive(const DMesh& m, int nb_nodes, cudaStream_t s);
 void quality_all(const DMesh& m, int nb_elems, bool fp32, cudaStream_t s);
 /* recompute the per-vertex tensor-logarithm cache of the FP64 or FP32 form */
