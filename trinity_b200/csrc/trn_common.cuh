@@ -110,11 +110,31 @@ __device__ __forceinline__ void trn_activate(const DMesh& m, int id) {
   if (trn_byte_cas01(m.activ + id) && m.act_next) trn_list_push(m.act_next, m.act_next_n, id);
 }
 
-/* append ids[0..k) to list[*n] with one atomic */
+/* append ids[0..k) to list[*n]; the lanes of a warp that push to the same
+ * counter at once share one atomic: their ids are laid out slot by slot
+ * (every lane's first id, then every lane's second, ...; lists are
+ * unordered). A flip or a collapse pushes a few ids onto the shared repair
+ * and activity lists, and one atomic per push serialises on those two
+ * counters in L2 (a few ns each, for every flip of a level). */
 __device__ __forceinline__ void trn_list_push_n(int* list, int* n, const int* ids, int k) {
-  if (k <= 0) return;
-  const int base = atomicAdd(n, k);
-  for (int j = 0; j < k; ++j) list[base + j] = ids[j];
+  const unsigned mask = __activemask();
+  const unsigned peers = __match_any_sync(mask, (unsigned long long) (uintptr_t) n);
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int kmax = (int) __reduce_max_sync(peers, (unsigned) (k > 0 ? k : 0));
+  if (kmax == 0) return;
+  int total = 0;
+  for (int j = 0; j < kmax; ++j) total += __popc(__ballot_sync(peers, j < k));
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(n, total);
+  base = __shfl_sync(peers, base, leader);
+  int off = 0;
+  for (int j = 0; j < kmax; ++j) {
+    const unsigned b = __ballot_sync(peers, j < k);
+    if (j < k) list[base + off + __popc(b & lt)] = ids[j];
+    off += __popc(b);
+  }
 }
 
 /* once any kernel raised the error word, later kernels of the call do no
