@@ -697,8 +697,8 @@ __global__ void k_smooth_gradient(DMesh m, const int* __restrict__ list, int n, 
     tasks++;
     commit += move_gradient<F32>(m, v, max_len, mode);
   }
-  if (tasks) atomicAdd(counters, tasks);
-  if (commit) atomicAdd(counters + 1, commit);
+  trn_warp_add(counters, tasks);
+  trn_warp_add(counters + 1, commit);
 }
 
 void smooth_gradient_color(const DMesh& m, const int* list, int n, double max_len, int mode,

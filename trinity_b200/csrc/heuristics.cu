@@ -380,7 +380,7 @@ __device__ __forceinline__ void match_accept_item(const MatchArgs& a, int ntasks
   if (ok) {
     a.mate[c] = n;
     a.mate[n] = c;
-    const int p = atomicAdd(npairs, 1);
+    const int p = trn_warp_reserve(npairs);
     pairs[2 * p] = c;
     pairs[2 * p + 1] = n;
   }
@@ -578,7 +578,7 @@ __device__ __forceinline__ bool greedy_act(const GreedyArgs& a, int ntasks, int 
     if (greedy_is_row(a, ntasks, n)) break;
   }
   if (partner >= 0) {
-    const int p = atomicAdd(npairs, 1);
+    const int p = trn_warp_reserve(npairs);
     pairs[2 * p] = c;
     pairs[2 * p + 1] = partner;
   }

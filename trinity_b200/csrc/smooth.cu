@@ -189,8 +189,8 @@ __global__ void __launch_bounds__(256, MinB) k_smooth_move(DMesh m, const int* _
     tasks++;
     commit += move_laplacian<F32>(m, v, jc, kj);
   }
-  if (tasks) atomicAdd(counters, tasks);
-  if (commit) atomicAdd(counters + 1, commit);
+  trn_warp_add(counters, tasks);
+  trn_warp_add(counters + 1, commit);
   if (bytes) atomicAdd(bc.bytes, bytes);
 }
 
@@ -400,11 +400,10 @@ __global__ void __launch_bounds__(256, MinB) k_smooth_move_grp(DMesh m, const in
     tasks++;
     commit += move_laplacian_grp<F32, G>(m, v, lane, gmask);
   }
-  if (lane == 0) {
-    if (tasks) atomicAdd(counters, tasks);
-    if (commit) atomicAdd(counters + 1, commit);
-    if (bytes) atomicAdd(bc.bytes, bytes);
-  }
+  /* the group's tallies sit on its first lane (0 on the others) */
+  trn_warp_add(counters, tasks * (lane == 0));
+  trn_warp_add(counters + 1, commit * (lane == 0));
+  if (lane == 0 && bytes) atomicAdd(bc.bytes, bytes);
 }
 
 void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s) {

@@ -326,7 +326,7 @@ __global__ void k_swap_flip2(DMesh m, const int* __restrict__ pairs, const int* 
     const int r = flip_pair2<F32>(m, k1, k2, index, map, dual, dual_n, ntasks, strict_map != 0, half, mask);
     if (!half) local += r;
   }
-  if (local) atomicAdd(commit, local);
+  trn_warp_add(commit, local);
 }
 
 void swap_init(const DMesh& m, int nb_nodes, int nb_elems, int* map, bool fp32, cudaStream_t s, int* act,

@@ -110,6 +110,26 @@ __device__ __forceinline__ void trn_activate(const DMesh& m, int id) {
   if (trn_byte_cas01(m.activ + id) && m.act_next) trn_list_push(m.act_next, m.act_next_n, id);
 }
 
+/* *dst += the sum of v over the lanes of the warp that run this together,
+ * with one atomic (per-thread tallies at a kernel's end otherwise add up to
+ * tens of thousands of atomics on one word) */
+__device__ __forceinline__ void trn_warp_add(int* dst, int v) {
+  const unsigned mask = __activemask();
+  const int s = (int) __reduce_add_sync(mask, (unsigned) v);
+  if ((int) (threadIdx.x & 31) == __ffs(mask) - 1 && s) atomicAdd(dst, s);
+}
+
+/* a slot of *counter for each lane of the warp that calls this together,
+ * reserved with one atomic; every such lane must pass the same counter */
+__device__ __forceinline__ int trn_warp_reserve(int* counter) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(mask & ((1u << lane) - 1));
+}
+
 /* append ids[0..k) to list[*n]; the lanes of a warp that push to the same
  * counter at once share one atomic: their ids are laid out slot by slot
  * (every lane's first id, then every lane's second, ...; lists are
