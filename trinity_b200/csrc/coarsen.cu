@@ -128,6 +128,7 @@ template <bool F32>
 __global__ void k_coarse_filter_append(DMesh m, const int* __restrict__ act, const int* act_n,
                                        int* __restrict__ target, int* __restrict__ cand, int* count,
                                        uint8_t* __restrict__ state, int min_n) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) trn_level_clear(m, nullptr);
   if (trn_failed(m)) return;
   const int n = *act_n;
   if (n < min_n) return;
@@ -161,6 +162,7 @@ template <bool F32, int G>
 __global__ void k_coarse_filter_group(DMesh m, const int* __restrict__ act, const int* act_n,
                                       int* __restrict__ target, int* __restrict__ cand, int* count,
                                       uint8_t* __restrict__ state, int max_n) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) trn_level_clear(m, nullptr);
   if (trn_failed(m)) return;
   const int n = *act_n;
   if (n > max_n) return;
@@ -378,7 +380,6 @@ void coarsen_filter(const DMesh& m, int nb_nodes, int* target, uint8_t* flag, bo
 void coarsen_filter_append(const DMesh& m, const int* act, const int* act_n, int* target, int* cand,
                            int* count, uint8_t* state, bool fp32, cudaStream_t s, long long bound) {
   ProfScope ps("coarsen_filter", s, 0.0);
-  cudaMemsetAsync(count, 0, sizeof(int), s);
   /* a level listing at most group_max vertices runs the grouped search
    * (measured on B200 with 8 lanes: faster below ~16k listed vertices, 2x
    * slower on full-mesh levels), a larger one the one-lane search. A known

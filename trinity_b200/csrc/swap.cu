@@ -218,7 +218,8 @@ template <bool F32>
 __global__ void k_swap_filter_dual(DMesh m, const int* __restrict__ act, const int* act_n,
                                    int* __restrict__ dual, int* __restrict__ dual_n,
                                    int* __restrict__ map, uint32_t* __restrict__ rank, int* count,
-                                   GreedyReset gr) {
+                                   GreedyReset gr, int* flips) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) trn_level_clear(m, flips);
   if (trn_failed(m)) return;
   const int na = *act_n;
   for (int q = trn_tid(); q < na; q += trn_grid_stride()) {
@@ -359,13 +360,12 @@ void swap_dual(const DMesh& m, const int* list, int ntasks, int* dual, int* dual
 
 void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,
                       int* map, uint32_t* rank, int* count, bool fp32, cudaStream_t s, long long bound,
-                      GreedyReset gr) {
+                      GreedyReset gr, int* flips) {
   ProfScope ps("swap_filter", s, 0.0);
-  cudaMemsetAsync(count, 0, sizeof(int), s);
   const int g = grid_bounded(bound, m.capa_elem);
   auto* kern = fp32 ? k_swap_filter_dual<true> : k_swap_filter_dual<false>;
   kern<<<grid_resident(reinterpret_cast<const void*>(kern), TRN_THREADS, g), TRN_THREADS, 0, s>>>(
-      m, act, act_n, dual, dual_n, map, rank, count, gr);
+      m, act, act_n, dual, dual_n, map, rank, count, gr, flips);
   note_launch();
   check_launch("swap_filter_dual");
 }

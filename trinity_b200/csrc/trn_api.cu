@@ -934,7 +934,7 @@ Seed seed_of(trn_mesh* m, uint64_t mix) {
 
 void stats_reset(trn_mesh* m, cudaStream_t s) {
   cudaMemsetAsync(m->status + S_EVAL, 0, sizeof(int) * 3, s);
-  cudaMemsetAsync(m->status + S_LEVEL, 0, sizeof(int), s);
+  cudaMemsetAsync(m->status + S_NTASK, 0, sizeof(int) * 2, s);   /* S_NTASK, S_LEVEL */
 }
 
 int* act_list(trn_mesh* m, int k) { return k ? m->hws.list_b : m->hws.list_a; }
@@ -967,8 +967,9 @@ void enq_coarsen_begin(trn_mesh* m, cudaStream_t s, bool capture) {
 void enq_coarsen_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphConditionalHandle h,
                        bool use_h) {
   DMesh dl = level_mesh(m);
-  cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s);
-  cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s);
+  /* no memsets before the filter: the previous level's end cleared the
+   * candidate count and the filter clears the activity and repair list
+   * counters, so after the host's read back the device starts at once */
   coarsen_filter_append(dl, act_list(m, 0), m->status + S_ACT, m->target, m->list, m->status + S_NTASK,
                         m->hws.state, m->fp32, s, bound);
   mis_jp_rounds(dl, m->list, m->status + S_NTASK, kMisRounds, seed_of(m, 0x9e37ULL), m->hws, m->indep,
@@ -988,13 +989,12 @@ void enq_swap_begin(trn_mesh* m, cudaStream_t s, bool capture) {
 void enq_swap_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphConditionalHandle h,
                     bool use_h) {
   DMesh dl = level_mesh(m);
-  cudaMemsetAsync(dl.act_next_n, 0, sizeof(int), s);
-  cudaMemsetAsync(dl.fix_n, 0, sizeof(int), s);
+  /* as for coarsening; the dual filter also clears the flip count */
   uint32_t* rank = m->swap_match == TRN_SWAP_GAIN ? m->hws.rank : nullptr;
   GreedyReset gr;
   if (m->swap_match == TRN_SWAP_GREEDY) gr = GreedyReset{m->hws.mate, m->hws.prop, m->hws.prop2};
   swap_filter_dual(dl, act_list(m, 0), m->status + S_ACT, m->dual, m->dual_n, m->map, rank,
-                   m->status + S_NTASK, m->fp32, s, bound, gr);
+                   m->status + S_NTASK, m->fp32, s, bound, gr, m->status + S_COMMIT);
   /* a captured round knows no list length, but the capacity bounds it and
    * sizes the matching's rounds for the mesh at hand */
   if (m->swap_match == TRN_SWAP_GREEDY)
@@ -1003,7 +1003,6 @@ void enq_swap_level(trn_mesh* m, cudaStream_t s, long long bound, cudaGraphCondi
   else
     match_handshake(dl, m->capa_elem, m->dual, m->dual_n, m->status + S_NTASK, m->map, rank,
                     seed_of(m, 0x51edULL), m->hws, m->pairs, m->status + S_NPAIRS, s, bound);
-  cudaMemsetAsync(m->status + S_COMMIT, 0, sizeof(int), s);
   swap_flip(dl, m->pairs, m->status + S_NPAIRS, m->map, m->dual, m->dual_n, m->status + S_NTASK,
             m->status + S_COMMIT, true, m->fp32, s, bound);
   fix_list_level_end(dl, dl.fix_list, dl.fix_n, bound < 0 ? -1 : 4 * bound, m->status, kLevelSwap,

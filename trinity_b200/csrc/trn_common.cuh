@@ -323,6 +323,16 @@ __device__ __forceinline__ void trn_append(int* list, int* count, int id) {
   list[base + __popc(mask & ((1u << lane) - 1))] = id;
 }
 
+/* a free-mode level's first kernel, one thread: the activity and repair
+ * list counters (and the flip count, when given) start the level empty; the
+ * level's later kernels fill them (its candidate count was cleared by the
+ * previous level's end) */
+__device__ __forceinline__ void trn_level_clear(const DMesh& m, int* flips) {
+  if (m.act_next_n) *m.act_next_n = 0;
+  if (m.fix_n) *m.fix_n = 0;
+  if (flips) *flips = 0;
+}
+
 /* trn_failed read once for the whole block, so that every thread of a block
  * that goes on to trn_block_append takes the same branch */
 __device__ __forceinline__ bool trn_failed_block(const DMesh& m) {

@@ -45,7 +45,9 @@ constexpr int kLevelCap = 100000;
 
 /* the decision at the end of a coarsening / swapping level, by one thread:
  * the call's statistics, the level cap, the seed counter, and whether
- * another level runs (S_CONT; also the captured loop's condition) */
+ * another level runs (S_CONT; also the captured loop's condition); it also
+ * clears the candidate count the next level's filter appends to (no other
+ * thread of the level's end reads it) */
 __device__ __forceinline__ void level_end_decide(int* status, int kind, int cap,
                                                  cudaGraphConditionalHandle h, int use_h) {
   const int ntask = status[S_NTASK];
@@ -68,6 +70,7 @@ __device__ __forceinline__ void level_end_decide(int* status, int kind, int cap,
   }
   status[S_ACT] = status[S_ACT + 1];
   status[S_CONT] = go;
+  status[S_NTASK] = 0;   /* the next level's candidate count starts empty */
   ++*reinterpret_cast<unsigned*>(status + S_TICK);
   if (use_h) cudaGraphSetConditional(h, go);
 }
@@ -251,7 +254,7 @@ struct GreedyReset {
 };
 void swap_filter_dual(const DMesh& m, const int* act, const int* act_n, int* dual, int* dual_n,
                       int* map, uint32_t* rank, int* count, bool fp32, cudaStream_t s,
-                      long long bound = -1, GreedyReset gr = GreedyReset());
+                      long long bound = -1, GreedyReset gr = GreedyReset(), int* flips = nullptr);
 
 /* smoothing (smooth.cu) */
 void smooth_pre(const DMesh& m, int nb_nodes, cudaStream_t s);
