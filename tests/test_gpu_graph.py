@@ -108,7 +108,9 @@ def test_launch_shapes_change_no_result(graph):
     for cfg in (None, ODD_TUNE, dict(ODD_TUNE, group_lanes=16, group_max=0, smooth_threads=256, smooth_lanes=8),
                 dict(ODD_TUNE, smooth_lanes=1, smooth_regs=1),
                 dict(ODD_TUNE, group_lanes=1, smooth_regs=2),
-                dict(ODD_TUNE, smooth_lanes=2, smooth_regs=1)):
+                dict(ODD_TUNE, smooth_lanes=2, smooth_regs=1),
+                dict(ODD_TUNE, smooth_threads=256, smooth_regs=3),
+                dict(ODD_TUNE, smooth_lanes=2, smooth_regs=3)):
         g = gpu_mesh(m, u, c)
         if cfg:
             g.set_tune(cfg)

@@ -257,14 +257,22 @@ __device__ __forceinline__ void reg_put(T (&a)[K], int j, T v) {
     if (j == k) a[k] = v;
 }
 
-template <bool F32, int G>
-__device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmask) {
+/* JS: the element metrics live in shared memory (KQ slots a thread, stride
+ * blockDim.x) instead of registers, and the lane's element records are
+ * prefetched into L1 while the stencil minimum is read: at the 64-register
+ * cap the register-resident metrics spill */
+template <bool F32, int G, bool JS>
+__device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmask, JmT<F32>* js) {
   const int* vc = m.vic + (size_t) i * m.bucket;
   const int* st = m.stenc + (size_t) i * m.bucket;
   const int deg = trn_deg(m, i);
   const int nb_neigh = m.vdeg[i];
   double q_min = 1.7976931348623157e308;
-  for (int a = lane; a < deg; a += G) q_min = trn_dmin(q_min, m.qual[st[a]]);
+  for (int a = lane; a < deg; a += G) {
+    const int e = st[a];
+    if constexpr (JS) asm volatile("prefetch.global.L1 [%0];" ::"l"(m.tri + e));
+    q_min = trn_dmin(q_min, m.qual[e]);
+  }
 #pragma unroll
   for (int o = G / 2; o > 0; o >>= 1) q_min = trn_dmin(q_min, __shfl_xor_sync(gmask, q_min, o, G));
   const double2 pini = m.pts[i];
@@ -317,14 +325,17 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
   double qv[KQ];
   /* the element metrics of this lane's first KQ elements: they do not depend
    * on where the vertex sits, so the tries below only redo the geometry */
-  JmT<F32> jv[KQ];
+  JmT<F32> jv[JS ? 1 : KQ];
 #pragma unroll
   for (int j = 0; j < KQ; ++j) {
     const int a = lane + j * G;
     if (a < deg) {
       const int4 n = m.tri[st[a]];
-      jv[j] = qmetric_x((n.x == i) ? lnew : log_load<F32>(m, n.x), (n.y == i) ? lnew : log_load<F32>(m, n.y),
-                        (n.z == i) ? lnew : log_load<F32>(m, n.z));
+      const JmT<F32> q = qmetric_x((n.x == i) ? lnew : log_load<F32>(m, n.x),
+                                   (n.y == i) ? lnew : log_load<F32>(m, n.y),
+                                   (n.z == i) ? lnew : log_load<F32>(m, n.z));
+      if constexpr (JS) js[(size_t) j * blockDim.x] = q;
+      else jv[j] = q;
     }
   }
   bool valid;
@@ -345,7 +356,8 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
         const double2 p2 = (n.z == i) ? pa : m.pts[n.z];
         ok = trn_ccw(p0, p1, p2);
         if (ok) {
-          q = qgeom_x(p0, p1, p2, reg_pick(jv, j));
+          if constexpr (JS) q = qgeom_x(p0, p1, p2, js[(size_t) j * blockDim.x]);
+          else q = qgeom_x(p0, p1, p2, reg_pick(jv, j));
           ok = q > q_min;
         }
         reg_put(qv, j, q);
@@ -373,10 +385,12 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
   return valid ? 1 : 0;
 }
 
-template <bool F32, int G, int MinB>
+template <bool F32, int G, int MinB, bool JS>
 __global__ void __launch_bounds__(256, MinB) k_smooth_move_grp(DMesh m, const int* __restrict__ list,
                                                                        int n, const int* off, int c,
                                                                        int* counters, ByteCount bc) {
+  extern __shared__ __align__(16) unsigned char smooth_smem[];
+  JmT<F32>* js = reinterpret_cast<JmT<F32>*>(smooth_smem) + threadIdx.x;
   if (trn_failed(m)) return;
   if (off) {
     list += off[c];
@@ -398,7 +412,7 @@ __global__ void __launch_bounds__(256, MinB) k_smooth_move_grp(DMesh m, const in
     if (bc.bytes && lane == 0) bytes += smooth_bytes<F32>(m, v, moved, bc.seen);
     if (!moved) continue;
     tasks++;
-    commit += move_laplacian_grp<F32, G>(m, v, lane, gmask);
+    commit += move_laplacian_grp<F32, G, JS>(m, v, lane, gmask, js);
   }
   /* the group's tallies sit on its first lane (0 on the others) */
   trn_warp_add(counters, tasks * (lane == 0));
@@ -427,14 +441,23 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
   const int g = grid_for((long long) hint * lanes, t);
   const int regs = tune().smooth_regs;
   if (lanes == 8 || lanes == 4 || lanes == 2) {
-#define TRN_GRP(F, G, B)                                                                     \
-  do {                                                                                       \
-    auto* kern = k_smooth_move_grp<F, G, B>;                                                 \
-    kern<<<grid_resident(reinterpret_cast<const void*>(kern), t, g), t, 0, s>>>(m, list, n, off, c, \
-                                                                                counters, bc); \
+    /* smooth_regs 3: the 64-register cap with the element metrics in shared
+     * memory (KQ = 2 slots a thread for 4 or 8 lanes, 3 for 2) */
+    const size_t js_smem = (size_t) (lanes >= 4 ? 2 : 3) * t * (fp32 ? sizeof(float4) : sizeof(double4));
+#define TRN_GRP(F, G, B, J)                                                                   \
+  do {                                                                                        \
+    auto* kern = k_smooth_move_grp<F, G, B, J>;                                               \
+    const size_t sm = J ? js_smem : 0;                                                        \
+    kern<<<grid_resident(reinterpret_cast<const void*>(kern), t, g, sm), t, sm, s>>>(m, list, n, off, c, \
+                                                                                     counters, bc); \
   } while (0)
-#define TRN_GRP_B(F, G) \
-  do { if (regs == 0) TRN_GRP(F, G, 2); else if (regs == 1) TRN_GRP(F, G, 3); else TRN_GRP(F, G, 4); } while (0)
+#define TRN_GRP_B(F, G)                                                                       \
+  do {                                                                                        \
+    if (regs == 0) TRN_GRP(F, G, 2, false);                                                   \
+    else if (regs == 1) TRN_GRP(F, G, 3, false);                                              \
+    else if (regs == 2) TRN_GRP(F, G, 4, false);                                              \
+    else TRN_GRP(F, G, 4, true);                                                              \
+  } while (0)
     if (lanes == 8) {
       if (fp32) TRN_GRP_B(true, 8);
       else TRN_GRP_B(false, 8);

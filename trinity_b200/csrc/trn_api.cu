@@ -1401,7 +1401,7 @@ int trn_set_tune(trn_mesh* m, const int cfg[TRN_TUNE_N]) {
   auto pow2_in = [](int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; };
   if (!pow2_in(cfg[0], 32, 256) || !pow2_in(cfg[1], 32, 1024) || (cfg[2] != 1 && cfg[2] != 4 && cfg[2] != 8 && cfg[2] != 16) ||
       cfg[3] < 0 || !pow2_in(cfg[4], 32, 1024) || (cfg[5] != 1 && cfg[5] != 2 && cfg[5] != 4 && cfg[5] != 8) ||
-      cfg[6] < 0 || cfg[6] > 2)
+      cfg[6] < 0 || cfg[6] > 3)
     return fail(m, TRN_ERR_INVALID, "set_tune: value out of range");
   m->tune.smooth_threads = cfg[0];
   m->tune.filter_threads = cfg[1];
@@ -1452,7 +1452,7 @@ int trn_autotune(trn_mesh* m, double target_factor, int norm, double h_min, doub
                              &m->tune.filter_threads, &m->tune.group_lanes, &m->tune.group_max,
                              &m->tune.flip_threads};
   const std::vector<std::vector<int>> cands = {
-      {1, 2, 4, 8}, {64, 128, 256}, {0, 1, 2}, {128, 256, 512}, {4, 8, 16}, {4096, 16384, 65536}, {128, 256, 512}};
+      {1, 2, 4, 8}, {64, 128, 256}, {0, 1, 2, 3}, {128, 256, 512}, {4, 8, 16}, {4096, 16384, 65536}, {128, 256, 512}};
   for (int f = 0; f < TRN_TUNE_N && rc == TRN_OK; ++f) {
     int best_v = *fields[f];
     double best_ms;

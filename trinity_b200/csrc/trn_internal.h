@@ -96,7 +96,8 @@ struct Tune {
   int flip_threads = 256;     /* k_swap_flip block: 128, 256, 512 */
   int smooth_lanes = 4;       /* lanes per smoothed vertex: 1, 2, 4, 8 */
   int smooth_regs = 2;        /* smoothing registers: 0 up to 128, 1 capped at 80 (three 256-thread
-                                 blocks an SM), 2 at 64 (four) */
+                                 blocks an SM), 2 at 64 (four), 3 at 64 with the grouped form's
+                                 element metrics in shared memory */
   bool operator==(const Tune& o) const {
     return smooth_threads == o.smooth_threads && filter_threads == o.filter_threads &&
            group_lanes == o.group_lanes && group_max == o.group_max && flip_threads == o.flip_threads &&
