@@ -9,6 +9,7 @@ import pytest
 
 from tests.helpers import gpu_mesh, gpu_state, oracle_run, run_gpu_stages
 from tests.oracle_lib import Oracle, digest, run_pipeline
+from tests.test_reference_decisions import REF_DECIDE, reference_decisions
 from trinity_b200 import meshgen
 
 CASES = [("c1", 40, 2), ("c1", None, 3), ("c2", 60, 2), ("c4", 50, 2)]
@@ -57,6 +58,39 @@ def test_grouped_smoothing_same_results(oracle_built, lanes, prec):
         assert not st.diff(runs[1][stage]), stage
         if prec == "fp64":
             assert not st.diff(states[stage]), stage
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(REF_DECIDE), reason="reference build (oracle/_ref) absent")
+@pytest.mark.parametrize("name", ["c2_n60", "c4_n50"])
+def test_replay_of_the_reference_decisions_matches_reference_digests(name, tmp_path):
+    """No oracle in the loop: the GPU is fed the independent sets, matchings
+    and colorings that trinity's own build records on one thread
+    (oracle/_ref/trinity_ref_decide), and its state after the metric and
+    after every stage hashes to the digests of the reference's run."""
+    gold = GOLD[name]
+    m, u, c = meshgen.make_config(gold["config"]["name"], gold["config"]["n"])
+    params = dict(c)
+    params.update(gold["params"])
+    mp, bp = str(tmp_path / "in.mesh"), str(tmp_path / "in.bb")
+    meshgen.write_mesh(mp, m)
+    meshgen.write_bb(bp, u)
+    log = reference_decisions(mp, bp, params, tmp_path)
+    want = gold["stages"]
+    g = gpu_mesh(m, u, params)
+    assert digest(gpu_state(g)) == want["load"], "load"
+    g.set_replay(log)
+    seen = []
+
+    def check(stage):
+        got = digest(gpu_state(g))
+        bad = [k for k in got if got[k] != want[stage][k]]
+        assert not bad, f"{name} stage {stage}: {bad} differ from the reference"
+        seen.append(stage)
+
+    run_gpu_stages(g, params, check)
+    g.close()
+    assert len(seen) == 1 + 4 * params["rounds"]
 
 
 @pytest.mark.gpu
