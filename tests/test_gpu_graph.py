@@ -110,7 +110,11 @@ def test_launch_shapes_change_no_result(graph):
                 dict(ODD_TUNE, group_lanes=1, smooth_regs=2),
                 dict(ODD_TUNE, smooth_lanes=2, smooth_regs=1),
                 dict(ODD_TUNE, smooth_threads=256, smooth_regs=3),
-                dict(ODD_TUNE, smooth_lanes=2, smooth_regs=3)):
+                dict(ODD_TUNE, smooth_lanes=2, smooth_regs=3),
+                dict(ODD_TUNE, smooth_threads=256, smooth_regs=4),
+                dict(ODD_TUNE, smooth_lanes=8, smooth_regs=6),
+                dict(ODD_TUNE, smooth_lanes=2, smooth_threads=256, smooth_regs=7),
+                dict(ODD_TUNE, smooth_regs=8)):
         g = gpu_mesh(m, u, c)
         if cfg:
             g.set_tune(cfg)
@@ -128,7 +132,7 @@ def test_autotune_picks_valid_shapes_and_reloads():
     g = gpu_mesh(m, u, c)
     cfg = g.autotune(c["target"], c["norm"], depth=c["depth"], rounds=1)
     assert cfg["smooth_threads"] in (64, 128, 256) and cfg["group_lanes"] in (4, 8, 16)
-    assert cfg["smooth_lanes"] in (1, 4, 8)
+    assert cfg["smooth_lanes"] in (1, 2, 4, 8) and cfg["smooth_regs"] in range(9)
     assert g.get_tune() == cfg
     assert g.counts()[:2] == (m.nb_nodes, m.nb_elems)
     ref = gpu_mesh(m, u, c)

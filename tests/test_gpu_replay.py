@@ -35,11 +35,13 @@ def test_replay_bit_exact(oracle_built, name, n, rounds):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("lanes,prec", [(4, "fp64"), (8, "fp64"), (8, "mixed")])
-def test_grouped_smoothing_same_results(oracle_built, lanes, prec):
-    """4 or 8 lanes per smoothed vertex give the one-lane results after every
-    stage: FP64 in replay, bit-identical to the oracle too; the mixed form
-    (free mode only) identical to its one-lane run."""
+@pytest.mark.parametrize("lanes,prec,regs", [(4, "fp64", 2), (8, "fp64", 2), (8, "mixed", 2), (4, "fp64", 4),
+                                             (4, "mixed", 6), (2, "fp64", 5), (2, "fp64", 7), (4, "mixed", 8)])
+def test_grouped_smoothing_same_results(oracle_built, lanes, prec, regs):
+    """2, 4 or 8 lanes per smoothed vertex, the tries in turn or in one sweep
+    (smooth_regs 4-8), give the one-lane results after every stage: FP64 in
+    replay, bit-identical to the oracle too; the mixed form (free mode only)
+    identical to its one-lane run."""
     m, u, c, states, log = oracle_run("c2", 60, 2)
     runs = {}
     for ln in (1, lanes):
@@ -49,6 +51,7 @@ def test_grouped_smoothing_same_results(oracle_built, lanes, prec):
         g.set_precision(prec)
         t = g.get_tune()
         t["smooth_lanes"] = ln
+        t["smooth_regs"] = regs if ln > 1 else 2
         g.set_tune(t)
         snaps = {}
         run_gpu_stages(g, c, lambda s: snaps.__setitem__(s, gpu_state(g)))

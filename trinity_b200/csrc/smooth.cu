@@ -257,12 +257,29 @@ __device__ __forceinline__ void reg_put(T (&a)[K], int j, T v) {
     if (j == k) a[k] = v;
 }
 
-/* JS: the element metrics live in shared memory (KQ slots a thread, stride
- * blockDim.x) instead of registers, and the lane's element records are
- * prefetched into L1 while the stencil minimum is read: at the 64-register
- * cap the register-resident metrics spill */
-template <bool F32, int G, bool JS>
-__device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmask, JmT<F32>* js) {
+/* V selects how the back-off runs:
+ *   0  the tries in turn, element metrics in registers;
+ *   1  the same with the element metrics in shared memory (KQ slots a
+ *      thread, stride blockDim.x) and the lane's element records prefetched
+ *      into L1 while the stencil minimum is read;
+ *   2  one sweep over the lane's elements evaluates all five tries (the
+ *      element's points loaded once, five independent geometry chains), the
+ *      group ANDs the lanes' five-bit pass masks and keeps the first try that
+ *      passes; the qualities wait in shared memory (5 x KQ a thread). A
+ *      warp of 8 groups almost always runs all five tries in turn anyway
+ *      (half the moves fail every try), so this costs no extra issue and
+ *      turns a serial chain into parallel ones. Same tries, same arithmetic,
+ *      same first passing try: the same bits;
+ *   3  the sweep of 2 with the element metrics in shared memory too (before
+ *      the qualities), which frees the registers the five chains need. */
+template <bool F32, int G, int V>
+__device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmask, unsigned char* smem) {
+  constexpr bool JS = V == 1 || V == 3;
+  constexpr bool SW = V >= 2;
+  constexpr int KQ = G >= 4 ? 2 : 3;
+  JmT<F32>* js = reinterpret_cast<JmT<F32>*>(smem) + threadIdx.x;
+  double* qs = reinterpret_cast<double*>(smem + (JS ? (size_t) KQ * blockDim.x * sizeof(JmT<F32>) : 0)) +
+               threadIdx.x;
   const int* vc = m.vic + (size_t) i * m.bucket;
   const int* st = m.stenc + (size_t) i * m.bucket;
   const int deg = trn_deg(m, i);
@@ -321,7 +338,6 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
   const LogT<F32> lnew = log_of<F32>(tn[0], tn[1], tn[2]);
   /* qualities and element metrics kept per lane (a stencil of 6 elements
    * fits: 2 a lane with 4 lanes, 3 with 2); later ones are recomputed */
-  constexpr int KQ = G >= 4 ? 2 : 3;
   double qv[KQ];
   /* the element metrics of this lane's first KQ elements: they do not depend
    * on where the vertex sits, so the tries below only redo the geometry */
@@ -337,6 +353,68 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
       if constexpr (JS) js[(size_t) j * blockDim.x] = q;
       else jv[j] = q;
     }
+  }
+  if constexpr (SW) {
+    unsigned okm = 0x1fu;   /* bit w: every element of this lane passes try w */
+    int j = 0;
+    for (int a = lane; a < deg; a += G, ++j) {
+      if (j < KQ) {
+        const int4 n = m.tri[st[a]];
+        const double2 b0 = (n.x == i) ? pini : m.pts[n.x];
+        const double2 b1 = (n.y == i) ? pini : m.pts[n.y];
+        const double2 b2 = (n.z == i) ? pini : m.pts[n.z];
+        JmT<F32> jm;
+        if constexpr (JS) jm = js[(size_t) j * blockDim.x];
+        else jm = reg_pick(jv, j);
+        double weight = 1;
+#pragma unroll
+        for (int w = 0; w < 5; ++w) {
+          double2 pw;
+          pw.x = (1 - weight) * pini.x + weight * ox;
+          pw.y = (1 - weight) * pini.y + weight * oy;
+          const double2 p0 = (n.x == i) ? pw : b0;
+          const double2 p1 = (n.y == i) ? pw : b1;
+          const double2 p2 = (n.z == i) ? pw : b2;
+          const bool ccw = trn_ccw(p0, p1, p2);
+          const double q = qgeom_x(p0, p1, p2, jm);
+          qs[(size_t) (w * KQ + j) * blockDim.x] = q;
+          if (!(ccw && q > q_min)) okm &= ~(1u << w);
+          weight *= 0.5;
+        }
+      } else {
+        double weight = 1;
+        for (int w = 0; w < 5; ++w) {
+          double2 pw;
+          pw.x = (1 - weight) * pini.x + weight * ox;
+          pw.y = (1 - weight) * pini.y + weight * oy;
+          double q = 0;
+          if (!(elem_quality_at<F32>(m, i, m.tri[st[a]], pw, lnew, &q) && q > q_min)) okm &= ~(1u << w);
+          weight *= 0.5;
+        }
+      }
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) okm &= __shfl_xor_sync(gmask, okm, o, G);
+    if (!okm) return 0;
+    const int wsel = __ffs(okm) - 1;
+    double weight = 1;
+    for (int w = 0; w < wsel; ++w) weight *= 0.5;
+    double2 pa;
+    pa.x = (1 - weight) * pini.x + weight * ox;
+    pa.y = (1 - weight) * pini.y + weight * oy;
+    j = 0;
+    for (int a = lane; a < deg; a += G, ++j) {
+      double q = 0;
+      if (j < KQ) q = qs[(size_t) (wsel * KQ + j) * blockDim.x];
+      else elem_quality_at<F32>(m, i, m.tri[st[a]], pa, lnew, &q);
+      m.qual[st[a]] = q;
+    }
+    if (lane == 0) {
+      m.pts[i] = pa;
+      ten_store<F32>(m, i, tnew);
+      log_store<F32>(m, i, lnew);
+    }
+    return 1;
   }
   bool valid;
   int retry = 0;
@@ -385,12 +463,11 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
   return valid ? 1 : 0;
 }
 
-template <bool F32, int G, int MinB, bool JS>
+template <bool F32, int G, int MinB, int V>
 __global__ void __launch_bounds__(256, MinB) k_smooth_move_grp(DMesh m, const int* __restrict__ list,
                                                                        int n, const int* off, int c,
                                                                        int* counters, ByteCount bc) {
   extern __shared__ __align__(16) unsigned char smooth_smem[];
-  JmT<F32>* js = reinterpret_cast<JmT<F32>*>(smooth_smem) + threadIdx.x;
   if (trn_failed(m)) return;
   if (off) {
     list += off[c];
@@ -412,7 +489,7 @@ __global__ void __launch_bounds__(256, MinB) k_smooth_move_grp(DMesh m, const in
     if (bc.bytes && lane == 0) bytes += smooth_bytes<F32>(m, v, moved, bc.seen);
     if (!moved) continue;
     tasks++;
-    commit += move_laplacian_grp<F32, G, JS>(m, v, lane, gmask, js);
+    commit += move_laplacian_grp<F32, G, V>(m, v, lane, gmask, smooth_smem);
   }
   /* the group's tallies sit on its first lane (0 on the others) */
   trn_warp_add(counters, tasks * (lane == 0));
@@ -442,21 +519,33 @@ static void smooth_launch(const DMesh& m, const int* list, int n, const int* off
   const int regs = tune().smooth_regs;
   if (lanes == 8 || lanes == 4 || lanes == 2) {
     /* smooth_regs 3: the 64-register cap with the element metrics in shared
-     * memory (KQ = 2 slots a thread for 4 or 8 lanes, 3 for 2) */
-    const size_t js_smem = (size_t) (lanes >= 4 ? 2 : 3) * t * (fp32 ? sizeof(float4) : sizeof(double4));
-#define TRN_GRP(F, G, B, J)                                                                   \
+     * memory (KQ = 2 slots a thread for 4 or 8 lanes, 3 for 2); 4, 5, 6: all
+     * five tries in one sweep, registers capped at 64, 80, 128, with 5 x KQ
+     * qualities a thread in shared memory; 7, 8: the sweep with the element
+     * metrics in shared memory too, capped at 128, 80 */
+    const int kq = lanes >= 4 ? 2 : 3;
+    const size_t js_smem = (size_t) kq * t * (fp32 ? sizeof(float4) : sizeof(double4));
+    const size_t sw_smem = (size_t) 5 * kq * t * sizeof(double);
+#define TRN_GRP(F, G, B, V)                                                                   \
   do {                                                                                        \
-    auto* kern = k_smooth_move_grp<F, G, B, J>;                                               \
-    const size_t sm = J ? js_smem : 0;                                                        \
+    auto* kern = k_smooth_move_grp<F, G, B, V>;                                               \
+    const size_t sm = V == 1 ? js_smem : V == 2 ? sw_smem : V == 3 ? js_smem + sw_smem : 0;   \
+    if (sm > (48u << 10))                                                                     \
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);      \
     kern<<<grid_resident(reinterpret_cast<const void*>(kern), t, g, sm), t, sm, s>>>(m, list, n, off, c, \
                                                                                      counters, bc); \
   } while (0)
 #define TRN_GRP_B(F, G)                                                                       \
   do {                                                                                        \
-    if (regs == 0) TRN_GRP(F, G, 2, false);                                                   \
-    else if (regs == 1) TRN_GRP(F, G, 3, false);                                              \
-    else if (regs == 2) TRN_GRP(F, G, 4, false);                                              \
-    else TRN_GRP(F, G, 4, true);                                                              \
+    if (regs == 0) TRN_GRP(F, G, 2, 0);                                                       \
+    else if (regs == 1) TRN_GRP(F, G, 3, 0);                                                  \
+    else if (regs == 2) TRN_GRP(F, G, 4, 0);                                                  \
+    else if (regs == 3) TRN_GRP(F, G, 4, 1);                                                  \
+    else if (regs == 4) TRN_GRP(F, G, 4, 2);                                                  \
+    else if (regs == 5) TRN_GRP(F, G, 3, 2);                                                  \
+    else if (regs == 6) TRN_GRP(F, G, 2, 2);                                                  \
+    else if (regs == 7) TRN_GRP(F, G, 2, 3);                                                  \
+    else TRN_GRP(F, G, 3, 3);                                                                 \
   } while (0)
     if (lanes == 8) {
       if (fp32) TRN_GRP_B(true, 8);

@@ -1401,7 +1401,7 @@ int trn_set_tune(trn_mesh* m, const int cfg[TRN_TUNE_N]) {
   auto pow2_in = [](int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; };
   if (!pow2_in(cfg[0], 32, 256) || !pow2_in(cfg[1], 32, 1024) || (cfg[2] != 1 && cfg[2] != 4 && cfg[2] != 8 && cfg[2] != 16) ||
       cfg[3] < 0 || !pow2_in(cfg[4], 32, 1024) || (cfg[5] != 1 && cfg[5] != 2 && cfg[5] != 4 && cfg[5] != 8) ||
-      cfg[6] < 0 || cfg[6] > 3)
+      cfg[6] < 0 || cfg[6] > 8)
     return fail(m, TRN_ERR_INVALID, "set_tune: value out of range");
   m->tune.smooth_threads = cfg[0];
   m->tune.filter_threads = cfg[1];
@@ -1413,10 +1413,12 @@ int trn_set_tune(trn_mesh* m, const int cfg[TRN_TUNE_N]) {
   return TRN_OK;
 }
 
-/* Coordinate descent over the launch shapes on this mesh: for each parameter
- * in turn, the current value and then every other candidate is timed (the
- * best of three runs of metric + rounds from the loaded input, device time
- * of the rounds) with the others at their best so far; a candidate replaces
+/* Launch shapes timed on this mesh (the best of three runs of metric +
+ * rounds from the loaded input, device time of the rounds). First the
+ * smoothing's lanes a vertex and register / back-off variant jointly (they
+ * interact: two lanes a vertex pay off only with the one-sweep tries), then
+ * coordinate descent over every parameter: the current value and then every
+ * other candidate with the others at their best so far. A candidate replaces
  * the value kept only when it is at least 1 % faster (run-to-run noise is
  * about that). The shapes change no result, only the time. The mesh is
  * reloaded at the end. */
@@ -1452,7 +1454,29 @@ int trn_autotune(trn_mesh* m, double target_factor, int norm, double h_min, doub
                              &m->tune.filter_threads, &m->tune.group_lanes, &m->tune.group_max,
                              &m->tune.flip_threads};
   const std::vector<std::vector<int>> cands = {
-      {1, 2, 4, 8}, {64, 128, 256}, {0, 1, 2, 3}, {128, 256, 512}, {4, 8, 16}, {4096, 16384, 65536}, {128, 256, 512}};
+      {1, 2, 4, 8}, {64, 128, 256}, {0, 1, 2, 3, 4, 5, 6, 7, 8}, {128, 256, 512}, {4, 8, 16}, {4096, 16384, 65536}, {128, 256, 512}};
+  {
+    int best_l = m->tune.smooth_lanes, best_r = m->tune.smooth_regs;
+    double best_ms;
+    rc = measure(&best_ms);
+    for (int l : cands[0]) {
+      for (int r : cands[2]) {
+        if (rc != TRN_OK) break;
+        if ((l == best_l && r == best_r) || (l == 1 && r > 2)) continue;  /* one lane: 0-2 only */
+        m->tune.smooth_lanes = l;
+        m->tune.smooth_regs = r;
+        double ms;
+        if ((rc = measure(&ms))) break;
+        if (ms < 0.99 * best_ms) {
+          best_ms = ms;
+          best_l = l;
+          best_r = r;
+        }
+      }
+    }
+    m->tune.smooth_lanes = best_l;
+    m->tune.smooth_regs = best_r;
+  }
   for (int f = 0; f < TRN_TUNE_N && rc == TRN_OK; ++f) {
     int best_v = *fields[f];
     double best_ms;

@@ -85,7 +85,8 @@ void fix_list_level_end(const DMesh& m, const int* list, const int* count, long 
 
 /* launch shapes the autotuner (trn_autotune) chooses; none of them changes
  * a result. The defaults are the tuner's choice on the 2M-triangle workload
- * (the smoothing by 4 lanes a vertex in 256-thread blocks). Each mesh keeps
+ * in FP64 (the smoothing by 2 lanes a vertex in 256-thread blocks, the five
+ * back-off tries in one sweep). Each mesh keeps
  * its own table; the C-ABI entry that drives a mesh makes it the calling
  * thread's table for the launchers. */
 struct Tune {
@@ -94,10 +95,12 @@ struct Tune {
   int group_lanes = 16;       /* lanes per vertex of the grouped search: 1 (one-lane search), 4, 8, 16 */
   int group_max = 16384;      /* longest level list the grouped search takes */
   int flip_threads = 256;     /* k_swap_flip block: 128, 256, 512 */
-  int smooth_lanes = 4;       /* lanes per smoothed vertex: 1, 2, 4, 8 */
-  int smooth_regs = 2;        /* smoothing registers: 0 up to 128, 1 capped at 80 (three 256-thread
+  int smooth_lanes = 2;       /* lanes per smoothed vertex: 1, 2, 4, 8 */
+  int smooth_regs = 7;        /* smoothing registers: 0 up to 128, 1 capped at 80 (three 256-thread
                                  blocks an SM), 2 at 64 (four), 3 at 64 with the grouped form's
-                                 element metrics in shared memory */
+                                 element metrics in shared memory; 4, 5, 6: the grouped form's
+                                 five tries in one sweep, capped at 64, 80, 128; 7, 8: the sweep
+                                 with the element metrics in shared memory, capped at 128, 80 */
   bool operator==(const Tune& o) const {
     return smooth_threads == o.smooth_threads && filter_threads == o.filter_threads &&
            group_lanes == o.group_lanes && group_max == o.group_max && flip_threads == o.flip_threads &&
