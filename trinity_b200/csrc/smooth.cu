@@ -257,6 +257,41 @@ __device__ __forceinline__ void reg_put(T (&a)[K], int j, T v) {
     if (j == k) a[k] = v;
 }
 
+/* The moved vertex's new tensor (the exponentiated mean of its neighbours'
+ * logarithms) and its logarithm, computed by every lane of a group: the two
+ * eigenvalues' exp (log) go to the two lanes of a pair, one each, and are
+ * swapped by a shuffle, so the group issues one transcendental chain where
+ * it issued two. Same functions on the same inputs, composed as
+ * trn_interp_finish / trn_log_tensor do: the same bits. FP64 form. */
+template <int G>
+__device__ __forceinline__ void finish_pair(double* lm, int nb, double* res, int lane, unsigned gmask) {
+  double val[2], vec[4], cache[4];
+  for (int i = 0; i < 4; ++i) lm[i] /= nb;
+  trn_eigen(lm, val, vec);
+  const bool h = lane & 1;
+  const double mine = trn_exp(h ? val[1] : val[0]);
+  const double other = __shfl_xor_sync(gmask, mine, 1, G);
+  val[0] = h ? other : mine;
+  val[1] = h ? mine : other;
+  trn_eigen_compose(val, vec, cache);
+  res[0] = cache[0];
+  res[1] = cache[1];
+  res[2] = cache[3];
+}
+
+template <int G>
+__device__ __forceinline__ double4 log_pair(double t0, double t1, double t2, int lane, unsigned gmask) {
+  double copy[4] = {t0, t1, t1, t2}, val[2], vec[4], cache[4];
+  trn_eigen(copy, val, vec);
+  const bool h = lane & 1;
+  const double mine = trn_log(h ? val[1] : val[0]);
+  const double other = __shfl_xor_sync(gmask, mine, 1, G);
+  val[0] = h ? other : mine;
+  val[1] = h ? mine : other;
+  trn_eigen_compose(val, vec, cache);
+  return make_double4(cache[0], cache[1], cache[2], cache[3]);
+}
+
 /* V selects how the back-off runs:
  *   0  the tries in turn, element metrics in registers;
  *   1  the same with the element metrics in shared memory (KQ slots a
@@ -274,6 +309,7 @@ __device__ __forceinline__ void reg_put(T (&a)[K], int j, T v) {
  *      the qualities), which frees the registers the five chains need. */
 template <bool F32, int G, int V>
 __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmask, unsigned char* smem) {
+  static_assert(G >= 2, "lane groups of two or more");
   constexpr bool JS = V == 1 || V == 3;
   constexpr bool SW = V >= 2;
   constexpr int KQ = G >= 4 ? 2 : 3;
@@ -333,9 +369,15 @@ __device__ int move_laplacian_grp(const DMesh& m, int i, int lane, unsigned gmas
     oy = sy / nb_neigh;
   }
   double tn[3];
-  lsum.finish(nb_neigh, tn);
+  LogT<F32> lnew;
+  if constexpr (!F32) {
+    finish_pair<G>(lsum.lm, nb_neigh, tn, lane, gmask);
+    lnew = log_pair<G>(tn[0], tn[1], tn[2], lane, gmask);
+  } else {
+    lsum.finish(nb_neigh, tn);
+    lnew = log_of<F32>(tn[0], tn[1], tn[2]);
+  }
   const double4 tnew = make_double4(tn[0], tn[1], tn[2], 0.0);
-  const LogT<F32> lnew = log_of<F32>(tn[0], tn[1], tn[2]);
   /* qualities and element metrics kept per lane (a stencil of 6 elements
    * fits: 2 a lane with 4 lanes, 3 with 2); later ones are recomputed */
   double qv[KQ];

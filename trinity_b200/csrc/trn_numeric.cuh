@@ -61,6 +61,21 @@ __device__ __forceinline__ void trn_eigen(const double* mat, double* val, double
   vec[3] /= n1;
 }
 
+/* P diag(val) P^T from an eigen pair (vec = the columns of P), the last
+ * step of numeric::interpolateTensor's logarithm and exponentiation
+ * (numeric.cpp:131-154, 196-216), all four entries */
+__device__ __forceinline__ void trn_eigen_compose(const double* val, const double* vec, double* cache) {
+  double copy[4];
+  copy[0] = val[0] * vec[0];
+  copy[1] = val[0] * vec[2];
+  copy[2] = val[1] * vec[1];
+  copy[3] = val[1] * vec[3];
+  cache[0] = vec[0] * copy[0] + vec[1] * copy[2];
+  cache[1] = vec[0] * copy[1] + vec[1] * copy[3];
+  cache[2] = vec[2] * copy[0] + vec[3] * copy[2];
+  cache[3] = vec[2] * copy[1] + vec[3] * copy[3];
+}
+
 /* the logarithm P log(D) P^T of one tensor as numeric::interpolateTensor
  * forms it (numeric.cpp:115-154), all four entries (not exactly symmetric).
  * It depends on the tensor alone, so a cached copy summed in the same order
@@ -74,14 +89,7 @@ __device__ __forceinline__ double4 trn_log_tensor(double t0, double t1, double t
   trn_eigen(copy, val, vec);
   val[0] = trn_log(val[0]);
   val[1] = trn_log(val[1]);
-  copy[0] = val[0] * vec[0];
-  copy[1] = val[0] * vec[2];
-  copy[2] = val[1] * vec[1];
-  copy[3] = val[1] * vec[3];
-  cache[0] = vec[0] * copy[0] + vec[1] * copy[2];
-  cache[1] = vec[0] * copy[1] + vec[1] * copy[3];
-  cache[2] = vec[2] * copy[0] + vec[3] * copy[2];
-  cache[3] = vec[2] * copy[1] + vec[3] * copy[3];
+  trn_eigen_compose(val, vec, cache);
   return make_double4(cache[0], cache[1], cache[2], cache[3]);
 }
 
@@ -100,18 +108,12 @@ __device__ __forceinline__ void trn_interp_add(double* log_mat, double t0, doubl
 
 /* the exponentiation half of numeric::interpolateTensor (numeric.cpp:189-216) */
 __device__ __forceinline__ void trn_interp_finish(double* log_mat, int nb, double* res) {
-  double copy[4], cache[4], val[2], vec[4];
+  double cache[4], val[2], vec[4];
   for (int i = 0; i < 4; ++i) log_mat[i] /= nb;
   trn_eigen(log_mat, val, vec);
   val[0] = trn_exp(val[0]);
   val[1] = trn_exp(val[1]);
-  copy[0] = val[0] * vec[0];
-  copy[1] = val[0] * vec[2];
-  copy[2] = val[1] * vec[1];
-  copy[3] = val[1] * vec[3];
-  cache[0] = vec[0] * copy[0] + vec[1] * copy[2];
-  cache[1] = vec[0] * copy[1] + vec[1] * copy[3];
-  cache[3] = vec[2] * copy[1] + vec[3] * copy[3];
+  trn_eigen_compose(val, vec, cache);
   res[0] = cache[0];
   res[1] = cache[1];
   res[2] = cache[3];
