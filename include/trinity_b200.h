@@ -187,14 +187,20 @@ int trn_smooth_gradient_run(trn_mesh* mesh, int max_colors, int steps, double ma
  * grouped search (4, 8, 16; 1: the one-lane search at every level), cfg[3]
  * longest level list the grouped search takes (longer ones run the one-lane
  * search), cfg[4] flip block, cfg[5] lanes per smoothed vertex (1, 2, 4,
- * 8), cfg[6] registers of the smoothing kernel (0: up to 128, two 256-thread
- * blocks per SM; 1: capped for three; 2: for four). Per mesh; a captured
- * round is recaptured when they change. trn_autotune chooses them on the
- * loaded mesh by coordinate descent over candidates, timing metric +
- * `rounds` rounds from the input (the best of three runs; a candidate
- * replaces the value kept only when at least 1 % faster), then reloads the
- * mesh; meshes of similar size can share the result through trn_set_tune.
- * No counterpart in the reference. */
+ * 8), cfg[6] variant of the smoothing kernel with 2 or more lanes (0: the
+ * back-off tries in turn, up to 128 registers, two 256-thread blocks per SM;
+ * 1: capped for three; 2: for four; 3: as 2, element metrics in shared
+ * memory; 4, 5, 6: the five tries in one sweep, capped for four, three,
+ * two blocks; 7, 8: the sweep with the element metrics in shared memory,
+ * two or three blocks; one lane a vertex reads 0-2 only and treats 3-8 as
+ * 2). Defaults: 2 lanes, variant 7, 256-thread blocks. Per mesh; a
+ * captured round is recaptured when they change. trn_autotune chooses them
+ * on the loaded mesh, timing metric + `rounds` rounds from the input (the
+ * best of three runs; a candidate replaces the value kept only when at
+ * least 1 % faster): first the smoothing's lanes and variant jointly, then
+ * coordinate descent over all seven; then it reloads the mesh; meshes of
+ * similar size can share the result through trn_set_tune. No counterpart in
+ * the reference. */
 #define TRN_TUNE_N 7
 int trn_get_tune(trn_mesh* mesh, int cfg[TRN_TUNE_N]);
 int trn_set_tune(trn_mesh* mesh, const int cfg[TRN_TUNE_N]);
